@@ -1,0 +1,147 @@
+/*
+ * cueva.h -- C-ABI of the B200 (sm_100a) implementation of the CUEVA per-step
+ * hot path (ByMar09/MHD-KH-instability, directory cueva_2D_base/).
+ *
+ * The reference is Fortran 95 whose hot routines take no arguments and read
+ * and write module arrays dimensioned (-6:imax+6, -6:jmax+6[, 1:kmax, 1:lmax])
+ * (threevectors.f95:12-81, fourvectors.f95:12-170).  A Fortran caller keeps
+ * those arrays and binds them here once with c_loc(array(-6,-6,1[,1]))
+ * (see fortran/cueva_gpu.f90 and INTEGRATION.md); this library mirrors them on
+ * the GPU and replaces the routines listed next to each entry point.
+ *
+ * Conventions: every entry point returns 0 (CUEVA_OK) or a positive error
+ * class; the message of the last failure on the calling thread is in
+ * cueva_last_error().  A context is bound to one CUDA device and one stream,
+ * is not re-entrant, and must be driven from one host thread (the reference
+ * calls its routines from the serial driver, main_cueva_code.f95:202-328).
+ * Where the reference prints and STOPs (non-physical states), the kernels set
+ * bits of a device status word instead; cueva_step() and the routine mirrors
+ * report them as CUEVA_ERR_PHYSICS at the next synchronisation.
+ */
+#ifndef CUEVA_H
+#define CUEVA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUEVA_OK 0
+#define CUEVA_ERR_ARG 1       /* invalid argument or unsupported configuration */
+#define CUEVA_ERR_CUDA 2      /* CUDA runtime failure (no device, out of memory, ...) */
+#define CUEVA_ERR_UNBOUND 3   /* a field the call needs was never bound */
+#define CUEVA_ERR_PHYSICS 4   /* a kernel hit a reference STOP condition, see cueva_status */
+
+/* status bits reported by cueva_status (reference STOP sites) */
+#define CUEVA_ST_C2P_FAIL 1u        /* 12_varprimitive.f95:382-428,485 */
+#define CUEVA_ST_SUPERLUMINAL 2u    /* 12_varprimitive.f95:678,691; 12_varprimitive_nr.f95:217 */
+#define CUEVA_ST_HLLC_NOCONV 4u     /* funciones.f95:240-245 */
+#define CUEVA_ST_HLLC_VSTAR 8u      /* 16_hllc_flow_mpx.f95:4294,4605 */
+
+typedef struct cueva_ctx cueva_ctx;
+
+/* Run configuration: the compile-time constants of parameters.f95 that the
+ * hot path reads, as runtime values. */
+typedef struct cueva_params {
+  int32_t imax, jmax;   /* grid points 0..imax x 0..jmax (parameters.f95:110-111), both >= 6 */
+  int32_t order;        /* IMEX tableau (parameters.f95:10): 1, 2 SSP2(2,2,2), 3 SSP2(3,3,2), 4 SSP3(4,3,3), 5, 6, 8 */
+  int32_t flux_solver;  /* 5 HLL+MPX, 7 HLLC+MPX (main_cueva_code.f95:263-273) */
+  int32_t rec_mp;       /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
+  int32_t c2p;          /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37), 2 learned seed + Newton */
+  int32_t bc_x, bc_y;   /* per-axis ghost rule: 0 copy, 1 periodic (BOUND 1 / 2 / 6 of 04_boundary.f95) */
+  int32_t precision;    /* 0 FP64 throughout; 1 FP32 reconstruction + Riemann, FP64 elsewhere */
+  int32_t device;       /* CUDA device ordinal */
+  double lx, ly, lz;    /* Longx, Longy, Longz (Delx = lx/imax, Dely = ly/jmax, Delz = lz) */
+  double cfl, sigma, gamma;
+  double dt;            /* <= 0 selects CFL*min(Delx,Dely,Delz) (parameters.f95:312) */
+} cueva_params;
+
+/* Field ids for cueva_bind_field.  Base = address of element (-6,-6) of the
+ * Fortran array (and stage 1 for the stage arrays); layout column-major with
+ * leading dimension imax+13, second dimension jmax+13, stage stride
+ * (imax+13)*(jmax+13). */
+enum cueva_field {
+  /* carried primitives (threevectors.f95:32-64) */
+  CUEVA_RHO = 0, CUEVA_P, CUEVA_VX, CUEVA_VY, CUEVA_VZ, CUEVA_PSI, CUEVA_PHI,
+  CUEVA_EX, CUEVA_EY, CUEVA_EZ, CUEVA_BX, CUEVA_BY, CUEVA_BZ, CUEVA_Q,
+  /* startconvar outputs at time n (threevectors.f95:38,64) */
+  CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W,
+  /* stage state, (.., 1:lmax) arrays of fourvectors.f95:18-50 */
+  CUEVA_PSIINT, CUEVA_PHIINT, CUEVA_EXINT, CUEVA_EYINT, CUEVA_EZINT,
+  CUEVA_BXINT, CUEVA_BYINT, CUEVA_BZINT, CUEVA_QINT, CUEVA_DDINT, CUEVA_TAUINT,
+  CUEVA_SXINT, CUEVA_SYINT, CUEVA_SZINT, CUEVA_JXINT, CUEVA_JYINT, CUEVA_JZINT,
+  CUEVA_EXAST, CUEVA_EYAST, CUEVA_EZAST,
+  /* stage right-hand sides, fourvectors.f95:140-145 */
+  CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
+  CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,
+  CUEVA_SXFLUX, CUEVA_SYFLUX, CUEVA_SZFLUX, CUEVA_EXASTSOUR, CUEVA_EYASTSOUR, CUEVA_EZASTSOUR,
+  CUEVA_NFIELDS
+};
+
+/* transfer groups for cueva_upload / cueva_download */
+#define CUEVA_G_PRIMS 1u   /* the 14 carried primitives */
+#define CUEVA_G_CONS 2u    /* D, tau, Sx, Sy, Sz, W */
+
+/* ---- lifecycle ------------------------------------------------------- */
+int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out);
+int32_t cueva_ctx_destroy(cueva_ctx* ctx);
+const char* cueva_last_error(void);
+int32_t cueva_set_stream(cueva_ctx* ctx, void* cuda_stream); /* NULL: the context's own stream */
+double cueva_dt(const cueva_ctx* ctx);
+int32_t cueva_tableau_stages(const cueva_ctx* ctx);
+
+/* ---- fields and transfers -------------------------------------------- */
+int32_t cueva_bind_field(cueva_ctx* ctx, int32_t field, double* base);
+/* page-lock a host range (e.g. a bound Fortran array) so transfers run at full PCIe rate */
+int32_t cueva_pin_host(void* ptr, uint64_t bytes);
+int32_t cueva_unpin_host(void* ptr);
+/* host -> device of the bound interior points; uploading CUEVA_G_PRIMS also
+ * runs startconvar and prepares stage 1, so cueva_step can follow directly */
+int32_t cueva_upload(cueva_ctx* ctx, uint32_t groups);
+/* device -> host of the bound interior points (ghost cells are left to the
+ * caller's boundary routine, as main_cueva_code.f95:328 does); synchronises
+ * and reports kernel status */
+int32_t cueva_download(cueva_ctx* ctx, uint32_t groups);
+
+/* ---- the hot path ----------------------------------------------------- */
+/* nsteps executions of the body of the time loop, main_cueva_code.f95:53-328
+ * (boundary, startconvar, cleanvarint, RK stages with sumint / varint /
+ * electricvarint / flowinit / {hll,hllc}_flow_mpx / fluxandsource / sumfin,
+ * varfin, electricfield, varprimitivecardano or varprimitive_nr), on the
+ * device-resident state.  Asynchronous on the context stream. */
+int32_t cueva_step(cueva_ctx* ctx, int32_t nsteps);
+int32_t cueva_sync(cueva_ctx* ctx);
+int32_t cueva_status(cueva_ctx* ctx, uint32_t* status_bits);
+int32_t cueva_counters(cueva_ctx* ctx, int64_t out3[3]);   /* contador_r, contador_p, contador_v */
+
+/* ---- routine mirrors (synchronous; bound host arrays in and out) ------- */
+/* startconvar, 06_conserved_var.f95:79-140: prims -> D, tau, S, W */
+int32_t cueva_startconvar(cueva_ctx* ctx);
+/* electricvarint (IMEX), 11_elecvarint.f95:279-328, plus the current J of
+ * flowinit, 14_flowinit.f95:280-302: Exast(l), Bxint(l).., qint(l), W, V ->
+ * Exint(l).., Jxint(l).. */
+int32_t cueva_electricvarint(cueva_ctx* ctx, int32_t l);
+/* {hll,hllc}_flow_mpx 2D + fluxandsource for stage l:
+ * psiint(l)..Szint(l), Exint(l).., Jxint(l).., V, p, rho, W ->
+ * psiflux(l)..Szflux(l), Exastsour(l).. */
+int32_t cueva_flux_rhs(cueva_ctx* ctx, int32_t l);
+/* varprimitivecardano / varprimitive_nr with l_swap = 1: D, tau, S, E, B and
+ * the seeds V, rho, p -> V, rho, p */
+int32_t cueva_con2prim(cueva_ctx* ctx);
+
+/* ---- synthetic input ------------------------------------------------- */
+/* Kelvin-Helmholtz initial data on the Fortran-layout prim arrays bound to
+ * ctx (interior points; reference orientation: x = shear normal with copy
+ * boundaries, y = periodic flow direction), conventions of
+ * 03_init_var_primitive.f95:2297-2336:
+ *   vy = v0 tanh(x/a), vx = amp sin(kpert y + phase) exp(-x^2/width),
+ *   B = (0, bshear, 0), E = -v x B, rho = rho0, p = p0, psi = phi = q = 0,
+ * with x = -lx/2 + i*Delx, y = -ly/2 + j*Dely. */
+int32_t cueva_kh_init(cueva_ctx* ctx, double v0, double a, double amp, double width, double kpert,
+                      double phase, double bshear, double rho0, double p0);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUEVA_H */

@@ -1,0 +1,546 @@
+// cueva_abi.cu -- the C-ABI of include/cueva.h: contexts, Fortran-layout
+// transfers, step orchestration with CUDA graphs, routine mirrors.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cueva.h"
+#include "cueva_common.cuh"
+#include "cueva_launch.h"
+
+using namespace cueva;
+
+namespace {
+
+thread_local std::string g_err;
+
+int32_t fail(int32_t code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CUDA_TRY(x)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (x);                                                                    \
+    if (e_ != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// IMEX tableaux, imex_scheme.f95:13-507 (MIRK = 0)
+struct Tableau { int s = 0; double wb[8] = {}, wbt[8] = {}, Ab[8][8] = {}, Abt[8][8] = {}; };
+
+bool make_tableau(int order, Tableau& T) {
+  T = Tableau();
+  const double cst = 1.0 - 1.0 / std::sqrt(2.0);
+  const double alpha1 = 0.24169426078821, beta1 = 0.06042356519705, etha1 = 0.12915286960590;
+  switch (order) {
+  case 1: T.s = 1; T.wb[0] = 1.0; T.Ab[0][0] = 1.0; return true;
+  case 2:
+    T.s = 2; T.wb[0] = T.wb[1] = 0.5; T.wbt[0] = T.wbt[1] = 0.5; T.Ab[1][0] = 1.0;
+    T.Abt[0][0] = cst; T.Abt[1][0] = 1.0 - 2.0 * cst; T.Abt[1][1] = cst; return true;
+  case 3:
+    T.s = 3; for (int k = 0; k < 3; ++k) { T.wb[k] = 1.0 / 3.0; T.wbt[k] = 1.0 / 3.0; }
+    T.Ab[1][0] = 0.5; T.Ab[2][0] = 0.5; T.Ab[2][1] = 0.5;
+    T.Abt[0][0] = 1.0 / 5.0; T.Abt[1][0] = 1.0 / 10.0; T.Abt[1][1] = 1.0 / 5.0;
+    T.Abt[2][0] = 1.0 / 3.0; T.Abt[2][1] = 1.0 / 3.0; T.Abt[2][2] = 1.0 / 3.0; return true;
+  case 4:
+    T.s = 4; T.wb[1] = 1.0 / 6.0; T.wb[2] = 1.0 / 6.0; T.wb[3] = 2.0 / 3.0;
+    for (int k = 0; k < 4; ++k) T.wbt[k] = T.wb[k];
+    T.Ab[2][1] = 1.0; T.Ab[3][1] = 0.25; T.Ab[3][2] = 0.25;
+    T.Abt[0][0] = alpha1; T.Abt[1][0] = -1.0 * alpha1; T.Abt[1][1] = alpha1;
+    T.Abt[2][1] = 1.0 - alpha1; T.Abt[2][2] = alpha1;
+    T.Abt[3][0] = beta1; T.Abt[3][1] = etha1; T.Abt[3][2] = 0.5 - beta1 - etha1 - alpha1; T.Abt[3][3] = alpha1;
+    return true;
+  case 5: {
+    T.s = 5;
+    const double wb[5] = {1.0 / 4.0, 7.0 / 4.0, 3.0 / 4.0, -7.0 / 4.0, 0.0};
+    const double wbt[5] = {0.0, 3.0 / 2.0, -3.0 / 2.0, 0.5, 0.5};
+    const double A[5][5] = {{0, 0, 0, 0, 0}, {0.5, 0, 0, 0, 0}, {11.0 / 18.0, 1.0 / 18.0, 0, 0, 0},
+                            {5.0 / 6.0, -5.0 / 6.0, 0.5, 0, 0}, {1.0 / 4.0, 7.0 / 4.0, 3.0 / 4.0, -7.0 / 4.0, 0}};
+    const double At[5][5] = {{0, 0, 0, 0, 0}, {0, 0.5, 0, 0, 0}, {0, 1.0 / 6.0, 0.5, 0, 0},
+                             {0, -0.5, 0.5, 0.5, 0}, {0, 3.0 / 2.0, -3.0 / 2.0, 0.5, 0.5}};
+    for (int a = 0; a < 5; ++a) { T.wb[a] = wb[a]; T.wbt[a] = wbt[a];
+      for (int b = 0; b < 5; ++b) { T.Ab[a][b] = A[a][b]; T.Abt[a][b] = At[a][b]; } }
+    return true; }
+  case 6: {
+    T.s = 6;
+    const double w[6] = {-0.035877095577305, 0.673080876788404, 0.149064711243777,
+                         0.137173305022086, 0.150219587614740, -0.073661385091702};
+    const double A[6][6] = {
+      {0, 0, 0, 0, 0, 0}, {0.342975342284516, 0, 0, 0, 0, 0},
+      {0.016193013787920, 0.309787886268879, 0, 0, 0, 0},
+      {-0.135950059698287, 0.640189764616023, 0.342154021907072, 0, 0, 0},
+      {-0.042056958294301, 0.660781723165128, -0.381308869908091, 1.001236515566727, 0, 0},
+      {0.099109299514465, -0.466919631638661, 1.030492210860962, 0.564549736036252, -0.119257987827582, 0}};
+    const double At[6][6] = {
+      {0.449855695709406, 0, 0, 0, 0, 0}, {-0.295189486209790, 0.449855695709406, 0, 0, 0, 0},
+      {0.879036496969614, -0.042071370873823, 0.449855695709406, 0, 0, 0},
+      {0.751731896214317, -0.222508174774298, 0.220689305480633, 0.449855695709406, 0, 0},
+      {-0.039570781554756, 0.788509712948086, 0.685131268735182, -0.144071924307435, 0.449855695709406, 0},
+      {0.382760589609172, -0.196622622060158, 0.904049611197476, 0.680864149962184, 0.571862669923976,
+       0.449855695709406}};
+    for (int a = 0; a < 6; ++a) { T.wb[a] = w[a]; T.wbt[a] = w[a];
+      for (int b = 0; b < 6; ++b) { T.Ab[a][b] = A[a][b]; T.Abt[a][b] = At[a][b]; } }
+    return true; }
+  case 8: {
+    T.s = 8;
+    const double w[8] = {0.0, 277.0 / 1720.0, 385.0 / 1314.0, 587.0 / 1885.0, 31.0 / 18247.0, 665.0 / 2906.0,
+                         0.0, 23.0 / 5731.0};
+    const double A[8][8] = {
+      {0, 0, 0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0, 0, 0}, {0, 966.0 / 2039.0, 0, 0, 0, 0, 0, 0},
+      {0, 199.0 / 5291.0, 735.0 / 1709.0, 0, 0, 0, 0, 0},
+      {0, 306.0 / 4373.0, 533.0 / 1060.0, 773.0 / 628.0, 0, 0, 0, 0},
+      {0, 61.0 / 10399.0, 552.0 / 8267.0, 881.0 / 1054.0, 52.0 / 9395.0, 0, 0, 0},
+      {184.0 / 2869.0, 141.0 / 3059.0, 826.0 / 1929.0, 1567.0 / 757.0, 1754.0 / 977.0, 161.0 / 599.0, 0, 0},
+      {0, 27.0 / 359.0, 227.0 / 2338.0, 53.0 / 557.0, 569.0 / 4644.0, 859.0 / 1966.0, 0, 0}};
+    const double g = 1026.0 / 3919.0;
+    const double At[8][8] = {
+      {g, 0, 0, 0, 0, 0, 0, 0}, {-1148.0 / 4385.0, g, 0, 0, 0, 0, 0, 0},
+      {-1165.0 / 2683.0, 904.0 / 1399.0, g, 0, 0, 0, 0, 0},
+      {1480.0 / 2439.0, -1469.0 / 4070.0, -121.0 / 3026.0, g, 0, 0, 0, 0},
+      {-2788.0 / 397.0, 2069.0 / 294.0, 722.0 / 339.0, -411.0 / 682.0, g, 0, 0, 0},
+      {-165.0 / 12667.0, 105.0 / 671.0, 133.0 / 500.0, 1307.0 / 5430.0, 55.0 / 26474.0, g, 0, 0},
+      {837.0 / 1003.0, 629.0 / 1976.0, 1195.0 / 149.0, -5209.0 / 618.0, 1045.0 / 1459.0, 2767.0 / 911.0, g, 0},
+      {-752.0 / 647.0, -771.0 / 2338.0, 3197.0 / 469.0, 2313.0 / 586.0, -2267.0 / 2341.0, -2128.0 / 275.0, 0, g}};
+    for (int a = 0; a < 8; ++a) { T.wb[a] = w[a]; T.wbt[a] = w[a];
+      for (int b = 0; b < 8; ++b) { T.Ab[a][b] = A[a][b]; T.Abt[a][b] = At[a][b]; } }
+    return true; }
+  default: return false;
+  }
+}
+
+}  // namespace
+
+struct cueva_ctx {
+  cueva_params P{};
+  Tableau T;
+  int dev = 0;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  int imax = 0, jmax = 0, nx = 0, ny = 0, pitch = 0;
+  long long fstride = 0;
+  double delx = 0, dely = 0, delz = 0, dt = 0;
+  // device memory
+  double* slab = nullptr;
+  uint32_t* d_status = nullptr;
+  unsigned long long* d_counters = nullptr;
+  InstDesc* d_inst = nullptr;
+  InstDesc h_inst{};
+  int nkslot = 0;
+  int kslot_of[8];        // slot of K_m (0-based m) or -1
+  int nblocks = 0;
+  int cur = 0, qin = 0;
+  bool primed = false;
+  double* bound[CUEVA_NFIELDS] = {};
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+};
+
+namespace {
+
+int32_t check_ctx(cueva_ctx* c) {
+  if (!c) return fail(CUEVA_ERR_ARG, "null context");
+  return CUEVA_OK;
+}
+
+size_t host_field_elems(const cueva_ctx* c) { return (size_t)(c->imax + 13) * (size_t)(c->jmax + 13); }
+double* host_interior(const cueva_ctx* c, double* base, int l) {
+  // element (0, 0) of stage l of a (-6:imax+6, -6:jmax+6, 1:lmax) array
+  return base + (size_t)(l - 1) * host_field_elems(c) + 6 + (size_t)6 * (c->imax + 13);
+}
+
+int32_t h2d(cueva_ctx* c, double* dst, int field, int l) {
+  if (!c->bound[field]) return fail(CUEVA_ERR_UNBOUND, "field " + std::to_string(field) + " not bound");
+  CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)c->pitch * 8, host_interior(c, c->bound[field], l),
+                             (size_t)(c->imax + 13) * 8, (size_t)c->nx * 8, (size_t)c->ny, cudaMemcpyHostToDevice,
+                             c->stream));
+  return CUEVA_OK;
+}
+int32_t d2h(cueva_ctx* c, const double* src, int field, int l) {
+  if (!c->bound[field]) return fail(CUEVA_ERR_UNBOUND, "field " + std::to_string(field) + " not bound");
+  CUDA_TRY(cudaMemcpy2DAsync(host_interior(c, c->bound[field], l), (size_t)(c->imax + 13) * 8, src,
+                             (size_t)c->pitch * 8, (size_t)c->nx * 8, (size_t)c->ny, cudaMemcpyDeviceToHost,
+                             c->stream));
+  return CUEVA_OK;
+}
+
+double* prim_f(cueva_ctx* c, int buf, int f) { return c->h_inst.prim[buf] + (long long)f * c->fstride; }
+double* aux_f(cueva_ctx* c, int buf, int f) { return c->h_inst.aux[buf] + (long long)f * c->fstride; }
+double* stage_f(cueva_ctx* c, int buf, int f) { return c->h_inst.stage[buf] + (long long)f * c->fstride; }
+
+int32_t read_status(cueva_ctx* c) {
+  uint32_t st = 0;
+  CUDA_TRY(cudaMemcpyAsync(&st, c->d_status, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (st) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite)", st);
+    return fail(CUEVA_ERR_PHYSICS, buf);
+  }
+  return CUEVA_OK;
+}
+
+StageArgs stage_args(const cueva_ctx* c, int l, int mode) {
+  StageArgs sa{};
+  const Tableau& T = c->T;
+  sa.l = l; sa.s = T.s; sa.cur = c->cur; sa.qin = c->qin; sa.mode = mode;
+  sa.wb = T.wb[l - 1]; sa.wbt = T.wbt[l - 1];
+  for (int m = 0; m < 8; ++m) { sa.kslot[m] = -1; sa.ab_next[m] = 0.0; sa.abt_next[m] = 0.0; }
+  if (l < T.s) {
+    for (int m = 1; m <= l; ++m) { sa.ab_next[m - 1] = T.Ab[l][m - 1]; sa.abt_next[m - 1] = T.Abt[l][m - 1]; }
+    sa.abt_diag_next = T.Abt[l][l];
+  }
+  sa.abt_diag_first = T.Abt[0][0];
+  for (int m = 1; m < l; ++m) sa.kslot[m - 1] = c->kslot_of[m - 1];
+  sa.store_k_slot = (l < T.s) ? c->kslot_of[l - 1] : -1;
+  sa.need_intsum_load = (l >= 2 && l < T.s) ? 1 : 0;
+  sa.need_intsum_store = (l + 1 < T.s) ? 1 : 0;
+  return sa;
+}
+
+int32_t run_begin_step(cueva_ctx* c) {
+  CUDA_TRY(launch_begin_step((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur, c->qin, c->T.Abt[0][0]));
+  c->primed = true;
+  return CUEVA_OK;
+}
+
+int32_t enqueue_step(cueva_ctx* c) {
+  for (int l = 1; l <= c->T.s; ++l) {
+    const StageArgs sa = stage_args(c, l, 0);
+    CUDA_TRY(launch_sweep(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nblocks, c->stream, c->d_inst, 1, sa));
+    c->qin ^= 1;
+  }
+  c->cur ^= 1;
+  return CUEVA_OK;
+}
+
+void destroy_graphs(cueva_ctx* c) {
+  for (auto& row : c->graph)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cueva_last_error(void) { return g_err.c_str(); }
+
+int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
+  if (!p || !out) return fail(CUEVA_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
+  if (p->flux_solver != 5 && p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
+  if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
+  if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
+  if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
+    return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
+  if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
+  cueva_ctx* c = new cueva_ctx();
+  c->P = *p;
+  if (!make_tableau(p->order, c->T)) { delete c; return fail(CUEVA_ERR_ARG, "unsupported IMEX order"); }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    delete c; cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, "no CUDA device available");
+  }
+  if (p->device < 0 || p->device >= ndev) { delete c; return fail(CUEVA_ERR_ARG, "device ordinal out of range"); }
+  c->dev = p->device;
+  if (cudaSetDevice(c->dev) != cudaSuccess) { delete c; return fail(CUEVA_ERR_CUDA, "cudaSetDevice failed"); }
+  c->imax = p->imax; c->jmax = p->jmax; c->nx = p->imax + 1; c->ny = p->jmax + 1;
+  c->pitch = (c->nx + 31) / 32 * 32;
+  c->fstride = (long long)c->pitch * c->ny;
+  c->delx = p->lx / (double)p->imax;
+  c->dely = p->ly / (double)p->jmax;
+  c->delz = p->lz / 1.0;
+  {
+    const double a = c->delx, b = c->dely, z = c->delz;
+    double mn = (b < a) ? b : a;
+    mn = (z < mn) ? z : mn;
+    c->dt = (p->dt > 0.0) ? p->dt : p->cfl * mn;
+  }
+  // K_m storage: needed when a row r >= m+2 of the tableau uses column m
+  for (int m = 0; m < 8; ++m) c->kslot_of[m] = -1;
+  for (int m = 0; m < c->T.s; ++m) {
+    bool need = false;
+    for (int r = m + 2; r < c->T.s; ++r) need = need || c->T.Ab[r][m] != 0.0 || c->T.Abt[r][m] != 0.0;
+    if (need) c->kslot_of[m] = c->nkslot++;
+  }
+  const long long fs = c->fstride;
+  const long long nfields = 2LL * NPRIM + 2LL * NAUX + 2LL * NSTAGE + 2LL * NCONS + (long long)c->nkslot * NRHS + NRHS;
+  if (cudaMalloc(&c->slab, (size_t)(nfields * fs) * sizeof(double)) != cudaSuccess) {
+    delete c; cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, "cudaMalloc of the field slab failed");
+  }
+  cudaMemset(c->slab, 0, (size_t)(nfields * fs) * sizeof(double));
+  double* q = c->slab;
+  InstDesc& I = c->h_inst;
+  I.prim[0] = q; q += NPRIM * fs; I.prim[1] = q; q += NPRIM * fs;
+  I.aux[0] = q; q += NAUX * fs; I.aux[1] = q; q += NAUX * fs;
+  I.stage[0] = q; q += NSTAGE * fs; I.stage[1] = q; q += NSTAGE * fs;
+  I.intsum = q; q += NCONS * fs;
+  I.finsum = q; q += NCONS * fs;
+  I.kbuf = q; q += (long long)c->nkslot * NRHS * fs;
+  I.rhs_out = q; q += NRHS * fs;
+  if (cudaMalloc(&c->d_status, 4) != cudaSuccess || cudaMalloc(&c->d_counters, 3 * 8) != cudaSuccess ||
+      cudaMalloc(&c->d_inst, sizeof(InstDesc)) != cudaSuccess) {
+    cueva_ctx_destroy(c); cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, "cudaMalloc of the context descriptors failed");
+  }
+  cudaMemset(c->d_status, 0, 4);
+  cudaMemset(c->d_counters, 0, 24);
+  I.status = c->d_status;
+  I.counters = c->d_counters;
+  I.mlp = nullptr;
+  I.imax = c->imax; I.jmax = c->jmax; I.pitch = c->pitch; I.fstride = fs;
+  I.bc_x = p->bc_x; I.bc_y = p->bc_y;
+  I.delx = c->delx; I.dely = c->dely; I.dt = c->dt; I.sigma = p->sigma; I.gamma = p->gamma;
+  const double mn = (c->dely < c->delx) ? c->dely : c->delx;   // parameters.f95:329-334
+  const double cp = std::sqrt(mn / 1.0);
+  I.kappa_psi = 1.0 / (cp * cp);
+  I.kappa_phi = 1.0 / (cp * cp);
+  // the Fortran module variable eps1 keeps the value the flux routine stored last
+  I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
+  I.c2p = p->c2p;
+  I.strips_x = (c->nx + STRIP - 1) / STRIP;
+  I.blocks_y = (c->ny + SWEEP_ROWS - 1) / SWEEP_ROWS;
+  I.block_begin = 0;
+  I.block_count = ((I.strips_x + SWEEP_WARPS - 1) / SWEEP_WARPS) * I.blocks_y;
+  c->nblocks = I.block_count;
+  if (cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cueva_ctx_destroy(c); cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, "context set-up failed");
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ctx_destroy(cueva_ctx* c) {
+  if (!c) return CUEVA_OK;
+  cudaSetDevice(c->dev);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  destroy_graphs(c);
+  if (c->slab) cudaFree(c->slab);
+  if (c->d_status) cudaFree(c->d_status);
+  if (c->d_counters) cudaFree(c->d_counters);
+  if (c->d_inst) cudaFree(c->d_inst);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return CUEVA_OK;
+}
+
+int32_t cueva_set_stream(cueva_ctx* c, void* s) {
+  if (int32_t e = check_ctx(c)) return e;
+  destroy_graphs(c);
+  c->stream = s ? (cudaStream_t)s : c->own_stream;
+  return CUEVA_OK;
+}
+
+double cueva_dt(const cueva_ctx* c) { return c ? c->dt : 0.0; }
+int32_t cueva_tableau_stages(const cueva_ctx* c) { return c ? c->T.s : 0; }
+
+int32_t cueva_bind_field(cueva_ctx* c, int32_t field, double* base) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (field < 0 || field >= CUEVA_NFIELDS) return fail(CUEVA_ERR_ARG, "field id out of range");
+  c->bound[field] = base;
+  return CUEVA_OK;
+}
+
+int32_t cueva_pin_host(void* ptr, uint64_t bytes) {
+  CUDA_TRY(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+  return CUEVA_OK;
+}
+int32_t cueva_unpin_host(void* ptr) {
+  CUDA_TRY(cudaHostUnregister(ptr));
+  return CUEVA_OK;
+}
+
+int32_t cueva_upload(cueva_ctx* c, uint32_t groups) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  if (groups & CUEVA_G_PRIMS) {
+    for (int f = 0; f < NPRIM; ++f)
+      if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+    if (int32_t e = run_begin_step(c)) return e;
+  }
+  if (groups & CUEVA_G_CONS) {
+    const int map[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
+    for (int f = 0; f < NAUX; ++f)
+      if (int32_t e = h2d(c, aux_f(c, c->cur, f), map[f], 1)) return e;
+  }
+  return CUEVA_OK;
+}
+
+int32_t cueva_download(cueva_ctx* c, uint32_t groups) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  if (groups & CUEVA_G_PRIMS)
+    for (int f = 0; f < NPRIM; ++f)
+      if (int32_t e = d2h(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  if (groups & CUEVA_G_CONS) {
+    const int map[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
+    for (int f = 0; f < NAUX; ++f)
+      if (int32_t e = d2h(c, aux_f(c, c->cur, f), map[f], 1)) return e;
+  }
+  return read_status(c);
+}
+
+int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (nsteps < 0) return fail(CUEVA_ERR_ARG, "nsteps < 0");
+  if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int n = 0; n < nsteps; ++n) {
+    cudaGraphExec_t& g = c->graph[c->cur][c->qin];
+    if (!g) {
+      // capture one step starting from this (cur, qin) parity
+      const int cur0 = c->cur, qin0 = c->qin;
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int32_t e = enqueue_step(c);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      if (e) { if (graph) cudaGraphDestroy(graph); return e; }
+      if (ce != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&g, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      c->cur = cur0; c->qin = qin0;
+    }
+    CUDA_TRY(cudaGraphLaunch(g, c->stream));
+    for (int l = 0; l < c->T.s; ++l) c->qin ^= 1;
+    c->cur ^= 1;
+  }
+  return CUEVA_OK;
+}
+
+int32_t cueva_sync(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  return read_status(c);
+}
+
+int32_t cueva_status(cueva_ctx* c, uint32_t* st) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  CUDA_TRY(cudaMemcpyAsync(st, c->d_status, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CUEVA_OK;
+}
+
+int32_t cueva_counters(cueva_ctx* c, int64_t out3[3]) {
+  if (int32_t e = check_ctx(c)) return e;
+  unsigned long long h[3];
+  CUDA_TRY(cudaMemcpyAsync(h, c->d_counters, 24, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
+  return CUEVA_OK;
+}
+
+// ------------------------------------------------------------ routine mirrors
+int32_t cueva_startconvar(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int f = 0; f < NPRIM; ++f)
+    if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  CUDA_TRY(launch_startconvar((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur));
+  c->primed = false;
+  const int map[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
+  for (int f = 0; f < NAUX; ++f)
+    if (c->bound[map[f]])
+      if (int32_t e = d2h(c, aux_f(c, c->cur, f), map[f], 1)) return e;
+  return read_status(c);
+}
+
+int32_t cueva_electricvarint(cueva_ctx* c, int32_t l) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (l < 1 || l > c->T.s) return fail(CUEVA_ERR_ARG, "stage index out of range");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  const int q = c->qin;
+  const int in[7] = {CUEVA_EXAST, CUEVA_EYAST, CUEVA_EZAST, CUEVA_BXINT, CUEVA_BYINT, CUEVA_BZINT, CUEVA_QINT};
+  const int slot[7] = {Q_EX, Q_EY, Q_EZ, Q_BX, Q_BY, Q_BZ, Q_Q};
+  for (int k = 0; k < 7; ++k)
+    if (int32_t e = h2d(c, stage_f(c, q, slot[k]), in[k], l)) return e;
+  for (int f : {P_VX, P_VY, P_VZ})
+    if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  if (int32_t e = h2d(c, aux_f(c, c->cur, A_W), CUEVA_W, 1)) return e;
+  CUDA_TRY(launch_electricvarint((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur, q, c->T.Abt[l - 1][l - 1]));
+  c->primed = false;
+  const int out[6] = {CUEVA_EXINT, CUEVA_EYINT, CUEVA_EZINT, CUEVA_JXINT, CUEVA_JYINT, CUEVA_JZINT};
+  const int oslot[6] = {Q_EX, Q_EY, Q_EZ, Q_JX, Q_JY, Q_JZ};
+  for (int k = 0; k < 6; ++k)
+    if (c->bound[out[k]] || k < 3)
+      if (int32_t e = d2h(c, stage_f(c, q, oslot[k]), out[k], l)) return e;
+  return read_status(c);
+}
+
+int32_t cueva_flux_rhs(cueva_ctx* c, int32_t l) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (l < 1 || l > c->T.s) return fail(CUEVA_ERR_ARG, "stage index out of range");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  const int q = c->qin;
+  const int in[NSTAGE] = {CUEVA_PSIINT, CUEVA_PHIINT, CUEVA_EXINT, CUEVA_EYINT, CUEVA_EZINT, CUEVA_BXINT,
+                          CUEVA_BYINT, CUEVA_BZINT, CUEVA_QINT, CUEVA_DDINT, CUEVA_TAUINT, CUEVA_SXINT,
+                          CUEVA_SYINT, CUEVA_SZINT, CUEVA_JXINT, CUEVA_JYINT, CUEVA_JZINT};
+  for (int k = 0; k < NSTAGE; ++k)
+    if (int32_t e = h2d(c, stage_f(c, q, k), in[k], l)) return e;
+  for (int f : {P_VX, P_VY, P_VZ, P_P, P_RHO})
+    if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  if (int32_t e = h2d(c, aux_f(c, c->cur, A_W), CUEVA_W, 1)) return e;
+  const StageArgs sa = stage_args(c, l, 1);
+  CUDA_TRY(launch_sweep(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nblocks, c->stream, c->d_inst, 1, sa));
+  c->primed = false;
+  const int out[NRHS] = {CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
+                         CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,
+                         CUEVA_SXFLUX, CUEVA_SYFLUX, CUEVA_SZFLUX, CUEVA_EXASTSOUR, CUEVA_EYASTSOUR,
+                         CUEVA_EZASTSOUR};
+  for (int k = 0; k < NRHS; ++k)
+    if (int32_t e = d2h(c, c->h_inst.rhs_out + (long long)k * c->fstride, out[k], l)) return e;
+  return read_status(c);
+}
+
+int32_t cueva_con2prim(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int f = 0; f < NPRIM; ++f)
+    if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  const int map[5] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ};
+  for (int f = 0; f < 5; ++f)
+    if (int32_t e = h2d(c, aux_f(c, c->cur, f), map[f], 1)) return e;
+  CUDA_TRY(launch_con2prim((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur));
+  c->primed = false;
+  for (int f : {P_RHO, P_P, P_VX, P_VY, P_VZ})
+    if (int32_t e = d2h(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  return read_status(c);
+}
+
+// --------------------------------------------------------------- KH input
+int32_t cueva_kh_init(cueva_ctx* c, double v0, double a, double amp, double width, double kpert, double phase,
+                      double bshear, double rho0, double p0) {
+  if (int32_t e = check_ctx(c)) return e;
+  for (int f = 0; f < NPRIM; ++f)
+    if (!c->bound[CUEVA_RHO + f]) return fail(CUEVA_ERR_UNBOUND, "kh_init needs all 14 prim fields bound");
+  const double lx = c->P.lx, ly = c->P.ly;
+  for (int j = 0; j <= c->jmax; ++j)
+    for (int i = 0; i <= c->imax; ++i) {
+      const size_t k = (size_t)(i + 6) + (size_t)(j + 6) * (c->imax + 13);
+      const double posx = -0.5 * lx + i * c->delx;
+      const double posy = -0.5 * ly + j * c->dely;
+      const double vx = amp * std::sin(kpert * posy + phase) * std::exp(-(posx * posx) / width);
+      const double vy = v0 * std::tanh(posx / a);
+      const double vz = 0.0;
+      const double Bx = 0.0, By = bshear, Bz = 0.0;
+      c->bound[CUEVA_RHO][k] = rho0; c->bound[CUEVA_P][k] = p0;
+      c->bound[CUEVA_VX][k] = vx; c->bound[CUEVA_VY][k] = vy; c->bound[CUEVA_VZ][k] = vz;
+      c->bound[CUEVA_PSI][k] = 0.0; c->bound[CUEVA_PHI][k] = 0.0; c->bound[CUEVA_Q][k] = 0.0;
+      c->bound[CUEVA_BX][k] = Bx; c->bound[CUEVA_BY][k] = By; c->bound[CUEVA_BZ][k] = Bz;
+      c->bound[CUEVA_EX][k] = -(vy * Bz - vz * By);
+      c->bound[CUEVA_EY][k] = -(vz * Bx - vx * Bz);
+      c->bound[CUEVA_EZ][k] = -(vx * By - vy * Bx);
+    }
+  return CUEVA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// cueva_common.cuh -- shared definitions of the B200 CUEVA kernels.
+//
+// Device data layout (HBM): structure of arrays, one slab per field group,
+// interior points only.  Point (i, j), 0 <= i <= imax, 0 <= j <= jmax, of
+// field f lives at base + f * fstride + j * pitch + i, with pitch a multiple
+// of 32 doubles (256 B rows) so every warp-wide row access is one aligned
+// 256 B segment.  Ghost cells of the Fortran arrays are never stored: loads
+// outside the interior go through the per-axis index map of the reference's
+// boundary routines (copy = clamp to [0, N]; periodic = node duplicate,
+// -k -> N-k and N+k -> k; 04_boundary.f95:1390-1533, 2867-3033).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cueva {
+
+// ---- field groups --------------------------------------------------------
+// carried primitive state, order of the C-ABI prims (include/cueva.h)
+enum Prim { P_RHO = 0, P_P, P_VX, P_VY, P_VZ, P_PSI, P_PHI, P_EX, P_EY, P_EZ, P_BX, P_BY, P_BZ, P_Q, NPRIM };
+// conserved D, tau, S and the Lorentz factor at time n (startconvar)
+enum Aux { A_D = 0, A_TAU, A_SX, A_SY, A_SZ, A_W, NAUX };
+// RK stage state: the 14 conserved of stage l (E already implicit) + J
+enum Stage { Q_PSI = 0, Q_PHI, Q_EX, Q_EY, Q_EZ, Q_BX, Q_BY, Q_BZ, Q_Q, Q_D, Q_TAU, Q_SX, Q_SY, Q_SZ,
+             Q_JX, Q_JY, Q_JZ, NSTAGE };
+constexpr int NCONS = 14;   // first 14 stage fields are the conserved set
+// stage right-hand side: F (14, same order as the conserved set) + E sources
+enum Rhs { K_SEX = 14, K_SEY, K_SEZ, NRHS };
+
+// ---- status bits (host maps them to C-ABI error codes) -------------------
+enum StatusBits : uint32_t {
+  ST_C2P_FAIL = 1u,        // Cardano "stop" branches, 12_varprimitive.f95:382-428,485
+  ST_SUPERLUMINAL = 2u,    // 12_varprimitive.f95:678,691 ; 12_varprimitive_nr.f95:217
+  ST_HLLC_NOCONV = 4u,     // funciones.f95:240-245
+  ST_HLLC_VSTAR = 8u,      // 16_hllc_flow_mpx.f95:4294,4605
+  ST_NONFINITE = 16u,
+};
+
+// ---- per-instance descriptor (one grid of the ensemble) -------------------
+struct InstDesc {
+  // device buffers
+  double* prim[2];     // double-buffered NPRIM slabs
+  double* aux[2];      // double-buffered NAUX slabs
+  double* stage[2];    // double-buffered NSTAGE slabs
+  double* intsum;      // NCONS slab (needed when the tableau has >= 3 stages)
+  double* finsum;      // NCONS slab
+  double* kbuf;        // nk * NRHS slabs of stored stage right-hand sides
+  double* rhs_out;     // NRHS slab written in the store-rhs mode
+  uint32_t* status;    // status word
+  unsigned long long* counters;  // [3] fix-up counters (rho, p, v)
+  // learned con2prim seed network (null unless c2p method 2)
+  const void* mlp;
+  // geometry
+  int imax, jmax;      // interior points 0..imax, 0..jmax
+  int pitch;           // doubles per row
+  long long fstride;   // doubles per field slab
+  int bc_x, bc_y;      // 0 copy, 1 periodic
+  // scalars
+  double delx, dely, dt, sigma, gamma, kappa_psi, kappa_phi;
+  double eps1_c2p;     // value of the Fortran module variable eps1 when con2prim runs
+  int c2p;             // 1 Cardano, 0 NR, 2 learned seed + Newton (Cardano fallback)
+  // work decomposition of the sweep launches
+  int strips_x;        // column strips of 31 cells
+  int blocks_y;        // row blocks of SWEEP_ROWS cells
+  int block_begin;     // first CTA index of this instance in the launch
+  int block_count;
+};
+
+// ---- tableau data of one stage launch (by value, kernel parameter space) -----
+struct StageArgs {
+  int l;               // 1-based RK stage being swept
+  int s;               // number of stages
+  int cur;             // which prim/aux buffer holds time n
+  int qin;             // which stage buffer holds stage l
+  double wb, wbt;      // wb(l), wbt(l)
+  double ab_next[8];   // Ab(l+1, 1..l)
+  double abt_next[8];  // Abt(l+1, 1..l)
+  double abt_diag_next;// Abt(l+1, l+1)
+  double abt_diag_first;// Abt(1,1) (next step's stage 1)
+  int kslot[8];        // slot of stored K_m in kbuf, -1 if not stored
+  int store_k_slot;    // slot to store K_l, -1 if not needed
+  int need_intsum_load;  // stage l >= 2 and s >= 3: intsum_l is stored
+  int need_intsum_store; // l + 1 < s
+  int mode;            // 0 fused (next stage / final), 1 store rhs only
+};
+
+// ---- small math helpers (Fortran semantics) ------------------------------
+template <typename T> __device__ __forceinline__ T pw2(T x) { return x * x; }
+template <typename T> __device__ __forceinline__ T pw3(T x) { return (x * x) * x; }
+template <typename T> __device__ __forceinline__ T pw4(T x) { T t = x * x; return t * t; }
+template <typename T> __device__ __forceinline__ T fmin2(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T fmax2(T a, T b) { return (b > a) ? b : a; }
+template <typename T> __device__ __forceinline__ T fsgn1(T b) { return copysign(T(1), b); }
+
+// ghost index maps of the reference's boundary routines
+__device__ __forceinline__ int map_idx(int i, int n, int periodic) {
+  if (i < 0) return periodic ? i + n : 0;
+  if (i > n) return periodic ? i - n : n;
+  return i;
+}
+
+constexpr int SWEEP_WARPS = 4;     // column strips per CTA
+constexpr int SWEEP_ROWS = 16;     // output rows per strip march
+constexpr int STRIP = 31;          // output columns per warp (lane 0 is the halo column)
+
+}  // namespace cueva

@@ -1,0 +1,138 @@
+// cueva_mp.cuh -- MP5 / MP7 / MP9 monotonicity-preserving reconstruction
+// (Suresh & Huynh 1997) as one interface pair per thread.
+//
+// The reference reconstructs whole grid lines (mp5.f95:2-278, mp7.f95:2-315,
+// mp9.f95:2-320): for every cell k it forms the limited left value up(k) at
+// k+1/2 and right value um(k) at k-1/2, and the interface between cells i and
+// i+1 takes L = up(i), R = um(i+1) (16_hll_flow_mpx.f95:942-1036).  Every
+// (cell, slot) value depends only on the cells k-R..k+R of its own slot, so a
+// thread that owns interface i loads the 2R+2 cells i-R..i+1+R into registers
+// and evaluates exactly the two values it needs.  Operation order follows the
+// Fortran so the FP64 build without FMA contraction is bit-identical.
+#pragma once
+#include "cueva_common.cuh"
+
+namespace cueva {
+
+template <typename T>
+__device__ __forceinline__ T DMM(T x, T y) {  // funciones.f95:148-162
+  return T(0.5) * (fsgn1(x) + fsgn1(y)) * fmin2(fabs(x), fabs(y));
+}
+template <typename T>
+__device__ __forceinline__ T DM4(T w, T xx, T y, T z) {  // funciones.f95:165-185
+  const T sw = fsgn1(w);
+  return T(0.125) * (sw + fsgn1(xx)) * fabs((sw + fsgn1(y)) * (sw + fsgn1(z))) *
+         fmin2(fmin2(fmin2(fabs(w), fabs(xx)), fabs(y)), fabs(z));
+}
+
+// stencil radius of the unlimited interface formula
+template <int RM> struct MPR { static constexpr int R = RM + 2; };
+
+// unlimited left value at k+1/2 (SH97 eq. 2.1 / 2.31) around register index C
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_vorp(const T (&u)[N]) {
+  if constexpr (RM == 0) {
+    const T b1 = T(1.0 / 60.0);
+    return b1 * (T(2.0) * u[C - 2] - T(13.0) * u[C - 1] + T(47.0) * u[C] + T(27.0) * u[C + 1] - T(3.0) * u[C + 2]);
+  } else if constexpr (RM == 1) {
+    const T b1 = T(1.0 / 420.0);
+    return b1 * (-T(3.0) * u[C - 3] + T(25.0) * u[C - 2] - T(101.0) * u[C - 1] + T(319.0) * u[C] +
+                 T(214.0) * u[C + 1] - T(38.0) * u[C + 2] + T(4.0) * u[C + 3]);
+  } else {
+    const T b1 = T(1.0 / 2520.0);
+    return b1 * (T(4.0) * u[C - 4] - T(41.0) * u[C - 3] + T(199.0) * u[C - 2] - T(641.0) * u[C - 1] +
+                 T(1879.0) * u[C] + T(1375.0) * u[C + 1] - T(305.0) * u[C + 2] + T(55.0) * u[C + 3] -
+                 T(5.0) * u[C + 4]);
+  }
+}
+// unlimited right value at k-1/2 (mirror formulas, same term order as the Fortran)
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_vorm(const T (&u)[N]) {
+  if constexpr (RM == 0) {
+    const T b1 = T(1.0 / 60.0);
+    return b1 * (-T(3.0) * u[C - 2] + T(27.0) * u[C - 1] + T(47.0) * u[C] - T(13.0) * u[C + 1] + T(2.0) * u[C + 2]);
+  } else if constexpr (RM == 1) {
+    const T b1 = T(1.0 / 420.0);
+    return b1 * (-T(3.0) * u[C + 3] + T(25.0) * u[C + 2] - T(101.0) * u[C + 1] + T(319.0) * u[C] +
+                 T(214.0) * u[C - 1] - T(38.0) * u[C - 2] + T(4.0) * u[C - 3]);
+  } else {
+    const T b1 = T(1.0 / 2520.0);
+    return b1 * (T(4.0) * u[C + 4] - T(41.0) * u[C + 3] + T(199.0) * u[C + 2] - T(641.0) * u[C + 1] +
+                 T(1879.0) * u[C] + T(1375.0) * u[C - 1] - T(305.0) * u[C - 2] + T(55.0) * u[C - 3] -
+                 T(5.0) * u[C - 4]);
+  }
+}
+
+// limited up(k) for the cell at register index C (mp5.f95:104-136)
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_up(const T (&u)[N]) {
+  const T alpha = T(2.0), b2 = T(4.0 / 3.0), epsm = T(1.0e-10);
+  const T du0 = u[C] - u[C - 1];
+  const T du1 = u[C + 1] - u[C];
+  const T vorp = mp_vorp<RM, C>(u);
+  const T vmpp = u[C] + DMM(du1, alpha * du0);
+  if ((vorp - u[C]) * (vorp - vmpp) <= epsm) return vorp;
+  const T d2m = u[C - 2] - T(2.0) * u[C - 1] + u[C];
+  const T d20 = u[C - 1] - T(2.0) * u[C] + u[C + 1];
+  const T d2p = u[C] - T(2.0) * u[C + 1] + u[C + 2];
+  const T dm4jph = DM4(T(4.0) * d20 - d2p, T(4.0) * d2p - d20, d20, d2p);
+  const T dm4jmh = DM4(T(4.0) * d20 - d2m, T(4.0) * d2m - d20, d20, d2m);
+  const T vul = u[C] + alpha * du0;
+  const T vav = T(0.5) * (u[C] + u[C + 1]);
+  const T vmd = vav - T(0.5) * dm4jph;
+  const T vlc = u[C] + T(0.5) * du0 + b2 * dm4jmh;
+  const T vmin = fmax2(fmin2(fmin2(u[C], u[C + 1]), vmd), fmin2(fmin2(u[C], vul), vlc));
+  const T vmax = fmin2(fmax2(fmax2(u[C], u[C + 1]), vmd), fmax2(fmax2(u[C], vul), vlc));
+  return vorp + DMM(vmin - vorp, vmax - vorp);
+}
+
+// limited um(k) for the cell at register index C (mp5.f95:142-167)
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_um(const T (&u)[N]) {
+  const T alpha = T(2.0), b2 = T(4.0 / 3.0), epsm = T(1.0e-10);
+  const T du0 = u[C] - u[C - 1];
+  const T du1 = u[C + 1] - u[C];
+  const T vorm = mp_vorm<RM, C>(u);
+  const T vmpm = u[C] + DMM(-du0, -alpha * du1);
+  if ((vorm - u[C]) * (vorm - vmpm) <= epsm) return vorm;
+  const T d2m = u[C - 2] - T(2.0) * u[C - 1] + u[C];
+  const T d20 = u[C - 1] - T(2.0) * u[C] + u[C + 1];
+  const T d2p = u[C] - T(2.0) * u[C + 1] + u[C + 2];
+  const T dm4jph = DM4(T(4.0) * d20 - d2p, T(4.0) * d2p - d20, d20, d2p);
+  const T dm4jmh = DM4(T(4.0) * d20 - d2m, T(4.0) * d2m - d20, d20, d2m);
+  const T vul = u[C] - alpha * du1;
+  const T vav = T(0.5) * (u[C] + u[C - 1]);
+  const T vmd = vav - T(0.5) * dm4jmh;
+  const T vlc = u[C] - T(0.5) * du1 + b2 * dm4jph;
+  const T vmin = fmax2(fmin2(fmin2(u[C], u[C - 1]), vmd), fmin2(fmin2(u[C], vul), vlc));
+  const T vmax = fmin2(fmax2(fmax2(u[C], u[C - 1]), vmd), fmax2(fmax2(u[C], vul), vlc));
+  return vorm + DMM(vmin - vorm, vmax - vorm);
+}
+
+// interface pair: u holds cells i-R .. i+1+R; returns L = up(i), R = um(i+1)
+template <int RM, typename T, int N>
+__device__ __forceinline__ void mp_pair(const T (&u)[N], T& L, T& R) {
+  constexpr int C = MPR<RM>::R;
+  L = mp_up<RM, C>(u);
+  R = mp_um<RM, C + 1>(u);
+}
+
+// pair for the p / rho slots: the positivity fix-up of mp5.f95:177-216 makes
+// the final up(k) depend on um(k) and the final um(k) on up(k)
+template <typename T>
+__device__ __forceinline__ void posfix_point(T uk, T duk, T duk1, T& up, T& um) {
+  if (up < T(0.0)) { up = uk + T(0.50) * DMM(duk, duk1); um = uk; }
+  if (um < T(0.0)) { um = uk - T(0.50) * DMM(duk, duk1); up = uk; }
+}
+template <int RM, typename T, int N>
+__device__ __forceinline__ void mp_pair_pos(const T (&u)[N], T& L, T& R) {
+  constexpr int C = MPR<RM>::R;
+  T up0 = mp_up<RM, C>(u), um0 = mp_um<RM, C>(u);
+  T up1 = mp_up<RM, C + 1>(u), um1 = mp_um<RM, C + 1>(u);
+  posfix_point(u[C], u[C] - u[C - 1], u[C + 1] - u[C], up0, um0);
+  posfix_point(u[C + 1], u[C + 1] - u[C], u[C + 2] - u[C + 1], up1, um1);
+  L = up0;
+  R = um1;
+}
+
+}  // namespace cueva

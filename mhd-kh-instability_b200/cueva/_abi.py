@@ -1,0 +1,90 @@
+"""ctypes binding of include/cueva.h (libcueva_b200.so).
+
+The library is built in-tree (mhd-kh-instability_b200/lib); there is no CPU
+fallback: if the shared object is missing or no GPU is present the calls fail
+loudly with the library's own error message.
+"""
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.normpath(os.path.join(_PKG, "..", "lib"))
+_LIBS = {}
+
+CUEVA_OK, CUEVA_ERR_ARG, CUEVA_ERR_CUDA, CUEVA_ERR_UNBOUND, CUEVA_ERR_PHYSICS = 0, 1, 2, 3, 4
+G_PRIMS, G_CONS = 1, 2
+
+PRIM_FIELDS = ["rho", "p", "vx", "vy", "vz", "psi", "phi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "q"]
+CONS_FIELDS = ["D", "tau", "Sx", "Sy", "Sz", "W"]
+STAGE_FIELDS = ["psiint", "phiint", "Exint", "Eyint", "Ezint", "Bxint", "Byint", "Bzint", "qint", "DDint",
+                "tauint", "Sxint", "Syint", "Szint", "Jxint", "Jyint", "Jzint", "Exast", "Eyast", "Ezast"]
+RHS_FIELDS = ["psiflux", "phiflux", "Exastflux", "Eyastflux", "Ezastflux", "Bxflux", "Byflux", "Bzflux",
+              "qflux", "Dflux", "tauflux", "Sxflux", "Syflux", "Szflux", "Exastsour", "Eyastsour", "Ezastsour"]
+FIELDS = PRIM_FIELDS + CONS_FIELDS + STAGE_FIELDS + RHS_FIELDS
+FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
+PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS)
+
+EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
+           "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
+           "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
+           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init"]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("imax", ctypes.c_int32), ("jmax", ctypes.c_int32), ("order", ctypes.c_int32),
+                ("flux_solver", ctypes.c_int32), ("rec_mp", ctypes.c_int32), ("c2p", ctypes.c_int32),
+                ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("lz", ctypes.c_double), ("cfl", ctypes.c_double), ("sigma", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("dt", ctypes.c_double)]
+
+
+class CuevaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cueva error {code}: {msg}")
+        self.code = code
+
+
+def lib_path(exact=False):
+    return os.path.join(LIBDIR, "libcueva_b200_exact.so" if exact else "libcueva_b200.so")
+
+
+def load(exact=False):
+    """Load the C-ABI library (production build, or the no-FMA parity build)."""
+    key = bool(exact)
+    if key in _LIBS:
+        return _LIBS[key]
+    path = lib_path(exact)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `make -C mhd-kh-instability_b200/csrc`")
+    L = ctypes.CDLL(path)
+    vp, i32, u32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32, ctypes.c_double
+    L.cueva_ctx_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.cueva_ctx_destroy.argtypes = [vp]
+    L.cueva_last_error.restype = ctypes.c_char_p
+    L.cueva_set_stream.argtypes = [vp, vp]
+    L.cueva_dt.restype = dbl
+    L.cueva_dt.argtypes = [vp]
+    L.cueva_tableau_stages.argtypes = [vp]
+    L.cueva_bind_field.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_double)]
+    L.cueva_pin_host.argtypes = [vp, ctypes.c_uint64]
+    L.cueva_unpin_host.argtypes = [vp]
+    L.cueva_upload.argtypes = [vp, u32]
+    L.cueva_download.argtypes = [vp, u32]
+    L.cueva_step.argtypes = [vp, i32]
+    L.cueva_sync.argtypes = [vp]
+    L.cueva_status.argtypes = [vp, ctypes.POINTER(u32)]
+    L.cueva_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.cueva_startconvar.argtypes = [vp]
+    L.cueva_electricvarint.argtypes = [vp, i32]
+    L.cueva_flux_rhs.argtypes = [vp, i32]
+    L.cueva_con2prim.argtypes = [vp]
+    L.cueva_kh_init.argtypes = [vp] + [dbl] * 9
+    _LIBS[key] = L
+    return L
+
+
+def check(L, rc):
+    if rc != CUEVA_OK:
+        raise CuevaError(rc, L.cueva_last_error().decode())
+    return rc

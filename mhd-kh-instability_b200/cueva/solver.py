@@ -1,0 +1,134 @@
+"""Host-side mirror of the reference driver over the C-ABI.
+
+`Cueva` owns Fortran-layout host arrays exactly like the reference's module
+arrays -- each field is dimensioned (-6:imax+6, -6:jmax+6) column-major
+(threevectors.f95:12-81), stage arrays add a slowest 1:lmax index
+(fourvectors.f95:12-170) -- binds them to a context, and exposes the
+routines the way main_cueva_code.f95 calls them: ``step`` replaces the body
+of the time loop (main_cueva_code.f95:53-328), and ``startconvar``,
+``electricvarint``, ``flux_rhs``, ``con2prim`` mirror the single routines.
+In numpy terms a field is an array of shape (jmax+13, imax+13) (C order,
+i fastest) and ``interior(name)`` is its [6:jmax+7, 6:imax+7] view.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+
+class Cueva:
+    def __init__(self, imax, jmax, order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1, precision=0,
+                 device=0, lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, exact=False,
+                 pinned=False):
+        self.L = _abi.load(exact)
+        self.imax, self.jmax = int(imax), int(jmax)
+        self.params = _abi.Params(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, precision, device,
+                                  lx, ly, lz, cfl, sigma, gamma, dt)
+        h = ctypes.c_void_p()
+        _abi.check(self.L, self.L.cueva_ctx_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self.ctx = h
+        self.lmax = self.L.cueva_tableau_stages(self.ctx)
+        self.arrays = {}
+        self._pinned = []
+        self.pinned = pinned
+        for name in _abi.PRIM_FIELDS + _abi.CONS_FIELDS:
+            self._alloc(name)
+
+    # ---------------------------------------------------------------- arrays
+    @property
+    def field_shape(self):
+        return (self.jmax + 13, self.imax + 13)
+
+    def _alloc(self, name):
+        shape = ((self.lmax,) if name in _abi.PER_STAGE else ()) + self.field_shape
+        a = np.zeros(shape, dtype=np.float64)
+        if self.pinned:
+            _abi.check(self.L, self.L.cueva_pin_host(a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
+            self._pinned.append(a)
+        self.arrays[name] = a
+        _abi.check(self.L, self.L.cueva_bind_field(self.ctx, _abi.FIELD_ID[name],
+                                                  a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return a
+
+    def array(self, name):
+        """Fortran-layout host array bound to the context (allocated on first use)."""
+        a = self.arrays.get(name)
+        return a if a is not None else self._alloc(name)
+
+    def interior(self, name, l=None):
+        a = self.array(name)
+        if l is not None:
+            a = a[l - 1]
+        return a[..., 6:self.jmax + 7, 6:self.imax + 7]
+
+    def set_interior(self, name, values, l=None):
+        self.interior(name, l)[...] = values
+
+    def prims(self):
+        return {n: self.interior(n).copy() for n in _abi.PRIM_FIELDS}
+
+    # ------------------------------------------------------------- hot path
+    @property
+    def dt(self):
+        return self.L.cueva_dt(self.ctx)
+
+    def kh_init(self, v0=0.5, a=0.01, amp=0.01, width=0.01, kpert=2 * np.pi, phase=0.0, bshear=0.1, rho0=1.0,
+                p0=1.0):
+        _abi.check(self.L, self.L.cueva_kh_init(self.ctx, v0, a, amp, width, kpert, phase, bshear, rho0, p0))
+
+    def upload(self, groups=_abi.G_PRIMS):
+        _abi.check(self.L, self.L.cueva_upload(self.ctx, groups))
+
+    def download(self, groups=_abi.G_PRIMS):
+        _abi.check(self.L, self.L.cueva_download(self.ctx, groups))
+
+    def step(self, n=1):
+        _abi.check(self.L, self.L.cueva_step(self.ctx, int(n)))
+
+    def sync(self):
+        _abi.check(self.L, self.L.cueva_sync(self.ctx))
+
+    def status(self):
+        s = ctypes.c_uint32()
+        _abi.check(self.L, self.L.cueva_status(self.ctx, ctypes.byref(s)))
+        return s.value
+
+    def counters(self):
+        c = (ctypes.c_int64 * 3)()
+        _abi.check(self.L, self.L.cueva_counters(self.ctx, c))
+        return list(c)
+
+    def set_stream(self, stream_ptr):
+        _abi.check(self.L, self.L.cueva_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
+
+    # ------------------------------------------------------- routine mirrors
+    def startconvar(self):
+        _abi.check(self.L, self.L.cueva_startconvar(self.ctx))
+
+    def electricvarint(self, l):
+        for n in ("Exint", "Eyint", "Ezint", "Jxint", "Jyint", "Jzint"):
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_electricvarint(self.ctx, int(l)))
+
+    def flux_rhs(self, l):
+        for n in _abi.RHS_FIELDS:
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_flux_rhs(self.ctx, int(l)))
+
+    def con2prim(self):
+        _abi.check(self.L, self.L.cueva_con2prim(self.ctx))
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.cueva_ctx_destroy(self.ctx)
+            self.ctx = None
+        for a in self._pinned:
+            self.L.cueva_unpin_host(a.ctypes.data_as(ctypes.c_void_p))
+        self._pinned = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

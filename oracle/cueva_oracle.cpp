@@ -1,0 +1,1457 @@
+// cueva_oracle.cpp -- CPU restatement (test infrastructure only) of the CUEVA
+// per-step hot path.  See cueva_oracle.h for scope and parity status.
+//
+// Every routine mirrors one Fortran routine of cueva_2D_base/ (paths relative
+// to the reference project) and keeps its array layout: fields live on
+// (-6:imax+6, -6:jmax+6), i fastest, exactly like the Fortran module arrays
+// (threevectors.f95:12-81, fourvectors.f95:12-170).  Ghost cells are filled
+// by the boundary maps of 04_boundary.f95 / 24_boundary_conserved.f95 /
+// 24_boundary_flux_conserved.f95 / 25_boundary_electric.f95 (per-axis copy or
+// periodic, node-duplicate convention).
+//
+// Build: g++ -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC
+#include "cueva_oracle.h"
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <map>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// gfortran expands constant integer powers with powi: x**2 = x*x,
+// x**3 = (x*x)*x, x**4 = (x*x)*(x*x).
+inline double pw2(double x) { return x * x; }
+inline double pw3(double x) { return (x * x) * x; }
+inline double pw4(double x) { double t = x * x; return t * t; }
+// Fortran SIGN(a,b) with signed zeros (gfortran -fsign-zero default)
+inline double fsign(double a, double b) { return std::copysign(std::fabs(a), b); }
+inline double fmin2(double a, double b) { return (b < a) ? b : a; }
+inline double fmax2(double a, double b) { return (b > a) ? b : a; }
+inline double fmin3(double a, double b, double c) { return fmin2(fmin2(a, b), c); }
+inline double fmax3(double a, double b, double c) { return fmax2(fmax2(a, b), c); }
+
+constexpr double PI = 3.14159265358979323846264338327950288419716939937510582097494459230781640628620899862803;
+constexpr double THIRD = 0.33333333333333333333333333333333333333333333333333333333333333333333333333333333333;
+
+enum Status : int32_t {
+  ST_OK = 0,
+  ST_C2P_FAIL = 1,        // Cardano "stop" branches (12_varprimitive.f95:382-428,485)
+  ST_SUPERLUMINAL = 2,    // 12_varprimitive.f95:678,691 ; 12_varprimitive_nr.f95:217
+  ST_HLLC_NOCONV = 4,     // funciones.f95:240-245
+  ST_HLLC_VSTAR = 8,      // 16_hllc_flow_mpx.f95:4294,4605
+  ST_NONFINITE = 16,
+};
+
+// ---------------------------------------------------------------- tableaux
+// imex_scheme.f95:13-507 (MIRK = 0 branches)
+struct Tableau { int s; double wb[8], wbt[8], Ab[8][8], Abt[8][8]; };
+
+bool make_tableau(int order, Tableau& T) {
+  std::memset(&T, 0, sizeof(T));
+  const double cst = 1.0 - 1.0 / std::sqrt(2.0);            // parameters.f95:240
+  const double alpha1 = 0.24169426078821, beta1 = 0.06042356519705, etha1 = 0.12915286960590;
+  switch (order) {
+  case 1:  // imex_scheme.f95:15-20
+    T.s = 1; T.wb[0] = 1.0; T.wbt[0] = 0.0; T.Ab[0][0] = 1.0; T.Abt[0][0] = 0.0; return true;
+  case 2:  // SSP2(2,2,2) imex_scheme.f95:42-49
+    T.s = 2; T.wb[0] = 0.5; T.wb[1] = 0.5; T.wbt[0] = 0.5; T.wbt[1] = 0.5;
+    T.Ab[1][0] = 1.0;
+    T.Abt[0][0] = cst; T.Abt[1][0] = 1.0 - 2.0 * cst; T.Abt[1][1] = cst; return true;
+  case 3:  // SSP2(3,3,2)-LUM imex_scheme.f95:77-86
+    T.s = 3; for (int k = 0; k < 3; ++k) { T.wb[k] = 1.0 / 3.0; T.wbt[k] = 1.0 / 3.0; }
+    T.Ab[1][0] = 0.5; T.Ab[2][0] = 0.5; T.Ab[2][1] = 0.5;
+    T.Abt[0][0] = 1.0 / 5.0; T.Abt[1][0] = 1.0 / 10.0; T.Abt[1][1] = 1.0 / 5.0;
+    T.Abt[2][0] = 1.0 / 3.0; T.Abt[2][1] = 1.0 / 3.0; T.Abt[2][2] = 1.0 / 3.0; return true;
+  case 4:  // SSP3(4,3,3) imex_scheme.f95:280-291
+    T.s = 4;
+    T.wb[0] = 0.0; T.wb[1] = 1.0 / 6.0; T.wb[2] = 1.0 / 6.0; T.wb[3] = 2.0 / 3.0;
+    for (int k = 0; k < 4; ++k) T.wbt[k] = T.wb[k];
+    T.Ab[2][1] = 1.0; T.Ab[3][1] = 0.25; T.Ab[3][2] = 0.25;
+    T.Abt[0][0] = alpha1;
+    T.Abt[1][0] = -1.0 * alpha1; T.Abt[1][1] = alpha1;
+    T.Abt[2][1] = 1.0 - alpha1; T.Abt[2][2] = alpha1;
+    T.Abt[3][0] = beta1; T.Abt[3][1] = etha1; T.Abt[3][2] = 0.5 - beta1 - etha1 - alpha1; T.Abt[3][3] = alpha1;
+    return true;
+  case 5: {  // ARS(4,4,3) imex_scheme.f95:328-341
+    T.s = 5;
+    const double wb[5] = {1.0 / 4.0, 7.0 / 4.0, 3.0 / 4.0, -7.0 / 4.0, 0.0};
+    const double wbt[5] = {0.0, 3.0 / 2.0, -3.0 / 2.0, 0.5, 0.5};
+    const double Ab[5][5] = {{0, 0, 0, 0, 0}, {0.5, 0, 0, 0, 0}, {11.0 / 18.0, 1.0 / 18.0, 0, 0, 0},
+                             {5.0 / 6.0, -5.0 / 6.0, 0.5, 0, 0}, {1.0 / 4.0, 7.0 / 4.0, 3.0 / 4.0, -7.0 / 4.0, 0}};
+    const double Abt[5][5] = {{0, 0, 0, 0, 0}, {0, 0.5, 0, 0, 0}, {0, 1.0 / 6.0, 0.5, 0, 0},
+                              {0, -0.5, 0.5, 0.5, 0}, {0, 3.0 / 2.0, -3.0 / 2.0, 0.5, 0.5}};
+    for (int a = 0; a < 5; ++a) { T.wb[a] = wb[a]; T.wbt[a] = wbt[a];
+      for (int b = 0; b < 5; ++b) { T.Ab[a][b] = Ab[a][b]; T.Abt[a][b] = Abt[a][b]; } }
+    return true; }
+  case 6: {  // IMEX-RK36S_E imex_scheme.f95:366-395
+    T.s = 6;
+    const double w[6] = {-0.035877095577305, 0.673080876788404, 0.149064711243777,
+                         0.137173305022086, 0.150219587614740, -0.073661385091702};
+    const double A[6][6] = {
+      {0, 0, 0, 0, 0, 0},
+      {0.342975342284516, 0, 0, 0, 0, 0},
+      {0.016193013787920, 0.309787886268879, 0, 0, 0, 0},
+      {-0.135950059698287, 0.640189764616023, 0.342154021907072, 0, 0, 0},
+      {-0.042056958294301, 0.660781723165128, -0.381308869908091, 1.001236515566727, 0, 0},
+      {0.099109299514465, -0.466919631638661, 1.030492210860962, 0.564549736036252, -0.119257987827582, 0}};
+    const double At[6][6] = {
+      {0.449855695709406, 0, 0, 0, 0, 0},
+      {-0.295189486209790, 0.449855695709406, 0, 0, 0, 0},
+      {0.879036496969614, -0.042071370873823, 0.449855695709406, 0, 0, 0},
+      {0.751731896214317, -0.222508174774298, 0.220689305480633, 0.449855695709406, 0, 0},
+      {-0.039570781554756, 0.788509712948086, 0.685131268735182, -0.144071924307435, 0.449855695709406, 0},
+      {0.382760589609172, -0.196622622060158, 0.904049611197476, 0.680864149962184, 0.571862669923976, 0.449855695709406}};
+    for (int a = 0; a < 6; ++a) { T.wb[a] = w[a]; T.wbt[a] = w[a];
+      for (int b = 0; b < 6; ++b) { T.Ab[a][b] = A[a][b]; T.Abt[a][b] = At[a][b]; } }
+    return true; }
+  case 8: {  // IMEX-RK48SSP imex_scheme.f95:469-507
+    T.s = 8;
+    const double w[8] = {0.0, 277.0 / 1720.0, 385.0 / 1314.0, 587.0 / 1885.0, 31.0 / 18247.0, 665.0 / 2906.0, 0.0, 23.0 / 5731.0};
+    const double A[8][8] = {
+      {0, 0, 0, 0, 0, 0, 0, 0},
+      {0, 0, 0, 0, 0, 0, 0, 0},
+      {0, 966.0 / 2039.0, 0, 0, 0, 0, 0, 0},
+      {0, 199.0 / 5291.0, 735.0 / 1709.0, 0, 0, 0, 0, 0},
+      {0, 306.0 / 4373.0, 533.0 / 1060.0, 773.0 / 628.0, 0, 0, 0, 0},
+      {0, 61.0 / 10399.0, 552.0 / 8267.0, 881.0 / 1054.0, 52.0 / 9395.0, 0, 0, 0},
+      {184.0 / 2869.0, 141.0 / 3059.0, 826.0 / 1929.0, 1567.0 / 757.0, 1754.0 / 977.0, 161.0 / 599.0, 0, 0},
+      {0, 27.0 / 359.0, 227.0 / 2338.0, 53.0 / 557.0, 569.0 / 4644.0, 859.0 / 1966.0, 0, 0}};
+    const double g = 1026.0 / 3919.0;
+    const double At[8][8] = {
+      {g, 0, 0, 0, 0, 0, 0, 0},
+      {-1148.0 / 4385.0, g, 0, 0, 0, 0, 0, 0},
+      {-1165.0 / 2683.0, 904.0 / 1399.0, g, 0, 0, 0, 0, 0},
+      {1480.0 / 2439.0, -1469.0 / 4070.0, -121.0 / 3026.0, g, 0, 0, 0, 0},
+      {-2788.0 / 397.0, 2069.0 / 294.0, 722.0 / 339.0, -411.0 / 682.0, g, 0, 0, 0},
+      {-165.0 / 12667.0, 105.0 / 671.0, 133.0 / 500.0, 1307.0 / 5430.0, 55.0 / 26474.0, g, 0, 0},
+      {837.0 / 1003.0, 629.0 / 1976.0, 1195.0 / 149.0, -5209.0 / 618.0, 1045.0 / 1459.0, 2767.0 / 911.0, g, 0},
+      {-752.0 / 647.0, -771.0 / 2338.0, 3197.0 / 469.0, 2313.0 / 586.0, -2267.0 / 2341.0, -2128.0 / 275.0, 0, g}};
+    for (int a = 0; a < 8; ++a) { T.wb[a] = w[a]; T.wbt[a] = w[a];
+      for (int b = 0; b < 8; ++b) { T.Ab[a][b] = A[a][b]; T.Abt[a][b] = At[a][b]; } }
+    return true; }
+  default: return false;
+  }
+}
+
+// ------------------------------------------------------------ MP5/7/9 line
+// mp5.f95:2-278, mp7.f95:2-315, mp9.f95:2-320 for ONE slot of one grid line.
+// The Fortran routine processes 68 slots at once, but every slot is computed
+// independently (the only cross-slot code is the positivity fix, which reads
+// and writes its own slot), so one slot at a time is the same arithmetic.
+// u, up, um are indexed -6..n+6 (pointer offset +6).  posfix selects the
+// p/rho positivity fix of mp5.f95:177-262 (applied to slots 24,25 / 61,62).
+
+inline double DMM(double x, double y) {  // funciones.f95:148-162
+  return 0.5 * (fsign(1.0, x) + fsign(1.0, y)) * fmin2(std::fabs(x), std::fabs(y));
+}
+inline double DM4(double w, double xx, double y, double z) {  // funciones.f95:165-185
+  return 0.125 * (fsign(1.0, w) + fsign(1.0, xx))
+         * std::fabs((fsign(1.0, w) + fsign(1.0, y)) * (fsign(1.0, w) + fsign(1.0, z)))
+         * fmin2(fmin2(fmin2(std::fabs(w), std::fabs(xx)), std::fabs(y)), std::fabs(z));
+}
+
+void mp_line(int rec_mp, int n, const double* U, int posfix, double* UP, double* UM) {
+  const double* u = U + 6;
+  double* up = UP + 6;
+  double* um = UM + 6;
+  const double b2 = 4.0 / 3.0, epsm = 1.0e-10, alpha_mp = 2.0;
+  const int mm = 0, nn = n;
+  // du, d2 over mm-3..nn+3 (mm-4/mm-5 for MP7/MP9; the extra points are never read)
+  std::vector<double> duv(n + 13, 0.0), d2v(n + 13, 0.0), vorpv(n + 13, 0.0), vormv(n + 13, 0.0),
+      vmppv(n + 13, 0.0), vmpmv(n + 13, 0.0);
+  double* du = duv.data() + 6;
+  double* d2 = d2v.data() + 6;
+  double* vorp = vorpv.data() + 6;
+  double* vorm = vormv.data() + 6;
+  double* vmpp = vmppv.data() + 6;
+  double* vmpm = vmpmv.data() + 6;
+  for (int i = mm - 3; i <= nn + 3; ++i) {
+    du[i] = u[i] - u[i - 1];
+    d2[i] = u[i - 1] - 2.0 * u[i] + u[i + 1];
+  }
+  for (int i = mm - 2; i <= nn + 2; ++i) {
+    if (rec_mp == 0) {
+      const double b1 = 1.0 / 60.0;   // mp5.f95:23, 79-83
+      vorp[i] = b1 * (2.0 * u[i - 2] - 13.0 * u[i - 1] + 47.0 * u[i] + 27.0 * u[i + 1] - 3.0 * u[i + 2]);
+      vorm[i] = b1 * (-3.0 * u[i - 2] + 27.0 * u[i - 1] + 47.0 * u[i] - 13.0 * u[i + 1] + 2.0 * u[i + 2]);
+    } else if (rec_mp == 1) {
+      const double b1 = 1.0 / 420.0;  // mp7.f95:23, 110-117
+      vorp[i] = b1 * (-3.0 * u[i - 3] + 25.0 * u[i - 2] - 101.0 * u[i - 1] + 319.0 * u[i] + 214.0 * u[i + 1]
+                      - 38.0 * u[i + 2] + 4.0 * u[i + 3]);
+      vorm[i] = b1 * (-3.0 * u[i + 3] + 25.0 * u[i + 2] - 101.0 * u[i + 1] + 319.0 * u[i] + 214.0 * u[i - 1]
+                      - 38.0 * u[i - 2] + 4.0 * u[i - 3]);
+    } else {
+      const double b1 = 1.0 / 2520.0; // mp9.f95:25, 114-124
+      vorp[i] = b1 * (4.0 * u[i - 4] - 41.0 * u[i - 3] + 199.0 * u[i - 2] - 641.0 * u[i - 1] + 1879.0 * u[i]
+                      + 1375.0 * u[i + 1] - 305.0 * u[i + 2] + 55.0 * u[i + 3] - 5.0 * u[i + 4]);
+      vorm[i] = b1 * (4.0 * u[i + 4] - 41.0 * u[i + 3] + 199.0 * u[i + 2] - 641.0 * u[i + 1] + 1879.0 * u[i]
+                      + 1375.0 * u[i - 1] - 305.0 * u[i - 2] + 55.0 * u[i - 3] - 5.0 * u[i - 4]);
+    }
+    vmpp[i] = u[i] + DMM(du[i + 1], alpha_mp * du[i]);
+    vmpm[i] = u[i] + DMM(-du[i], -alpha_mp * du[i + 1]);
+  }
+  for (int i = mm - 2; i <= nn + 2; ++i) { up[i] = vorp[i]; um[i] = vorm[i]; }
+  for (int i = mm - 2; i <= nn + 2; ++i) {  // mp5.f95:104-136
+    if ((vorp[i] - u[i]) * (vorp[i] - vmpp[i]) <= epsm) {
+      up[i] = vorp[i];
+    } else {
+      const double dm4jph = DM4(4.0 * d2[i] - d2[i + 1], 4.0 * d2[i + 1] - d2[i], d2[i], d2[i + 1]);
+      const double dm4jmh = DM4(4.0 * d2[i] - d2[i - 1], 4.0 * d2[i - 1] - d2[i], d2[i], d2[i - 1]);
+      const double vul = u[i] + alpha_mp * du[i];
+      const double vav = 0.5 * (u[i] + u[i + 1]);
+      const double vmd = vav - 0.5 * dm4jph;
+      const double vlc = u[i] + 0.5 * du[i] + b2 * dm4jmh;
+      const double vmin = fmax2(fmin3(u[i], u[i + 1], vmd), fmin3(u[i], vul, vlc));
+      const double vmax = fmin2(fmax3(u[i], u[i + 1], vmd), fmax3(u[i], vul, vlc));
+      up[i] = vorp[i] + DMM(vmin - vorp[i], vmax - vorp[i]);
+    }
+  }
+  for (int i = mm - 2; i <= nn + 2; ++i) {  // mp5.f95:142-167
+    if ((vorm[i] - u[i]) * (vorm[i] - vmpm[i]) <= epsm) {
+      um[i] = vorm[i];
+    } else {
+      const double dm4jph = DM4(4.0 * d2[i] - d2[i + 1], 4.0 * d2[i + 1] - d2[i], d2[i], d2[i + 1]);
+      const double dm4jmh = DM4(4.0 * d2[i] - d2[i - 1], 4.0 * d2[i - 1] - d2[i], d2[i], d2[i - 1]);
+      const double vul = u[i] - alpha_mp * du[i + 1];
+      const double vav = 0.5 * (u[i] + u[i - 1]);
+      const double vmd = vav - 0.5 * dm4jmh;
+      const double vlc = u[i] - 0.5 * du[i + 1] + b2 * dm4jph;
+      const double vmin = fmax2(fmin3(u[i], u[i - 1], vmd), fmin3(u[i], vul, vlc));
+      const double vmax = fmin2(fmax3(u[i], u[i - 1], vmd), fmax3(u[i], vul, vlc));
+      um[i] = vorm[i] + DMM(vmin - vorm[i], vmax - vorm[i]);
+    }
+  }
+  if (posfix) {  // mp5.f95:177-216 (and 226-262 for the y slots)
+    for (int i = mm - 2; i <= nn + 2; ++i) {
+      if (up[i] < 0.0) { up[i] = u[i] + 0.50 * DMM(du[i], du[i + 1]); um[i] = u[i]; }
+    }
+    for (int i = mm - 2; i <= nn + 2; ++i) {
+      if (um[i] < 0.0) { um[i] = u[i] - 0.50 * DMM(du[i], du[i + 1]); up[i] = u[i]; }
+    }
+  }
+}
+
+// ---------------------------------------------------------- get_hllc_vel
+// funciones.f95:188-259.  The Fortran evaluates f at the local v before it
+// is ever assigned (line 229); this restatement starts from v = oldv, the
+// seed the routine documents ("Initial seed ... limited to [-1,1]").
+double get_hllc_vel(double a, double b, double c, double rt, int32_t* st) {
+  const int maxiter = 100;
+  const double minerr = 1.0e-12, diferr = 1.0e-3;
+  double oldv = fmax2(-1.0, fmin2(1.0, rt));
+  double v = oldv;
+  int iter = 0;
+  for (;;) {
+    const double fv = a * v * v - b * v + c;
+    const double dfdv = 2.0 * a * v - b;
+    v = fmax2(-1.0, fmin2(1.0, oldv - fv / dfdv));
+    const double err = std::fabs(oldv - v);
+    oldv = v;
+    iter = iter + 1;
+    if (iter >= maxiter) { if (st) *st |= ST_HLLC_NOCONV; break; }
+    if (!(err > minerr)) break;
+  }
+  return fmax2(-1.0 + diferr, fmin2(1.0 - diferr, v));
+}
+
+// -------------------------------------------------------- con2prim, point
+struct C2PIn { double D, tau, Sx, Sy, Sz, Ex, Ey, Ez, Bx, By, Bz, vx0, vy0, vz0, rho0, p0; };
+struct C2POut { double vx, vy, vz, rho, p, W; };
+
+// 12_varprimitive.f95:48-813 with l_swap = 1, VDRIFT = 0, low_vel = 0, REC_ELEC = 0
+int32_t c2p_cardano(const C2PIn& in, double gamma, double eps1, C2POut& o, int64_t* cnt) {
+  int32_t st = 0;
+  const double TOL = 1.0e-10;
+  const int nrmax = 40;
+  double Vx_elec_0 = in.vx0, Vy_elec_0 = in.vy0, Vz_elec_0 = in.vz0;
+  const double Ex_elec_0 = in.Ex, Ey_elec_0 = in.Ey, Ez_elec_0 = in.Ez;
+  const double Bx_elec = in.Bx, By_elec = in.By, Bz_elec = in.Bz;
+  const double D_elec = in.D, Sx_elec = in.Sx, Sy_elec = in.Sy, Sz_elec = in.Sz;
+  double tau_elec = in.tau;
+  double rho_elec = in.rho0, p_elec = in.p0, enthpy_elec = 0.0;
+  double W_elec, V2c, Vx_elec = 0, Vy_elec = 0, Vz_elec = 0;
+  double E2B2 = 0.5 * (Ex_elec_0 * Ex_elec_0 + Ey_elec_0 * Ey_elec_0 + Ez_elec_0 * Ez_elec_0 +
+                       Bx_elec * Bx_elec + By_elec * By_elec + Bz_elec * Bz_elec);
+  double gamma_1 = (gamma - 1.0) / gamma;
+  // do while loop with REC_ELEC = 0 runs exactly once (12_varprimitive.f95:222,756-767)
+  {
+    V2c = pw2(Vx_elec_0) + pw2(Vy_elec_0) + pw2(Vz_elec_0);
+    W_elec = 1.0 / std::sqrt(1.0 - V2c);
+    if (V2c > 1.0) {
+      V2c = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V2c));
+      W_elec = 1.0 / std::sqrt(1.0 - V2c);
+    }
+    E2B2 = 0.5 * (pw2(Ex_elec_0) + pw2(Ey_elec_0) + pw2(Ez_elec_0) + pw2(Bx_elec) + pw2(By_elec) + pw2(Bz_elec));
+    gamma_1 = (gamma - 1.0) / gamma;
+    const double C_1 = pw2(Sx_elec - Ey_elec_0 * Bz_elec + Ez_elec_0 * By_elec)
+                     + pw2(Sy_elec - Ez_elec_0 * Bx_elec + Ex_elec_0 * Bz_elec)
+                     + pw2(Sz_elec - Ex_elec_0 * By_elec + Ey_elec_0 * Bx_elec);
+    const double C_2 = tau_elec - E2B2;
+    const double a_4 = C_1 - pw2(C_2);
+    const double a_3 = 2.0 * gamma_1 * C_2 * D_elec;
+    const double a_2 = pw2(C_2) - 2.0 * gamma_1 * C_1 - pw2(gamma_1) * pw2(D_elec);
+    const double a_1 = -2.0 * gamma_1 * C_2 * D_elec;
+    const double a_0 = pw2(gamma_1) * (C_1 + pw2(D_elec));
+    const double b_3 = a_3 / a_4, b_2 = a_2 / a_4, b_1 = a_1 / a_4, b_0 = a_0 / a_4;
+    const double d_2 = b_2 - (3.0 * pw2(b_3)) / 8.0;
+    const double d_1 = b_1 - (b_3 * b_2) / 2.0 + (pw3(b_3)) / 8.0;
+    const double d_0 = b_0 - (b_3 * b_1) / 4.0 + (pw2(b_3) * b_2) / 16.0 - (3.0 * pw4(b_3)) / 256.0;
+    double Wnro = NAN;
+    const double e = (20.0 * d_2) / 8.0;
+    const double f = -(d_0 - 2.0 * pw2(d_2));
+    const double g = -(pw2(d_1) + 4.0 * d_2 * d_0 - 4.0 * pw3(d_2)) / 8.0;
+    const double Q_1 = (pw2(e) - 3.0 * f) / 9.0;
+    const double R_1 = (2.0 * pw3(e) - 9.0 * e * f + 27.0 * g) / 54.0;
+    double s = 0, t = 0, det = 0, z_1 = 0;
+    if (pw2(R_1) < pw3(Q_1)) {
+      const double T_1 = std::acos(R_1 / std::fabs(std::sqrt(pw3(Q_1))));
+      const double z_1a = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1) / 3.0) - e / 3.0;
+      const double s_1a = d_2 + 2.0 * z_1a;
+      const double t_1a = pw2(z_1a) + 2.0 * d_2 * z_1a + pw2(d_2) - d_0;
+      const double z_1b = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1 + 2.0 * PI) / 3.0) - e / 3.0;
+      const double s_1b = d_2 + 2.0 * z_1b;
+      const double t_1b = pw2(z_1b) + 2.0 * d_2 * z_1b + pw2(d_2) - d_0;
+      const double z_1c = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1 - 2.0 * PI) / 3.0) - e / 3.0;
+      const double s_1c = d_2 + 2.0 * z_1c;
+      const double t_1c = pw2(z_1c) + 2.0 * d_2 * z_1c + pw2(d_2) - d_0;
+      if (s_1a >= 0.0 && t_1a >= 0.0) {
+        s = std::fabs(std::sqrt(s_1a)); t = std::fabs(std::sqrt(t_1a));
+        det = pw2(s) - 4.0 * (d_2 + z_1a - t); z_1 = z_1a;
+        if (det < 0.0) st |= ST_C2P_FAIL;
+      } else if (s_1b >= 0.0 && t_1b >= 0.0) {
+        s = std::fabs(std::sqrt(s_1b)); t = std::fabs(std::sqrt(t_1b));
+        det = pw2(s) - 4.0 * (d_2 + z_1b - t); z_1 = z_1b;
+        if (det < 0.0) st |= ST_C2P_FAIL;
+      } else if (s_1c >= 0.0 && t_1c >= 0.0) {
+        s = std::fabs(std::sqrt(s_1c)); t = std::fabs(std::sqrt(t_1c));
+        det = pw2(s) - 4.0 * (d_2 + z_1c - t); z_1 = z_1c;
+        if (det < 0.0) st |= ST_C2P_FAIL;
+      } else {
+        st |= ST_C2P_FAIL;
+      }
+    } else {
+      const double xx1 = std::fabs(R_1) + std::fabs(std::sqrt(pw2(R_1) - pw3(Q_1)));
+      const double AA_1 = -fsign(1.0, R_1) * fsign(std::fabs(std::pow(xx1, THIRD)), xx1);
+      const double BB_1 = (AA_1 != 0.0) ? Q_1 / AA_1 : 0.0;
+      z_1 = (AA_1 + BB_1) - e / 3.0;
+      s = std::fabs(std::sqrt(d_2 + 2.0 * z_1));
+      t = std::fabs(std::sqrt(pw2(z_1) + 2.0 * d_2 * z_1 + pw2(d_2) - d_0));
+      det = pw2(s) - 4.0 * (d_2 + z_1 - t);
+    }
+    const double Q_2 = -0.5 * (-s + fsign(1.0, -s) * std::fabs(std::sqrt(det)));
+    const double y_1 = Q_2 - b_3 / 4.0;
+    const double y_2 = (d_2 + z_1 - t) / Q_2 - b_3 / 4.0;
+    if (y_1 >= 1.0 && y_2 >= 1.0) Wnro = fmin2(y_1, y_2);
+    if (y_1 <= 1.0 && y_2 <= 1.0) st |= ST_C2P_FAIL;
+    if (y_1 >= 1.0 && y_2 <= 1.0) Wnro = y_1;
+    if (y_1 <= 1.0 && y_2 >= 1.0) Wnro = y_2;
+    // Newton-Raphson polish of W (12_varprimitive.f95:510-526)
+    int nrw = 1;
+    double CHA1 = 1.0;
+    while (CHA1 > TOL && nrw < nrmax) {
+      const double Wnr = Wnro - (pw4(Wnro) + b_3 * pw3(Wnro) + b_2 * pw2(Wnro) + b_1 * Wnro + b_0) /
+                                (4.0 * pw3(Wnro) + 3.0 * b_3 * pw2(Wnro) + 2.0 * b_2 * Wnro + b_1);
+      CHA1 = std::fabs(Wnr - Wnro) / (0.5 * (Wnr + Wnro));
+      Wnro = Wnr;
+      nrw = nrw + 1;
+    }
+    W_elec = Wnro;
+    rho_elec = D_elec / W_elec;
+    if (rho_elec < 0.0) {  // 12_varprimitive.f95:536-548
+      if (cnt) cnt[0] += 1;
+      rho_elec = fmax2(in.rho0 * 1.0e-1, rho_elec);
+    }
+    enthpy_elec = (tau_elec - E2B2 - gamma_1 * rho_elec) / (pw2(W_elec) - gamma_1);
+    p_elec = gamma_1 * (enthpy_elec - rho_elec);
+    // "pressure NR" with frozen epsilon (12_varprimitive.f95:558-587)
+    double pnro = p_elec;
+    int nr = 1;
+    const double epsilonnr = (tau_elec - E2B2 - D_elec * W_elec + pnro * (1.0 - pw2(W_elec))) / (D_elec * W_elec);
+    const double Cs2 = (gamma * (gamma - 1.0) * epsilonnr) / (1.0 + gamma * epsilonnr);
+    double CHA = 1.0;
+    while (CHA >= TOL && nr <= nrmax) {
+      const double pnr = pnro - ((gamma - 1.0) * rho_elec * epsilonnr - pnro) / (V2c * Cs2 - 1.0);
+      CHA = std::fabs(pnr - pnro) / (0.5 * (pnr + pnro));
+      pnro = pnr;
+      nr = nr + 1;
+    }
+    if (pnro < 0.0) {  // 12_varprimitive.f95:592-607
+      if (cnt) cnt[1] += 1;
+      pnro = fmax2(in.p0 * 1.0e-4, pnro);
+    }
+    p_elec = pnro;
+    tau_elec = E2B2 + enthpy_elec * pw2(W_elec) - p_elec;
+    Vx_elec = (Sx_elec - Ey_elec_0 * Bz_elec + Ez_elec_0 * By_elec) / (tau_elec - E2B2 + p_elec);
+    Vy_elec = (Sy_elec - Ez_elec_0 * Bx_elec + Ex_elec_0 * Bz_elec) / (tau_elec - E2B2 + p_elec);
+    Vz_elec = (Sz_elec - Ex_elec_0 * By_elec + Ey_elec_0 * Bx_elec) / (tau_elec - E2B2 + p_elec);
+    V2c = pw2(Vx_elec) + pw2(Vy_elec) + pw2(Vz_elec);
+    W_elec = 1.0 / std::sqrt(1.0 - V2c);
+    if (V2c >= 1.0) {  // 12_varprimitive.f95:627-696
+      const double ErotB = Ey_elec_0 * Bz_elec - Ez_elec_0 * By_elec + Ez_elec_0 * Bx_elec - Ex_elec_0 * Bz_elec +
+                           Ex_elec_0 * By_elec - Ey_elec_0 * Bx_elec;
+      const double B2_drift = pw2(Bx_elec) + pw2(By_elec) + pw2(Bz_elec);
+      if (B2_drift / rho_elec >= 10.0) {
+        const double v_drift = ErotB / B2_drift;
+        const double W_drift = 1.0 / std::sqrt(1.0 - pw2(v_drift));
+        rho_elec = D_elec / W_drift;
+        enthpy_elec = (tau_elec - E2B2 - gamma_1 * rho_elec) / (pw2(W_drift) - gamma_1);
+        p_elec = gamma_1 * (enthpy_elec - rho_elec);
+        tau_elec = E2B2 + enthpy_elec * pw2(W_elec) - p_elec;
+        Vx_elec = (Sx_elec - Ey_elec_0 * Bz_elec + Ez_elec_0 * By_elec) / (tau_elec - E2B2 + p_elec);
+        Vy_elec = (Sy_elec - Ez_elec_0 * Bx_elec + Ex_elec_0 * Bz_elec) / (tau_elec - E2B2 + p_elec);
+        Vz_elec = (Sz_elec - Ex_elec_0 * By_elec + Ey_elec_0 * Bx_elec) / (tau_elec - E2B2 + p_elec);
+        V2c = pw2(Vx_elec) + pw2(Vy_elec) + pw2(Vz_elec);
+        W_elec = 1.0 / std::sqrt(1.0 - V2c);
+        if (cnt) cnt[2] += 1;
+        if (V2c >= 1.0) st |= ST_SUPERLUMINAL;
+      } else {
+        st |= ST_SUPERLUMINAL;
+      }
+    }
+    Vx_elec_0 = Vx_elec; Vy_elec_0 = Vy_elec; Vz_elec_0 = Vz_elec;  // label 111
+  }
+  o.vx = Vx_elec_0; o.vy = Vy_elec_0; o.vz = Vz_elec_0;
+  o.rho = rho_elec; o.p = p_elec; o.W = W_elec;
+  return st;
+}
+
+// 12_varprimitive_nr.f95:28-338 with l_swap = 1, REC_ELEC = 0
+int32_t c2p_nr(const C2PIn& in, double gamma, C2POut& o) {
+  int32_t st = 0;
+  const double TOL = 1.0e-10;
+  const int nrmax = 40;
+  const double Ex = in.Ex, Ey = in.Ey, Ez = in.Ez, Bx = in.Bx, By = in.By, Bz = in.Bz;
+  const double D = in.D, tau = in.tau, Sx = in.Sx, Sy = in.Sy, Sz = in.Sz;
+  double p_elec = in.p0;
+  const double E2B2 = 0.5 * (pw2(Ex) + pw2(Ey) + pw2(Ez) + pw2(Bx) + pw2(By) + pw2(Bz));
+  double Vx = (Sx - Ey * Bz + Ez * By) / (tau - E2B2 + p_elec);
+  double Vy = (Sy - Ez * Bx + Ex * Bz) / (tau - E2B2 + p_elec);
+  double Vz = (Sz - Ex * By + Ey * Bx) / (tau - E2B2 + p_elec);
+  double V2c = pw2(Vx) + pw2(Vy) + pw2(Vz);
+  double W = 1.0 / std::sqrt(1.0 - V2c);
+  double W_2 = 1.0 / (1.0 - V2c);
+  double rho = D / W;
+  const double epsilonnr = (tau - E2B2 - D * W + p_elec * (1.0 - W_2)) / (D * W);
+  const double Cs2 = (gamma * (gamma - 1.0) * epsilonnr) / (1.0 + gamma * epsilonnr);
+  double CHA = 1.0;
+  int nr = 1;
+  double pnro = p_elec;
+  while (CHA >= TOL && nr <= nrmax) {
+    const double pnr = pnro - ((gamma - 1.0) * rho * epsilonnr - pnro) / (V2c * Cs2 - 1.0);
+    CHA = std::fabs(pnr - pnro) / (0.5 * (pnr + pnro));
+    pnro = pnr;
+    nr = nr + 1;
+  }
+  p_elec = pnro;
+  Vx = (Sx - Ey * Bz + Ez * By) / (tau - E2B2 + p_elec);
+  Vy = (Sy - Ez * Bx + Ex * Bz) / (tau - E2B2 + p_elec);
+  Vz = (Sz - Ex * By + Ey * Bx) / (tau - E2B2 + p_elec);
+  V2c = pw2(Vx) + pw2(Vy) + pw2(Vz);
+  W = 1.0 / std::sqrt(1.0 - V2c);
+  W_2 = 1.0 / (1.0 - V2c);
+  (void)W_2;
+  rho = D / W;
+  if (V2c >= 1.0) st |= ST_SUPERLUMINAL;
+  o.vx = Vx; o.vy = Vy; o.vz = Vz; o.rho = rho; o.p = p_elec; o.W = W;
+  return st;
+}
+
+// ------------------------------------------------------------------ state
+struct Arr {
+  std::vector<double> v;
+};
+
+struct Oracle {
+  oracle_params P;
+  int imax, jmax, nxg, nyg;
+  size_t ng;
+  double Delx, Dely, Delz, Delt, kappa_psi, kappa_phi, gamma, sigma;
+  double eps1_c2p;
+  Tableau T;
+  int lmax;
+  int32_t status = 0;
+  int64_t counters[3] = {0, 0, 0};
+
+  std::map<std::string, std::vector<double>> A;    // named ghosted arrays
+  std::vector<std::map<std::string, std::vector<double>>> K;  // per-stage fluxes/sources
+
+  size_t id(int i, int j) const { return (size_t)(i + 6) + (size_t)(j + 6) * nxg; }
+  double* a(const char* n) { return A[n].data(); }
+
+  void alloc(const char* n) { A[n].assign(ng, 0.0); }
+
+  // ghost map: copy (clamp to [0,N]) or periodic (node duplicate: -k -> N-k, N+k -> k)
+  int mapi(int i) const {
+    if (i >= 0 && i <= imax) return i;
+    if (P.bc_x == 1) return i < 0 ? i + imax : i - imax;
+    return i < 0 ? 0 : imax;
+  }
+  int mapj(int j) const {
+    if (j >= 0 && j <= jmax) return j;
+    if (P.bc_y == 1) return j < 0 ? j + jmax : j - jmax;
+    return j < 0 ? 0 : jmax;
+  }
+  // composite of the per-axis ghost fills (same final values for the y-then-x
+  // order of 04_boundary.f95:2867-3033 and the x-then-y order of
+  // 24_boundary_flux_conserved.f95:2088-2788 when imax, jmax >= 6)
+  void fill_ghosts(double* f) {
+    for (int j = -6; j <= jmax + 6; ++j)
+      for (int i = -6; i <= imax + 6; ++i) {
+        if (i >= 0 && i <= imax && j >= 0 && j <= jmax) continue;
+        f[id(i, j)] = f[id(mapi(i), mapj(j))];
+      }
+  }
+
+  explicit Oracle(const oracle_params& p) : P(p) {
+    imax = p.imax; jmax = p.jmax;
+    nxg = imax + 13; nyg = jmax + 13; ng = (size_t)nxg * nyg;
+    Delx = p.lx / (double)imax;             // parameters.f95:306-308
+    Dely = p.ly / (double)jmax;
+    Delz = p.lz / 1.0;
+    const double mn = fmin2(fmin2(Delx, Dely), Delz);
+    Delt = (p.dt > 0.0) ? p.dt : p.cfl * mn; // parameters.f95:312
+    const double cp_psi = std::sqrt(fmin2(Delx, Dely) / 1.0);  // parameters.f95:329-334
+    const double cp_phi = std::sqrt(fmin2(Delx, Dely) / 1.0);
+    kappa_psi = 1.0 / pw2(cp_psi);
+    kappa_phi = 1.0 / pw2(cp_phi);
+    gamma = p.gamma; sigma = p.sigma;
+    // value the module variable eps1 holds when con2prim runs (set last by the flux routine)
+    eps1_c2p = (p.flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
+    make_tableau(p.order, T);
+    lmax = T.s;
+    const char* names[] = {
+      "psi", "phi", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "Vx", "Vy", "Vz", "q", "p", "rho",
+      "V2", "W", "E2", "B2", "epsiln", "enthpy", "D", "tau", "Sx", "Sy", "Sz",
+      "psiintsum", "phiintsum", "Bxintsum", "Byintsum", "Bzintsum", "Exastsum", "Eyastsum", "Ezastsum",
+      "qintsum", "Dintsum", "tauintsum", "Sxintsum", "Syintsum", "Szintsum",
+      "psifinsum", "phifinsum", "Bxfinsum", "Byfinsum", "Bzfinsum", "Exfinsum", "Eyfinsum", "Ezfinsum",
+      "qfinsum", "Dfinsum", "taufinsum", "Sxfinsum", "Syfinsum", "Szfinsum",
+      "psiint", "phiint", "Exast", "Eyast", "Ezast", "Exint", "Eyint", "Ezint", "Bxint", "Byint", "Bzint",
+      "qint", "DDint", "tauint", "Sxint", "Syint", "Szint", "Jxint", "Jyint", "Jzint",
+      // interface fluxes (16_*_flow_mpx.f95 outputs read by 17_fluxandsource.f95)
+      "Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "EzlaxBx", "EzlaxBy", "philaxBy",
+      "EylaxBz", "ExlaxBz", "psilaxEx", "BzlaxEx", "BzlaxEy", "psilaxEy", "BylaxEz", "BxlaxEz",
+      "Jxlax", "Jylax", "FDxlax", "FDylax", "Ftauxlax", "Ftauylax",
+      "FSxxlax", "FSxylax", "FSxzlax", "FSyxlax", "FSyylax", "FSyzlax"};
+    for (const char* n : names) alloc(n);
+    K.resize(lmax);
+    const char* kn[] = {"psiflux", "phiflux", "Bxflux", "Byflux", "Bzflux", "Exastflux", "Eyastflux",
+                        "Ezastflux", "qflux", "Dflux", "tauflux", "Sxflux", "Syflux", "Szflux",
+                        "Exastsour", "Eyastsour", "Ezastsour"};
+    for (int l = 0; l < lmax; ++l)
+      for (const char* n : kn) K[l][n].assign(ng, 0.0);
+  }
+
+  // ------------------------------------------------- 06_conserved_var.f95:79-140
+  void startconvar() {
+    double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *Ex = a("Ex"), *Ey = a("Ey"), *Ez = a("Ez");
+    double *Bx = a("Bx"), *By = a("By"), *Bz = a("Bz"), *p = a("p"), *rho = a("rho");
+    double *V2 = a("V2"), *W = a("W"), *E2 = a("E2"), *B2 = a("B2"), *eps = a("epsiln"), *h = a("enthpy");
+    double *D = a("D"), *tau = a("tau"), *Sx = a("Sx"), *Sy = a("Sy"), *Sz = a("Sz");
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        V2[k] = pw2(Vx[k]) + pw2(Vy[k]) + pw2(Vz[k]);
+        W[k] = 1.0 / std::sqrt(1.0 - V2[k]);
+        E2[k] = pw2(Ex[k]) + pw2(Ey[k]) + pw2(Ez[k]);
+        B2[k] = pw2(Bx[k]) + pw2(By[k]) + pw2(Bz[k]);
+        eps[k] = p[k] / ((gamma - 1.0) * rho[k]);
+        h[k] = rho[k] * (1.0 + eps[k]) + p[k];
+        D[k] = rho[k] * W[k];
+        tau[k] = 0.5 * (E2[k] + B2[k]) + h[k] * pw2(W[k]) - p[k];
+        Sx[k] = (Bz[k] * Ey[k] - By[k] * Ez[k]) + h[k] * pw2(W[k]) * Vx[k];
+        Sy[k] = (Bx[k] * Ez[k] - Bz[k] * Ex[k]) + h[k] * pw2(W[k]) * Vy[k];
+        Sz[k] = (By[k] * Ex[k] - Bx[k] * Ey[k]) + h[k] * pw2(W[k]) * Vz[k];
+      }
+  }
+
+  // ---------------------------------------------------- 07_clean_var.f95:18-58
+  void cleanvarint() {
+    const char* s[] = {"psiintsum", "phiintsum", "Bxintsum", "Byintsum", "Bzintsum", "Exastsum", "Eyastsum",
+                       "Ezastsum", "qintsum", "Dintsum", "tauintsum", "Sxintsum", "Syintsum", "Szintsum",
+                       "psifinsum", "phifinsum", "Bxfinsum", "Byfinsum", "Bzfinsum", "Exfinsum", "Eyfinsum",
+                       "Ezfinsum", "qfinsum", "Dfinsum", "taufinsum", "Sxfinsum", "Syfinsum", "Szfinsum"};
+    for (const char* n : s) std::fill(A[n].begin(), A[n].end(), 0.0);
+  }
+
+  // ------------------------------------------------------- 09_sumint.f95:18-67
+  // EGLM terms carry FAC_EGLM = 0 (parameters.f95:44) and are dropped.
+  void sumint(int l, int m) {  // l, m are 1-based like the Fortran
+    const double ab = T.Ab[l - 1][m - 1], abt = T.Abt[l - 1][m - 1];
+    auto& Km = K[m - 1];
+    const char* s[] = {"psiintsum", "phiintsum", "Bxintsum", "Byintsum", "Bzintsum", "qintsum", "Dintsum",
+                       "tauintsum", "Sxintsum", "Syintsum", "Szintsum"};
+    const char* f[] = {"psiflux", "phiflux", "Bxflux", "Byflux", "Bzflux", "qflux", "Dflux",
+                       "tauflux", "Sxflux", "Syflux", "Szflux"};
+    for (int c = 0; c < 11; ++c) {
+      double* S = a(s[c]);
+      const double* F = Km[f[c]].data();
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); S[k] = S[k] + ab * F[k]; }
+    }
+    const char* es[] = {"Exastsum", "Eyastsum", "Ezastsum"};
+    const char* ef[] = {"Exastflux", "Eyastflux", "Ezastflux"};
+    const char* eo[] = {"Exastsour", "Eyastsour", "Ezastsour"};
+    for (int c = 0; c < 3; ++c) {
+      double* S = a(es[c]);
+      const double* F = Km[ef[c]].data();
+      const double* O = Km[eo[c]].data();
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); S[k] = S[k] + (ab * F[k] - abt * O[k]); }
+    }
+  }
+
+  // -------------------------------------------------------- 10_varint.f95:18-72
+  void varint() {
+    const char* dst[] = {"psiint", "phiint", "Bxint", "Byint", "Bzint", "Exast", "Eyast", "Ezast",
+                         "qint", "DDint", "tauint", "Sxint", "Syint", "Szint"};
+    const char* src[] = {"psi", "phi", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "q", "D", "tau", "Sx", "Sy", "Sz"};
+    const char* sum[] = {"psiintsum", "phiintsum", "Bxintsum", "Byintsum", "Bzintsum", "Exastsum", "Eyastsum",
+                         "Ezastsum", "qintsum", "Dintsum", "tauintsum", "Sxintsum", "Syintsum", "Szintsum"};
+    for (int c = 0; c < 14; ++c) {
+      double* d = a(dst[c]);
+      const double* s = a(src[c]);
+      const double* S = a(sum[c]);
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); d[k] = s[k] + Delt * S[k]; }
+    }
+    const char* bc[] = {"psiint", "phiint", "Bxint", "Byint", "Bzint", "qint", "DDint", "tauint",
+                        "Sxint", "Syint", "Szint"};
+    for (const char* n : bc) fill_ghosts(a(n));   // boundary_conserved
+  }
+
+  // ------------------------------------------- 11_elecvarint.f95:279-328 (IMEX)
+  // a(l) and matx(l) are per-cell temporaries here (the Fortran shares them
+  // between OpenMP threads, 11_elecvarint.f95:13).
+  void electricvarint(int l) {
+    const double abtll = T.Abt[l - 1][l - 1];
+    double *W = a("W"), *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz");
+    double *Bx = a("Bxint"), *By = a("Byint"), *Bz = a("Bzint");
+    double *Exa = a("Exast"), *Eya = a("Eyast"), *Eza = a("Ezast");
+    double *Exi = a("Exint"), *Eyi = a("Eyint"), *Ezi = a("Ezint");
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        const double al = abtll * sigma * Delt;
+        const double Wk = W[k], vx = Vx[k], vy = Vy[k], vz = Vz[k];
+        const double matx = pw2(Wk) * al + Wk * pw2(al) + Wk + al;
+        const double vrotB_x = (Bz[k] * vy - By[k] * vz);
+        const double vrotB_y = (Bx[k] * vz - Bz[k] * vx);
+        const double vrotB_z = (By[k] * vx - Bx[k] * vy);
+        Exi[k] = (1.0 / matx) * (
+            (al + Wk + al * pw2(Wk) * pw2(vx)) * Exa[k] +
+            al * pw2(Wk) * vx * vy * Eya[k] +
+            al * pw2(Wk) * vx * vz * Eza[k] -
+            abtll * sigma * Wk * Delt * (
+              (al + Wk + al * pw2(Wk) * pw2(vx)) * vrotB_x +
+              al * pw2(Wk) * vx * vy * vrotB_y +
+              al * pw2(Wk) * vx * vz * vrotB_z));
+        Eyi[k] = (1.0 / matx) * (
+            al * pw2(Wk) * vx * vy * Exa[k] +
+            (al + Wk + al * pw2(Wk) * pw2(vy)) * Eya[k] +
+            al * pw2(Wk) * vy * vz * Eza[k] -
+            abtll * sigma * Wk * Delt * (
+              al * pw2(Wk) * vx * vy * vrotB_x +
+              (al + Wk + al * pw2(Wk) * pw2(vy)) * vrotB_y +
+              al * pw2(Wk) * vy * vz * vrotB_z));
+        Ezi[k] = (1.0 / matx) * (
+            al * pw2(Wk) * vx * vz * Exa[k] +
+            al * pw2(Wk) * vy * vz * Eya[k] +
+            (al + Wk + al * pw2(Wk) * pw2(vz)) * Eza[k] -
+            abtll * sigma * Wk * Delt * (
+              al * pw2(Wk) * vx * vz * vrotB_x +
+              al * pw2(Wk) * vy * vz * vrotB_y +
+              (al + Wk + al * pw2(Wk) * pw2(vz)) * vrotB_z));
+      }
+    fill_ghosts(Exi); fill_ghosts(Eyi); fill_ghosts(Ezi);   // boundary_electric
+  }
+
+  // ------------------------------------------- 14_flowinit.f95:264-302 (J only;
+  // the centre fluxes are only read when flux_rec_mp5 = 1)
+  void flowinit() {
+    double *W = a("W"), *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz");
+    double *Ex = a("Exint"), *Ey = a("Eyint"), *Ez = a("Ezint");
+    double *Bx = a("Bxint"), *By = a("Byint"), *Bz = a("Bzint"), *q = a("qint");
+    double *Jx = a("Jxint"), *Jy = a("Jyint"), *Jz = a("Jzint");
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        const double Edotv = Ex[k] * Vx[k] + Ey[k] * Vy[k] + Ez[k] * Vz[k];
+        const double vrotB_x = (Bz[k] * Vy[k] - By[k] * Vz[k]);
+        const double vrotB_y = (Bx[k] * Vz[k] - Bz[k] * Vx[k]);
+        const double vrotB_z = (By[k] * Vx[k] - Bx[k] * Vy[k]);
+        Jx[k] = sigma * W[k] * (Ex[k] + vrotB_x - Edotv * Vx[k]) + q[k] * Vx[k];
+        Jy[k] = sigma * W[k] * (Ey[k] + vrotB_y - Edotv * Vy[k]) + q[k] * Vy[k];
+        Jz[k] = sigma * W[k] * (Ez[k] + vrotB_z - Edotv * Vz[k]) + q[k] * Vz[k];
+      }
+    fill_ghosts(Jx); fill_ghosts(Jy); fill_ghosts(Jz);   // boundary_flux_conserved
+  }
+
+  // ----------------------------------------- reconstruction passes (MPX 2D)
+  // x slots of 16_hll_flow_mpx.f95:784-894 and y slots of :1086-1197
+  enum XS { X_PSI = 0, X_PHI, X_EX, X_EY, X_EZ, X_EXM, X_EYM, X_EZM, X_BX, X_BY, X_BZ, X_BXM, X_BYM, X_BZM,
+            X_Q, X_D, X_TAU, X_SX, X_SY, X_SZ, X_VX, X_VY, X_VZ, X_P, X_RHO, X_JX, X_JZ, X_N };
+  enum YS { Y_PSI = 0, Y_PHI, Y_EX, Y_EY, Y_EZ, Y_EXM, Y_EYM, Y_EZM, Y_BX, Y_BY, Y_BZ, Y_BXM, Y_BYM, Y_BZM,
+            Y_Q, Y_D, Y_TAU, Y_SX, Y_SY, Y_SZ, Y_VX, Y_VY, Y_VZ, Y_P, Y_RHO, Y_JY, Y_N };
+  std::vector<std::vector<double>> XL, XR, YL, YR;   // [slot][ghosted 2D]
+
+  void slot_src(int slot, bool xdir, const double*& src, double& sgn) {
+    sgn = 1.0;
+    // identical ordering for x and y up to the current slot
+    switch (slot) {
+      case X_PSI: src = a("psiint"); break;
+      case X_PHI: src = a("phiint"); break;
+      case X_EX: src = a("Exint"); break;
+      case X_EY: src = a("Eyint"); break;
+      case X_EZ: src = a("Ezint"); break;
+      case X_EXM: src = a("Exint"); sgn = -1.0; break;
+      case X_EYM: src = a("Eyint"); sgn = -1.0; break;
+      case X_EZM: src = a("Ezint"); sgn = -1.0; break;
+      case X_BX: src = a("Bxint"); break;
+      case X_BY: src = a("Byint"); break;
+      case X_BZ: src = a("Bzint"); break;
+      case X_BXM: src = a("Bxint"); sgn = -1.0; break;
+      case X_BYM: src = a("Byint"); sgn = -1.0; break;
+      case X_BZM: src = a("Bzint"); sgn = -1.0; break;
+      case X_Q: src = a("qint"); break;
+      case X_D: src = a("DDint"); break;
+      case X_TAU: src = a("tauint"); break;
+      case X_SX: src = a("Sxint"); break;
+      case X_SY: src = a("Syint"); break;
+      case X_SZ: src = a("Szint"); break;
+      case X_VX: src = a("Vx"); break;
+      case X_VY: src = a("Vy"); break;
+      case X_VZ: src = a("Vz"); break;
+      case X_P: src = a("p"); break;
+      case X_RHO: src = a("rho"); break;
+      case X_JX: src = xdir ? a("Jxint") : a("Jyint"); break;   // slot 26 (x) / 63 (y)
+      case X_JZ: src = a("Jzint"); break;                      // slot 27 (x only)
+      default: src = nullptr;
+    }
+  }
+
+  void reconstruct() {
+    const int rec = P.rec_mp;
+    XL.assign(X_N, std::vector<double>(ng, 0.0)); XR.assign(X_N, std::vector<double>(ng, 0.0));
+    YL.assign(Y_N, std::vector<double>(ng, 0.0)); YR.assign(Y_N, std::vector<double>(ng, 0.0));
+    // x pass: lines imp = -1..jmax+1 (16_hll_flow_mpx.f95:781)
+#pragma omp parallel
+    {
+      std::vector<double> u(imax + 13), up(imax + 13), um(imax + 13);
+#pragma omp for schedule(static)
+      for (int jj = -1; jj <= jmax + 1; ++jj) {
+        for (int s = 0; s < X_N; ++s) {
+          const double* src; double sg;
+          slot_src(s, true, src, sg);
+          for (int i = -6; i <= imax + 6; ++i) u[i + 6] = (sg < 0) ? -src[id(i, jj)] : src[id(i, jj)];
+          mp_line(rec, imax, u.data(), (s == X_P || s == X_RHO), up.data(), um.data());
+          for (int i = -1; i <= imax + 1; ++i) {    // :942-1036
+            XL[s][id(i, jj)] = up[i + 6];
+            XR[s][id(i, jj)] = um[i + 1 + 6];
+          }
+        }
+      }
+    }
+    // y pass: lines imp = -1..imax+1 (16_hll_flow_mpx.f95:1083)
+#pragma omp parallel
+    {
+      std::vector<double> u(jmax + 13), up(jmax + 13), um(jmax + 13);
+#pragma omp for schedule(static)
+      for (int ii = -1; ii <= imax + 1; ++ii) {
+        for (int s = 0; s < Y_N; ++s) {
+          const double* src; double sg;
+          slot_src(s, false, src, sg);
+          for (int j = -6; j <= jmax + 6; ++j) u[j + 6] = (sg < 0) ? -src[id(ii, j)] : src[id(ii, j)];
+          mp_line(rec, jmax, u.data(), (s == Y_P || s == Y_RHO), up.data(), um.data());
+          for (int j = -1; j <= jmax + 1; ++j) {    // :1240-1329
+            YL[s][id(ii, j)] = up[j + 6];
+            YR[s][id(ii, j)] = um[j + 1 + 6];
+          }
+        }
+      }
+    }
+  }
+
+  // per-interface reconstructed state of one side
+  struct Side {
+    double psi, phi, Ex, Ey, Ez, Exm, Eym, Ezm, Bx, By, Bz, Bxm, Bym, Bzm, q, D, tau, Sx, Sy, Sz;
+    double vx, vy, vz, p, rho, J;   // J = Jx (x side) or Jy (y side)
+  };
+  Side side(const std::vector<std::vector<double>>& R, size_t k) {
+    Side s;
+    s.psi = R[X_PSI][k]; s.phi = R[X_PHI][k];
+    s.Ex = R[X_EX][k]; s.Ey = R[X_EY][k]; s.Ez = R[X_EZ][k];
+    s.Exm = R[X_EXM][k]; s.Eym = R[X_EYM][k]; s.Ezm = R[X_EZM][k];
+    s.Bx = R[X_BX][k]; s.By = R[X_BY][k]; s.Bz = R[X_BZ][k];
+    s.Bxm = R[X_BXM][k]; s.Bym = R[X_BYM][k]; s.Bzm = R[X_BZM][k];
+    s.q = R[X_Q][k]; s.D = R[X_D][k]; s.tau = R[X_TAU][k];
+    s.Sx = R[X_SX][k]; s.Sy = R[X_SY][k]; s.Sz = R[X_SZ][k];
+    s.vx = R[X_VX][k]; s.vy = R[X_VY][k]; s.vz = R[X_VZ][k];
+    s.p = R[X_P][k]; s.rho = R[X_RHO][k]; s.J = R[X_JX][k];
+    return s;
+  }
+
+  // physical fluxes of one side (16_hll_flow_mpx.f95:1464-1733, flux_rec_mp5 = 0)
+  struct PhysX { double W, h, FD, Ftau, FSx, FSy, FSz; };
+  PhysX physx(const Side& s) {  // x direction
+    PhysX f;
+    const double V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
+    f.W = 1.0 / std::sqrt(1.0 - V2);
+    const double E2B2 = pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez) + pw2(s.Bx) + pw2(s.By) + pw2(s.Bz);
+    const double eps = s.p / ((gamma - 1.0) * s.rho);
+    f.h = s.rho * (1.0 + eps) + s.p;
+    f.FD = s.D * s.vx;
+    f.Ftau = (s.Bz * s.Ey - s.By * s.Ez) + f.h * pw2(f.W) * s.vx;
+    f.FSx = -pw2(s.Ex) - pw2(s.Bx) + f.h * pw2(f.W) * pw2(s.vx) + 0.5 * E2B2 + s.p;
+    f.FSy = -s.Ex * s.Ey - s.Bx * s.By + f.h * pw2(f.W) * s.vx * s.vy;
+    f.FSz = -s.Ex * s.Ez - s.Bx * s.Bz + f.h * pw2(f.W) * s.vx * s.vz;
+    return f;
+  }
+  PhysX physy(const Side& s) {  // y direction: FSx is FSyx, FSy is FSyy, FSz is FSyz
+    PhysX f;
+    const double V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
+    f.W = 1.0 / std::sqrt(1.0 - V2);
+    const double E2B2 = pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez) + pw2(s.Bx) + pw2(s.By) + pw2(s.Bz);
+    const double eps = s.p / ((gamma - 1.0) * s.rho);
+    f.h = s.rho * (1.0 + eps) + s.p;
+    f.FD = s.D * s.vy;
+    f.Ftau = (s.Bx * s.Ez - s.Bz * s.Ex) + f.h * pw2(f.W) * s.vy;
+    f.FSx = -s.Ex * s.Ey - s.Bx * s.By + f.h * pw2(f.W) * s.vx * s.vy;
+    f.FSy = -pw2(s.Ey) - pw2(s.By) + f.h * pw2(f.W) * pw2(s.vy) + 0.5 * E2B2 + s.p;
+    f.FSz = -s.Ey * s.Ez - s.By * s.Bz + f.h * pw2(f.W) * s.vy * s.vz;
+    return f;
+  }
+  // HLLE variant of the physical fluxes: W from 1 - vx^2 - vy^2 - vz^2
+  // (16_hlle_flow_mpx.f95:2289-2292)
+  void hlle_w(PhysX& f, const Side& s) {
+    f.W = 1.0 / std::sqrt(1.0 - pw2(s.vx) - pw2(s.vy) - pw2(s.vz));
+  }
+
+  static double hllf(double FL, double FR, double UL, double UR) {
+    const double s1 = -1.0, s2 = 1.0;   // parameters.f95:283-284
+    return (s2 * FL - s1 * FR + s1 * s2 * (UR - UL)) / (s2 - s1);
+  }
+
+  // ------------------------------------------- Riemann loop (2D, i=-1..imax, j=-1..jmax)
+  void riemann() {
+    const int solver = P.flux_solver;
+    double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *rho = a("rho");
+    double* o[28];
+    const char* on[] = {"Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "EzlaxBx", "EzlaxBy",
+                        "philaxBy", "EylaxBz", "ExlaxBz", "psilaxEx", "BzlaxEx", "BzlaxEy", "psilaxEy",
+                        "BylaxEz", "BxlaxEz", "Jxlax", "Jylax", "FDxlax", "FDylax", "Ftauxlax", "Ftauylax",
+                        "FSxxlax", "FSxylax", "FSxzlax", "FSyxlax", "FSyylax", "FSyzlax"};
+    for (int c = 0; c < 28; ++c) o[c] = a(on[c]);
+    int32_t st_acc = 0;
+#pragma omp parallel for schedule(static) reduction(| : st_acc)
+    for (int j = -1; j <= jmax; ++j)
+      for (int i = -1; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        Side xl = side(XL, k), xr = side(XR, k);
+        Side yl = side(YL, k), yr = side(YR, k);
+        yl.J = YL[Y_JY][k]; yr.J = YR[Y_JY][k];
+        if (solver == 5 || solver == 7) {
+          // superluminal fall-back, 16_hll_flow_mpx.f95:1393-1462
+          double V2xl = pw2(xl.vx) + pw2(xl.vy) + pw2(xl.vz);
+          double V2xr = pw2(xr.vx) + pw2(xr.vy) + pw2(xr.vz);
+          double V2yl = pw2(yl.vx) + pw2(yl.vy) + pw2(yl.vz);
+          double V2yr = pw2(yr.vx) + pw2(yr.vy) + pw2(yr.vz);
+          auto fallback = [&]() {
+            xl.vx = Vx[id(i, j)]; xr.vx = Vx[id(i - 1, j)];
+            xl.vy = Vy[id(i, j)]; xr.vy = Vy[id(i - 1, j)];
+            xl.vz = Vz[id(i, j)]; xr.vz = Vz[id(i - 1, j)];
+            yl.vx = Vx[id(i, j)]; yr.vx = Vx[id(i, j - 1)];
+            yl.vy = Vy[id(i, j)]; yr.vy = Vy[id(i, j - 1)];
+            yl.vz = Vz[id(i, j)]; yr.vz = Vz[id(i, j - 1)];
+            V2yl = pw2(yl.vx) + pw2(yl.vy) + pw2(yl.vz);
+            V2yr = pw2(yr.vx) + pw2(yr.vy) + pw2(yr.vz);
+            V2xl = pw2(xl.vx) + pw2(xl.vy) + pw2(xl.vz);
+            V2xr = pw2(xr.vx) + pw2(xr.vy) + pw2(xr.vz);
+          };
+          if (V2xl >= 1.0 || V2xr >= 1.0) fallback();
+          if (V2yl >= 1.0 || V2yr >= 1.0) fallback();
+        }
+        if (solver == 7) {
+          // density fix-up chain, 16_hllc_flow_mpx.f95:2663-2690
+          if (yl.rho < 0.0) yl.rho = rho[k] * 1.0e-1;
+          else if (yr.rho < 0.0) yr.rho = rho[k] * 1.0e-1;
+          else if (xl.rho < 0.0) xl.rho = rho[k] * 1.0e-1;
+          else if (xr.rho < 0.0) xr.rho = rho[k] * 1.0e-1;
+        }
+        PhysX fxl = physx(xl), fxr = physx(xr), fyl = physy(yl), fyr = physy(yr);
+        if (solver == 6) { hlle_w(fxl, xl); hlle_w(fxr, xr); hlle_w(fyl, yl); hlle_w(fyr, yr);
+          fxl = physx_w(xl, fxl.W); fxr = physx_w(xr, fxr.W); fyl = physy_w(yl, fyl.W); fyr = physy_w(yr, fyr.W); }
+        double out[28];
+        // EM + charge fluxes are HLL for every solver (HLLC star EM fluxes equal the HLL ones)
+        out[0] = hllf(xl.Ex, xr.Ex, xl.psi, xr.psi);                 // Exlaxpsi
+        out[1] = hllf(yl.Ey, yr.Ey, yl.psi, yr.psi);                 // Eylaxpsi
+        out[2] = hllf(xl.Bx, xr.Bx, xl.phi, xr.phi);                 // Bxlaxphi
+        out[3] = hllf(yl.By, yr.By, yl.phi, yr.phi);                 // Bylaxphi
+        out[4] = hllf(xl.phi, xr.phi, xl.Bx, xr.Bx);                 // philaxBx
+        out[5] = hllf(yl.Ez, yr.Ez, yl.Bx, yr.Bx);                   // EzlaxBx
+        out[6] = -hllf(xl.Ezm, xr.Ezm, xl.By, xr.By);                // EzlaxBy
+        out[7] = hllf(yl.phi, yr.phi, yl.By, yr.By);                 // philaxBy
+        out[8] = hllf(xl.Ey, xr.Ey, xl.Bz, xr.Bz);                   // EylaxBz
+        out[9] = -hllf(yl.Exm, yr.Exm, yl.Bz, yr.Bz);                // ExlaxBz
+        out[10] = hllf(xl.psi, xr.psi, xl.Ex, xr.Ex);                // psilaxEx
+        out[11] = -hllf(yl.Bzm, yr.Bzm, yl.Ex, yr.Ex);               // BzlaxEx
+        out[12] = hllf(xl.Bz, xr.Bz, xl.Ey, xr.Ey);                  // BzlaxEy
+        out[13] = hllf(yl.psi, yr.psi, yl.Ey, yr.Ey);                // psilaxEy
+        out[14] = -hllf(xl.Bym, xr.Bym, xl.Ez, xr.Ez);               // BylaxEz
+        out[15] = hllf(yl.Bx, yr.Bx, yl.Ez, yr.Ez);                  // BxlaxEz
+        out[16] = hllf(xl.J, xr.J, xl.q, xr.q);                      // Jxlax
+        out[17] = hllf(yl.J, yr.J, yl.q, yr.q);                      // Jylax
+        if (solver == 5) {  // 16_hll_flow_mpx.f95:1871-1924
+          out[18] = hllf(fxl.FD, fxr.FD, xl.D, xr.D);
+          out[19] = hllf(fyl.FD, fyr.FD, yl.D, yr.D);
+          out[20] = hllf(fxl.Ftau, fxr.Ftau, xl.tau, xr.tau);
+          out[21] = hllf(fyl.Ftau, fyr.Ftau, yl.tau, yr.tau);
+          out[22] = hllf(fxl.FSx, fxr.FSx, xl.Sx, xr.Sx);
+          out[23] = hllf(fxl.FSy, fxr.FSy, xl.Sy, xr.Sy);
+          out[24] = hllf(fxl.FSz, fxr.FSz, xl.Sz, xr.Sz);
+          out[25] = hllf(fyl.FSx, fyr.FSx, yl.Sx, yr.Sx);
+          out[26] = hllf(fyl.FSy, fyr.FSy, yl.Sy, yr.Sy);
+          out[27] = hllf(fyl.FSz, fyr.FSz, yl.Sz, yr.Sz);
+        } else if (solver == 7) {
+          st_acc |= hllc_x(xl, xr, fxl, fxr, out);
+          st_acc |= hllc_y(yl, yr, fyl, fyr, out);
+        } else {
+          st_acc |= hlle_x(xl, xr, fxl, fxr, out);
+          st_acc |= hlle_y(yl, yr, fyl, fyr, out);
+        }
+        for (int c = 0; c < 28; ++c) o[c][k] = out[c];
+      }
+    status |= st_acc;
+  }
+
+  PhysX physx_w(const Side& s, double W) {
+    PhysX f = physx(s); f.W = W;
+    const double eps = s.p / ((gamma - 1.0) * s.rho);
+    f.h = s.rho * (1.0 + eps) + s.p;
+    const double E2B2 = pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez) + pw2(s.Bx) + pw2(s.By) + pw2(s.Bz);
+    f.Ftau = (s.Bz * s.Ey - s.By * s.Ez) + f.h * pw2(f.W) * s.vx;
+    f.FSx = -pw2(s.Ex) - pw2(s.Bx) + f.h * pw2(f.W) * pw2(s.vx) + 0.5 * E2B2 + s.p;
+    f.FSy = -s.Ex * s.Ey - s.Bx * s.By + f.h * pw2(f.W) * s.vx * s.vy;
+    f.FSz = -s.Ex * s.Ez - s.Bx * s.Bz + f.h * pw2(f.W) * s.vx * s.vz;
+    return f;
+  }
+  PhysX physy_w(const Side& s, double W) {
+    PhysX f = physy(s); f.W = W;
+    const double eps = s.p / ((gamma - 1.0) * s.rho);
+    f.h = s.rho * (1.0 + eps) + s.p;
+    const double E2B2 = pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez) + pw2(s.Bx) + pw2(s.By) + pw2(s.Bz);
+    f.Ftau = (s.Bx * s.Ez - s.Bz * s.Ex) + f.h * pw2(f.W) * s.vy;
+    f.FSx = -s.Ex * s.Ey - s.Bx * s.By + f.h * pw2(f.W) * s.vx * s.vy;
+    f.FSy = -pw2(s.Ey) - pw2(s.By) + f.h * pw2(f.W) * pw2(s.vy) + 0.5 * E2B2 + s.p;
+    f.FSz = -s.Ey * s.Ez - s.By * s.Bz + f.h * pw2(f.W) * s.vy * s.vz;
+    return f;
+  }
+
+  // ----------------------------------------- HLLC, x direction
+  // 16_hllc_flow_mpx.f95:2816-3100 (HLL states/fluxes), 3184-3335 (v*),
+  // 3485-3520 (star states), 3592-3740 (star fluxes), 3908-4300 (selection)
+  int32_t hllc_x(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+    int32_t st = 0;
+    const double s1 = -1.0, s2 = 1.0;
+    const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ex - R.Ex) / (s2 - s1);
+    const double phi_hll = (s2 * R.phi - s1 * L.phi + L.Bx - R.Bx) / (s2 - s1);
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.psi - R.psi) / (s2 - s1);
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.Bz - R.Bz) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bym - R.Bym) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.phi - R.phi) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.Ezm - R.Ezm) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Ey - R.Ey) / (s2 - s1);
+    const double DD_hll = (s2 * R.D - s1 * L.D + fl.FD - fr.FD) / (s2 - s1);
+    const double tau_hll = (s2 * R.tau - s1 * L.tau + fl.Ftau - fr.Ftau) / (s2 - s1);
+    const double Sx_hll = (s2 * R.Sx - s1 * L.Sx + fl.FSx - fr.FSx) / (s2 - s1);
+    const double Sy_hll = (s2 * R.Sy - s1 * L.Sy + fl.FSy - fr.FSy) / (s2 - s1);
+    const double Sz_hll = (s2 * R.Sz - s1 * L.Sz + fl.FSz - fr.FSz) / (s2 - s1);
+    const double psi_f = 0.5 * (L.Ex + R.Ex - (R.psi - L.psi));
+    const double phi_f = 0.5 * (L.Bx + R.Bx - (R.phi - L.phi));
+    const double Bx_f = 0.5 * (L.phi + R.phi - (R.Bx - L.Bx));
+    const double By_f = 0.5 * (L.Ezm + R.Ezm - (R.By - L.By));
+    const double Bz_f = 0.5 * (L.Ey + R.Ey - (R.Bz - L.Bz));
+    const double Ex_f = 0.5 * (L.psi + R.psi - (R.Ex - L.Ex));
+    const double Ey_f = 0.5 * (L.Bz + R.Bz - (R.Ey - L.Ey));
+    const double Ez_f = 0.5 * (L.Bym + R.Bym - (R.Ez - L.Ez));
+    const double q_f = 0.5 * (L.J + R.J - (R.q - L.q));
+    const double DD_f = 0.5 * (fl.FD + fr.FD - (R.D - L.D));
+    const double tau_f = 0.5 * (fl.Ftau + fr.Ftau - (R.tau - L.tau));
+    const double Sx_f = 0.5 * (fl.FSx + fr.FSx - (R.Sx - L.Sx));
+    const double Sy_f = 0.5 * (fl.FSy + fr.FSy - (R.Sy - L.Sy));
+    const double Sz_f = 0.5 * (fl.FSz + fr.FSz - (R.Sz - L.Sz));
+    // star E, B are the HLL averages (L and R identical)
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Eys) + pw2(Ezs));
+    const double B2_perp = (pw2(Bys) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_x;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sx_f;
+    const double c_hll = Sx_hll - ErotB_x;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = 1.0e-6;  // 16_hllc_flow_mpx.f95:3217
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sx_f + (pw2(Exs) + pw2(Bxs)) - (tau_f - ErotB_x) * V;
+    const double psiR = (s2 * psi_hll - V * Ex_f) / (s2 - V);
+    const double psiL = (-s1 * psi_hll + V * Ex_f) / (V - s1);
+    const double phiR = (s2 * phi_hll - V * Bx_f) / (s2 - V);
+    const double phiL = (-s1 * phi_hll + V * Bx_f) / (V - s1);
+    const double SxR = (s2 * Sx_hll - tau_f * V) / (s2 - V);
+    const double SxL = (-s1 * Sx_hll + tau_f * V) / (V - s1);
+    const double SyR = (s2 * Sy_hll - Sy_f - ErotB_y * V - Exs * Eys - Bxs * Bys) / (s2 - V);
+    const double SyL = (-s1 * Sy_hll + Sy_f + ErotB_y * V + Exs * Eys + Bxs * Bys) / (V - s1);
+    const double SzR = (s2 * Sz_hll - Sz_f - ErotB_z * V - Exs * Ezs - Bxs * Bzs) / (s2 - V);
+    const double SzL = (-s1 * Sz_hll + Sz_f + ErotB_z * V + Exs * Ezs + Bxs * Bzs) / (V - s1);
+    const double tauR = (SxR - ErotB_x) / V - pstr + E2B2_str;
+    const double tauL = (SxL - ErotB_x) / V - pstr + E2B2_str;
+    const double DR = (s2 * DD_hll - DD_f) / (s2 - V);
+    const double DL = (-s1 * DD_hll + DD_f) / (V - s1);
+    double fpsiR, fpsiL, fphiR, fphiL, fDR, fDL, ftR, ftL, fSxR, fSxL, fSyR, fSyL, fSzR, fSzL;
+    if (V == 0.0) {
+      fpsiR = fpsiL = psi_f; fphiR = fphiL = phi_f; fDR = fDL = DD_f; ftR = ftL = tau_f;
+      fSxR = fSxL = Sx_f; fSyR = fSyL = Sy_f; fSzR = fSzL = Sz_f;
+    } else {
+      fpsiR = psi_f + (s2 * (V - s1) * (psiR - psiL)) / (s2 - s1);
+      fpsiL = psi_f - (s1 * (s2 - V) * (psiR - psiL)) / (s2 - s1);
+      fphiR = phi_f + (s2 * (V - s1) * (phiR - phiL)) / (s2 - s1);
+      fphiL = phi_f - (s1 * (s2 - V) * (phiR - phiL)) / (s2 - s1);
+      fDR = DD_f + s2 * (V - s1) * (DR - DL) / (s2 - s1);
+      fDL = DD_f - s1 * (s2 - V) * (DR - DL) / (s2 - s1);
+      ftR = tau_f + s2 * (V - s1) * (tauR - tauL) / (s2 - s1);
+      ftL = tau_f - s1 * (s2 - V) * (tauR - tauL) / (s2 - s1);
+      fSxR = Sx_f + s2 * (V - s1) * (SxR - SxL) / (s2 - s1);
+      fSxL = Sx_f - s1 * (s2 - V) * (SxR - SxL) / (s2 - s1);
+      fSyR = Sy_f + s2 * (V - s1) * (SyR - SyL) / (s2 - s1);
+      fSyL = Sy_f - s1 * (s2 - V) * (SyR - SyL) / (s2 - s1);
+      fSzR = Sz_f + s2 * (V - s1) * (SzR - SzL) / (s2 - s1);
+      fSzL = Sz_f - s1 * (s2 - V) * (SzR - SzL) / (s2 - s1);
+    }
+    if (s1 < 0.0 && 0.0 < V) {
+      out[0] = fpsiL; out[2] = fphiL; out[18] = fDL; out[20] = ftL; out[22] = fSxL; out[23] = fSyL; out[24] = fSzL;
+      out[4] = Bx_f; out[6] = -By_f; out[8] = Bz_f; out[10] = Ex_f; out[12] = Ey_f; out[14] = -Ez_f; out[16] = q_f;
+    } else if (V < 0.0 && 0.0 < s2) {
+      out[0] = fpsiR; out[2] = fphiR; out[18] = fDR; out[20] = ftR; out[22] = fSxR; out[23] = fSyR; out[24] = fSzR;
+      out[4] = Bx_f; out[6] = -By_f; out[8] = Bz_f; out[10] = Ex_f; out[12] = Ey_f; out[14] = -Ez_f; out[16] = q_f;
+    } else if (V == 0.0) {
+      out[0] = 0.5 * (fpsiR + fpsiL); out[2] = 0.5 * (fphiR + fphiL);
+      out[4] = 0.5 * (Bx_f + Bx_f); out[6] = -0.5 * (By_f + By_f); out[8] = 0.5 * (Bz_f + Bz_f);
+      out[10] = 0.5 * (Ex_f + Ex_f); out[12] = 0.5 * (Ey_f + Ey_f); out[14] = -0.5 * (Ez_f + Ez_f);
+      out[16] = 0.5 * (q_f + q_f); out[18] = 0.5 * (fDR + fDL); out[20] = 0.5 * (ftR + ftL);
+      out[22] = 0.5 * (fSxR + fSxL); out[23] = 0.5 * (fSyR + fSyL); out[24] = 0.5 * (fSzR + fSzL);
+    } else {
+      st |= ST_HLLC_VSTAR;
+      for (int c : {0, 2, 4, 6, 8, 10, 12, 14, 16, 18, 20, 22, 23, 24}) out[c] = NAN;
+    }
+    return st;
+  }
+
+  // ----------------------------------------- HLLC, y direction
+  // 16_hllc_flow_mpx.f95:2960-3100, 3340-3475, 3522-3570, 3742-3905, 4305-4610
+  int32_t hllc_y(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+    int32_t st = 0;
+    const double s1 = -1.0, s2 = 1.0;
+    const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ey - R.Ey) / (s2 - s1);
+    const double phi_hll = (s2 * R.phi - s1 * L.phi + L.By - R.By) / (s2 - s1);
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.psi - R.psi) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bx - R.Bx) / (s2 - s1);
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.Bzm - R.Bzm) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.phi - R.phi) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Exm - R.Exm) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.Ez - R.Ez) / (s2 - s1);
+    const double DD_hll = (s2 * R.D - s1 * L.D + fl.FD - fr.FD) / (s2 - s1);
+    const double tau_hll = (s2 * R.tau - s1 * L.tau + fl.Ftau - fr.Ftau) / (s2 - s1);
+    const double Sy_hll = (s2 * R.Sy - s1 * L.Sy + fl.FSy - fr.FSy) / (s2 - s1);
+    const double Sz_hll = (s2 * R.Sz - s1 * L.Sz + fl.FSz - fr.FSz) / (s2 - s1);
+    const double Sx_hll = (s2 * R.Sx - s1 * L.Sx + fl.FSx - fr.FSx) / (s2 - s1);
+    const double psi_f = 0.5 * (L.Ey + R.Ey - (R.psi - L.psi));
+    const double phi_f = 0.5 * (L.By + R.By - (R.phi - L.phi));
+    const double By_f = 0.5 * (L.phi + R.phi - (R.By - L.By));
+    const double Bz_f = 0.5 * (L.Exm + R.Exm - (R.Bz - L.Bz));
+    const double Bx_f = 0.5 * (L.Ez + R.Ez - (R.Bx - L.Bx));
+    const double Ey_f = 0.5 * (L.psi + R.psi - (R.Ey - L.Ey));
+    const double Ez_f = 0.5 * (L.Bx + R.Bx - (R.Ez - L.Ez));
+    const double Ex_f = 0.5 * (L.Bzm + R.Bzm - (R.Ex - L.Ex));
+    const double q_f = 0.5 * (L.J + R.J - (R.q - L.q));
+    const double DD_f = 0.5 * (fl.FD + fr.FD - (R.D - L.D));
+    const double tau_f = 0.5 * (fl.Ftau + fr.Ftau - (R.tau - L.tau));
+    const double Sy_f = 0.5 * (fl.FSy + fr.FSy - (R.Sy - L.Sy));
+    const double Sz_f = 0.5 * (fl.FSz + fr.FSz - (R.Sz - L.Sz));
+    const double Sx_f = 0.5 * (fl.FSx + fr.FSx - (R.Sx - L.Sx));
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Exs) + pw2(Ezs));
+    const double B2_perp = (pw2(Bxs) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_y;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sy_f;
+    const double c_hll = Sy_hll - ErotB_y;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = (double)1.0e-6f;  // single-precision literal, 16_hllc_flow_mpx.f95:3354
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sy_f + (pw2(Eys) + pw2(Bys)) - (tau_f - ErotB_y) * V;
+    const double psiR = (s2 * psi_hll - V * Ey_f) / (s2 - V);
+    const double psiL = (-s1 * psi_hll + V * Ey_f) / (V - s1);
+    const double phiR = (s2 * phi_hll - V * By_f) / (s2 - V);
+    const double phiL = (-s1 * phi_hll + V * By_f) / (V - s1);
+    const double SyR = (s2 * Sy_hll - tau_f * V) / (s2 - V);
+    const double SyL = (-s1 * Sy_hll + tau_f * V) / (V - s1);
+    const double SzR = (s2 * Sz_hll - Sz_f - ErotB_z * V - Eys * Ezs - Bys * Bzs) / (s2 - V);
+    const double SzL = (-s1 * Sz_hll + Sz_f + ErotB_z * V + Eys * Ezs + Bys * Bzs) / (V - s1);
+    const double SxR = (s2 * Sx_hll - Sx_f - ErotB_x * V - Eys * Exs - Bys * Bxs) / (s2 - V);
+    const double SxL = (-s1 * Sx_hll + Sx_f + ErotB_x * V + Eys * Exs + Bys * Bxs) / (V - s1);
+    const double tauR = (SyR - ErotB_y) / V - pstr + E2B2_str;
+    const double tauL = (SyL - ErotB_y) / V - pstr + E2B2_str;
+    const double DR = (s2 * DD_hll - DD_f) / (s2 - V);
+    const double DL = (-s1 * DD_hll + DD_f) / (V - s1);
+    double fpsiR, fpsiL, fphiR, fphiL, fDR, fDL, ftR, ftL, fSxR, fSxL, fSyR, fSyL, fSzR, fSzL;
+    if (V == 0.0) {
+      fpsiR = fpsiL = psi_f; fphiR = fphiL = phi_f; fDR = fDL = DD_f; ftR = ftL = tau_f;
+      fSxR = fSxL = Sx_f; fSyR = fSyL = Sy_f; fSzR = fSzL = Sz_f;
+    } else {
+      fpsiR = psi_f + (s2 * (V - s1) * (psiR - psiL)) / (s2 - s1);
+      fpsiL = psi_f - (s1 * (s2 - V) * (psiR - psiL)) / (s2 - s1);
+      fphiR = phi_f + (s2 * (V - s1) * (phiR - phiL)) / (s2 - s1);
+      fphiL = phi_f - (s1 * (s2 - V) * (phiR - phiL)) / (s2 - s1);
+      fDR = DD_f + s2 * (V - s1) * (DR - DL) / (s2 - s1);
+      fDL = DD_f - s1 * (s2 - V) * (DR - DL) / (s2 - s1);
+      ftR = tau_f + s2 * (V - s1) * (tauR - tauL) / (s2 - s1);
+      ftL = tau_f - s1 * (s2 - V) * (tauR - tauL) / (s2 - s1);
+      fSxR = Sx_f + s2 * (V - s1) * (SxR - SxL) / (s2 - s1);
+      fSxL = Sx_f - s1 * (s2 - V) * (SxR - SxL) / (s2 - s1);
+      fSyR = Sy_f + s2 * (V - s1) * (SyR - SyL) / (s2 - s1);
+      fSyL = Sy_f - s1 * (s2 - V) * (SyR - SyL) / (s2 - s1);
+      fSzR = Sz_f + s2 * (V - s1) * (SzR - SzL) / (s2 - s1);
+      fSzL = Sz_f - s1 * (s2 - V) * (SzR - SzL) / (s2 - s1);
+    }
+    if (s1 < 0.0 && 0.0 < V) {
+      out[1] = fpsiL; out[3] = fphiL; out[19] = fDL; out[21] = ftL; out[25] = fSxL; out[26] = fSyL; out[27] = fSzL;
+      out[5] = Bx_f; out[7] = By_f; out[9] = -Bz_f; out[11] = -Ex_f; out[13] = Ey_f; out[15] = Ez_f; out[17] = q_f;
+    } else if (V < 0.0 && 0.0 < s2) {
+      out[1] = fpsiR; out[3] = fphiR; out[19] = fDR; out[21] = ftR; out[25] = fSxR; out[26] = fSyR; out[27] = fSzR;
+      out[5] = Bx_f; out[7] = By_f; out[9] = -Bz_f; out[11] = -Ex_f; out[13] = Ey_f; out[15] = Ez_f; out[17] = q_f;
+    } else if (V == 0.0) {
+      out[1] = 0.5 * (fpsiR + fpsiL); out[3] = 0.5 * (fphiR + fphiL);
+      out[5] = 0.5 * (Bx_f + Bx_f); out[7] = 0.5 * (By_f + By_f); out[9] = -0.5 * (Bz_f + Bz_f);
+      out[11] = -0.5 * (Ex_f + Ex_f); out[13] = 0.5 * (Ey_f + Ey_f); out[15] = 0.5 * (Ez_f + Ez_f);
+      out[17] = 0.5 * (q_f + q_f); out[19] = 0.5 * (fDR + fDL); out[21] = 0.5 * (ftR + ftL);
+      out[25] = 0.5 * (fSxR + fSxL); out[26] = 0.5 * (fSyR + fSyL); out[27] = 0.5 * (fSzR + fSzL);
+    } else {
+      st |= ST_HLLC_VSTAR;
+      for (int c : {1, 3, 5, 7, 9, 11, 13, 15, 17, 19, 21, 25, 26, 27}) out[c] = NAN;
+    }
+    return st;
+  }
+
+  // HLLE is restated separately (16_hlle_flow_mpx.f95); until then the
+  // solver id 6 is rejected at creation.
+  int32_t hlle_x(const Side&, const Side&, const PhysX&, const PhysX&, double*) { return ST_NONFINITE; }
+  int32_t hlle_y(const Side&, const Side&, const PhysX&, const PhysX&, double*) { return ST_NONFINITE; }
+
+  // ---------------------------------------------- 17_fluxandsource.f95:441-635
+  // z differences (X(i,j)-X(i,j))/Delz are kept as literal zeros.
+  void fluxandsource(int l) {
+    auto& Kl = K[l - 1];
+    double *Ex = a("Exint"), *Ey = a("Eyint"), *Ez = a("Ezint"), *Bx = a("Bxint"), *By = a("Byint"),
+           *Bz = a("Bzint"), *q = a("qint"), *psi = a("psiint"), *phi = a("phiint");
+    double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *W = a("W");
+    double *Exlaxpsi = a("Exlaxpsi"), *Eylaxpsi = a("Eylaxpsi"), *Bxlaxphi = a("Bxlaxphi"), *Bylaxphi = a("Bylaxphi");
+    double *philaxBx = a("philaxBx"), *EzlaxBx = a("EzlaxBx"), *EzlaxBy = a("EzlaxBy"), *philaxBy = a("philaxBy");
+    double *EylaxBz = a("EylaxBz"), *ExlaxBz = a("ExlaxBz"), *psilaxEx = a("psilaxEx"), *BzlaxEx = a("BzlaxEx");
+    double *BzlaxEy = a("BzlaxEy"), *psilaxEy = a("psilaxEy"), *BylaxEz = a("BylaxEz"), *BxlaxEz = a("BxlaxEz");
+    double *Jxlax = a("Jxlax"), *Jylax = a("Jylax"), *FDxlax = a("FDxlax"), *FDylax = a("FDylax");
+    double *Ftauxlax = a("Ftauxlax"), *Ftauylax = a("Ftauylax");
+    double *FSxxlax = a("FSxxlax"), *FSxylax = a("FSxylax"), *FSxzlax = a("FSxzlax");
+    double *FSyxlax = a("FSyxlax"), *FSyylax = a("FSyylax"), *FSyzlax = a("FSyzlax");
+    double *psiflux = Kl["psiflux"].data(), *phiflux = Kl["phiflux"].data(), *Bxflux = Kl["Bxflux"].data(),
+           *Byflux = Kl["Byflux"].data(), *Bzflux = Kl["Bzflux"].data(), *Exf = Kl["Exastflux"].data(),
+           *Eyf = Kl["Eyastflux"].data(), *Ezf = Kl["Ezastflux"].data(), *qflux = Kl["qflux"].data(),
+           *Dflux = Kl["Dflux"].data(), *tauflux = Kl["tauflux"].data(), *Sxflux = Kl["Sxflux"].data(),
+           *Syflux = Kl["Syflux"].data(), *Szflux = Kl["Szflux"].data(), *Exs = Kl["Exastsour"].data(),
+           *Eys = Kl["Eyastsour"].data(), *Ezs = Kl["Ezastsour"].data();
+    const double z = 0.0;  // (X(i,j,1,l) - X(i,j,1,l))/Delz for finite X
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j), km = id(i - 1, j), kn = id(i, j - 1);
+        const double Edotv = Ex[k] * Vx[k] + Ey[k] * Vy[k] + Ez[k] * Vz[k];
+        const double vrotB_x = (Bz[k] * Vy[k] - By[k] * Vz[k]);
+        const double vrotB_y = (Bx[k] * Vz[k] - Bz[k] * Vx[k]);
+        const double vrotB_z = (By[k] * Vx[k] - Bx[k] * Vy[k]);
+        const double Vx_elec = Vx[k], Vy_elec = Vy[k], Vz_elec = Vz[k], W_elec = W[k];
+        psiflux[k] = -(Exlaxpsi[k] - Exlaxpsi[km]) / Delx - (Eylaxpsi[k] - Eylaxpsi[kn]) / Dely - z / Delz
+                     + q[k] - kappa_psi * psi[k];
+        phiflux[k] = -(Bxlaxphi[k] - Bxlaxphi[km]) / Delx - (Bylaxphi[k] - Bylaxphi[kn]) / Dely - z / Delz
+                     - kappa_phi * phi[k];
+        Bxflux[k] = -(EzlaxBx[k] - EzlaxBx[kn]) / Dely + z / Delz - (philaxBx[k] - philaxBx[km]) / Delx;
+        Byflux[k] = -(z) / Delz + (EzlaxBy[k] - EzlaxBy[km]) / Delx - (philaxBy[k] - philaxBy[kn]) / Dely;
+        Bzflux[k] = -(EylaxBz[k] - EylaxBz[km]) / Delx + (ExlaxBz[k] - ExlaxBz[kn]) / Dely - z / Delz;
+        Exf[k] = (BzlaxEx[k] - BzlaxEx[kn]) / Dely - z / Delz - (psilaxEx[k] - psilaxEx[km]) / Delx - q[k] * Vx_elec;
+        Eyf[k] = z / Delz - (BzlaxEy[k] - BzlaxEy[km]) / Delx - (psilaxEy[k] - psilaxEy[kn]) / Dely - q[k] * Vy_elec;
+        Ezf[k] = (BylaxEz[k] - BylaxEz[km]) / Delx - (BxlaxEz[k] - BxlaxEz[kn]) / Dely - z / Delz - q[k] * Vz_elec;
+        Exs[k] = sigma * W_elec * (Ex[k] + vrotB_x - Edotv * Vx_elec);
+        Eys[k] = sigma * W_elec * (Ey[k] + vrotB_y - Edotv * Vy_elec);
+        Ezs[k] = sigma * W_elec * (Ez[k] + vrotB_z - Edotv * Vz_elec);
+        qflux[k] = -(Jxlax[k] - Jxlax[km]) / Delx - (Jylax[k] - Jylax[kn]) / Dely - z / Delz;
+        Dflux[k] = -(FDxlax[k] - FDxlax[km]) / Delx - (FDylax[k] - FDylax[kn]) / Dely - z / Delz;
+        tauflux[k] = -(Ftauxlax[k] - Ftauxlax[km]) / Delx - (Ftauylax[k] - Ftauylax[kn]) / Dely - z / Delz;
+        Sxflux[k] = -(FSxxlax[k] - FSxxlax[km]) / Delx - (FSyxlax[k] - FSyxlax[kn]) / Dely - z / Delz;
+        Syflux[k] = -(FSxylax[k] - FSxylax[km]) / Delx - (FSyylax[k] - FSyylax[kn]) / Dely - z / Delz;
+        Szflux[k] = -(FSxzlax[k] - FSxzlax[km]) / Delx - (FSyzlax[k] - FSyzlax[kn]) / Dely - z / Delz;
+      }
+  }
+
+  // ------------------------------------------------------- 18_sumfin.f95:20-66
+  void sumfin(int l) {
+    auto& Kl = K[l - 1];
+    const double w = T.wb[l - 1], wt = T.wbt[l - 1];
+    const char* s[] = {"psifinsum", "phifinsum", "Bxfinsum", "Byfinsum", "Bzfinsum", "qfinsum", "Dfinsum",
+                       "taufinsum", "Sxfinsum", "Syfinsum", "Szfinsum"};
+    const char* f[] = {"psiflux", "phiflux", "Bxflux", "Byflux", "Bzflux", "qflux", "Dflux",
+                       "tauflux", "Sxflux", "Syflux", "Szflux"};
+    for (int c = 0; c < 11; ++c) {
+      double* S = a(s[c]);
+      const double* F = Kl[f[c]].data();
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); S[k] = S[k] + w * F[k]; }
+    }
+    const char* es[] = {"Exfinsum", "Eyfinsum", "Ezfinsum"};
+    const char* ef[] = {"Exastflux", "Eyastflux", "Ezastflux"};
+    const char* eo[] = {"Exastsour", "Eyastsour", "Ezastsour"};
+    for (int c = 0; c < 3; ++c) {
+      double* S = a(es[c]);
+      const double* F = Kl[ef[c]].data();
+      const double* O = Kl[eo[c]].data();
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); S[k] = S[k] + (w * F[k] - wt * O[k]); }
+    }
+  }
+
+  // ----------------------------- 19_varfin.f95:16-54, 20_electricfield.f95:153-167
+  void varfin_electricfield() {
+    const char* dst[] = {"psi", "phi", "Bx", "By", "Bz", "q", "D", "tau", "Sx", "Sy", "Sz", "Ex", "Ey", "Ez"};
+    const char* sum[] = {"psifinsum", "phifinsum", "Bxfinsum", "Byfinsum", "Bzfinsum", "qfinsum", "Dfinsum",
+                         "taufinsum", "Sxfinsum", "Syfinsum", "Szfinsum", "Exfinsum", "Eyfinsum", "Ezfinsum"};
+    for (int c = 0; c < 14; ++c) {
+      double* d = a(dst[c]);
+      const double* S = a(sum[c]);
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) { const size_t k = id(i, j); d[k] = d[k] + Delt * S[k]; }
+    }
+  }
+
+  // ------------------------------------------------------ con2prim (l_swap = 1)
+  void con2prim() {
+    double *D = a("D"), *tau = a("tau"), *Sx = a("Sx"), *Sy = a("Sy"), *Sz = a("Sz");
+    double *Ex = a("Ex"), *Ey = a("Ey"), *Ez = a("Ez"), *Bx = a("Bx"), *By = a("By"), *Bz = a("Bz");
+    double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *rho = a("rho"), *p = a("p"), *W = a("W");
+    int32_t st_acc = 0;
+    int64_t c0 = 0, c1 = 0, c2 = 0;
+#pragma omp parallel for schedule(static) reduction(| : st_acc) reduction(+ : c0, c1, c2)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        C2PIn in{D[k], tau[k], Sx[k], Sy[k], Sz[k], Ex[k], Ey[k], Ez[k], Bx[k], By[k], Bz[k],
+                 Vx[k], Vy[k], Vz[k], rho[k], p[k]};
+        C2POut o;
+        int64_t cnt[3] = {0, 0, 0};
+        int32_t st = (P.c2p == 1) ? c2p_cardano(in, gamma, eps1_c2p, o, cnt) : c2p_nr(in, gamma, o);
+        st_acc |= st;
+        c0 += cnt[0]; c1 += cnt[1]; c2 += cnt[2];
+        Vx[k] = o.vx; Vy[k] = o.vy; Vz[k] = o.vz; rho[k] = o.rho; p[k] = o.p; W[k] = o.W;
+      }
+    status |= st_acc;
+    counters[0] += c0; counters[1] += c1; counters[2] += c2;
+  }
+
+  void boundary_prims() {
+    const char* n[] = {"psi", "phi", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "Vx", "Vy", "Vz", "q", "p", "rho"};
+    for (const char* s : n) fill_ghosts(a(s));
+  }
+
+  // main_cueva_code.f95:53-328 stages part
+  void begin_step() {
+    boundary_prims();   // :53
+    startconvar();      // :181
+    cleanvarint();      // :184
+  }
+  void stage(int l) {
+    for (int m = 1; m <= l - 1; ++m) sumint(l, m);   // :205-211
+    varint();                                       // :214
+    {
+      // Exast ghosts are never read; only E_l carries boundary data
+    }
+    electricvarint(l);                              // :216
+    flowinit();                                     // :238 (+ boundary_flux_conserved :242)
+    reconstruct();                                  // 16_*_flow_mpx.f95 passes
+    riemann();
+    fluxandsource(l);                               // :284
+    sumfin(l);                                      // :286
+  }
+  void finish_step() {
+    varfin_electricfield();                         // :295-297
+    con2prim();                                     // :312-326
+    boundary_prims();                               // :328
+  }
+  int32_t step(int n) {
+    for (int h = 0; h < n; ++h) {
+      begin_step();
+      for (int l = 1; l <= lmax; ++l) stage(l);
+      finish_step();
+    }
+    return status;
+  }
+};
+
+const char* prim_names[OR_NPRIM] = {"rho", "p", "Vx", "Vy", "Vz", "psi", "phi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "q"};
+
+}  // namespace
+
+// ============================================================== C API
+extern "C" {
+
+void* oracle_create(const oracle_params* p) {
+  if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
+  if (p->flux_solver != 5 && p->flux_solver != 7) return nullptr;
+  if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
+  Tableau T;
+  if (!make_tableau(p->order, T)) return nullptr;
+  return new Oracle(*p);
+}
+void oracle_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void oracle_set_threads(int32_t n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
+}
+double oracle_dt(void* h) { return static_cast<Oracle*>(h)->Delt; }
+
+void oracle_set_prims(void* h, const double* const* f) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int c = 0; c < OR_NPRIM; ++c) {
+    double* d = o->a(prim_names[c]);
+    for (int j = 0; j <= o->jmax; ++j)
+      for (int i = 0; i <= o->imax; ++i) d[o->id(i, j)] = f[c][(size_t)i + (size_t)j * (o->imax + 1)];
+  }
+  o->boundary_prims();
+}
+void oracle_get_prims(void* h, double* const* f) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int c = 0; c < OR_NPRIM; ++c) {
+    const double* d = o->a(prim_names[c]);
+    for (int j = 0; j <= o->jmax; ++j)
+      for (int i = 0; i <= o->imax; ++i) f[c][(size_t)i + (size_t)j * (o->imax + 1)] = d[o->id(i, j)];
+  }
+}
+int32_t oracle_step(void* h, int32_t n) { return static_cast<Oracle*>(h)->step(n); }
+int32_t oracle_run_stages(void* h, int32_t upto) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->begin_step();
+  for (int l = 1; l <= upto && l <= o->lmax; ++l) o->stage(l);
+  return o->status;
+}
+int32_t oracle_get_named(void* h, const char* name, int32_t l, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const double* src = nullptr;
+  auto it = o->A.find(name);
+  if (it != o->A.end()) src = it->second.data();
+  else if (l >= 1 && l <= o->lmax) {
+    auto jt = o->K[l - 1].find(name);
+    if (jt != o->K[l - 1].end()) src = jt->second.data();
+  }
+  if (!src) return -1;
+  for (int j = 0; j <= o->jmax; ++j)
+    for (int i = 0; i <= o->imax; ++i) out[(size_t)i + (size_t)j * (o->imax + 1)] = src[o->id(i, j)];
+  return 0;
+}
+void oracle_counters(void* h, int64_t* out3) {
+  Oracle* o = static_cast<Oracle*>(h);
+  for (int c = 0; c < 3; ++c) out3[c] = o->counters[c];
+}
+
+void oracle_kh_init(int32_t imax, int32_t jmax, double lx, double ly, double v0, double a, double amp,
+                    double width, double kpert, double phase, double bshear, double rho0, double p0,
+                    double* const* f) {
+  const double Delx = lx / (double)imax, Dely = ly / (double)jmax;
+  for (int j = 0; j <= jmax; ++j)
+    for (int i = 0; i <= imax; ++i) {
+      const size_t k = (size_t)i + (size_t)j * (imax + 1);
+      const double posx = -0.5 * lx + i * Delx;   // reference x = BASELINE y (shear normal)
+      const double posy = -0.5 * ly + j * Dely;   // reference y = BASELINE x (periodic)
+      const double vx = amp * std::sin(kpert * posy + phase) * std::exp(-(posx * posx) / width);
+      const double vy = v0 * std::tanh(posx / a);
+      const double vz = 0.0;
+      const double Bx = 0.0, By = bshear, Bz = 0.0;
+      f[OR_RHO][k] = rho0; f[OR_P][k] = p0;
+      f[OR_VX][k] = vx; f[OR_VY][k] = vy; f[OR_VZ][k] = vz;
+      f[OR_PSI][k] = 0.0; f[OR_PHI][k] = 0.0; f[OR_Q][k] = 0.0;
+      f[OR_BX][k] = Bx; f[OR_BY][k] = By; f[OR_BZ][k] = Bz;
+      f[OR_EX][k] = -(vy * Bz - vz * By);
+      f[OR_EY][k] = -(vz * Bx - vx * Bz);
+      f[OR_EZ][k] = -(vx * By - vy * Bx);
+    }
+}
+
+void oracle_mp_line(int32_t rec_mp, int32_t n, const double* u, int32_t posfix, double* up, double* um) {
+  mp_line(rec_mp, n, u, posfix, up, um);
+}
+double oracle_hllc_vel(double a, double b, double c, double rt) { return get_hllc_vel(a, b, c, rt, nullptr); }
+int32_t oracle_c2p_cardano(const double* in, double gamma, double eps1, double* out) {
+  C2PIn i{in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], in[9], in[10],
+          in[11], in[12], in[13], in[14], in[15]};
+  C2POut o;
+  int32_t st = c2p_cardano(i, gamma, eps1, o, nullptr);
+  out[0] = o.vx; out[1] = o.vy; out[2] = o.vz; out[3] = o.rho; out[4] = o.p; out[5] = o.W;
+  return st;
+}
+int32_t oracle_c2p_nr(const double* in, double gamma, double* out) {
+  C2PIn i{in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], in[9], in[10],
+          in[11], in[12], in[13], in[14], in[15]};
+  C2POut o;
+  int32_t st = c2p_nr(i, gamma, o);
+  out[0] = o.vx; out[1] = o.vy; out[2] = o.vz; out[3] = o.rho; out[4] = o.p; out[5] = o.W;
+  return st;
+}
+int32_t oracle_tableau(int32_t order, double* wb8, double* wbt8, double* ab64, double* abt64) {
+  Tableau T;
+  if (!make_tableau(order, T)) return -1;
+  for (int a = 0; a < 8; ++a) {
+    wb8[a] = T.wb[a]; wbt8[a] = T.wbt[a];
+    for (int b = 0; b < 8; ++b) { ab64[a * 8 + b] = T.Ab[a][b]; abt64[a * 8 + b] = T.Abt[a][b]; }
+  }
+  return T.s;
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+/*
+ * cueva_oracle.h -- CPU restatement of the CUEVA (ByMar09/MHD-KH-instability)
+ * per-step hot path, used ONLY as test infrastructure: the checker that the
+ * B200 kernels are compared against in tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py.  Nothing in the product links this library.
+ *
+ * Parity status: UNPINNED against the reference itself.  The reference is
+ * Fortran 95 and no Fortran compiler exists on either machine, and the
+ * reference ships no golden vectors or known-answer tests.  The restatement
+ * follows the Fortran line by line (each routine cites the file:line it
+ * mirrors) and is pinned by analytic/structural tests (polynomial exactness
+ * of MP5/7/9, odd symmetry, HLL consistency, con2prim round trips, uniform
+ * state preservation, periodic conservation, tableau sums, 1-thread vs
+ * N-thread bit identity) plus regression fixtures under tests/golden/.
+ *
+ * Arithmetic follows the Fortran evaluation order (left to right, integer
+ * powers expanded as gfortran's powi does: x**2 = x*x, x**3 = (x*x)*x,
+ * x**4 = (x*x)*(x*x)) and must be compiled with -ffp-contract=off.
+ */
+#ifndef CUEVA_ORACLE_H
+#define CUEVA_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_params {
+  int32_t imax, jmax;      /* grid points 0..imax x 0..jmax (parameters.f95:110-111) */
+  int32_t order;           /* IMEX tableau: 1,2,3,4,5,6,8 (imex_scheme.f95) */
+  int32_t flux_solver;     /* 5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX (main_cueva_code.f95:263-273) */
+  int32_t rec_mp;          /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
+  int32_t c2p;             /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37) */
+  int32_t bc_x, bc_y;      /* 0 copy, 1 periodic (04_boundary.f95 BOUND 1/2/6) */
+  int32_t pad;
+  double lx, ly, lz;       /* Longx, Longy, Longz */
+  double cfl, sigma, gamma;
+  double dt;               /* <= 0: CFL*min(Delx,Dely,Delz) (parameters.f95:312) */
+} oracle_params;
+
+/* carried primitive fields, interior (imax+1)*(jmax+1), i fastest */
+enum {
+  OR_RHO = 0, OR_P, OR_VX, OR_VY, OR_VZ, OR_PSI, OR_PHI,
+  OR_EX, OR_EY, OR_EZ, OR_BX, OR_BY, OR_BZ, OR_Q, OR_NPRIM
+};
+
+void*   oracle_create(const oracle_params* p);
+void    oracle_destroy(void* h);
+void    oracle_set_threads(int32_t n);
+double  oracle_dt(void* h);
+void    oracle_set_prims(void* h, const double* const* prims14);
+void    oracle_get_prims(void* h, double* const* prims14);
+/* one full time step h of main_cueva_code.f95:47-356; returns status (0 ok) */
+int32_t oracle_step(void* h, int32_t nsteps);
+/* runs boundary+startconvar+cleanvarint and RK stages 1..upto only */
+int32_t oracle_run_stages(void* h, int32_t upto);
+/* interior copy of a named internal array ("psiflux", "Exastsour", "Exlaxpsi",
+ * "Exint", "Jxint", "D", "tau", ...); l selects the stage for per-stage arrays */
+int32_t oracle_get_named(void* h, const char* name, int32_t l, double* out);
+void    oracle_counters(void* h, int64_t* out3);
+
+/* KH initial data in the reference orientation (x_ref = BASELINE y, copy;
+ * y_ref = BASELINE x, periodic), conventions of 03_init_var_primitive.f95:2297-2336 */
+void    oracle_kh_init(int32_t imax, int32_t jmax, double lx, double ly,
+                       double v0, double a, double amp, double width,
+                       double kpert, double phase, double bshear,
+                       double rho0, double p0, double* const* prims14);
+
+/* unit entry points for the pins */
+void    oracle_mp_line(int32_t rec_mp, int32_t n, const double* u /* n+13, starts at -6 */,
+                       int32_t posfix, double* up, double* um /* n+13 */);
+double  oracle_hllc_vel(double a, double b, double c, double rt);
+/* Cardano con2prim of one point (12_varprimitive.f95:48-813, l_swap=1);
+ * in: D tau Sx Sy Sz Ex Ey Ez Bx By Bz vx0 vy0 vz0 rho0 p0 ; out: vx vy vz rho p W */
+int32_t oracle_c2p_cardano(const double* in16, double gamma, double eps1, double* out6);
+int32_t oracle_c2p_nr(const double* in16, double gamma, double* out6);
+int32_t oracle_tableau(int32_t order, double* wb8, double* wbt8, double* ab64, double* abt64);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,221 @@
+"""Pins of the CPU oracle (the checker): analytic and structural properties of
+the restated Fortran that must hold whatever the reference would print.
+
+The reference ships no tests or golden vectors and cannot be compiled here
+(no Fortran compiler), so these are the anchors of the restatement."""
+import numpy as np
+import pytest
+
+from conftest import rel_l1
+
+
+def _line(vals):
+    return np.ascontiguousarray(vals, dtype=np.float64)
+
+
+@pytest.mark.parametrize("rec", [0, 1, 2])
+def test_mp_linear_exact(oracle_mod, rec):
+    n = 24
+    x = np.arange(-6, n + 7, dtype=np.float64)
+    u = 0.3 + 0.7 * x
+    up, um = oracle_mod.mp_line(_line(u), rec)
+    k = np.arange(-2, n + 3) + 6
+    np.testing.assert_allclose(up[k], 0.3 + 0.7 * (x[k] + 0.5), rtol=0, atol=1e-13)
+    np.testing.assert_allclose(um[k], 0.3 + 0.7 * (x[k] - 0.5), rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("rec,deg", [(0, 4), (1, 6), (2, 8)])
+def test_mp_polynomial_exact(oracle_mod, rec, deg):
+    """Unlimited MP5/7/9 interface values are exact for cell averages of
+    polynomials of degree <= 4/6/8; a gentle monotone polynomial keeps the
+    limiter off (SH97 eq. 2.1/2.31)."""
+    n, h = 32, 1.0 / 64
+    rng = np.random.default_rng(7 + rec)
+    coef = rng.uniform(-0.3, 0.3, deg + 1) * (0.2 ** np.arange(deg + 1))
+    coef[1] = 1.0
+    P = np.polynomial.Polynomial(coef)
+    Pi = P.integ()
+    xe = (np.arange(-6, n + 8) - 0.5) * h          # cell edges
+    avg = (Pi(xe[1:]) - Pi(xe[:-1])) / h            # cell averages of cells -6..n+6
+    up, um = oracle_mod.mp_line(_line(avg), rec)
+    k = np.arange(-2, n + 3) + 6
+    xc = (np.arange(-6, n + 7)) * h
+    np.testing.assert_allclose(up[k], P(xc[k] + 0.5 * h), rtol=0, atol=2e-12)
+    np.testing.assert_allclose(um[k], P(xc[k] - 0.5 * h), rtol=0, atol=2e-12)
+
+
+@pytest.mark.parametrize("rec", [0, 1, 2])
+@pytest.mark.parametrize("posfix", [False, True])
+def test_mp_odd_symmetry_bitwise(oracle_mod, rec, posfix):
+    """MP5/7/9 are odd: the reference's separately reconstructed -E/-B slots
+    equal the negated E/B values bit for bit (basis of the kernels' shortcut).
+    The p/rho positivity fix is not odd, so only posfix=False is compared."""
+    rng = np.random.default_rng(11 + rec)
+    u = rng.standard_normal(40 + 13).cumsum() * 0.1 + rng.standard_normal(53) * 0.5
+    up, um = oracle_mod.mp_line(_line(u), rec, posfix)
+    upn, umn = oracle_mod.mp_line(_line(-u), rec, posfix)
+    k = np.arange(-2, 40 + 3) + 6
+    if not posfix:
+        assert np.array_equal(upn[k], -up[k]) and np.array_equal(umn[k], -um[k])
+    else:
+        assert np.all(np.isfinite(up[k]))
+
+
+def test_mp_positivity_fix(oracle_mod):
+    """p/rho slots never reconstruct negative values next to positive cells
+    (mp5.f95:177-216)."""
+    u = np.full(40 + 13, 1.0)
+    u[20:] = 1e-6        # strong jump that overshoots below zero unlimited
+    up, um = oracle_mod.mp_line(_line(u), 0, True)
+    k = np.arange(-2, 43) + 6
+    assert (up[k] >= 0).all() and (um[k] >= 0).all()
+
+
+def test_hllc_vel_root(oracle_mod):
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        v = rng.uniform(-0.9, 0.9)
+        a = rng.uniform(0.5, 2.0)
+        w = rng.uniform(1.5, 4.0) * np.sign(rng.standard_normal())  # second root outside [-1, 1]
+        # a (x - v)(x - w) = a x^2 - a (v + w) x + a v w = a x^2 - b x + c
+        b, c = a * (v + w), a * v * w
+        got = oracle_mod.hllc_vel(a, b, c, v + 0.05)
+        assert abs(got - v) < 1e-10
+
+
+def _random_prims(rng, n):
+    rho = 10 ** rng.uniform(-1, 1, n)
+    p = 10 ** rng.uniform(-2, 1, n)
+    W = rng.uniform(1.0, 3.0, n)
+    vdir = rng.standard_normal((n, 3))
+    vdir /= np.linalg.norm(vdir, axis=1)[:, None]
+    v = vdir * np.sqrt(1 - 1 / W ** 2)[:, None]
+    B = rng.standard_normal((n, 3)) * 0.5
+    E = -np.cross(v, B) + rng.standard_normal((n, 3)) * 1e-3
+    return rho, p, v, E, B
+
+
+def _cons(rho, p, v, E, B, gamma=4 / 3):
+    V2 = (v ** 2).sum(1)
+    W = 1 / np.sqrt(1 - V2)
+    h = rho * (1 + p / ((gamma - 1) * rho)) + p
+    D = rho * W
+    tau = 0.5 * ((E ** 2).sum(1) + (B ** 2).sum(1)) + h * W ** 2 - p
+    S = np.cross(E, B) + (h * W ** 2)[:, None] * v
+    return D, tau, S
+
+
+@pytest.mark.parametrize("method", [1, 0])
+def test_c2p_round_trip(oracle_mod, method):
+    """prim -> cons -> prim: Cardano recovers the primitives to ~1e-9 from a
+    seed at the true state (the reference seeds with the time-n prims)."""
+    rng = np.random.default_rng(5)
+    rho, p, v, E, B = _random_prims(rng, 300)
+    D, tau, S = _cons(rho, p, v, E, B)
+    worst = 0.0
+    for k in range(300):
+        inp = np.r_[D[k], tau[k], S[k], E[k], B[k], v[k], rho[k], p[k]]
+        st, out = oracle_mod.c2p(inp, method=method)
+        assert st == 0
+        if method == 1:
+            worst = max(worst, abs(out[3] / rho[k] - 1), abs(out[4] / p[k] - 1),
+                        np.abs(out[:3] - v[k]).max())
+    assert worst < 1e-8
+
+
+def test_tableaux_consistent(oracle_mod):
+    for order in (1, 2, 3, 4, 5, 6, 8):
+        s, wb, wbt, ab, abt = oracle_mod.tableau(order)
+        assert s >= 1
+        # IMEX-RK48SSP stores rational approximations that sum to 1 - 1.2e-7
+        assert abs(wb.sum() - 1) < 1e-6 and abs(wbt[:s].sum() - (0 if order == 1 else 1)) < 1e-6
+        if order != 1:   # order 1 stores Ab(1,1) = 1, never read (sumint runs m = 1..l-1)
+            assert np.all(np.triu(ab[:s, :s]) == 0)             # explicit part strictly lower
+        assert np.all(np.triu(abt[:s, :s], 1) == 0)             # implicit part lower (DIRK)
+
+
+@pytest.mark.parametrize("solver,order,rec", [(5, 2, 0), (7, 4, 0), (7, 2, 1), (5, 3, 2)])
+def test_uniform_state_stays_uniform(oracle_mod, solver, order, rec):
+    imax, jmax = 20, 12
+    o = oracle_mod.Oracle(imax, jmax, order=order, flux_solver=solver, rec_mp=rec, bc_x=0, bc_y=1, sigma=1e3)
+    v = np.array([0.3, -0.2, 0.1])
+    B = np.array([0.1, 0.2, -0.05])
+    E = -np.cross(v, B)
+    shape = (jmax + 1, imax + 1)
+    pr = {"rho": np.full(shape, 1.3), "p": np.full(shape, 0.7), "psi": np.zeros(shape), "phi": np.zeros(shape),
+          "q": np.zeros(shape)}
+    for c, n in enumerate("xyz"):
+        pr["v" + n] = np.full(shape, v[c])
+        pr["E" + n] = np.full(shape, E[c])
+        pr["B" + n] = np.full(shape, B[c])
+    o.set_prims(pr)
+    assert o.step(3) == 0
+    out = o.get_prims()
+    for n, a in out.items():
+        # round-off of the stiff source sigma W (E + v x B ...) is amplified by sigma
+        np.testing.assert_allclose(a, pr[n], rtol=1e-11, atol=1e-13, err_msg=n)
+
+
+def test_periodic_mass_conservation(oracle_mod):
+    """Fully periodic box: the flux divergence telescopes, so sum(D) over the
+    unique points changes only by the con2prim tolerance."""
+    imax, jmax = 24, 24
+    o = oracle_mod.Oracle(imax, jmax, order=2, flux_solver=5, bc_x=1, bc_y=1, lx=1.0, ly=1.0, sigma=1e3)
+    pr = oracle_mod.kh_init(imax, jmax, lx=1.0, ly=1.0, v0=0.3, a=0.1)
+    o.set_prims(pr)
+    o.run_stages(0)
+    d0 = o.named("D")[:-1, :-1].sum()
+    o2 = oracle_mod.Oracle(imax, jmax, order=2, flux_solver=5, bc_x=1, bc_y=1, lx=1.0, ly=1.0, sigma=1e3)
+    o2.set_prims(pr)
+    o2.step(5)
+    o2.run_stages(0)
+    d1 = o2.named("D")[:-1, :-1].sum()
+    assert abs(d1 / d0 - 1) < 1e-9
+
+
+def test_implicit_e_residual(oracle_mod):
+    """electricvarint solves E - E* + a W (E + v x B - (E.v) v) = 0 with a = Abt(l,l) sigma dt."""
+    imax, jmax = 32, 16
+    sigma = 1e6
+    o = oracle_mod.Oracle(imax, jmax, order=2, flux_solver=5, sigma=sigma)
+    pr = oracle_mod.kh_init(imax, jmax)
+    pr["Ex"] = pr["Ex"] + 1e-3 * np.sin(np.arange(pr["Ex"].size)).reshape(pr["Ex"].shape)
+    o.set_prims(pr)
+    o.run_stages(1)
+    s, wb, wbt, ab, abt = oracle_mod.tableau(2)
+    a = abt[0, 0] * sigma * o.dt
+    W = o.named("W")
+    E = np.stack([o.named("Exint"), o.named("Eyint"), o.named("Ezint")], -1)
+    Ea = np.stack([o.named("Exast"), o.named("Eyast"), o.named("Ezast")], -1)
+    B = np.stack([o.named("Bxint"), o.named("Byint"), o.named("Bzint")], -1)
+    v = np.stack([pr["vx"], pr["vy"], pr["vz"]], -1)
+    Edv = (E * v).sum(-1)
+    res = E - Ea + (a * W)[..., None] * (E + np.cross(v, B) - Edv[..., None] * v)
+    scale = np.abs(Ea).max() + np.abs(E).max()
+    assert np.abs(res).max() < 1e-12 * max(1.0, a) * max(scale, 1e-3)
+
+
+def test_threads_bit_identical(oracle_mod):
+    imax, jmax = 40, 20
+    outs = []
+    for nt in (1, 4):
+        oracle_mod.set_threads(nt)
+        o = oracle_mod.Oracle(imax, jmax, order=4, flux_solver=7, sigma=1e4)
+        o.set_prims(oracle_mod.kh_init(imax, jmax))
+        o.step(3)
+        outs.append(o.get_prims())
+    oracle_mod.set_threads(8)
+    for n in outs[0]:
+        assert np.array_equal(outs[0][n], outs[1][n]), n
+
+
+def test_kh_init_matches_formula(oracle_mod):
+    imax, jmax = 16, 8
+    pr = oracle_mod.kh_init(imax, jmax, v0=0.5, a=0.01)
+    x = -1.0 + np.arange(imax + 1) * (2.0 / imax)
+    y = -0.5 + np.arange(jmax + 1) * (1.0 / jmax)
+    X, Y = np.meshgrid(x, y)
+    np.testing.assert_allclose(pr["vy"], 0.5 * np.tanh(X / 0.01), rtol=1e-15, atol=1e-16)
+    np.testing.assert_allclose(pr["vx"], 0.01 * np.sin(2 * np.pi * Y) * np.exp(-(X * X) / 0.01), atol=1e-17)
+    np.testing.assert_allclose(pr["Ez"], -(pr["vx"] * 0.1), rtol=1e-15)
+    assert rel_l1(pr["By"], np.full_like(pr["By"], 0.1)) == 0
