@@ -52,6 +52,11 @@ typedef struct cueva_params {
   int32_t bc_x, bc_y;   /* per-axis ghost rule: 0 copy, 1 periodic (BOUND 1 / 2 / 6 of 04_boundary.f95) */
   int32_t precision;    /* 0 FP64 throughout; 1 FP32 reconstruction + Riemann, FP64 elsewhere */
   int32_t device;       /* CUDA device ordinal */
+  int32_t intsum_reset; /* 0: the stage sums are zeroed once per step and accumulate over the stages
+                           (07_clean_var.f95 via main_cueva_code.f95:184, the reference); 1: zeroed
+                           before every stage (textbook IMEX-RK; the reference's SSP3(4,3,3) marked
+                           "NO" in imex_scheme.f95:278 is only stable this way) */
+  int32_t pad;
   double lx, ly, lz;    /* Longx, Longy, Longz (Delx = lx/imax, Dely = ly/jmax, Delz = lz) */
   double cfl, sigma, gamma;
   double dt;            /* <= 0 selects CFL*min(Delx,Dely,Delz) (parameters.f95:312) */

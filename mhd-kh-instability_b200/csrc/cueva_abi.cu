@@ -193,8 +193,10 @@ StageArgs stage_args(const cueva_ctx* c, int l, int mode) {
   sa.abt_diag_first = T.Abt[0][0];
   for (int m = 1; m < l; ++m) sa.kslot[m - 1] = c->kslot_of[m - 1];
   sa.store_k_slot = (l < T.s) ? c->kslot_of[l - 1] : -1;
-  sa.need_intsum_load = (l >= 2 && l < T.s) ? 1 : 0;
-  sa.need_intsum_store = (l + 1 < T.s) ? 1 : 0;
+  // the reference zeroes the stage sums once per step, so stage l+1 starts
+  // from the sums of stage l; with intsum_reset every stage starts from zero
+  sa.need_intsum_load = (!c->P.intsum_reset && l >= 2 && l < T.s) ? 1 : 0;
+  sa.need_intsum_store = (!c->P.intsum_reset && l + 1 < T.s) ? 1 : 0;
   return sa;
 }
 
@@ -237,6 +239,7 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
     return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
   if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
+  if (p->intsum_reset != 0 && p->intsum_reset != 1) return fail(CUEVA_ERR_ARG, "intsum_reset must be 0 or 1");
   cueva_ctx* c = new cueva_ctx();
   c->P = *p;
   if (!make_tableau(p->order, c->T)) { delete c; return fail(CUEVA_ERR_ARG, "unsupported IMEX order"); }

@@ -154,13 +154,52 @@ __device__ __forceinline__ double e2b2_half(const C2PIn& in) {
   return 0.5 * (pw2(in.Ex) + pw2(in.Ey) + pw2(in.Ez) + pw2(in.Bx) + pw2(in.By) + pw2(in.Bz));
 }
 
+// Cardano seed arithmetic with +,-,*,/ only, so host and device produce the
+// same bits (the last bit of the W seed is amplified by the limiter switches
+// of the reference scheme; libm-dependent acos/cos/pow would make CPU and GPU
+// runs drift apart by ~1e-5 over 200 steps).
+// Roots of 4c^3 - 3c = y, y in (-1, 1): by the triple-angle identity
+// cos 3a = 4 cos^3 a - 3 cos a they are cos((acos y + 2 pi k)/3); c0 in
+// (1/2, 1) and c1 in (-1, -1/2) by monotone Newton from c = 1 and c = -1,
+// c2 from -(c0 + c1) (the roots sum to zero) polished by Newton.
+__device__ __forceinline__ void chebyshev_roots(double y, double& c0, double& c1, double& c2) {
+  double c = 1.0;
+  for (int it = 0; it < 80; ++it) {
+    const double cn = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+    if (!(cn < c)) break;
+    c = cn;
+  }
+  c0 = c;
+  c = -1.0;
+  for (int it = 0; it < 80; ++it) {
+    const double cn = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+    if (!(cn > c)) break;
+    c = cn;
+  }
+  c1 = c;
+  c = -(c0 + c1);
+  for (int it = 0; it < 3; ++it) c = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+  c2 = c;
+}
+// x^(1/3), x >= 0: Newton cube root on the mantissa (frexp/ldexp are exact)
+__device__ __forceinline__ double cbrt_newton(double x) {
+  if (!(x > 0.0) || !(x < CUDART_INF)) return x;
+  int e;
+  double m = frexp(x, &e);
+  const int r = ((e % 3) + 3) % 3;
+  const int q = (e - r) / 3;
+  m = ldexp(m, r);
+  double y = 1.0;
+#pragma unroll
+  for (int it = 0; it < 8; ++it) y = y - (y * y * y - m) / (3.0 * y * y);
+  return ldexp(y, q);
+}
+
 // Cardano con2prim, 12_varprimitive.f95:48-813 (l_swap = 1, VDRIFT = 0,
 // low_vel = 0, REC_ELEC = 0): quartic in W by Ferrari-Cardano, Newton polish.
 __device__ __forceinline__ uint32_t c2p_cardano(const C2PIn& in, double gamma, double eps1, C2POut& o,
                                                 unsigned long long* cnt) {
   uint32_t st = 0;
-  const double PI = 3.14159265358979323846264338327950288;
-  const double THIRD = 0.333333333333333333333333333333333333;
   double V2c = pw2(in.vx0) + pw2(in.vy0) + pw2(in.vz0);
   if (V2c > 1.0) V2c = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V2c));
   const double E2B2 = e2b2_half(in);
@@ -184,11 +223,10 @@ __device__ __forceinline__ uint32_t c2p_cardano(const C2PIn& in, double gamma, d
   const double R_1 = (2.0 * pw3(e) - 9.0 * e * f + 27.0 * g) / 54.0;
   double s = 0.0, t = 0.0, det = 0.0, z_1 = 0.0;
   if (pw2(R_1) < pw3(Q_1)) {
-    const double T_1 = acos(R_1 / fabs(sqrt(pw3(Q_1))));
+    double ca, cb, cc;   // cos(T/3), cos((T+2pi)/3), cos((T-2pi)/3), T = acos(R/|Q|^1.5)
+    chebyshev_roots(R_1 / fabs(sqrt(pw3(Q_1))), ca, cb, cc);
     const double sq = fabs(sqrt(Q_1));
-    const double zs[3] = {-2.0 * sq * cos((T_1) / 3.0) - e / 3.0,
-                          -2.0 * sq * cos((T_1 + 2.0 * PI) / 3.0) - e / 3.0,
-                          -2.0 * sq * cos((T_1 - 2.0 * PI) / 3.0) - e / 3.0};
+    const double zs[3] = {-2.0 * sq * ca - e / 3.0, -2.0 * sq * cb - e / 3.0, -2.0 * sq * cc - e / 3.0};
     bool found = false;
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
@@ -207,7 +245,7 @@ __device__ __forceinline__ uint32_t c2p_cardano(const C2PIn& in, double gamma, d
     if (!found) st |= ST_C2P_FAIL;
   } else {
     const double xx1 = fabs(R_1) + fabs(sqrt(pw2(R_1) - pw3(Q_1)));
-    const double AA_1 = -fsgn1(R_1) * copysign(fabs(pow(xx1, THIRD)), xx1);
+    const double AA_1 = -fsgn1(R_1) * copysign(fabs(cbrt_newton(xx1)), xx1);
     const double BB_1 = (AA_1 != 0.0) ? Q_1 / AA_1 : 0.0;
     z_1 = (AA_1 + BB_1) - e / 3.0;
     s = fabs(sqrt(d_2 + 2.0 * z_1));

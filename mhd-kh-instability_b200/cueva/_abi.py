@@ -34,7 +34,8 @@ class Params(ctypes.Structure):
     _fields_ = [("imax", ctypes.c_int32), ("jmax", ctypes.c_int32), ("order", ctypes.c_int32),
                 ("flux_solver", ctypes.c_int32), ("rec_mp", ctypes.c_int32), ("c2p", ctypes.c_int32),
                 ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("device", ctypes.c_int32), ("intsum_reset", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double),
                 ("lz", ctypes.c_double), ("cfl", ctypes.c_double), ("sigma", ctypes.c_double),
                 ("gamma", ctypes.c_double), ("dt", ctypes.c_double)]
 
@@ -45,16 +46,17 @@ class CuevaError(RuntimeError):
         self.code = code
 
 
-def lib_path(exact=False):
-    return os.path.join(LIBDIR, "libcueva_b200_exact.so" if exact else "libcueva_b200.so")
+def lib_path(fma=False):
+    return os.path.join(LIBDIR, "libcueva_b200_fma.so" if fma else "libcueva_b200.so")
 
 
-def load(exact=False):
-    """Load the C-ABI library (production build, or the no-FMA parity build)."""
-    key = bool(exact)
+def load(fma=False):
+    """Load the C-ABI library: the default build keeps the reference's
+    operation order (no FMA contraction); fma=True loads the contracted one."""
+    key = bool(fma)
     if key in _LIBS:
         return _LIBS[key]
-    path = lib_path(exact)
+    path = lib_path(fma)
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is missing: build it with `make -C mhd-kh-instability_b200/csrc`")
     L = ctypes.CDLL(path)

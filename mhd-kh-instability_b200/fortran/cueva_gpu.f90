@@ -1,0 +1,159 @@
+! cueva_gpu.f90 -- ISO_C_BINDING interface of include/cueva.h for the CUEVA
+! Fortran driver (cueva_2D_base/main_cueva_code.f95).  Source only: no
+! Fortran compiler exists in the build image, so this module is not compiled
+! or tested here; the C++ stand-in driver (host/cueva_driver.cpp) exercises
+! the same calls on arrays with the Fortran layout.
+!
+! Use from the reference driver (see INTEGRATION.md):
+!   use cueva_gpu
+!   type(c_ptr) :: ctx
+!   call cueva_attach(ctx)                       ! after init_var_primitive
+!   do h = hini, hmax-1
+!      ierr = cueva_step(ctx, 1)                 ! replaces main_cueva_code.f95:53-326
+!      if (mod(h, hloc) == 0) ierr = cueva_download(ctx, CUEVA_G_PRIMS)
+!      call boundary ; call lector               ! unchanged Fortran I/O path
+!   end do
+module cueva_gpu
+  use iso_c_binding
+  implicit none
+
+  integer(c_int32_t), parameter :: CUEVA_OK = 0, CUEVA_ERR_ARG = 1, CUEVA_ERR_CUDA = 2
+  integer(c_int32_t), parameter :: CUEVA_ERR_UNBOUND = 3, CUEVA_ERR_PHYSICS = 4
+  integer(c_int32_t), parameter :: CUEVA_G_PRIMS = 1, CUEVA_G_CONS = 2
+
+  ! field ids, same order as enum cueva_field
+  integer(c_int32_t), parameter :: CUEVA_RHO = 0, CUEVA_P = 1, CUEVA_VX = 2, CUEVA_VY = 3, CUEVA_VZ = 4
+  integer(c_int32_t), parameter :: CUEVA_PSI = 5, CUEVA_PHI = 6, CUEVA_EX = 7, CUEVA_EY = 8, CUEVA_EZ = 9
+  integer(c_int32_t), parameter :: CUEVA_BX = 10, CUEVA_BY = 11, CUEVA_BZ = 12, CUEVA_Q = 13
+  integer(c_int32_t), parameter :: CUEVA_D = 14, CUEVA_TAU = 15, CUEVA_SX = 16, CUEVA_SY = 17, CUEVA_SZ = 18
+  integer(c_int32_t), parameter :: CUEVA_W = 19
+  integer(c_int32_t), parameter :: CUEVA_PSIINT = 20, CUEVA_PHIINT = 21, CUEVA_EXINT = 22, CUEVA_EYINT = 23
+  integer(c_int32_t), parameter :: CUEVA_EZINT = 24, CUEVA_BXINT = 25, CUEVA_BYINT = 26, CUEVA_BZINT = 27
+  integer(c_int32_t), parameter :: CUEVA_QINT = 28, CUEVA_DDINT = 29, CUEVA_TAUINT = 30, CUEVA_SXINT = 31
+  integer(c_int32_t), parameter :: CUEVA_SYINT = 32, CUEVA_SZINT = 33, CUEVA_JXINT = 34, CUEVA_JYINT = 35
+  integer(c_int32_t), parameter :: CUEVA_JZINT = 36, CUEVA_EXAST = 37, CUEVA_EYAST = 38, CUEVA_EZAST = 39
+  integer(c_int32_t), parameter :: CUEVA_PSIFLUX = 40, CUEVA_PHIFLUX = 41, CUEVA_EXASTFLUX = 42
+  integer(c_int32_t), parameter :: CUEVA_EYASTFLUX = 43, CUEVA_EZASTFLUX = 44, CUEVA_BXFLUX = 45
+  integer(c_int32_t), parameter :: CUEVA_BYFLUX = 46, CUEVA_BZFLUX = 47, CUEVA_QFLUX = 48, CUEVA_DFLUX = 49
+  integer(c_int32_t), parameter :: CUEVA_TAUFLUX = 50, CUEVA_SXFLUX = 51, CUEVA_SYFLUX = 52
+  integer(c_int32_t), parameter :: CUEVA_SZFLUX = 53, CUEVA_EXASTSOUR = 54, CUEVA_EYASTSOUR = 55
+  integer(c_int32_t), parameter :: CUEVA_EZASTSOUR = 56
+
+  type, bind(c) :: cueva_params
+     integer(c_int32_t) :: imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y
+     integer(c_int32_t) :: precision, device, intsum_reset, pad
+     real(c_double)     :: lx, ly, lz, cfl, sigma, gamma, dt
+  end type cueva_params
+
+  interface
+     integer(c_int32_t) function cueva_ctx_create(p, ctx) bind(c, name="cueva_ctx_create")
+       import :: c_int32_t, c_ptr, cueva_params
+       type(cueva_params), intent(in) :: p
+       type(c_ptr), intent(out) :: ctx
+     end function cueva_ctx_create
+     integer(c_int32_t) function cueva_ctx_destroy(ctx) bind(c, name="cueva_ctx_destroy")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_ctx_destroy
+     type(c_ptr) function cueva_last_error() bind(c, name="cueva_last_error")
+       import :: c_ptr
+     end function cueva_last_error
+     ! base(*): the whole module array is passed by reference, i.e. the
+     ! address of element (-6,-6[,1,1]); the library keeps that address, which
+     ! is valid for the life of the program for the static module arrays.
+     integer(c_int32_t) function cueva_bind_field(ctx, field, base) bind(c, name="cueva_bind_field")
+       import :: c_int32_t, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: field
+       real(c_double), intent(inout) :: base(*)
+     end function cueva_bind_field
+     integer(c_int32_t) function cueva_upload(ctx, groups) bind(c, name="cueva_upload")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: groups
+     end function cueva_upload
+     integer(c_int32_t) function cueva_download(ctx, groups) bind(c, name="cueva_download")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: groups
+     end function cueva_download
+     integer(c_int32_t) function cueva_step(ctx, nsteps) bind(c, name="cueva_step")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: nsteps
+     end function cueva_step
+     integer(c_int32_t) function cueva_sync(ctx) bind(c, name="cueva_sync")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_sync
+     integer(c_int32_t) function cueva_counters(ctx, out3) bind(c, name="cueva_counters")
+       import :: c_int32_t, c_int64_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), intent(out) :: out3(3)
+     end function cueva_counters
+     integer(c_int32_t) function cueva_startconvar(ctx) bind(c, name="cueva_startconvar")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_startconvar
+     integer(c_int32_t) function cueva_electricvarint(ctx, l) bind(c, name="cueva_electricvarint")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: l
+     end function cueva_electricvarint
+     integer(c_int32_t) function cueva_flux_rhs(ctx, l) bind(c, name="cueva_flux_rhs")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: l
+     end function cueva_flux_rhs
+     integer(c_int32_t) function cueva_con2prim(ctx) bind(c, name="cueva_con2prim")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_con2prim
+  end interface
+
+contains
+
+  ! Creates a context for the module-global run configuration, binds the
+  ! carried primitives of threevectors.f95 and uploads the initial state.
+  subroutine cueva_attach(ctx)
+    use parameters
+    use threevectors
+    type(c_ptr), intent(out) :: ctx
+    type(cueva_params) :: prm
+    integer(c_int32_t) :: ierr
+    prm%imax = imax; prm%jmax = jmax; prm%order = order; prm%flux_solver = flux_solver
+    prm%rec_mp = rec_mp; prm%c2p = conserved_to_primitive
+    prm%bc_x = 0; prm%bc_y = 1                   ! BOUND 6: x copy, y periodic
+    if (BOUND == 1) prm%bc_y = 0                 ! copy / copy
+    if (BOUND == 2) prm%bc_x = 1                 ! periodic / periodic
+    prm%precision = 0; prm%device = 0; prm%intsum_reset = 0; prm%pad = 0
+    prm%lx = Longx; prm%ly = Longy; prm%lz = Longz; prm%cfl = CFL
+    prm%sigma = sigma; prm%gamma = gamma; prm%dt = Delt
+    ierr = cueva_ctx_create(prm, ctx)
+    if (ierr /= CUEVA_OK) stop "cueva_ctx_create failed"
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_RHO, rho)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_P, p)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_VX, Vx)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_VY, Vy)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_VZ, Vz)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_PSI, psi)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_PHI, phi)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_EX, Ex)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_EY, Ey)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_EZ, Ez)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_BX, Bx)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_BY, By)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_BZ, Bz)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_Q, q)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_D, D)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_TAU, tau)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_SX, Sx)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_SY, Sy)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_SZ, Sz)
+    ierr = ierr + cueva_bind_field(ctx, CUEVA_W, W)
+    if (ierr /= CUEVA_OK) stop "cueva_bind_field failed"
+    ierr = cueva_upload(ctx, CUEVA_G_PRIMS)
+    if (ierr /= CUEVA_OK) stop "cueva_upload failed"
+  end subroutine cueva_attach
+
+end module cueva_gpu

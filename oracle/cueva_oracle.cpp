@@ -261,6 +261,55 @@ double get_hllc_vel(double a, double b, double c, double rt, int32_t* st) {
   return fmax2(-1.0 + diferr, fmin2(1.0 - diferr, v));
 }
 
+// ------------------------------------------------ Cardano seed arithmetic
+// The Cardano branch of 12_varprimitive.f95:351-452 needs acos, cos and
+// x**THIRD.  Their last bit depends on the math library (glibc here, CUDA's
+// on the device), and that last bit of the W seed is amplified by the
+// reference's limiter switches: a 1-ulp change of the seed moves config-1
+// prims by ~1e-5 (relative L1) after 200 steps.  The default "deterministic"
+// mode therefore evaluates the seed with +,-,*,/ only, identically on host
+// and device:
+//  * the three angles of the trigonometric solution, cos((acos(y)+2 pi k)/3),
+//    are the three roots of 4c^3 - 3c = y (triple-angle identity
+//    cos 3a = 4 cos^3 a - 3 cos a), found by monotone Newton iterations from
+//    c = 1 and c = -1 and, for the middle root, from -(c0 + c1) (the roots
+//    sum to zero);
+//  * x**(1/3) is a Newton cube root on the mantissa (frexp/ldexp are exact).
+// oracle_set_libm_seed(1) switches back to acos/cos/pow of the C library.
+int g_libm_seed = 0;
+
+void chebyshev_roots(double y, double& c0, double& c1, double& c2) {
+  double c = 1.0;
+  for (int it = 0; it < 80; ++it) {
+    const double cn = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+    if (!(cn < c)) break;
+    c = cn;
+  }
+  c0 = c;
+  c = -1.0;
+  for (int it = 0; it < 80; ++it) {
+    const double cn = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+    if (!(cn > c)) break;
+    c = cn;
+  }
+  c1 = c;
+  c = -(c0 + c1);
+  for (int it = 0; it < 3; ++it) c = c - ((4.0 * c * c - 3.0) * c - y) / (12.0 * c * c - 3.0);
+  c2 = c;
+}
+
+double cbrt_newton(double x) {
+  if (!(x > 0.0) || !(x < INFINITY)) return x;
+  int e;
+  double m = std::frexp(x, &e);
+  const int r = ((e % 3) + 3) % 3;
+  const int q = (e - r) / 3;
+  m = std::ldexp(m, r);                 // x = m 2^(3q), m in [0.5, 4)
+  double y = 1.0;
+  for (int it = 0; it < 8; ++it) y = y - (y * y * y - m) / (3.0 * y * y);
+  return std::ldexp(y, q);
+}
+
 // -------------------------------------------------------- con2prim, point
 struct C2PIn { double D, tau, Sx, Sy, Sz, Ex, Ey, Ez, Bx, By, Bz, vx0, vy0, vz0, rho0, p0; };
 struct C2POut { double vx, vy, vz, rho, p, W; };
@@ -311,14 +360,20 @@ int32_t c2p_cardano(const C2PIn& in, double gamma, double eps1, C2POut& o, int64
     const double R_1 = (2.0 * pw3(e) - 9.0 * e * f + 27.0 * g) / 54.0;
     double s = 0, t = 0, det = 0, z_1 = 0;
     if (pw2(R_1) < pw3(Q_1)) {
-      const double T_1 = std::acos(R_1 / std::fabs(std::sqrt(pw3(Q_1))));
-      const double z_1a = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1) / 3.0) - e / 3.0;
+      double ca, cb, cc;   // cos(T/3), cos((T+2pi)/3), cos((T-2pi)/3)
+      if (g_libm_seed) {
+        const double T_1 = std::acos(R_1 / std::fabs(std::sqrt(pw3(Q_1))));
+        ca = std::cos((T_1) / 3.0); cb = std::cos((T_1 + 2.0 * PI) / 3.0); cc = std::cos((T_1 - 2.0 * PI) / 3.0);
+      } else {
+        chebyshev_roots(R_1 / std::fabs(std::sqrt(pw3(Q_1))), ca, cb, cc);
+      }
+      const double z_1a = -2.0 * std::fabs(std::sqrt(Q_1)) * ca - e / 3.0;
       const double s_1a = d_2 + 2.0 * z_1a;
       const double t_1a = pw2(z_1a) + 2.0 * d_2 * z_1a + pw2(d_2) - d_0;
-      const double z_1b = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1 + 2.0 * PI) / 3.0) - e / 3.0;
+      const double z_1b = -2.0 * std::fabs(std::sqrt(Q_1)) * cb - e / 3.0;
       const double s_1b = d_2 + 2.0 * z_1b;
       const double t_1b = pw2(z_1b) + 2.0 * d_2 * z_1b + pw2(d_2) - d_0;
-      const double z_1c = -2.0 * std::fabs(std::sqrt(Q_1)) * std::cos((T_1 - 2.0 * PI) / 3.0) - e / 3.0;
+      const double z_1c = -2.0 * std::fabs(std::sqrt(Q_1)) * cc - e / 3.0;
       const double s_1c = d_2 + 2.0 * z_1c;
       const double t_1c = pw2(z_1c) + 2.0 * d_2 * z_1c + pw2(d_2) - d_0;
       if (s_1a >= 0.0 && t_1a >= 0.0) {
@@ -338,7 +393,8 @@ int32_t c2p_cardano(const C2PIn& in, double gamma, double eps1, C2POut& o, int64
       }
     } else {
       const double xx1 = std::fabs(R_1) + std::fabs(std::sqrt(pw2(R_1) - pw3(Q_1)));
-      const double AA_1 = -fsign(1.0, R_1) * fsign(std::fabs(std::pow(xx1, THIRD)), xx1);
+      const double cr = g_libm_seed ? std::pow(xx1, THIRD) : cbrt_newton(xx1);
+      const double AA_1 = -fsign(1.0, R_1) * fsign(std::fabs(cr), xx1);
       const double BB_1 = (AA_1 != 0.0) ? Q_1 / AA_1 : 0.0;
       z_1 = (AA_1 + BB_1) - e / 3.0;
       s = std::fabs(std::sqrt(d_2 + 2.0 * z_1));
@@ -1306,6 +1362,11 @@ struct Oracle {
     cleanvarint();      // :184
   }
   void stage(int l) {
+    if (P.intsum_reset) {   // optional textbook variant; the reference zeroes intsum once per step
+      const char* sn[] = {"psiintsum", "phiintsum", "Bxintsum", "Byintsum", "Bzintsum", "Exastsum", "Eyastsum",
+                          "Ezastsum", "qintsum", "Dintsum", "tauintsum", "Sxintsum", "Syintsum", "Szintsum"};
+      for (const char* n : sn) std::fill(A[n].begin(), A[n].end(), 0.0);
+    }
     for (int m = 1; m <= l - 1; ++m) sumint(l, m);   // :205-211
     varint();                                       // :214
     {
@@ -1349,6 +1410,9 @@ void* oracle_create(const oracle_params* p) {
   return new Oracle(*p);
 }
 void oracle_destroy(void* h) { delete static_cast<Oracle*>(h); }
+void oracle_set_libm_seed(int32_t on) { g_libm_seed = on ? 1 : 0; }
+void oracle_chebyshev_roots(double y, double* out3) { chebyshev_roots(y, out3[0], out3[1], out3[2]); }
+double oracle_cbrt(double x) { return cbrt_newton(x); }
 void oracle_set_threads(int32_t n) {
 #ifdef _OPENMP
   omp_set_num_threads(n > 0 ? n : 1);

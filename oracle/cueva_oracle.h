@@ -33,7 +33,8 @@ typedef struct oracle_params {
   int32_t rec_mp;          /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
   int32_t c2p;             /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37) */
   int32_t bc_x, bc_y;      /* 0 copy, 1 periodic (04_boundary.f95 BOUND 1/2/6) */
-  int32_t pad;
+  int32_t intsum_reset;    /* 0: intsum zeroed once per step (07_clean_var.f95, main_cueva_code.f95:184),
+                              as the reference; 1: zeroed before every stage (textbook IMEX-RK) */
   double lx, ly, lz;       /* Longx, Longy, Longz */
   double cfl, sigma, gamma;
   double dt;               /* <= 0: CFL*min(Delx,Dely,Delz) (parameters.f95:312) */
@@ -48,6 +49,10 @@ enum {
 void*   oracle_create(const oracle_params* p);
 void    oracle_destroy(void* h);
 void    oracle_set_threads(int32_t n);
+/* 0 (default): deterministic Cardano seed shared with the kernels; 1: C-library acos/cos/pow */
+void    oracle_set_libm_seed(int32_t on);
+void    oracle_chebyshev_roots(double y, double* out3);
+double  oracle_cbrt(double x);
 double  oracle_dt(void* h);
 void    oracle_set_prims(void* h, const double* const* prims14);
 void    oracle_get_prims(void* h, double* const* prims14);

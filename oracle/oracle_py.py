@@ -18,7 +18,7 @@ PRIM_NAMES = ["rho", "p", "vx", "vy", "vz", "psi", "phi", "Ex", "Ey", "Ez", "Bx"
 class OracleParams(ctypes.Structure):
     _fields_ = [("imax", ctypes.c_int32), ("jmax", ctypes.c_int32), ("order", ctypes.c_int32),
                 ("flux_solver", ctypes.c_int32), ("rec_mp", ctypes.c_int32), ("c2p", ctypes.c_int32),
-                ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("intsum_reset", ctypes.c_int32),
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
                 ("cfl", ctypes.c_double), ("sigma", ctypes.c_double), ("gamma", ctypes.c_double),
                 ("dt", ctypes.c_double)]
@@ -40,6 +40,10 @@ def lib():
         L.oracle_create.argtypes = [ctypes.POINTER(OracleParams)]
         L.oracle_destroy.argtypes = [ctypes.c_void_p]
         L.oracle_set_threads.argtypes = [ctypes.c_int32]
+        L.oracle_set_libm_seed.argtypes = [ctypes.c_int32]
+        L.oracle_chebyshev_roots.argtypes = [ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_cbrt.restype = ctypes.c_double
+        L.oracle_cbrt.argtypes = [ctypes.c_double]
         L.oracle_dt.restype = ctypes.c_double
         L.oracle_dt.argtypes = [ctypes.c_void_p]
         L.oracle_set_prims.argtypes = [ctypes.c_void_p, ctypes.POINTER(dp)]
@@ -79,13 +83,19 @@ def set_threads(n):
     lib().oracle_set_threads(int(n))
 
 
+def set_libm_seed(on):
+    """Cardano seed from the C library's acos/cos/pow (1) or the deterministic
+    basic-operation seed shared with the kernels (0, default)."""
+    lib().oracle_set_libm_seed(int(bool(on)))
+
+
 class Oracle:
     """One CUEVA run on the host: prims in, prims out, internal arrays by name."""
 
     def __init__(self, imax, jmax, order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1,
-                 lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0):
+                 lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, intsum_reset=0):
         self.imax, self.jmax = imax, jmax
-        self.p = OracleParams(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, 0,
+        self.p = OracleParams(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, intsum_reset,
                               lx, ly, lz, cfl, sigma, gamma, dt)
         self.h = lib().oracle_create(ctypes.byref(self.p))
         if not self.h:
@@ -165,3 +175,13 @@ def tableau(order):
     wb, wbt, ab, abt = np.zeros(8), np.zeros(8), np.zeros(64), np.zeros(64)
     s = lib().oracle_tableau(order, _dp(wb), _dp(wbt), _dp(ab), _dp(abt))
     return s, wb, wbt, ab.reshape(8, 8), abt.reshape(8, 8)
+
+
+def chebyshev_roots(y):
+    out = np.zeros(3)
+    lib().oracle_chebyshev_roots(float(y), _dp(out))
+    return out
+
+
+def cbrt(x):
+    return lib().oracle_cbrt(float(x))

@@ -219,3 +219,36 @@ def test_kh_init_matches_formula(oracle_mod):
     np.testing.assert_allclose(pr["vx"], 0.01 * np.sin(2 * np.pi * Y) * np.exp(-(X * X) / 0.01), atol=1e-17)
     np.testing.assert_allclose(pr["Ez"], -(pr["vx"] * 0.1), rtol=1e-15)
     assert rel_l1(pr["By"], np.full_like(pr["By"], 0.1)) == 0
+
+
+def test_cardano_seed_helpers_match_libm(oracle_mod):
+    """The deterministic seed arithmetic equals the C library's
+    cos((acos y + 2 pi k)/3) and x**(1/3) to a few ulp."""
+    rng = np.random.default_rng(9)
+    for y in np.r_[rng.uniform(-0.999999, 0.999999, 500), -0.5, 0.0, 0.5]:
+        t = np.arccos(y)
+        ref = np.cos(np.array([t, t + 2 * np.pi, t - 2 * np.pi]) / 3)
+        got = oracle_mod.chebyshev_roots(y)
+        # both sides are ill-conditioned next to the double roots y = +-1
+        assert np.abs(got - ref).max() < 4e-15 / (1 - abs(y)) ** 0.5, y
+    # x**THIRD of the reference is the cube root to within |ln x| * 1.9e-17
+    for x in np.r_[10 ** rng.uniform(-300, 300, 500), 1.0, 8.0, 27.0]:
+        assert abs(oracle_mod.cbrt(x) / np.cbrt(x) - 1) < 4e-16
+    assert oracle_mod.cbrt(0.0) == 0.0
+
+
+@pytest.mark.parametrize("solver", [5, 7])
+def test_seed_modes_agree_after_one_step(oracle_mod, solver):
+    """C-library and deterministic Cardano seeds give the same step to the
+    last few bits (they differ by ~1 ulp in W only)."""
+    imax, jmax = 64, 32
+    outs = []
+    for libm in (1, 0):
+        oracle_mod.set_libm_seed(libm)
+        o = oracle_mod.Oracle(imax, jmax, order=2, flux_solver=solver, sigma=1e3)
+        o.set_prims(oracle_mod.kh_init(imax, jmax, a=0.05))
+        assert o.step(1) == 0
+        outs.append(o.get_prims())
+    oracle_mod.set_libm_seed(0)
+    for n in outs[0]:
+        assert rel_l1(outs[0][n], outs[1][n]) <= 1e-14, n
