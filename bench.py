@@ -41,6 +41,22 @@ def alg_bytes_per_zone(s):
     return 8.0 * (48 * s + 8.5 * s * (s - 1) + 28)
 
 
+FACE_BYTES = 8.0 * (20 + 14)   # per interface: 20 reconstructed fields read once, 14 fluxes written
+KERNELS = ("k_face<x>", "k_face<y>", "k_update")
+
+
+def kernel_units(cfg):
+    """Units one launch of each kernel processes: x faces, y faces, points."""
+    return ((cfg.imax + 2) * (cfg.jmax + 1), (cfg.imax + 1) * (cfg.jmax + 2), (cfg.imax + 1) * (cfg.jmax + 1))
+
+
+def kernel_bytes_per_unit(s):
+    """Algorithmic bytes per unit: a face reads the 20 reconstructed fields
+    once and writes 14 fluxes; a point reads its 28 face fluxes (each face is
+    shared by two points) plus the stage's share of the resident state I/O."""
+    return (FACE_BYTES, FACE_BYTES, alg_bytes_per_zone(s) / s + 8.0 * 28)
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -166,10 +182,16 @@ def main():
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--grid", default=None, help="NXxNY override of the workload grid (profiling a small case)")
     args = ap.parse_args()
 
     from cueva.configs import C2
     cfg = C2
+    if args.grid:
+        import dataclasses
+        nx, ny = (int(v) for v in args.grid.lower().split("x"))
+        cfg = dataclasses.replace(C2, nx=nx, ny=ny, name=C2.name.replace("1024x2048", f"{nx}x{ny}"))
     if args.impl == "reference":
         return run_reference(args, cfg)
 
@@ -186,7 +208,9 @@ def main():
     from cueva import Cueva
 
     g = Cueva(device=local, pinned=True, **dict(cfg.solver_kwargs(), precision=args.precision))
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by the library and the CUDA events
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     g.set_stream(stream.cuda_stream)
     g.kh_init(**cfg.kh_kwargs())
     g.upload()
@@ -239,15 +263,26 @@ def main():
            "h2d_bytes_per_step": field_bytes, "d2h_bytes_per_step": field_bytes,
            "note": "per step: upload of the 14 prim fields from pinned host arrays, one time step, download"}
 
+    # per-kernel device time: a few steps launched kernel by kernel with
+    # events between the launches on the library's stream
     peak, peak_kind = measured_peaks()
-    launch_ms = ms_per_step / s
-    bytes_per_launch = alg_bytes_per_zone(s) * zones / s
-    achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
+    kms, kcnt = g.profile_steps(args.profile_steps)
+    g.sync()
+    units = kernel_units(cfg)
+    bpu = kernel_bytes_per_unit(s)
+    kernels = {}
+    for k, name in enumerate(KERNELS):
+        avg = kms[k] / max(kcnt[k], 1)
+        kernels[name] = {"avg_ms": avg, "launches": kcnt[k], "share": kms[k] / max(sum(kms), 1e-30),
+                         "alg_bytes_per_launch": bpu[k] * units[k],
+                         "gbs": bpu[k] * units[k] / (avg * 1e-3) / 1e9 if avg > 0 else None}
+    top = max(range(3), key=lambda k: kms[k])
+    achieved = kernels[KERNELS[top]]["gbs"]
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    tpath = os.path.join(ROOT, "profiles", "kernel_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch_full")
+            traffic = json.load(f).get(KERNELS[top], {}).get("dram_bytes_per_launch_full")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f64+f32",
@@ -261,9 +296,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,
-                         "note": f"k_sweep avg launch {launch_ms:.3f} ms; algorithmic bytes "
-                                 f"{alg_bytes_per_zone(s) / s:.0f} B per zone per launch"},
-            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": s * args.steps}
+                         "kernel": KERNELS[top], "kernels": kernels,
+                         "note": f"{KERNELS[top]}: {bpu[top]:.0f} algorithmic B per unit x {units[top]} units "
+                                 f"per launch / avg launch {kernels[KERNELS[top]]['avg_ms']:.3f} ms"},
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 3 * s * args.steps}
     if rank == 0 and not args.no_cpu_baseline:
         r, cores, sample = cpu_port_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

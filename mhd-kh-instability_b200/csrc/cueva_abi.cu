@@ -129,7 +129,7 @@ struct cueva_ctx {
   InstDesc h_inst{};
   int nkslot = 0;
   int kslot_of[8];        // slot of K_m (0-based m) or -1
-  int nblocks = 0;
+  int nb[3] = {0, 0, 0};  // CTAs of the x-face, y-face and point launches
   int cur = 0, qin = 0;
   bool primed = false;
   double* bound[CUEVA_NFIELDS] = {};
@@ -209,7 +209,7 @@ int32_t run_begin_step(cueva_ctx* c) {
 int32_t enqueue_step(cueva_ctx* c) {
   for (int l = 1; l <= c->T.s; ++l) {
     const StageArgs sa = stage_args(c, l, 0);
-    CUDA_TRY(launch_sweep(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nblocks, c->stream, c->d_inst, 1, sa));
+    CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1, sa));
     c->qin ^= 1;
   }
   c->cur ^= 1;
@@ -271,12 +271,17 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
     if (need) c->kslot_of[m] = c->nkslot++;
   }
   const long long fs = c->fstride;
+  // interface flux scratch: x faces -1/2 .. imax+1/2 (imax+2 per row) on
+  // jmax+1 rows, y faces on jmax+2 rows of imax+1
+  const int fpitch = (c->nx + 1 + 31) / 32 * 32;
+  const long long ffs = (long long)fpitch * (c->ny + 1);
   const long long nfields = 2LL * NPRIM + 2LL * NAUX + 2LL * NSTAGE + 2LL * NCONS + (long long)c->nkslot * NRHS + NRHS;
-  if (cudaMalloc(&c->slab, (size_t)(nfields * fs) * sizeof(double)) != cudaSuccess) {
+  const long long nslab = nfields * fs + 2LL * NFACE * ffs;
+  if (cudaMalloc(&c->slab, (size_t)nslab * sizeof(double)) != cudaSuccess) {
     delete c; cudaGetLastError();
     return fail(CUEVA_ERR_CUDA, "cudaMalloc of the field slab failed");
   }
-  cudaMemset(c->slab, 0, (size_t)(nfields * fs) * sizeof(double));
+  cudaMemset(c->slab, 0, (size_t)nslab * sizeof(double));
   double* q = c->slab;
   InstDesc& I = c->h_inst;
   I.prim[0] = q; q += NPRIM * fs; I.prim[1] = q; q += NPRIM * fs;
@@ -286,6 +291,9 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   I.finsum = q; q += NCONS * fs;
   I.kbuf = q; q += (long long)c->nkslot * NRHS * fs;
   I.rhs_out = q; q += NRHS * fs;
+  I.fx = q; q += NFACE * ffs;
+  I.fy = q; q += NFACE * ffs;
+  I.fpitch = fpitch; I.ffs = ffs;
   if (cudaMalloc(&c->d_status, 4) != cudaSuccess || cudaMalloc(&c->d_counters, 3 * 8) != cudaSuccess ||
       cudaMalloc(&c->d_inst, sizeof(InstDesc)) != cudaSuccess) {
     cueva_ctx_destroy(c); cudaGetLastError();
@@ -306,11 +314,11 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   // the Fortran module variable eps1 keeps the value the flux routine stored last
   I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
   I.c2p = p->c2p;
-  I.strips_x = (c->nx + STRIP - 1) / STRIP;
-  I.blocks_y = (c->ny + SWEEP_ROWS - 1) / SWEEP_ROWS;
-  I.block_begin = 0;
-  I.block_count = ((I.strips_x + SWEEP_WARPS - 1) / SWEEP_WARPS) * I.blocks_y;
-  c->nblocks = I.block_count;
+  // x faces i = -1..imax on rows 0..jmax; y faces i = 0..imax on rows -1..jmax
+  I.block_count[LK_XFACE] = ((c->nx + 1 + 31) / 32) * ((c->ny + FACE_ROWS - 1) / FACE_ROWS);
+  I.block_count[LK_YFACE] = ((c->nx + 31) / 32) * ((c->ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
+  I.block_count[LK_POINT] = ((c->nx + 31) / 32) * ((c->ny + POINT_THREADS / 32 - 1) / (POINT_THREADS / 32));
+  for (int k = 0; k < 3; ++k) { I.block_begin[k] = 0; c->nb[k] = I.block_count[k]; }
   if (cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cueva_ctx_destroy(c); cudaGetLastError();
@@ -419,6 +427,41 @@ int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {
   return CUEVA_OK;
 }
 
+int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int32_t launches_out[3]) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (nsteps < 0 || !ms_out || !launches_out) return fail(CUEVA_ERR_ARG, "bad profile arguments");
+  if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int k = 0; k < 3; ++k) { ms_out[k] = 0.0; launches_out[k] = 0; }
+  cudaEvent_t ev[4] = {};
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      for (auto& f : ev) if (f) cudaEventDestroy(f);
+      return fail(CUEVA_ERR_CUDA, "cudaEventCreate failed");
+    }
+  int32_t rc = CUEVA_OK;
+  for (int n = 0; n < nsteps && rc == CUEVA_OK; ++n) {
+    for (int l = 1; l <= c->T.s && rc == CUEVA_OK; ++l) {
+      const StageArgs sa = stage_args(c, l, 0);
+      cudaError_t ce = launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1,
+                                    sa, ev);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[3]);
+      if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
+      for (int k = 0; k < 3; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+        ms_out[k] += ms;
+        launches_out[k] += 1;
+      }
+      c->qin ^= 1;
+    }
+    c->cur ^= 1;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc) return rc;
+  return read_status(c);
+}
+
 int32_t cueva_sync(cueva_ctx* c) {
   if (int32_t e = check_ctx(c)) return e;
   CUDA_TRY(cudaSetDevice(c->dev));
@@ -493,7 +536,7 @@ int32_t cueva_flux_rhs(cueva_ctx* c, int32_t l) {
     if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
   if (int32_t e = h2d(c, aux_f(c, c->cur, A_W), CUEVA_W, 1)) return e;
   const StageArgs sa = stage_args(c, l, 1);
-  CUDA_TRY(launch_sweep(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nblocks, c->stream, c->d_inst, 1, sa));
+  CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1, sa));
   c->primed = false;
   const int out[NRHS] = {CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
                          CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,

@@ -58,11 +58,15 @@ struct InstDesc {
   double delx, dely, dt, sigma, gamma, kappa_psi, kappa_phi;
   double eps1_c2p;     // value of the Fortran module variable eps1 when con2prim runs
   int c2p;             // 1 Cardano, 0 NR, 2 learned seed + Newton (Cardano fallback)
-  // work decomposition of the sweep launches
-  int strips_x;        // column strips of 31 cells
-  int blocks_y;        // row blocks of SWEEP_ROWS cells
-  int block_begin;     // first CTA index of this instance in the launch
-  int block_count;
+  // interface flux scratch: Fx(i+1/2, j) at fx[(j) * fpitch + (i + 1)],
+  // Fy(i, j+1/2) at fy[(j + 1) * fpitch + i], NFACE fields each
+  double* fx;
+  double* fy;
+  int fpitch;
+  long long ffs;       // doubles per flux field
+  // work decomposition: CTAs of each launch kind (x faces, y faces, points)
+  int block_begin[3];
+  int block_count[3];
 };
 
 // ---- tableau data of one stage launch (by value, kernel parameter space) -----
@@ -98,8 +102,11 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
   return i;
 }
 
-constexpr int SWEEP_WARPS = 4;     // column strips per CTA
-constexpr int SWEEP_ROWS = 16;     // output rows per strip march
-constexpr int STRIP = 31;          // output columns per warp (lane 0 is the halo column)
+// launch geometry: 32 x FACE_ROWS threads per CTA for the face kernels,
+// 256 threads for the pointwise kernels
+constexpr int FACE_ROWS = 4;
+constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
+constexpr int POINT_THREADS = 256;
+enum LaunchKind { LK_XFACE = 0, LK_YFACE = 1, LK_POINT = 2 };
 
 }  // namespace cueva

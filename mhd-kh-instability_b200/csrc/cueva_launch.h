@@ -4,8 +4,10 @@
 #include "cueva_common.cuh"
 
 namespace cueva {
-cudaError_t launch_sweep(int rec_mp, int solver, int prec, int nblocks, cudaStream_t st, const InstDesc* d, int n,
-                         const StageArgs& sa);
+// one RK stage: x faces, y faces, update (nb = CTAs per launch kind); with
+// ev non-null, ev[0..3] are recorded before, between and after the launches
+cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[3], cudaStream_t st, const InstDesc* d,
+                         int n, const StageArgs& sa, cudaEvent_t* ev = nullptr);
 cudaError_t launch_begin_step(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
                               double abt11);
 cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);

@@ -135,4 +135,53 @@ __device__ __forceinline__ void mp_pair_pos(const T (&u)[N], T& L, T& R) {
   R = um1;
 }
 
+// Out-of-line entry points.  A sweep thread reconstructs ~45 slots per grid
+// point; inlining the limiter 45 times made the kernel larger than the
+// instruction cache (ncu: "no instruction" was the top stall).  One copy of
+// each limiter body is called with the stencil values in registers.
+template <typename T> struct Pair { T L, R; };
+
+template <int RM, typename T> struct MPCall;
+template <typename T> struct MPCall<0, T> {
+  static __device__ __noinline__ Pair<T> pair(T a0, T a1, T a2, T a3, T a4, T a5) {
+    const T u[6] = {a0, a1, a2, a3, a4, a5};
+    Pair<T> p; mp_pair<0>(u, p.L, p.R); return p;
+  }
+  static __device__ __noinline__ Pair<T> pos(T a0, T a1, T a2, T a3, T a4, T a5) {
+    const T u[6] = {a0, a1, a2, a3, a4, a5};
+    Pair<T> p; mp_pair_pos<0>(u, p.L, p.R); return p;
+  }
+  template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[6]) {
+    return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5]) : pair(u[0], u[1], u[2], u[3], u[4], u[5]);
+  }
+};
+template <typename T> struct MPCall<1, T> {
+  static __device__ __noinline__ Pair<T> pair(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7) {
+    const T u[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
+    Pair<T> p; mp_pair<1>(u, p.L, p.R); return p;
+  }
+  static __device__ __noinline__ Pair<T> pos(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7) {
+    const T u[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
+    Pair<T> p; mp_pair_pos<1>(u, p.L, p.R); return p;
+  }
+  template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[8]) {
+    return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7])
+               : pair(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7]);
+  }
+};
+template <typename T> struct MPCall<2, T> {
+  static __device__ __noinline__ Pair<T> pair(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7, T a8, T a9) {
+    const T u[10] = {a0, a1, a2, a3, a4, a5, a6, a7, a8, a9};
+    Pair<T> p; mp_pair<2>(u, p.L, p.R); return p;
+  }
+  static __device__ __noinline__ Pair<T> pos(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7, T a8, T a9) {
+    const T u[10] = {a0, a1, a2, a3, a4, a5, a6, a7, a8, a9};
+    Pair<T> p; mp_pair_pos<2>(u, p.L, p.R); return p;
+  }
+  template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[10]) {
+    return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9])
+               : pair(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9]);
+  }
+};
+
 }  // namespace cueva

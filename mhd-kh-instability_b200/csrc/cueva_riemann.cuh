@@ -27,6 +27,7 @@
 namespace cueva {
 
 enum Role { R_PSI = 0, R_PHI, R_BN, R_BT1, R_BT2, R_EN, R_ET1, R_ET2, R_Q, R_D, R_TAU, R_SN, R_ST1, R_ST2, NROLE };
+static_assert(NROLE == NFACE, "flux scratch holds one slab per role");
 
 template <typename T>
 struct Side {

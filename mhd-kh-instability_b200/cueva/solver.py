@@ -99,6 +99,14 @@ class Cueva:
         _abi.check(self.L, self.L.cueva_counters(self.ctx, c))
         return list(c)
 
+    def profile_steps(self, n=1):
+        """Advance n steps kernel by kernel (no graph) and return the summed
+        device ms and launch counts of the (x-face, y-face, update) kernels."""
+        ms = (ctypes.c_double * 3)()
+        cnt = (ctypes.c_int32 * 3)()
+        _abi.check(self.L, self.L.cueva_profile_steps(self.ctx, n, ms, cnt))
+        return list(ms), list(cnt)
+
     def set_stream(self, stream_ptr):
         _abi.check(self.L, self.L.cueva_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
 
