@@ -307,6 +307,12 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   I.imax = c->imax; I.jmax = c->jmax; I.pitch = c->pitch; I.fstride = fs;
   I.bc_x = p->bc_x; I.bc_y = p->bc_y;
   I.delx = c->delx; I.dely = c->dely; I.dt = c->dt; I.sigma = p->sigma; I.gamma = p->gamma;
+  auto inv_pow2 = [](double d) {
+    int e = 0;
+    return (std::frexp(d, &e) == 0.5 && std::isnormal(1.0 / d)) ? 1.0 / d : 0.0;
+  };
+  I.inv_delx_pow2 = inv_pow2(c->delx);
+  I.inv_dely_pow2 = inv_pow2(c->dely);
   const double mn = (c->dely < c->delx) ? c->dely : c->delx;   // parameters.f95:329-334
   const double cp = std::sqrt(mn / 1.0);
   I.kappa_psi = 1.0 / (cp * cp);
@@ -319,7 +325,8 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   I.block_count[LK_YFACE] = ((c->nx + 31) / 32) * ((c->ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
   I.block_count[LK_POINT] = ((c->nx + 31) / 32) * ((c->ny + POINT_THREADS / 32 - 1) / (POINT_THREADS / 32));
   for (int k = 0; k < 3; ++k) { I.block_begin[k] = 0; c->nb[k] = I.block_count[k]; }
-  if (cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
+  if (prepare_stage(p->rec_mp, p->flux_solver, p->precision) != cudaSuccess ||
+      cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     cueva_ctx_destroy(c); cudaGetLastError();
     return fail(CUEVA_ERR_CUDA, "context set-up failed");

@@ -56,6 +56,10 @@ struct InstDesc {
   int bc_x, bc_y;      // 0 copy, 1 periodic
   // scalars
   double delx, dely, dt, sigma, gamma, kappa_psi, kappa_phi;
+  // 1/delx, 1/dely when the spacing is a power of two (then v * inv == v / del
+  // exactly and the divisions of the flux divergence become multiplications);
+  // 0 otherwise
+  double inv_delx_pow2, inv_dely_pow2;
   double eps1_c2p;     // value of the Fortran module variable eps1 when con2prim runs
   int c2p;             // 1 Cardano, 0 NR, 2 learned seed + Newton (Cardano fallback)
   // interface flux scratch: Fx(i+1/2, j) at fx[(j) * fpitch + (i + 1)],
@@ -104,7 +108,7 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
 
 // launch geometry: 32 x FACE_ROWS threads per CTA for the face kernels,
 // 256 threads for the pointwise kernels
-constexpr int FACE_ROWS = 4;
+constexpr int FACE_ROWS = 8;
 constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
 constexpr int POINT_THREADS = 256;
 enum LaunchKind { LK_XFACE = 0, LK_YFACE = 1, LK_POINT = 2 };

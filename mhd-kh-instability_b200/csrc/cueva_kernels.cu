@@ -1,11 +1,11 @@
 // cueva_kernels.cu -- sm_100a kernels of the CUEVA per-step hot path.
 //
 // One RK stage = three launches:
-//  k_face<..., 0>  one thread per x interface (i+1/2, j): MP5/7/9
-//                  reconstruction of the 21 x slots plus the y velocities
-//                  (and y densities for HLLC) at (i, j) that the reference's
-//                  fix-ups couple in, then the HLL / HLLC flux; 14 fluxes
-//                  written to a scratch slab;
+//  k_face<..., 0>  one thread per x interface (i+1/2, j), stencils staged
+//                  in shared memory: MP5/7/9 reconstruction of the 21 x
+//                  slots plus the y velocities (and y densities for HLLC)
+//                  at (i, j) that the reference's fix-ups couple in, then
+//                  the HLL / HLLC flux; 14 fluxes written to a scratch slab;
 //  k_face<..., 1>  the same for the y interfaces (i, j+1/2);
 //  k_update<EP>    one thread per grid point: flux divergence and sources
 //                  (17_fluxandsource.f95:441-635) and a fused pointwise
@@ -169,84 +169,181 @@ __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
 }
 
 // ------------------------------------------------------------ face kernels
-// x faces: i in [-1, imax], j in [0, jmax]; y faces: i in [0, imax],
-// j in [-1, jmax] (the interfaces 17_fluxandsource.f95 differences)
+// A CTA covers 32 interfaces along the row times FACE_ROWS rows.  Every
+// value its stencils read is first copied into shared memory with cp.async
+// (all copies in flight at once, one wait), so the reconstruction and the
+// Riemann solve run from shared memory without global-load latency.
+//   x faces (D = 0): i = i0-1+lane in [-1, imax], j = j0+warp in [0, jmax];
+//   y faces (D = 1): i = i0+lane in [0, imax], j = j0-1+warp in [-1, jmax]
+// (the interfaces 17_fluxandsource.f95 differences).  Staged regions:
+//   normal:     NF fields x FACE_ROWS rows x (32 + 2R + 1) cells along the
+//               normal (x) or NF fields x (FACE_ROWS + 2R + 1) rows x 32
+//               columns (y);
+//   transverse: the NC velocity (+ density) fields the fix-ups couple in,
+//               along the other direction through the face's cell.
+__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
+
+template <int RM, int SOLVER>
+struct FaceGeom {
+  static constexpr int R = MPR<RM>::R;
+  static constexpr int NS = 2 * R + 2;                 // stencil points
+  static constexpr int LONG = 32 + 2 * R + 1;          // staged cells along a 32-face segment
+  static constexpr int DEEP = FACE_ROWS + 2 * R + 1;   // staged rows across FACE_ROWS faces
+  static constexpr int NC = (SOLVER == 7) ? 4 : 3;     // coupled fields: v (+ rho for HLLC)
+  // D = 0: normal [row][f][LONG], transverse [f][DEEP][32]
+  // D = 1: normal [f][DEEP][32],  transverse [row][f][LONG]
+  static constexpr int NORMAL0 = FACE_ROWS * NF_FACE * LONG;
+  static constexpr int NORMAL1 = NF_FACE * DEEP * 32;
+  static constexpr int TRANS0 = NC * DEEP * 32;
+  static constexpr int TRANS1 = FACE_ROWS * NC * LONG;
+  static constexpr size_t bytes(int D) {
+    return sizeof(double) * (size_t)(D == 0 ? NORMAL0 + TRANS0 : NORMAL1 + TRANS1);
+  }
+};
+
 template <int RM, int SOLVER, typename T, int D>
-__global__ void __launch_bounds__(32 * FACE_ROWS)
+__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
 k_face(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
-  constexpr int R = MPR<RM>::R;
-  constexpr int NS = 2 * R + 2;
+  using G = FaceGeom<RM, SOLVER>;
+  constexpr int R = G::R, NS = G::NS, LONG = G::LONG, DEEP = G::DEEP, NC = G::NC;
+  extern __shared__ double smem[];
   int b = blockIdx.x, k = 0;
   for (int t = 1; t < ninst; ++t)
     if (insts[t].block_begin[D] <= b) k = t;
   const InstDesc& I = insts[k];
   b -= I.block_begin[D];
   const int imax = I.imax, jmax = I.jmax, pitch = I.pitch, bcx = I.bc_x, bcy = I.bc_y;
-  const int nfx = (D == 0) ? imax + 2 : imax + 1;          // faces per row
-  const int bpr = (nfx + 31) / 32;
-  const int i = (b % bpr) * 32 + (int)threadIdx.x - (D == 0 ? 1 : 0);
-  const int j = (b / bpr) * FACE_ROWS + (int)threadIdx.y - (D == 1 ? 1 : 0);
-  if (i > imax || j > jmax) return;
+  const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+  const int nfr = (D == 0) ? imax + 2 : imax + 1;      // faces per row
+  const int bpr = (nfr + 31) / 32;
+  const int i0 = (b % bpr) * 32 - (D == 0 ? 1 : 0);      // first face of the segment
+  const int j0 = (b / bpr) * FACE_ROWS - (D == 1 ? 1 : 0);
+  const int i = i0 + lane, j = j0 + w;
   const long long fs = I.fstride;
-  const T gamma = T(I.gamma);
   const double* __restrict__ prim = I.prim[sa.cur];
   const double* __restrict__ Q = I.stage[sa.qin];
+  // staged field f: 0-4 primitive slots (vx, vy, vz, p, rho), 5-19 stage
+  // fields psi..Sz and the current along the normal
+  auto field = [&](int f) -> const double* {
+    if (f < 5) {
+      const int pf = (f < 3) ? P_VX + f : (f == 3 ? P_P : P_RHO);
+      return prim + (long long)pf * fs;
+    }
+    const int qf = (f < 19) ? f - 5 : (D == 0 ? Q_JX : Q_JY);
+    return Q + (long long)qf * fs;
+  };
+  // coupled field c: vx, vy, vz, rho
+  auto cfield = [&](int c) -> const double* { return prim + (long long)(c < 3 ? P_VX + c : P_RHO) * fs; };
+  double* sn = smem;
+  double* st = smem + (D == 0 ? G::NORMAL0 : G::NORMAL1);
+  const int ilast = min(i0 + 31, imax), jlast = min(j0 + FACE_ROWS - 1, jmax);  // last face of the tile
 
-  // stencil offsets: along the normal (cells n-R .. n+1+R) and, for the
-  // coupled fix-ups, along the other direction through the same point
-  int offn[NS], offt[NS];
-  const int ci = map_idx(i, imax, bcx), rj = map_idx(j, jmax, bcy);
+  // ---- stage the stencils (cells reaching beyond the last face are skipped)
+  if constexpr (D == 0) {
+    // normal: rows j0..jlast, cells i0-R .. ilast+R+1 along x
+    const int ncell = ilast + R + 1 - (i0 - R) + 1;
+    for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
+      const int r = e / LONG, c = e - r * LONG;
+      if (j0 + r > jlast || c >= ncell) continue;
+      const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
+      double* d = sn + (r * NF_FACE) * LONG + c;
 #pragma unroll
-  for (int q = 0; q < NS; ++q) {
-    if (D == 0) {
-      offn[q] = rj * pitch + map_idx(i - R + q, imax, bcx);
-      offt[q] = map_idx(j - R + q, jmax, bcy) * pitch + ci;
-    } else {
-      offn[q] = map_idx(j - R + q, jmax, bcy) * pitch + ci;
-      offt[q] = rj * pitch + map_idx(i - R + q, imax, bcx);
+      for (int f = 0; f < NF_FACE; ++f) cp_async8(d + f * LONG, field(f) + off);
+    }
+    // transverse: columns i0..ilast, rows j0-R .. jlast+R+1 along y
+    const int nrow = jlast + R + 1 - (j0 - R) + 1;
+    for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
+      const int r = e >> 5, c = e & 31;
+      if (r >= nrow || i0 + c > ilast) continue;
+      const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
+#pragma unroll
+      for (int f = 0; f < NC; ++f) cp_async8(st + (f * DEEP + r) * 32 + c, cfield(f) + off);
+    }
+  } else {
+    // normal: columns i0..ilast, rows j0-R .. jlast+R+1 along y
+    const int nrow = jlast + R + 1 - (j0 - R) + 1;
+    for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
+      const int r = e >> 5, c = e & 31;
+      if (r >= nrow || i0 + c > ilast) continue;
+      const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
+#pragma unroll
+      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (f * DEEP + r) * 32 + c, field(f) + off);
+    }
+    // transverse: rows j0..jlast, cells i0-R .. ilast+R+1 along x
+    const int ncell = ilast + R + 1 - (i0 - R) + 1;
+    for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
+      const int r = e / LONG, c = e - r * LONG;
+      if (j0 + r > jlast || c >= ncell) continue;
+      const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
+#pragma unroll
+      for (int f = 0; f < NC; ++f) cp_async8(st + (r * NC + f) * LONG + c, cfield(f) + off);
     }
   }
-  auto rec = [&](const double* f, const int (&off)[NS], T& L, T& Rv) {
+  cp_async_wait_all();
+  __syncthreads();
+  if (i > ilast || j > jlast) return;
+
+  // stencil of staged field f through this face (normal) / the face's cell (transverse)
+  auto nrmd = [&](int f, int q) -> double {
+    return (D == 0) ? sn[(w * NF_FACE + f) * LONG + lane + q] : sn[(f * DEEP + w + q) * 32 + lane];
+  };
+  auto nrm = [&](int f, int q) -> T { return T(nrmd(f, q)); };
+  auto trn = [&](int f, int q) -> T {
+    return (D == 0) ? T(st[(f * DEEP + w + q) * 32 + lane]) : T(st[(w * NC + f) * LONG + lane + q]);
+  };
+  auto rec = [&](int f, T& L, T& Rv) {
     T u[NS];
 #pragma unroll
-    for (int q = 0; q < NS; ++q) u[q] = ldT<T>(f + off[q]);
+    for (int q = 0; q < NS; ++q) u[q] = nrm(f, q);
     const Pair<T> p = MPCall<RM, T>::template call<false>(u);
     L = p.L; Rv = p.R;
   };
-  auto recp = [&](const double* f, const int (&off)[NS], T& L, T& Rv) {
+  auto recp = [&](int f, T& L, T& Rv) {
     T u[NS];
 #pragma unroll
-    for (int q = 0; q < NS; ++q) u[q] = ldT<T>(f + off[q]);
+    for (int q = 0; q < NS; ++q) u[q] = nrm(f, q);
     const Pair<T> p = MPCall<RM, T>::template call<true>(u);
     L = p.L; Rv = p.R;
   };
+  auto rect = [&](int f, bool pos, T& L, T& Rv) {
+    T u[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) u[q] = trn(f, q);
+    const Pair<T> p = pos ? MPCall<RM, T>::template call<true>(u) : MPCall<RM, T>::template call<false>(u);
+    L = p.L; Rv = p.R;
+  };
 
-  uint32_t st = 0;
+  uint32_t stt = 0;
   Side<T> L, Rs;
   // primitive slots of this direction (21-25 for x, 58-62 for y)
-  rec(prim + P_VX * fs, offn, L.vx, Rs.vx);
-  rec(prim + P_VY * fs, offn, L.vy, Rs.vy);
-  rec(prim + P_VZ * fs, offn, L.vz, Rs.vz);
-  recp(prim + P_P * fs, offn, L.p, Rs.p);
-  recp(prim + P_RHO * fs, offn, L.rho, Rs.rho);
+  rec(0, L.vx, Rs.vx);
+  rec(1, L.vy, Rs.vy);
+  rec(2, L.vz, Rs.vz);
+  recp(3, L.p, Rs.p);
+  recp(4, L.rho, Rs.rho);
   if constexpr (SOLVER == 5 || SOLVER == 7) {
     // superluminal fall-back, 16_hll_flow_mpx.f95:1393-1462: the x and y
     // reconstructions of the point fall back together if either is
     // superluminal; left states take cell (i,j), right states cell i-1 (x)
     // or j-1 (y), as in the reference
     T ovx, ovy, ovz, wvx, wvy, wvz;
-    rec(prim + P_VX * fs, offt, ovx, wvx);
-    rec(prim + P_VY * fs, offt, ovy, wvy);
-    rec(prim + P_VZ * fs, offt, ovz, wvz);
+    rect(0, false, ovx, wvx);
+    rect(1, false, ovy, wvy);
+    rect(2, false, ovz, wvz);
     const T V2l = pw2(L.vx) + pw2(L.vy) + pw2(L.vz);
     const T V2r = pw2(Rs.vx) + pw2(Rs.vy) + pw2(Rs.vz);
     const T V2ol = pw2(ovx) + pw2(ovy) + pw2(ovz);
     const T V2or = pw2(wvx) + pw2(wvy) + pw2(wvz);
     if (V2l >= T(1) || V2r >= T(1) || V2ol >= T(1) || V2or >= T(1)) {
-      const int c0 = rj * pitch + ci;
-      const int cm = (D == 0) ? rj * pitch + map_idx(i - 1, imax, bcx) : map_idx(j - 1, jmax, bcy) * pitch + ci;
-      L.vx = ldT<T>(prim + P_VX * fs + c0); L.vy = ldT<T>(prim + P_VY * fs + c0); L.vz = ldT<T>(prim + P_VZ * fs + c0);
-      Rs.vx = ldT<T>(prim + P_VX * fs + cm); Rs.vy = ldT<T>(prim + P_VY * fs + cm); Rs.vz = ldT<T>(prim + P_VZ * fs + cm);
+      // cell (i, j) is stencil point R of the normal stencil; i-1 / j-1 is R-1
+      L.vx = nrm(0, R); L.vy = nrm(1, R); L.vz = nrm(2, R);
+      Rs.vx = nrm(0, R - 1); Rs.vy = nrm(1, R - 1); Rs.vz = nrm(2, R - 1);
     }
   }
   if constexpr (SOLVER == 7) {
@@ -257,39 +354,40 @@ k_face(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
       bool other_neg = false;
       if (D == 0) {
         T oL, oR;
-        recp(prim + P_RHO * fs, offt, oL, oR);
+        rect(3, true, oL, oR);
         other_neg = (oL < T(0)) || (oR < T(0));
       }
       if (!other_neg) {
-        const T r10 = T(__ldg(prim + P_RHO * fs + rj * pitch + ci) * 1.0e-1);
+        const T r10 = T(nrmd(4, R) * 1.0e-1);
         if (L.rho < T(0)) L.rho = r10;
         else Rs.rho = r10;
       }
     }
   }
-  rec(Q + Q_PSI * fs, offn, L.psi, Rs.psi);
-  rec(Q + Q_PHI * fs, offn, L.phi, Rs.phi);
-  rec(Q + Q_EX * fs, offn, L.Ex, Rs.Ex);
-  rec(Q + Q_EY * fs, offn, L.Ey, Rs.Ey);
-  rec(Q + Q_EZ * fs, offn, L.Ez, Rs.Ez);
-  rec(Q + Q_BX * fs, offn, L.Bx, Rs.Bx);
-  rec(Q + Q_BY * fs, offn, L.By, Rs.By);
-  rec(Q + Q_BZ * fs, offn, L.Bz, Rs.Bz);
-  rec(Q + Q_Q * fs, offn, L.q, Rs.q);
-  rec(Q + Q_D * fs, offn, L.D, Rs.D);
-  rec(Q + Q_TAU * fs, offn, L.tau, Rs.tau);
-  rec(Q + Q_SX * fs, offn, L.Sx, Rs.Sx);
-  rec(Q + Q_SY * fs, offn, L.Sy, Rs.Sy);
-  rec(Q + Q_SZ * fs, offn, L.Sz, Rs.Sz);
-  rec(Q + (D == 0 ? Q_JX : Q_JY) * fs, offn, L.J, Rs.J);
+  rec(5 + Q_PSI, L.psi, Rs.psi);
+  rec(5 + Q_PHI, L.phi, Rs.phi);
+  rec(5 + Q_EX, L.Ex, Rs.Ex);
+  rec(5 + Q_EY, L.Ey, Rs.Ey);
+  rec(5 + Q_EZ, L.Ez, Rs.Ez);
+  rec(5 + Q_BX, L.Bx, Rs.Bx);
+  rec(5 + Q_BY, L.By, Rs.By);
+  rec(5 + Q_BZ, L.Bz, Rs.Bz);
+  rec(5 + Q_Q, L.q, Rs.q);
+  rec(5 + Q_D, L.D, Rs.D);
+  rec(5 + Q_TAU, L.tau, Rs.tau);
+  rec(5 + Q_SX, L.Sx, Rs.Sx);
+  rec(5 + Q_SY, L.Sy, Rs.Sy);
+  rec(5 + Q_SZ, L.Sz, Rs.Sz);
+  rec(19, L.J, Rs.J);
+  const T gamma = T(I.gamma);
   T F[NROLE];
   if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, F);
-  else hllc_fluxes<D>(L, Rs, gamma, F, st);
+  else hllc_fluxes<D>(L, Rs, gamma, F, stt);
   double* out = (D == 0) ? I.fx : I.fy;
   const long long fo = (D == 0) ? (long long)j * I.fpitch + (i + 1) : (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
   for (int c = 0; c < NROLE; ++c) out[c * I.ffs + fo] = double(F[c]);
-  if (st) atomicOr(I.status, st);
+  if (stt) atomicOr(I.status, stt);
 }
 
 // ------------------------------------------------------------ update kernel
@@ -323,7 +421,9 @@ k_update(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   const double* __restrict__ fy = I.fy;
   auto dxv = [&](int r) { return fx[r * I.ffs + fxo] - fx[r * I.ffs + fxo - 1]; };
   auto dyv = [&](int r) { return fy[r * I.ffs + fyo] - fy[r * I.ffs + fyo - I.fpitch]; };
-  const double dlx = I.delx, dly = I.dely;
+  const double dlx = I.delx, dly = I.dely, ix2 = I.inv_delx_pow2, iy2 = I.inv_dely_pow2;
+  auto dxq = [&](int r) { return ix2 != 0.0 ? dxv(r) * ix2 : dxv(r) / dlx; };   // (dx)/dlx
+  auto dyq = [&](int r) { return iy2 != 0.0 ? dyv(r) * iy2 : dyv(r) / dly; };   // (dy)/dly
   // centre values of stage l and time n
   const double q = Q[Q_Q * fs + pc], psi = Q[Q_PSI * fs + pc], phi = Q[Q_PHI * fs + pc];
   const double Ex = Q[Q_EX * fs + pc], Ey = Q[Q_EY * fs + pc], Ez = Q[Q_EZ * fs + pc];
@@ -332,20 +432,21 @@ k_update(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   const double W = aux[A_W * fs + pc];
   double K[NRHS];
   // 17_fluxandsource.f95:488-598; z differences are (X - X)/Delz = 0
-  K[Q_PSI] = -(dxv(R_PSI)) / dlx - (dyv(R_PSI)) / dly + q - I.kappa_psi * psi;
-  K[Q_PHI] = -(dxv(R_PHI)) / dlx - (dyv(R_PHI)) / dly - I.kappa_phi * phi;
-  K[Q_BX] = -(dyv(R_BT2)) / dly + 0.0 - (dxv(R_BN)) / dlx;
-  K[Q_BY] = (dxv(R_BT1)) / dlx - (dyv(R_BN)) / dly;
-  K[Q_BZ] = -(dxv(R_BT2)) / dlx + (dyv(R_BT1)) / dly;
-  K[Q_EX] = (dyv(R_ET2)) / dly - (dxv(R_EN)) / dlx - q * vx;
-  K[Q_EY] = 0.0 - (dxv(R_ET1)) / dlx - (dyv(R_EN)) / dly - q * vy;
-  K[Q_EZ] = (dxv(R_ET2)) / dlx - (dyv(R_ET1)) / dly - q * vz;
-  K[Q_Q] = -(dxv(R_Q)) / dlx - (dyv(R_Q)) / dly;
-  K[Q_D] = -(dxv(R_D)) / dlx - (dyv(R_D)) / dly;
-  K[Q_TAU] = -(dxv(R_TAU)) / dlx - (dyv(R_TAU)) / dly;
-  K[Q_SX] = -(dxv(R_SN)) / dlx - (dyv(R_ST2)) / dly;
-  K[Q_SY] = -(dxv(R_ST1)) / dlx - (dyv(R_SN)) / dly;
-  K[Q_SZ] = -(dxv(R_ST2)) / dlx - (dyv(R_ST1)) / dly;
+  // (-a)/d == -(a/d) exactly, so every term is -/+ the quotient of a difference
+  K[Q_PSI] = -dxq(R_PSI) - dyq(R_PSI) + q - I.kappa_psi * psi;
+  K[Q_PHI] = -dxq(R_PHI) - dyq(R_PHI) - I.kappa_phi * phi;
+  K[Q_BX] = -dyq(R_BT2) + 0.0 - dxq(R_BN);
+  K[Q_BY] = dxq(R_BT1) - dyq(R_BN);
+  K[Q_BZ] = -dxq(R_BT2) + dyq(R_BT1);
+  K[Q_EX] = dyq(R_ET2) - dxq(R_EN) - q * vx;
+  K[Q_EY] = 0.0 - dxq(R_ET1) - dyq(R_EN) - q * vy;
+  K[Q_EZ] = dxq(R_ET2) - dyq(R_ET1) - q * vz;
+  K[Q_Q] = -dxq(R_Q) - dyq(R_Q);
+  K[Q_D] = -dxq(R_D) - dyq(R_D);
+  K[Q_TAU] = -dxq(R_TAU) - dyq(R_TAU);
+  K[Q_SX] = -dxq(R_SN) - dyq(R_ST2);
+  K[Q_SY] = -dxq(R_ST1) - dyq(R_SN);
+  K[Q_SZ] = -dxq(R_ST2) - dyq(R_ST1);
   stiff_source(I.sigma, W, vx, vy, vz, Ex, Ey, Ez, Bx, By, Bz, K[K_SEX], K[K_SEY], K[K_SEZ]);
 
   if constexpr (EP == EP_RHS) {
@@ -441,12 +542,40 @@ k_update(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
 template <int RM, int SV, typename T>
 static void launch_faces(const int (&nb)[3], cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
                          cudaEvent_t* ev) {
+  using G = FaceGeom<RM, SV>;
   const dim3 blk(32, FACE_ROWS);
   if (ev) cudaEventRecord(ev[0], st);
-  k_face<RM, SV, T, 0><<<nb[LK_XFACE], blk, 0, st>>>(d, n, sa);
+  k_face<RM, SV, T, 0><<<nb[LK_XFACE], blk, G::bytes(0), st>>>(d, n, sa);
   if (ev) cudaEventRecord(ev[1], st);
-  k_face<RM, SV, T, 1><<<nb[LK_YFACE], blk, 0, st>>>(d, n, sa);
+  k_face<RM, SV, T, 1><<<nb[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sa);
   if (ev) cudaEventRecord(ev[2], st);
+}
+
+template <int RM, int SV, typename T>
+static cudaError_t prepare_faces() {
+  using G = FaceGeom<RM, SV>;
+  cudaError_t e = cudaFuncSetAttribute(k_face<RM, SV, T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)G::bytes(0));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_face<RM, SV, T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::bytes(1));
+  return e;
+}
+
+template <int RM, int SV>
+static cudaError_t prepare_rm_sv(int prec) {
+  return prec == 0 ? prepare_faces<RM, SV, double>() : prepare_faces<RM, SV, float>();
+}
+
+cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
+  switch (rec_mp * 10 + (solver == 7 ? 1 : 0)) {
+    case 0: return prepare_rm_sv<0, 5>(prec);
+    case 1: return prepare_rm_sv<0, 7>(prec);
+    case 10: return prepare_rm_sv<1, 5>(prec);
+    case 11: return prepare_rm_sv<1, 7>(prec);
+    case 20: return prepare_rm_sv<2, 5>(prec);
+    case 21: return prepare_rm_sv<2, 7>(prec);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <int RM, int SV>

@@ -4,6 +4,9 @@
 #include "cueva_common.cuh"
 
 namespace cueva {
+// sets the shared-memory limits of the stage kernels (call once per device
+// before the first launch or capture)
+cudaError_t prepare_stage(int rec_mp, int solver, int prec);
 // one RK stage: x faces, y faces, update (nb = CTAs per launch kind); with
 // ev non-null, ev[0..3] are recorded before, between and after the launches
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[3], cudaStream_t st, const InstDesc* d,

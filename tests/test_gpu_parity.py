@@ -125,6 +125,30 @@ def test_steps_vs_oracle(oracle_mod, fma, solver, order, rec, reset):
     g.close()
 
 
+@pytest.mark.parametrize("imax,jmax,solver,rec,bc_x", [
+    (45, 38, 7, 0, 0),    # ragged tiles, spacings 2/45 and 1/38 (not powers of two)
+    (70, 33, 5, 1, 0),
+    (37, 50, 7, 2, 1),    # fully periodic box
+    (6, 6, 7, 0, 0),      # smallest grid the ghost maps allow
+])
+def test_steps_ragged_grids(oracle_mod, imax, jmax, solver, rec, bc_x):
+    """Partial CTA tiles, non-power-of-two spacings (true divisions in the
+    divergence) and both boundary maps: 1 step <= 1e-12, 50 steps <= 1e-9."""
+    g, o = _pair(oracle_mod, imax, jmax, False, order=2, flux_solver=solver, rec_mp=rec, sigma=1e3, bc_x=bc_x)
+    g.kh_init(v0=0.5, a=0.05)
+    o.set_prims(g.prims())
+    g.upload()
+    for steps, bar in ((1, 1e-12), (49, 1e-9)):
+        g.step(steps)
+        g.download()
+        assert o.step(steps) == 0
+        ref = o.get_prims()
+        for n in PRIMS:
+            err = rel_l1_field(n, g.interior(n), ref[n], ref)
+            assert err <= bar, (steps, n, err)
+    g.close()
+
+
 @pytest.mark.parametrize("solver", [5, 7])
 def test_ssp433_reference_breakdown_reproduced(oracle_mod, solver):
     """The reference zeroes the stage sums once per step, which makes its
