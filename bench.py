@@ -42,19 +42,20 @@ def alg_bytes_per_zone(s):
 
 
 FACE_BYTES = 8.0 * (20 + 14)   # per interface: 20 reconstructed fields read once, 14 fluxes written
-KERNELS = ("k_face<x>", "k_face<y>", "k_update")
+KERNELS = ("k_yface", "k_xupd")
 
 
 def kernel_units(cfg):
-    """Units one launch of each kernel processes: x faces, y faces, points."""
-    return ((cfg.imax + 2) * (cfg.jmax + 1), (cfg.imax + 1) * (cfg.jmax + 2), (cfg.imax + 1) * (cfg.jmax + 1))
+    """Units one launch of each kernel processes: y faces, points."""
+    return ((cfg.imax + 1) * (cfg.jmax + 2), (cfg.imax + 1) * (cfg.jmax + 1))
 
 
 def kernel_bytes_per_unit(s):
-    """Algorithmic bytes per unit: a face reads the 20 reconstructed fields
-    once and writes 14 fluxes; a point reads its 28 face fluxes (each face is
-    shared by two points) plus the stage's share of the resident state I/O."""
-    return (FACE_BYTES, FACE_BYTES, alg_bytes_per_zone(s) / s + 8.0 * 28)
+    """Algorithmic bytes per unit: a y face reads the 20 reconstructed fields
+    once and writes 14 fluxes; a point of the x-face + update kernel reads
+    its 20 stencil fields and 14 y fluxes (each y face is shared by two
+    points) plus the stage's share of the resident state I/O."""
+    return (FACE_BYTES, 8.0 * (20 + 14) + alg_bytes_per_zone(s) / s)
 
 
 def measured_peaks():
@@ -276,7 +277,7 @@ def main():
         kernels[name] = {"avg_ms": avg, "launches": kcnt[k], "share": kms[k] / max(sum(kms), 1e-30),
                          "alg_bytes_per_launch": bpu[k] * units[k],
                          "gbs": bpu[k] * units[k] / (avg * 1e-3) / 1e9 if avg > 0 else None}
-    top = max(range(3), key=lambda k: kms[k])
+    top = max(range(len(KERNELS)), key=lambda k: kms[k])
     achieved = kernels[KERNELS[top]]["gbs"]
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "kernel_traffic.json")
@@ -299,7 +300,7 @@ def main():
                          "kernel": KERNELS[top], "kernels": kernels,
                          "note": f"{KERNELS[top]}: {bpu[top]:.0f} algorithmic B per unit x {units[top]} units "
                                  f"per launch / avg launch {kernels[KERNELS[top]]['avg_ms']:.3f} ms"},
-            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 3 * s * args.steps}
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 2 * s * args.steps}
     if rank == 0 and not args.no_cpu_baseline:
         r, cores, sample = cpu_port_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

@@ -121,9 +121,10 @@ int32_t cueva_status(cueva_ctx* ctx, uint32_t* status_bits);
 int32_t cueva_counters(cueva_ctx* ctx, int64_t out3[3]);   /* contador_r, contador_p, contador_v */
 /* nsteps steps launched one kernel at a time (no CUDA graph) with events
  * between the launches on the context stream; ms_out[k] receives the summed
- * device time of the x-face (k = 0), y-face (1) and update (2) kernels and
- * launches_out[k] their launch counts.  Synchronises.  No counterpart in the
- * reference (it is instrumentation for the per-kernel roofline). */
+ * device time of the y-face (k = 0) and the x-face + update (k = 1) kernels
+ * (k = 2 is reserved, 0) and launches_out[k] their launch counts.
+ * Synchronises.  No counterpart in the reference (it is instrumentation for
+ * the per-kernel roofline). */
 int32_t cueva_profile_steps(cueva_ctx* ctx, int32_t nsteps, double ms_out[3], int32_t launches_out[3]);
 
 /* ---- routine mirrors (synchronous; bound host arrays in and out) ------- */

@@ -129,7 +129,7 @@ struct cueva_ctx {
   InstDesc h_inst{};
   int nkslot = 0;
   int kslot_of[8];        // slot of K_m (0-based m) or -1
-  int nb[3] = {0, 0, 0};  // CTAs of the x-face, y-face and point launches
+  int nb[2] = {0, 0};     // CTAs of the x-face + update and the y-face launches
   int cur = 0, qin = 0;
   bool primed = false;
   double* bound[CUEVA_NFIELDS] = {};
@@ -320,11 +320,11 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   // the Fortran module variable eps1 keeps the value the flux routine stored last
   I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
   I.c2p = p->c2p;
-  // x faces i = -1..imax on rows 0..jmax; y faces i = 0..imax on rows -1..jmax
-  I.block_count[LK_XFACE] = ((c->nx + 1 + 31) / 32) * ((c->ny + FACE_ROWS - 1) / FACE_ROWS);
+  // x tiles: 31 points (32 faces) x FACE_ROWS rows; y tiles: 32 columns x
+  // FACE_ROWS face rows of j = -1..jmax
+  I.block_count[LK_XUPD] = ((c->nx + 30) / 31) * ((c->ny + FACE_ROWS - 1) / FACE_ROWS);
   I.block_count[LK_YFACE] = ((c->nx + 31) / 32) * ((c->ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
-  I.block_count[LK_POINT] = ((c->nx + 31) / 32) * ((c->ny + POINT_THREADS / 32 - 1) / (POINT_THREADS / 32));
-  for (int k = 0; k < 3; ++k) { I.block_begin[k] = 0; c->nb[k] = I.block_count[k]; }
+  for (int k = 0; k < 2; ++k) { I.block_begin[k] = 0; c->nb[k] = I.block_count[k]; }
   if (prepare_stage(p->rec_mp, p->flux_solver, p->precision) != cudaSuccess ||
       cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -440,7 +440,7 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
   if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
   CUDA_TRY(cudaSetDevice(c->dev));
   for (int k = 0; k < 3; ++k) { ms_out[k] = 0.0; launches_out[k] = 0; }
-  cudaEvent_t ev[4] = {};
+  cudaEvent_t ev[3] = {};
   for (auto& e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) {
       for (auto& f : ev) if (f) cudaEventDestroy(f);
@@ -452,9 +452,9 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
       const StageArgs sa = stage_args(c, l, 0);
       cudaError_t ce = launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1,
                                     sa, ev);
-      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[3]);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[2]);
       if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < 2; ++k) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
         ms_out[k] += ms;

@@ -68,9 +68,9 @@ struct InstDesc {
   double* fy;
   int fpitch;
   long long ffs;       // doubles per flux field
-  // work decomposition: CTAs of each launch kind (x faces, y faces, points)
-  int block_begin[3];
-  int block_count[3];
+  // work decomposition: CTAs of each launch kind (x faces + update, y faces)
+  int block_begin[2];
+  int block_count[2];
 };
 
 // ---- tableau data of one stage launch (by value, kernel parameter space) -----
@@ -106,11 +106,11 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
   return i;
 }
 
-// launch geometry: 32 x FACE_ROWS threads per CTA for the face kernels,
-// 256 threads for the pointwise kernels
+// launch geometry: 32 x FACE_ROWS threads per CTA for the face tiles
+// (x tiles update 31 points per row), 256 threads for the pointwise kernels
 constexpr int FACE_ROWS = 8;
 constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
 constexpr int POINT_THREADS = 256;
-enum LaunchKind { LK_XFACE = 0, LK_YFACE = 1, LK_POINT = 2 };
+enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1 };
 
 }  // namespace cueva

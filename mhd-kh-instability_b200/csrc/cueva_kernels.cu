@@ -1,22 +1,22 @@
 // cueva_kernels.cu -- sm_100a kernels of the CUEVA per-step hot path.
 //
-// One RK stage = three launches:
-//  k_face<..., 0>  one thread per x interface (i+1/2, j), stencils staged
-//                  in shared memory: MP5/7/9 reconstruction of the 21 x
-//                  slots plus the y velocities (and y densities for HLLC)
-//                  at (i, j) that the reference's fix-ups couple in, then
-//                  the HLL / HLLC flux; 14 fluxes written to a scratch slab;
-//  k_face<..., 1>  the same for the y interfaces (i, j+1/2);
-//  k_update<EP>    one thread per grid point: flux divergence and sources
-//                  (17_fluxandsource.f95:441-635) and a fused pointwise
-//                  epilogue -- sumfin, the next stage's sumint / varint /
-//                  electricvarint / flowinit, or, after the last stage,
-//                  varfin / electricfield, con2prim and the next step's
-//                  startconvar.
+// One RK stage = two launches:
+//  k_yface  one thread per y interface (i, j+1/2), stencils staged in shared
+//           memory: MP5/7/9 reconstruction of the 20 y slots plus the x
+//           velocities at (i, j) that the reference's superluminal fix-up
+//           couples in, then the HLL / HLLC flux; 14 fluxes to a scratch slab;
+//  k_xupd   one thread per x interface (i+1/2, j), same staging, plus the
+//           y densities for the HLLC density fix-up chain; the x flux of the
+//           neighbour interface arrives by warp shuffle, so each thread then
+//           updates its point: flux divergence and sources
+//           (17_fluxandsource.f95:441-635) and a fused pointwise epilogue --
+//           sumfin, the next stage's sumint / varint / electricvarint /
+//           flowinit, or, after the last stage, varfin / electricfield,
+//           con2prim and the next step's startconvar.
 // The reference computes both faces of a point in one loop iteration
-// (16_hll_flow_mpx.f95:1358-1965); splitting them keeps one direction's
-// state per thread (register pressure, occupancy) at the cost of the
-// 28-double flux round trip through L2/HBM.
+// (16_hll_flow_mpx.f95:1358-1965); splitting the directions keeps one
+// direction's state per thread (register pressure, occupancy) at the cost of
+// the 14-double y-flux round trip through L2/HBM.
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -168,17 +168,17 @@ __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
   if (st) atomicOr(I.status, st);
 }
 
-// ------------------------------------------------------------ face kernels
+// ------------------------------------------------------------ face tiles
 // A CTA covers 32 interfaces along the row times FACE_ROWS rows.  Every
 // value its stencils read is first copied into shared memory with cp.async
 // (all copies in flight at once, one wait), so the reconstruction and the
 // Riemann solve run from shared memory without global-load latency.
-//   x faces (D = 0): i = i0-1+lane in [-1, imax], j = j0+warp in [0, jmax];
-//   y faces (D = 1): i = i0+lane in [0, imax], j = j0-1+warp in [-1, jmax]
-// (the interfaces 17_fluxandsource.f95 differences).  Staged regions:
-//   normal:     NF fields x FACE_ROWS rows x (32 + 2R + 1) cells along the
-//               normal (x) or NF fields x (FACE_ROWS + 2R + 1) rows x 32
-//               columns (y);
+//   x faces (D = 0): i = i0+lane, j = j0+warp;  y faces (D = 1): i = i0+lane,
+//   j = j0+warp; face "i" is the interface i+1/2 (x) or j+1/2 (y).
+// Staged regions:
+//   normal:     NF_FACE fields x FACE_ROWS rows x (32 + 2R + 1) cells along
+//               x (D = 0), or NF_FACE fields x (FACE_ROWS + 2R + 1) rows x 32
+//               columns (D = 1);
 //   transverse: the NC velocity (+ density) fields the fix-ups couple in,
 //               along the other direction through the face's cell.
 __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
@@ -202,101 +202,84 @@ struct FaceGeom {
   static constexpr int NORMAL1 = NF_FACE * DEEP * 32;
   static constexpr int TRANS0 = NC * DEEP * 32;
   static constexpr int TRANS1 = FACE_ROWS * NC * LONG;
+  static constexpr __host__ __device__ int normal(int D) { return D == 0 ? NORMAL0 : NORMAL1; }
   static constexpr size_t bytes(int D) {
     return sizeof(double) * (size_t)(D == 0 ? NORMAL0 + TRANS0 : NORMAL1 + TRANS1);
   }
+  // staged offset of field f at the face's stencil point q (normal) and of
+  // coupled field f at stencil point q through the face's cell (transverse)
+  template <int D> static __device__ __forceinline__ int nrm(int f, int q, int w, int lane) {
+    return D == 0 ? (w * NF_FACE + f) * LONG + lane + q : (f * DEEP + w + q) * 32 + lane;
+  }
+  template <int D> static __device__ __forceinline__ int trn(int f, int q, int w, int lane) {
+    return D == 0 ? (f * DEEP + w + q) * 32 + lane : (w * NC + f) * LONG + lane + q;
+  }
 };
 
-template <int RM, int SOLVER, typename T, int D>
-__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
-k_face(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
+// staged field f: 0-4 primitive slots (vx, vy, vz, p, rho) of time n, 5-18
+// the stage's conserved psi..Sz, 19 the current along the normal
+template <int D>
+__device__ __forceinline__ const double* face_field(const double* prim, const double* Q, long long fs, int f) {
+  if (f < 5) {
+    const int pf = (f < 3) ? P_VX + f : (f == 3 ? P_P : P_RHO);
+    return prim + (long long)pf * fs;
+  }
+  const int qf = (f < 19) ? f - 5 : (D == 0 ? Q_JX : Q_JY);
+  return Q + (long long)qf * fs;
+}
+
+// issue the cp.async copies of one tile (first face i0, j0; last ilast, jlast);
+// cells reaching beyond the last face are not copied
+template <int RM, int SOLVER, int D>
+__device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& sa, double* sn, double* st, int i0,
+                                           int j0, int ilast, int jlast, int tid) {
   using G = FaceGeom<RM, SOLVER>;
-  constexpr int R = G::R, NS = G::NS, LONG = G::LONG, DEEP = G::DEEP, NC = G::NC;
-  extern __shared__ double smem[];
-  int b = blockIdx.x, k = 0;
-  for (int t = 1; t < ninst; ++t)
-    if (insts[t].block_begin[D] <= b) k = t;
-  const InstDesc& I = insts[k];
-  b -= I.block_begin[D];
+  constexpr int R = G::R, LONG = G::LONG, DEEP = G::DEEP, NC = G::NC;
   const int imax = I.imax, jmax = I.jmax, pitch = I.pitch, bcx = I.bc_x, bcy = I.bc_y;
-  const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
-  const int nfr = (D == 0) ? imax + 2 : imax + 1;      // faces per row
-  const int bpr = (nfr + 31) / 32;
-  const int i0 = (b % bpr) * 32 - (D == 0 ? 1 : 0);      // first face of the segment
-  const int j0 = (b / bpr) * FACE_ROWS - (D == 1 ? 1 : 0);
-  const int i = i0 + lane, j = j0 + w;
   const long long fs = I.fstride;
   const double* __restrict__ prim = I.prim[sa.cur];
   const double* __restrict__ Q = I.stage[sa.qin];
-  // staged field f: 0-4 primitive slots (vx, vy, vz, p, rho), 5-19 stage
-  // fields psi..Sz and the current along the normal
-  auto field = [&](int f) -> const double* {
-    if (f < 5) {
-      const int pf = (f < 3) ? P_VX + f : (f == 3 ? P_P : P_RHO);
-      return prim + (long long)pf * fs;
-    }
-    const int qf = (f < 19) ? f - 5 : (D == 0 ? Q_JX : Q_JY);
-    return Q + (long long)qf * fs;
-  };
-  // coupled field c: vx, vy, vz, rho
   auto cfield = [&](int c) -> const double* { return prim + (long long)(c < 3 ? P_VX + c : P_RHO) * fs; };
-  double* sn = smem;
-  double* st = smem + (D == 0 ? G::NORMAL0 : G::NORMAL1);
-  const int ilast = min(i0 + 31, imax), jlast = min(j0 + FACE_ROWS - 1, jmax);  // last face of the tile
-
-  // ---- stage the stencils (cells reaching beyond the last face are skipped)
-  if constexpr (D == 0) {
-    // normal: rows j0..jlast, cells i0-R .. ilast+R+1 along x
-    const int ncell = ilast + R + 1 - (i0 - R) + 1;
-    for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
-      const int r = e / LONG, c = e - r * LONG;
-      if (j0 + r > jlast || c >= ncell) continue;
-      const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
-      double* d = sn + (r * NF_FACE) * LONG + c;
+  const int ncell = ilast + R + 1 - (i0 - R) + 1;   // x cells i0-R .. ilast+R+1
+  const int nrow = jlast + R + 1 - (j0 - R) + 1;    // y rows j0-R .. jlast+R+1
+  // rows j0..jlast, cells along x: the normal stencils (D = 0) or the coupled ones (D = 1)
+  for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
+    const int r = e / LONG, c = e - r * LONG;
+    if (j0 + r > jlast || c >= ncell) continue;
+    const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
+    if constexpr (D == 0) {
 #pragma unroll
-      for (int f = 0; f < NF_FACE; ++f) cp_async8(d + f * LONG, field(f) + off);
-    }
-    // transverse: columns i0..ilast, rows j0-R .. jlast+R+1 along y
-    const int nrow = jlast + R + 1 - (j0 - R) + 1;
-    for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
-      const int r = e >> 5, c = e & 31;
-      if (r >= nrow || i0 + c > ilast) continue;
-      const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
-#pragma unroll
-      for (int f = 0; f < NC; ++f) cp_async8(st + (f * DEEP + r) * 32 + c, cfield(f) + off);
-    }
-  } else {
-    // normal: columns i0..ilast, rows j0-R .. jlast+R+1 along y
-    const int nrow = jlast + R + 1 - (j0 - R) + 1;
-    for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
-      const int r = e >> 5, c = e & 31;
-      if (r >= nrow || i0 + c > ilast) continue;
-      const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
-#pragma unroll
-      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (f * DEEP + r) * 32 + c, field(f) + off);
-    }
-    // transverse: rows j0..jlast, cells i0-R .. ilast+R+1 along x
-    const int ncell = ilast + R + 1 - (i0 - R) + 1;
-    for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
-      const int r = e / LONG, c = e - r * LONG;
-      if (j0 + r > jlast || c >= ncell) continue;
-      const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
+      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (r * NF_FACE + f) * LONG + c, face_field<D>(prim, Q, fs, f) + off);
+    } else {
 #pragma unroll
       for (int f = 0; f < NC; ++f) cp_async8(st + (r * NC + f) * LONG + c, cfield(f) + off);
     }
   }
-  cp_async_wait_all();
-  __syncthreads();
-  if (i > ilast || j > jlast) return;
+  // columns i0..ilast, rows along y: the coupled stencils (D = 0) or the normal ones (D = 1)
+  for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
+    const int r = e >> 5, c = e & 31;
+    if (r >= nrow || i0 + c > ilast) continue;
+    const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
+    if constexpr (D == 0) {
+#pragma unroll
+      for (int f = 0; f < NC; ++f) cp_async8(st + (f * DEEP + r) * 32 + c, cfield(f) + off);
+    } else {
+#pragma unroll
+      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (f * DEEP + r) * 32 + c, face_field<D>(prim, Q, fs, f) + off);
+    }
+  }
+}
 
-  // stencil of staged field f through this face (normal) / the face's cell (transverse)
-  auto nrmd = [&](int f, int q) -> double {
-    return (D == 0) ? sn[(w * NF_FACE + f) * LONG + lane + q] : sn[(f * DEEP + w + q) * 32 + lane];
-  };
+// flux of the face of (w, lane) from the staged tile (16_hll_flow_mpx.f95 /
+// 16_hllc_flow_mpx.f95 for one interface); returns status bits
+template <int RM, int SOLVER, typename T, int D>
+__device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
+                                              T (&F)[NROLE]) {
+  using G = FaceGeom<RM, SOLVER>;
+  constexpr int R = G::R, NS = G::NS;
+  auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
   auto nrm = [&](int f, int q) -> T { return T(nrmd(f, q)); };
-  auto trn = [&](int f, int q) -> T {
-    return (D == 0) ? T(st[(f * DEEP + w + q) * 32 + lane]) : T(st[(w * NC + f) * LONG + lane + q]);
-  };
+  auto trn = [&](int f, int q) -> T { return T(st[G::template trn<D>(f, q, w, lane)]); };
   auto rec = [&](int f, T& L, T& Rv) {
     T u[NS];
 #pragma unroll
@@ -379,74 +362,95 @@ k_face(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   rec(5 + Q_SY, L.Sy, Rs.Sy);
   rec(5 + Q_SZ, L.Sz, Rs.Sz);
   rec(19, L.J, Rs.J);
-  const T gamma = T(I.gamma);
-  T F[NROLE];
+  const T gamma = T(gamma_d);
   if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, F);
   else hllc_fluxes<D>(L, Rs, gamma, F, stt);
-  double* out = (D == 0) ? I.fx : I.fy;
-  const long long fo = (D == 0) ? (long long)j * I.fpitch + (i + 1) : (long long)(j + 1) * I.fpitch + i;
+  return stt;
+}
+
+__device__ __forceinline__ const InstDesc& tile_inst(const InstDesc* __restrict__ insts, int ninst, int kind, int& b) {
+  int k = 0;
+  for (int t = 1; t < ninst; ++t)
+    if (insts[t].block_begin[kind] <= b) k = t;
+  b -= insts[k].block_begin[kind];
+  return insts[k];
+}
+
+// y faces: 32 columns x FACE_ROWS face rows j = j0-1+warp in [-1, jmax];
+// writes Fy(i, j+1/2) to the flux scratch
+template <int RM, int SOLVER, typename T>
+__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
+k_yface(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
+  using G = FaceGeom<RM, SOLVER>;
+  extern __shared__ double smem[];
+  int b = blockIdx.x;
+  const InstDesc& I = tile_inst(insts, ninst, LK_YFACE, b);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int bpr = (I.imax + 1 + 31) / 32;
+  const int i0 = (b % bpr) * 32, j0 = (b / bpr) * FACE_ROWS - 1;
+  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + FACE_ROWS - 1, I.jmax);
+  double* sn = smem;
+  double* st = smem + G::normal(1);
+  stage_tile<RM, SOLVER, 1>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
+  cp_async_wait_all();
+  __syncthreads();
+  const int i = i0 + lane, j = j0 + w;
+  if (i > ilast || j > jlast) return;
+  T F[NROLE];
+  const uint32_t stt = face_flux<RM, SOLVER, T, 1>(sn, st, w, lane, I.gamma, F);
+  const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
-  for (int c = 0; c < NROLE; ++c) out[c * I.ffs + fo] = double(F[c]);
+  for (int c = 0; c < NROLE; ++c) I.fy[c * I.ffs + fo] = double(F[c]);
   if (stt) atomicOr(I.status, stt);
 }
 
-// ------------------------------------------------------------ update kernel
+// ------------------------------------------------- x faces + point update
 // EP selects the epilogue: EP_RHS stores the stage right-hand side only (the
 // routine mirror), EP_MID prepares stage l+1, EP_LAST finishes the step.
 enum Epilogue { EP_RHS = 0, EP_MID = 1, EP_LAST = 2 };
 
+// centre values of stage l (psi, phi, E, B, q) and time n (v) of a point
+struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
+
+// flux divergence + sources of point (i, j) (17_fluxandsource.f95:441-635)
+// and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
 template <int EP>
-__global__ void __launch_bounds__(POINT_THREADS)
-k_update(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
-  int b = blockIdx.x, k = 0;
-  for (int t = 1; t < ninst; ++t)
-    if (insts[t].block_begin[LK_POINT] <= b) k = t;
-  const InstDesc& I = insts[k];
-  b -= I.block_begin[LK_POINT];
-  const int nx = I.imax + 1;
-  const int bpr = (nx + 31) / 32;
-  const int i = (b % bpr) * 32 + (int)(threadIdx.x & 31);
-  const int j = (b / bpr) * (POINT_THREADS / 32) + (int)(threadIdx.x >> 5);
-  if (i > I.imax || j > I.jmax) return;
+__device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
+                                                 const double (&qx)[NROLE], const Centre& cv) {
   const int pitch = I.pitch;
   const long long fs = I.fstride;
   const double* __restrict__ prim = I.prim[sa.cur];
   const double* __restrict__ aux = I.aux[sa.cur];
-  const double* __restrict__ Q = I.stage[sa.qin];
   uint32_t st = 0;
   const long long pc = (long long)j * pitch + i;
-  const long long fxo = (long long)j * I.fpitch + (i + 1);      // Fx(i+1/2, j); Fx(i-1/2, j) at -1
   const long long fyo = (long long)(j + 1) * I.fpitch + i;      // Fy(i, j+1/2); Fy(i, j-1/2) at -fpitch
-  const double* __restrict__ fx = I.fx;
   const double* __restrict__ fy = I.fy;
-  auto dxv = [&](int r) { return fx[r * I.ffs + fxo] - fx[r * I.ffs + fxo - 1]; };
-  auto dyv = [&](int r) { return fy[r * I.ffs + fyo] - fy[r * I.ffs + fyo - I.fpitch]; };
-  const double dlx = I.delx, dly = I.dely, ix2 = I.inv_delx_pow2, iy2 = I.inv_dely_pow2;
-  auto dxq = [&](int r) { return ix2 != 0.0 ? dxv(r) * ix2 : dxv(r) / dlx; };   // (dx)/dlx
-  auto dyq = [&](int r) { return iy2 != 0.0 ? dyv(r) * iy2 : dyv(r) / dly; };   // (dy)/dly
-  // centre values of stage l and time n
-  const double q = Q[Q_Q * fs + pc], psi = Q[Q_PSI * fs + pc], phi = Q[Q_PHI * fs + pc];
-  const double Ex = Q[Q_EX * fs + pc], Ey = Q[Q_EY * fs + pc], Ez = Q[Q_EZ * fs + pc];
-  const double Bx = Q[Q_BX * fs + pc], By = Q[Q_BY * fs + pc], Bz = Q[Q_BZ * fs + pc];
-  const double vx = prim[P_VX * fs + pc], vy = prim[P_VY * fs + pc], vz = prim[P_VZ * fs + pc];
+  const double dly = I.dely, iy2 = I.inv_dely_pow2;
+  auto qy = [&](int r) {   // (dy)/dly
+    const double d = fy[r * I.ffs + fyo] - fy[r * I.ffs + fyo - I.fpitch];
+    return iy2 != 0.0 ? d * iy2 : d / dly;
+  };
+  auto qxf = [&](int r) { return qx[r]; };
+  const double q = cv.q, psi = cv.psi, phi = cv.phi, Ex = cv.Ex, Ey = cv.Ey, Ez = cv.Ez;
+  const double Bx = cv.Bx, By = cv.By, Bz = cv.Bz, vx = cv.vx, vy = cv.vy, vz = cv.vz;
   const double W = aux[A_W * fs + pc];
   double K[NRHS];
   // 17_fluxandsource.f95:488-598; z differences are (X - X)/Delz = 0
   // (-a)/d == -(a/d) exactly, so every term is -/+ the quotient of a difference
-  K[Q_PSI] = -dxq(R_PSI) - dyq(R_PSI) + q - I.kappa_psi * psi;
-  K[Q_PHI] = -dxq(R_PHI) - dyq(R_PHI) - I.kappa_phi * phi;
-  K[Q_BX] = -dyq(R_BT2) + 0.0 - dxq(R_BN);
-  K[Q_BY] = dxq(R_BT1) - dyq(R_BN);
-  K[Q_BZ] = -dxq(R_BT2) + dyq(R_BT1);
-  K[Q_EX] = dyq(R_ET2) - dxq(R_EN) - q * vx;
-  K[Q_EY] = 0.0 - dxq(R_ET1) - dyq(R_EN) - q * vy;
-  K[Q_EZ] = dxq(R_ET2) - dyq(R_ET1) - q * vz;
-  K[Q_Q] = -dxq(R_Q) - dyq(R_Q);
-  K[Q_D] = -dxq(R_D) - dyq(R_D);
-  K[Q_TAU] = -dxq(R_TAU) - dyq(R_TAU);
-  K[Q_SX] = -dxq(R_SN) - dyq(R_ST2);
-  K[Q_SY] = -dxq(R_ST1) - dyq(R_SN);
-  K[Q_SZ] = -dxq(R_ST2) - dyq(R_ST1);
+  K[Q_PSI] = -qxf(R_PSI) - qy(R_PSI) + q - I.kappa_psi * psi;
+  K[Q_PHI] = -qxf(R_PHI) - qy(R_PHI) - I.kappa_phi * phi;
+  K[Q_BX] = -qy(R_BT2) + 0.0 - qxf(R_BN);
+  K[Q_BY] = qxf(R_BT1) - qy(R_BN);
+  K[Q_BZ] = -qxf(R_BT2) + qy(R_BT1);
+  K[Q_EX] = qy(R_ET2) - qxf(R_EN) - q * vx;
+  K[Q_EY] = 0.0 - qxf(R_ET1) - qy(R_EN) - q * vy;
+  K[Q_EZ] = qxf(R_ET2) - qy(R_ET1) - q * vz;
+  K[Q_Q] = -qxf(R_Q) - qy(R_Q);
+  K[Q_D] = -qxf(R_D) - qy(R_D);
+  K[Q_TAU] = -qxf(R_TAU) - qy(R_TAU);
+  K[Q_SX] = -qxf(R_SN) - qy(R_ST2);
+  K[Q_SY] = -qxf(R_ST1) - qy(R_SN);
+  K[Q_SZ] = -qxf(R_ST2) - qy(R_ST1);
   stiff_source(I.sigma, W, vx, vy, vz, Ex, Ey, Ez, Bx, By, Bz, K[K_SEX], K[K_SEY], K[K_SEZ]);
 
   if constexpr (EP == EP_RHS) {
@@ -535,35 +539,93 @@ k_update(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
       begin_step_point(I, sa.abt_diag_first, I.aux[1 - sa.cur], I.stage[1 - sa.qin], pc, pv);
     }
   }
-  if (st) atomicOr(I.status, st);
+  return st;
+}
+
+template <int RM, int SOLVER, typename T, int EP>
+__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
+k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
+  using G = FaceGeom<RM, SOLVER>;
+  constexpr int R = G::R, LONG = G::LONG;
+  extern __shared__ double smem[];
+  int b = blockIdx.x;
+  const InstDesc& I = tile_inst(insts, ninst, LK_XUPD, b);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  // a tile updates 31 points per row: faces i0 .. i0+31 (i0 = first point - 1)
+  const int bpr = (I.imax + 1 + 30) / 31;
+  const int i0 = (b % bpr) * 31 - 1, j0 = (b / bpr) * FACE_ROWS;
+  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + FACE_ROWS - 1, I.jmax);
+  double* sn = smem;
+  double* st = smem + G::normal(0);
+  stage_tile<RM, SOLVER, 0>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
+  cp_async_wait_all();
+  __syncthreads();
+  const int i = i0 + lane, j = j0 + w;
+  if (j > jlast) return;   // whole warp
+  T F[NROLE];
+#pragma unroll
+  for (int c = 0; c < NROLE; ++c) F[c] = T(0);
+  uint32_t stt = 0;
+  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0>(sn, st, w, lane, I.gamma, F);
+  // Fx(i-1/2) of point i is the face of lane-1
+  const double dlx = I.delx, ix2 = I.inv_delx_pow2;
+  double qx[NROLE];
+#pragma unroll
+  for (int c = 0; c < NROLE; ++c) {
+    const double fr = double(F[c]);
+    const double fl = __shfl_up_sync(0xffffffffu, fr, 1);
+    const double d = fr - fl;
+    qx[c] = ix2 != 0.0 ? d * ix2 : d / dlx;
+  }
+  if (lane >= 1 && i <= ilast) {
+    // centre values: staged cell i is stencil point R of this lane's face
+    auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + lane + R]; };
+    const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
+                    cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
+    stt |= update_point<EP>(I, sa, i, j, qx, cv);
+  }
+  if (stt) atomicOr(I.status, stt);
 }
 
 // ---------------------------------------------------------------- launchers
 template <int RM, int SV, typename T>
-static void launch_faces(const int (&nb)[3], cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
+static void launch_tiles(const int (&nb)[2], cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
                          cudaEvent_t* ev) {
   using G = FaceGeom<RM, SV>;
   const dim3 blk(32, FACE_ROWS);
   if (ev) cudaEventRecord(ev[0], st);
-  k_face<RM, SV, T, 0><<<nb[LK_XFACE], blk, G::bytes(0), st>>>(d, n, sa);
+  k_yface<RM, SV, T><<<nb[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sa);
   if (ev) cudaEventRecord(ev[1], st);
-  k_face<RM, SV, T, 1><<<nb[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sa);
+  if (sa.mode == 1) k_xupd<RM, SV, T, EP_RHS><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
+  else if (sa.l < sa.s) k_xupd<RM, SV, T, EP_MID><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
+  else k_xupd<RM, SV, T, EP_LAST><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
   if (ev) cudaEventRecord(ev[2], st);
 }
 
 template <int RM, int SV, typename T>
-static cudaError_t prepare_faces() {
+static cudaError_t prepare_tiles() {
   using G = FaceGeom<RM, SV>;
-  cudaError_t e = cudaFuncSetAttribute(k_face<RM, SV, T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)G::bytes(0));
+  const int b0 = (int)G::bytes(0), b1 = (int)G::bytes(1);
+  cudaError_t e = cudaFuncSetAttribute(k_yface<RM, SV, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_face<RM, SV, T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::bytes(1));
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
   return e;
 }
 
 template <int RM, int SV>
+static void launch_rm_sv(int prec, const int (&nb)[2], cudaStream_t st, const InstDesc* d, int n,
+                         const StageArgs& sa, cudaEvent_t* ev) {
+  if (prec == 0) launch_tiles<RM, SV, double>(nb, st, d, n, sa, ev);
+  else launch_tiles<RM, SV, float>(nb, st, d, n, sa, ev);
+}
+
+template <int RM, int SV>
 static cudaError_t prepare_rm_sv(int prec) {
-  return prec == 0 ? prepare_faces<RM, SV, double>() : prepare_faces<RM, SV, float>();
+  return prec == 0 ? prepare_tiles<RM, SV, double>() : prepare_tiles<RM, SV, float>();
 }
 
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
@@ -578,14 +640,7 @@ cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
   }
 }
 
-template <int RM, int SV>
-static void launch_rm_sv(int prec, const int (&nb)[3], cudaStream_t st, const InstDesc* d, int n,
-                         const StageArgs& sa, cudaEvent_t* ev) {
-  if (prec == 0) launch_faces<RM, SV, double>(nb, st, d, n, sa, ev);
-  else launch_faces<RM, SV, float>(nb, st, d, n, sa, ev);
-}
-
-cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[3], cudaStream_t st, const InstDesc* d,
+cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[2], cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev) {
   switch (rec_mp * 10 + (solver == 7 ? 1 : 0)) {
     case 0: launch_rm_sv<0, 5>(prec, nb, st, d, n, sa, ev); break;
@@ -596,10 +651,6 @@ cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[3], c
     case 21: launch_rm_sv<2, 7>(prec, nb, st, d, n, sa, ev); break;
     default: return cudaErrorInvalidValue;
   }
-  if (sa.mode == 1) k_update<EP_RHS><<<nb[LK_POINT], POINT_THREADS, 0, st>>>(d, n, sa);
-  else if (sa.l < sa.s) k_update<EP_MID><<<nb[LK_POINT], POINT_THREADS, 0, st>>>(d, n, sa);
-  else k_update<EP_LAST><<<nb[LK_POINT], POINT_THREADS, 0, st>>>(d, n, sa);
-  if (ev) cudaEventRecord(ev[3], st);
   return cudaGetLastError();
 }
 
