@@ -186,6 +186,13 @@ __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// L2 prefetch of the n doubles at p, widened to 16-byte boundaries (which
+// stay inside the 256-byte-aligned row the doubles belong to)
+__device__ __forceinline__ void prefetch_l2(const double* p, int n) {
+  const unsigned long long a = (unsigned long long)p & ~15ull;
+  const unsigned long long e = ((unsigned long long)(p + n) + 15ull) & ~15ull;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
 
 constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
 
@@ -558,6 +565,40 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   double* sn = smem;
   double* st = smem + G::normal(0);
   stage_tile<RM, SOLVER, 0>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
+  if constexpr (EP != EP_RHS) {
+    // the update's other inputs go to L2 while the faces are computed: per
+    // row of the tile, the 6 aux and 9 time-n primitive fields, finsum and
+    // intsum when loaded, stored stage right-hand sides, and the y fluxes
+    const long long fs = I.fstride;
+    const int npt = ilast - i0, nr = jlast - j0 + 1;
+    const int nfin = (sa.l > 1) ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
+    int nk = 0;
+    for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
+    const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;   // fields read at the point
+    const int total = ncen * nr + NROLE * (nr + 1);
+    for (int e = w * 32 + lane; e < total && npt > 0; e += 32 * FACE_ROWS) {
+      if (e < ncen * nr) {
+        const int r = e % nr;
+        int f = e / nr;
+        const double* base;
+        if (f < NAUX) base = I.aux[sa.cur] + f * fs;
+        else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
+        else if ((f -= 9) < nfin) base = I.finsum + f * fs;
+        else if ((f -= nfin) < nint) base = I.intsum + f * fs;
+        else {
+          f -= nint;
+          int kk = f / NRHS, m = 1;
+          for (; m < sa.l; ++m)
+            if (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0) && kk-- == 0) break;
+          base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + f % NRHS) * fs;
+        }
+        prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
+      } else {
+        const int e2 = e - ncen * nr, r = e2 % (nr + 1), c = e2 / (nr + 1);
+        prefetch_l2(I.fy + c * I.ffs + (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
+      }
+    }
+  }
   cp_async_wait_all();
   __syncthreads();
   const int i = i0 + lane, j = j0 + w;
