@@ -142,6 +142,45 @@ int32_t cueva_flux_rhs(cueva_ctx* ctx, int32_t l);
  * the seeds V, rho, p -> V, rho, p */
 int32_t cueva_con2prim(cueva_ctx* ctx);
 
+/* ---- stage right-hand side without any device allocation -------------- */
+/* No counterpart in the reference.  Computes the same stage right-hand side
+ * as cueva_flux_rhs ({hll,hllc}_flow_mpx 2D + fluxandsource), but on device
+ * arrays the caller already owns and without a context, so it never calls
+ * cudaMalloc, cudaFree or anything else that allocates device memory.  It is
+ * meant for callers that cannot allocate at this point: code running under a
+ * fixed memory budget or a pre-sized arena whose free memory belongs to
+ * another framework, and loops that must not pay the device-wide
+ * synchronisation that cudaMalloc / cudaFree imply.
+ *
+ * Arrays (device memory, FP64, interior points only): point (i, j) of field
+ * f of a group is at base[f * fstride + j * pitch + i], 0 <= i <= imax,
+ * 0 <= j <= jmax, with pitch >= imax + 1 and fstride >= pitch * (jmax + 1):
+ *   prim   the 14 primitives of time n in cueva_field order (rho .. q);
+ *   W      the Lorentz factor of time n (one field);
+ *   stage  the stage's 14 conserved (psi, phi, E, B, q, D, tau, S, in
+ *          cueva_field order) followed by Jx, Jy, Jz (17 fields);
+ *   rhs    out: psiflux .. Szflux, Exastsour .. Ezastsour (17 fields).
+ * Only params' imax, jmax, flux_solver, rec_mp, bc_x, bc_y, precision,
+ * device, lx, ly, lz, gamma and sigma are read.
+ *
+ * The interface-flux scratch is a fixed 32 MiB block of static device
+ * memory inside the library (14 flux fields of (round32(imax + 2)) *
+ * (jmax + 2) doubles plus a small header): grids that need more are
+ * rejected with CUEVA_ERR_ARG and a message giving both sizes; 512 x 512
+ * fits.  The first call on a device looks up the block's address and sets
+ * the kernels' shared-memory limits there (no allocation); make that first
+ * call before any stream capture.  The status word in the block is zeroed
+ * by every call.  The block is shared by all calls on a device, so calls
+ * that overlap in time (on different streams or host threads) race on it;
+ * serialise them.
+ *
+ * Asynchronous on `stream` (0 = the legacy default stream).  If
+ * status_bits is non-null the call waits for the stream and stores the
+ * kernel status bits there; a non-zero status returns CUEVA_ERR_PHYSICS. */
+int32_t cueva_flux_rhs_noalloc(const cueva_params* params, const double* prim, const double* W,
+                               const double* stage, double* rhs, int32_t pitch, int64_t fstride, void* stream,
+                               uint32_t* status_bits);
+
 /* ---- synthetic input ------------------------------------------------- */
 /* Kelvin-Helmholtz initial data on the Fortran-layout prim arrays bound to
  * ctx (interior points; reference orientation: x = shear normal with copy

@@ -596,4 +596,106 @@ int32_t cueva_kh_init(cueva_ctx* c, double v0, double a, double amp, double widt
   return CUEVA_OK;
 }
 
+// ------------------------------------------- stage rhs without allocation
+// Scratch for cueva_flux_rhs_noalloc: a 256-byte header (status word and
+// fix-up counters, zeroed per call), the kernels' instance descriptor, then
+// the 14 y-flux fields.  Static device memory: nothing is allocated at run
+// time.
+namespace {
+constexpr size_t kNoallocBytes = size_t(32) << 20;
+constexpr size_t kNoallocHeader = 256;
+constexpr size_t kNoallocDesc = (sizeof(InstDesc) + 255) / 256 * 256;
+constexpr int kMaxDevices = 64;
+void* g_noalloc_base[kMaxDevices] = {};
+}  // namespace
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocBytes / sizeof(double)];
+
+int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const double* W, const double* stage,
+                               double* rhs, int32_t pitch, int64_t fstride, void* stream, uint32_t* status_bits) {
+  if (!p || !prim || !W || !stage || !rhs) return fail(CUEVA_ERR_ARG, "null argument");
+  if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
+  if (p->flux_solver != 5 && p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
+  if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
+  if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
+    return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
+  if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
+  const int nx = p->imax + 1, ny = p->jmax + 1;
+  if (pitch < nx || fstride < (int64_t)pitch * ny) return fail(CUEVA_ERR_ARG, "pitch < imax+1 or fstride < pitch*(jmax+1)");
+  const int fpitch = (nx + 1 + 31) / 32 * 32;
+  const long long ffs = (long long)fpitch * (ny + 1);
+  const size_t need = kNoallocHeader + kNoallocDesc + (size_t)NFACE * (size_t)ffs * sizeof(double);
+  if (need > kNoallocBytes)
+    return fail(CUEVA_ERR_ARG, "grid too large for the no-alloc scratch: needs " + std::to_string(need) +
+                                   " bytes, the static block holds " + std::to_string(kNoallocBytes));
+  if (p->device < 0 || p->device >= kMaxDevices) return fail(CUEVA_ERR_ARG, "device ordinal out of range");
+  CUDA_TRY(cudaSetDevice(p->device));
+  if (!g_noalloc_base[p->device]) {
+    // once per device, with that device current
+    void* base = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&base, g_noalloc_scratch));
+    for (int rm = 0; rm < 3; ++rm)
+      for (int sv : {5, 7})
+        for (int pr = 0; pr < 2; ++pr) CUDA_TRY(prepare_stage(rm, sv, pr));
+    g_noalloc_base[p->device] = base;
+  }
+  char* base = (char*)g_noalloc_base[p->device];
+  cudaStream_t st = (cudaStream_t)stream;
+  InstDesc I{};
+  I.status = (uint32_t*)base;
+  I.counters = (unsigned long long*)(base + 8);
+  // the kernels read prim[cur], aux[cur] + A_W * fstride and stage[qin] in
+  // the rhs-only mode; aux is placed so that its W slot is the caller's W
+  I.prim[0] = I.prim[1] = const_cast<double*>(prim);
+  I.aux[0] = I.aux[1] = (double*)((uintptr_t)W - (uintptr_t)A_W * (uintptr_t)fstride * sizeof(double));
+  I.stage[0] = I.stage[1] = const_cast<double*>(stage);
+  I.rhs_out = rhs;
+  I.fx = nullptr;
+  I.fy = (double*)(base + kNoallocHeader + kNoallocDesc);
+  I.fpitch = fpitch;
+  I.ffs = ffs;
+  I.imax = p->imax; I.jmax = p->jmax; I.pitch = pitch; I.fstride = fstride;
+  I.bc_x = p->bc_x; I.bc_y = p->bc_y;
+  I.delx = p->lx / (double)p->imax;
+  I.dely = p->ly / (double)p->jmax;
+  I.sigma = p->sigma; I.gamma = p->gamma;
+  {
+    const double mn = (I.dely < I.delx) ? I.dely : I.delx;   // parameters.f95:329-334
+    const double cp = std::sqrt(mn / 1.0);
+    I.kappa_psi = 1.0 / (cp * cp);
+    I.kappa_phi = 1.0 / (cp * cp);
+    auto inv_pow2 = [](double d) {
+      int e = 0;
+      return (std::frexp(d, &e) == 0.5 && std::isnormal(1.0 / d)) ? 1.0 / d : 0.0;
+    };
+    I.inv_delx_pow2 = inv_pow2(I.delx);
+    I.inv_dely_pow2 = inv_pow2(I.dely);
+  }
+  I.c2p = 1;
+  I.block_begin[LK_XUPD] = I.block_begin[LK_YFACE] = 0;
+  I.block_count[LK_XUPD] = ((nx + 30) / 31) * ((ny + FACE_ROWS - 1) / FACE_ROWS);
+  I.block_count[LK_YFACE] = ((nx + 31) / 32) * ((ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
+  const int nb[2] = {I.block_count[LK_XUPD], I.block_count[LK_YFACE]};
+  InstDesc* d_inst = (InstDesc*)(base + kNoallocHeader);
+  CUDA_TRY(cudaMemsetAsync(base, 0, kNoallocHeader, st));
+  CUDA_TRY(cudaMemcpyAsync(d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice, st));
+  StageArgs sa{};
+  sa.l = 1; sa.s = 1; sa.cur = 0; sa.qin = 0; sa.mode = 1;
+  for (int m = 0; m < 8; ++m) sa.kslot[m] = -1;
+  sa.store_k_slot = -1;
+  CUDA_TRY(launch_stage(p->rec_mp, p->flux_solver, p->precision, nb, st, d_inst, 1, sa));
+  if (status_bits) {
+    uint32_t h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, base, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *status_bits = h;
+    if (h) {
+      char buf[64];
+      snprintf(buf, sizeof buf, "kernel status 0x%x", h);
+      return fail(CUEVA_ERR_PHYSICS, buf);
+    }
+  }
+  return CUEVA_OK;
+}
+
 }  // extern "C"

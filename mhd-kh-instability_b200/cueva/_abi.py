@@ -27,7 +27,7 @@ PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS)
 EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
            "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
            "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
-           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps"]
+           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc"]
 
 
 class Params(ctypes.Structure):
@@ -83,6 +83,8 @@ def load(fma=False):
     L.cueva_con2prim.argtypes = [vp]
     L.cueva_kh_init.argtypes = [vp] + [dbl] * 9
     L.cueva_profile_steps.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(i32)]
+    L.cueva_flux_rhs_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp, vp, i32, ctypes.c_int64, vp,
+                                         ctypes.POINTER(u32)]
     _LIBS[key] = L
     return L
 
