@@ -174,6 +174,86 @@ def run_reference(args, cfg):
     return 0
 
 
+PRIM_NAMES = ["rho", "p", "vx", "vy", "vz", "psi", "phi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "q"]
+
+
+def vector_rel_l1(run, ref):
+    """Per-component L1 difference relative to the L1 norm of the whole
+    vector (|v|, |E|, |B|); components that are zero in the 2D problem, or
+    small against their vector, are then measured against the physics."""
+    import numpy as np
+    groups = {"v": ("vx", "vy", "vz"), "E": ("Ex", "Ey", "Ez"), "B": ("Bx", "By", "Bz")}
+    out = {}
+    for comps in groups.values():
+        den = max(float(sum(np.abs(ref[c]).sum() for c in comps)), 1e-300)
+        for c in comps:
+            out[c] = float(np.abs(run.interior(c) - ref[c]).sum()) / den
+    return out
+
+
+def mixed_study(args):
+    """Mixed precision (FP32 reconstruction + Riemann, FP64 update, implicit
+    E and con2prim) against plain FP64 on the 2048x4096 V0 = 0.8, sigma = 1e5
+    workload, MP7 and MP9: per-variable relative L1 after 1, 100 and 1000
+    steps, and the step time of both forms."""
+    import dataclasses
+    import torch
+    from cueva import Cueva
+    from cueva.configs import C3
+    from cueva.metrics import rel_l1_field
+    checkpoints = [int(c) for c in args.study_steps.split(",")]
+    cfg = C3
+    if args.grid:
+        nx, ny = (int(v) for v in args.grid.lower().split("x"))
+        cfg = dataclasses.replace(C3, nx=nx, ny=ny, name=C3.name.replace("2048x4096", f"{nx}x{ny}"))
+    out = {"study": "mixed precision vs plain FP64", "workload": cfg.name, "nx": cfg.nx, "ny": cfg.ny,
+           "checkpoints": checkpoints, "variants": {}}
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    for rec, label in ((1, "MP7"), (2, "MP9")):
+        runs = {}
+        for prec in (0, 1):
+            g = Cueva(pinned=False, **dict(cfg.solver_kwargs(), rec_mp=rec, precision=prec))
+            g.set_stream(stream.cuda_stream)
+            g.kh_init(**cfg.kh_kwargs())
+            g.upload()
+            runs[prec] = g
+        # step time of each form (after a few warm-up steps on a copy of the state)
+        times = {}
+        for prec, g in runs.items():
+            g.step(3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.step(10)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[prec] = e0.elapsed_time(e1) / 10
+            g.kh_init(**cfg.kh_kwargs())
+            g.upload()
+        errs, done, breakdown = {}, 0, None
+        from cueva import CuevaError
+        for cp in checkpoints:
+            try:
+                for g in runs.values():
+                    g.step(cp - done)
+                    g.download()
+            except CuevaError as e:
+                breakdown = {"before_step": cp, "error": str(e)}
+                break
+            done = cp
+            ref = {n: runs[0].interior(n).copy() for n in PRIM_NAMES}
+            errs[str(cp)] = {n: rel_l1_field(n, runs[1].interior(n), ref[n], ref) for n in PRIM_NAMES}
+            errs[str(cp) + "_vector"] = vector_rel_l1(runs[1], ref)
+        out["variants"][label] = {"ms_per_step_fp64": times[0], "ms_per_step_mixed": times[1],
+                                  "zone_updates_per_s_fp64": cfg.nx * cfg.ny / (times[0] * 1e-3),
+                                  "zone_updates_per_s_mixed": cfg.nx * cfg.ny / (times[1] * 1e-3),
+                                  "rel_l1_mixed_vs_fp64": errs, "breakdown": breakdown}
+        for g in runs.values():
+            g.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,6 +265,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--grid", default=None, help="NXxNY override of the workload grid (profiling a small case)")
+    ap.add_argument("--mixed-study", action="store_true",
+                    help="per-variable error and speed of mixed precision vs FP64 (2048x4096, MP7/MP9)")
+    ap.add_argument("--study-steps", default="1,100,150,1000")
     args = ap.parse_args()
 
     from cueva.configs import C2
@@ -195,6 +278,8 @@ def main():
         cfg = dataclasses.replace(C2, nx=nx, ny=ny, name=C2.name.replace("1024x2048", f"{nx}x{ny}"))
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.mixed_study:
+        return mixed_study(args)
 
     import numpy as np
     import torch

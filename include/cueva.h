@@ -38,6 +38,7 @@ extern "C" {
 #define CUEVA_ST_SUPERLUMINAL 2u    /* 12_varprimitive.f95:678,691; 12_varprimitive_nr.f95:217 */
 #define CUEVA_ST_HLLC_NOCONV 4u     /* funciones.f95:240-245 */
 #define CUEVA_ST_HLLC_VSTAR 8u      /* 16_hllc_flow_mpx.f95:4294,4605 */
+#define CUEVA_ST_NONFINITE 16u      /* con2prim returned NaN/Inf (the reference continues silently) */
 
 typedef struct cueva_ctx cueva_ctx;
 

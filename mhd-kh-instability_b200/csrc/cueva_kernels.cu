@@ -139,10 +139,15 @@ __global__ void k_electricvarint(const InstDesc* __restrict__ insts, int cur, in
 
 // con2prim with l_swap = 1: the evolved D, tau, S in aux[cur] and E, B in
 // prim[cur]; seeds v, rho, p are the prims in prim[cur]; result overwrites prim[cur]
+// The reference lets NaN states pass silently (its comparisons are false on
+// NaN); a non-finite recovered state is reported as ST_NONFINITE here.
 __device__ __forceinline__ uint32_t c2p_dispatch(const InstDesc& I, const C2PIn& in, C2POut& o) {
-  if (I.c2p == 1) return c2p_cardano(in, I.gamma, I.eps1_c2p, o, I.counters);
-  if (I.c2p == 0) return c2p_nr(in, I.gamma, o);
-  return c2p_learned(in, I.gamma, I.eps1_c2p, I.mlp, o, I.counters);
+  uint32_t st;
+  if (I.c2p == 1) st = c2p_cardano(in, I.gamma, I.eps1_c2p, o, I.counters);
+  else if (I.c2p == 0) st = c2p_nr(in, I.gamma, o);
+  else st = c2p_learned(in, I.gamma, I.eps1_c2p, I.mlp, o, I.counters);
+  if (!(isfinite(o.rho) && isfinite(o.p) && isfinite(o.vx) && isfinite(o.vy) && isfinite(o.vz))) st |= ST_NONFINITE;
+  return st;
 }
 
 __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {

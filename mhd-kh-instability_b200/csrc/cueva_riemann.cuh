@@ -125,8 +125,11 @@ __device__ __forceinline__ void hll_fluxes(const Side<T>& L, const Side<T>& R, T
 // get_hllc_vel, funciones.f95:188-259: Newton on a v^2 - b v + c = 0 in
 // [-1,1].  The Fortran's first f evaluation reads the local v before it is
 // assigned (line 229); this evaluates it at the seed oldv, like the oracle.
+// The reference's step tolerance 1e-12 is below FP32 resolution, so the FP32
+// (mixed-precision) instantiation stops at 4e-7, two ulps of |v| <= 1.
 template <typename T>
 __device__ __forceinline__ T hllc_vel(T a, T b, T c, T rt, uint32_t& st) {
+  const T tol = (sizeof(T) == sizeof(double)) ? T(1.0e-12) : T(4.0e-7);
   T oldv = fmax2(T(-1.0), fmin2(T(1.0), rt));
   T v = oldv;
   for (int iter = 1;; ++iter) {
@@ -136,7 +139,7 @@ __device__ __forceinline__ T hllc_vel(T a, T b, T c, T rt, uint32_t& st) {
     const T err = fabs(oldv - v);
     oldv = v;
     if (iter >= 100) { st |= ST_HLLC_NOCONV; break; }
-    if (!(err > T(1.0e-12))) break;
+    if (!(err > tol)) break;
   }
   return fmax2(T(-1.0) + T(1.0e-3), fmin2(T(1.0) - T(1.0e-3), v));
 }

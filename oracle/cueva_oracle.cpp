@@ -1342,6 +1342,10 @@ struct Oracle {
         C2POut o;
         int64_t cnt[3] = {0, 0, 0};
         int32_t st = (P.c2p == 1) ? c2p_cardano(in, gamma, eps1_c2p, o, cnt) : c2p_nr(in, gamma, o);
+        // NaN states pass the reference's checks silently; report them
+        if (!(std::isfinite(o.rho) && std::isfinite(o.p) && std::isfinite(o.vx) && std::isfinite(o.vy) &&
+              std::isfinite(o.vz)))
+          st |= ST_NONFINITE;
         st_acc |= st;
         c0 += cnt[0]; c1 += cnt[1]; c2 += cnt[2];
         Vx[k] = o.vx; Vy[k] = o.vy; Vz[k] = o.vz; rho[k] = o.rho; p[k] = o.p; W[k] = o.W;
