@@ -143,6 +143,53 @@ int32_t cueva_flux_rhs(cueva_ctx* ctx, int32_t l);
  * the seeds V, rho, p -> V, rho, p */
 int32_t cueva_con2prim(cueva_ctx* ctx);
 
+/* ---- learned con2prim seed (c2p = 2) ---------------------------------- */
+/* No counterpart in the reference.  A 6 -> 64 -> 64 -> 64 -> 1 SiLU network
+ * (bf16 weights, FP32 accumulation) predicts log p from the conserved state;
+ * a Newton-Raphson solve of the ideal-gas pressure equation refines it to a
+ * relative step of 1e-12, and the Cardano recovery (12_varprimitive.f95) is
+ * the fall-back whenever the refinement fails.  Training runs on the GPU with
+ * the library's own forward/backward kernels (minibatch Adam).
+ * Conserved arrays (d_cons) are device SoA blocks of 11 x n doubles:
+ * D, tau, Sx, Sy, Sz, Ex, Ey, Ez, Bx, By, Bz; primitive arrays 5 x n:
+ * rho, p, vx, vy, vz. */
+typedef struct cueva_mlp cueva_mlp;
+#define CUEVA_MLP_NPARAM 8833   /* W1[64][6] b1 W2[64][64] b2 W3[64][64] b3 W4[64] b4 */
+#define CUEVA_MLP_NNORM 14      /* feature mean[6], sd[6], target mean, sd */
+int32_t cueva_mlp_create(int32_t device, uint64_t seed, cueva_mlp** out);
+int32_t cueva_mlp_destroy(cueva_mlp* mlp);
+/* n = CUEVA_MLP_NPARAM + CUEVA_MLP_NNORM floats: parameters then normalisation */
+int32_t cueva_mlp_get_params(cueva_mlp* mlp, float* host, int32_t n);
+int32_t cueva_mlp_set_params(cueva_mlp* mlp, const float* host, int32_t n);
+/* n synthetic states (seeded, counter-based): rho log-uniform [1e-3,10],
+ * p log-uniform [1e-4,10], W uniform [1,20], |B|^2/(rho h) log-uniform
+ * [1e-3,10], isotropic v and B, E = -v x B + N(0,1e-3) */
+int32_t cueva_mlp_synthetic_pairs(int32_t device, int64_t n, uint64_t seed, double gamma, double* d_cons,
+                                  double* d_prims, void* stream);
+/* feature / target mean and deviation over a training set (d_p: n pressures) */
+int32_t cueva_mlp_fit_normalisation(cueva_mlp* mlp, const double* d_cons, const double* d_p, int64_t n);
+/* `steps` Adam steps on minibatches of `batch` rows drawn with replacement,
+ * cosine-decayed learning rate from lr; loss_out = last batch's MSE */
+int32_t cueva_mlp_train(cueva_mlp* mlp, const double* d_cons, const double* d_p, int64_t n, int32_t steps,
+                        int32_t batch, float lr, uint64_t seed, float* loss_out);
+/* loss and gradient (CUEVA_MLP_NPARAM floats, host) of the MSE over the first
+ * n rows, for checking the backward kernels */
+int32_t cueva_mlp_gradients(cueva_mlp* mlp, const double* d_cons, const double* d_p, int32_t n, float* grads,
+                            float* loss_out);
+/* network pressure seeds of n states (device out) */
+int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed);
+/* batch con2prim for comparisons: method 1 Cardano, 2 network seed + Newton,
+ * 3 Newton from d_seed; d_prev (5 x n) are the previous primitives the
+ * Cardano path seeds from; d_iters (optional) gets the Newton iterations
+ * (-1 = failed, then the Cardano result is stored; 0 for method 1) */
+int32_t cueva_c2p_batch(int32_t device, int32_t method, const cueva_mlp* mlp, double gamma, double eps1,
+                        const double* d_cons, const double* d_prev, const double* d_seed, int64_t n, double* d_out,
+                        int32_t* d_iters);
+/* copy a trained network into ctx; con2prim uses it when params.c2p == 2 */
+int32_t cueva_attach_mlp(cueva_ctx* ctx, const cueva_mlp* mlp);
+/* Newton iterations, points and Cardano fall-backs of the learned path so far */
+int32_t cueva_learned_stats(cueva_ctx* ctx, int64_t out3[3]);
+
 /* ---- stage right-hand side without any device allocation -------------- */
 /* No counterpart in the reference.  Computes the same stage right-hand side
  * as cueva_flux_rhs ({hll,hllc}_flow_mpx 2D + fluxandsource), but on device

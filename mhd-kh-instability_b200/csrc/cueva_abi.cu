@@ -11,6 +11,7 @@
 #include "../../include/cueva.h"
 #include "cueva_common.cuh"
 #include "cueva_launch.h"
+#include "cueva_mlp.cuh"
 
 using namespace cueva;
 
@@ -22,6 +23,12 @@ int32_t fail(int32_t code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+}  // namespace
+
+int32_t cueva_fail(int32_t code, const std::string& msg) { return fail(code, msg); }
+
+namespace {
+
 #define CUDA_TRY(x)                                                                          \
   do {                                                                                       \
     cudaError_t e_ = (x);                                                                    \
@@ -134,6 +141,8 @@ struct cueva_ctx {
   bool primed = false;
   double* bound[CUEVA_NFIELDS] = {};
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  MLPDevice* d_mlp = nullptr;                 // attached learned seed (c2p = 2)
+  unsigned long long* d_mlp_stats = nullptr;  // Newton iterations, points, fall-backs
 };
 
 namespace {
@@ -345,6 +354,8 @@ int32_t cueva_ctx_destroy(cueva_ctx* c) {
   if (c->d_status) cudaFree(c->d_status);
   if (c->d_counters) cudaFree(c->d_counters);
   if (c->d_inst) cudaFree(c->d_inst);
+  if (c->d_mlp) cudaFree(c->d_mlp);
+  if (c->d_mlp_stats) cudaFree(c->d_mlp_stats);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return CUEVA_OK;
@@ -567,6 +578,39 @@ int32_t cueva_con2prim(cueva_ctx* c) {
   for (int f : {P_RHO, P_P, P_VX, P_VY, P_VZ})
     if (int32_t e = d2h(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
   return read_status(c);
+}
+
+// ------------------------------------------------------- learned c2p seed
+int32_t cueva_attach_mlp(cueva_ctx* c, const cueva_mlp* mlp) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!mlp) return fail(CUEVA_ERR_ARG, "null network");
+  if (mlp_device_of(mlp) != c->dev) return fail(CUEVA_ERR_ARG, "network and context live on different devices");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  MLPDevice h;
+  if (int32_t e = mlp_device_image(mlp, &h)) return e;
+  if (!c->d_mlp) {
+    CUDA_TRY(cudaMalloc(&c->d_mlp, sizeof(MLPDevice)));
+    CUDA_TRY(cudaMalloc(&c->d_mlp_stats, 3 * sizeof(unsigned long long)));
+  }
+  h.stats = c->d_mlp_stats;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CUDA_TRY(cudaMemcpy(c->d_mlp, &h, sizeof(MLPDevice), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemset(c->d_mlp_stats, 0, 3 * sizeof(unsigned long long)));
+  c->h_inst.mlp = c->d_mlp;
+  CUDA_TRY(cudaMemcpy(c->d_inst, &c->h_inst, sizeof(InstDesc), cudaMemcpyHostToDevice));
+  return CUEVA_OK;
+}
+
+int32_t cueva_learned_stats(cueva_ctx* c, int64_t out3[3]) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!out3) return fail(CUEVA_ERR_ARG, "null argument");
+  unsigned long long h[3] = {0, 0, 0};
+  if (c->d_mlp_stats) {
+    CUDA_TRY(cudaMemcpyAsync(h, c->d_mlp_stats, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
+  return CUEVA_OK;
 }
 
 // --------------------------------------------------------------- KH input

@@ -1,9 +1,19 @@
 // cueva_launch.h -- host-side launchers of the kernels in cueva_kernels.cu
 #pragma once
 #include <cuda_runtime.h>
+#include <string>
 #include "cueva_common.cuh"
 
+struct cueva_mlp;
+
+// records msg as the thread's last error and returns code (cueva_last_error)
+int32_t cueva_fail(int32_t code, const std::string& msg);
+
 namespace cueva {
+struct MLPDevice;
+// the network in the layout the kernels read (host copy), and its device
+int32_t mlp_device_image(const cueva_mlp* M, MLPDevice* out);
+int mlp_device_of(const cueva_mlp* M);
 // sets the shared-memory limits of the stage kernels (call once per device
 // before the first launch or capture)
 cudaError_t prepare_stage(int rec_mp, int solver, int prec);

@@ -27,7 +27,11 @@ PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS)
 EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
            "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
            "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
-           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc"]
+           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
+           "cueva_mlp_destroy", "cueva_mlp_get_params", "cueva_mlp_set_params", "cueva_mlp_synthetic_pairs",
+           "cueva_mlp_fit_normalisation", "cueva_mlp_train", "cueva_mlp_gradients", "cueva_mlp_predict",
+           "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats"]
+MLP_NPARAM, MLP_NNORM = 8833, 14
 
 
 class Params(ctypes.Structure):
@@ -83,6 +87,19 @@ def load(fma=False):
     L.cueva_con2prim.argtypes = [vp]
     L.cueva_kh_init.argtypes = [vp] + [dbl] * 9
     L.cueva_profile_steps.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(i32)]
+    i64, u64, f32p = ctypes.c_int64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)
+    L.cueva_mlp_create.argtypes = [i32, u64, ctypes.POINTER(vp)]
+    L.cueva_mlp_destroy.argtypes = [vp]
+    L.cueva_mlp_get_params.argtypes = [vp, f32p, i32]
+    L.cueva_mlp_set_params.argtypes = [vp, f32p, i32]
+    L.cueva_mlp_synthetic_pairs.argtypes = [i32, i64, u64, dbl, vp, vp, vp]
+    L.cueva_mlp_fit_normalisation.argtypes = [vp, vp, vp, i64]
+    L.cueva_mlp_train.argtypes = [vp, vp, vp, i64, i32, i32, ctypes.c_float, u64, f32p]
+    L.cueva_mlp_gradients.argtypes = [vp, vp, vp, i32, f32p, f32p]
+    L.cueva_mlp_predict.argtypes = [vp, vp, i64, vp]
+    L.cueva_c2p_batch.argtypes = [i32, i32, vp, dbl, dbl, vp, vp, vp, i64, vp, vp]
+    L.cueva_attach_mlp.argtypes = [vp, vp]
+    L.cueva_learned_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.cueva_flux_rhs_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp, vp, i32, ctypes.c_int64, vp,
                                          ctypes.POINTER(u32)]
     _LIBS[key] = L
