@@ -254,6 +254,51 @@ def mixed_study(args):
     return 0
 
 
+def run_mixed_learned(args, cfg, stream, g, device, world, pg):
+    """FP32 reconstruction + Riemann with the learned con2prim seed (c2p = 2)
+    over the same warm-up + timed steps from the same initial state as the
+    FP64 run; its throughput and its per-variable error against that run."""
+    import torch
+    from cueva import Cueva
+    from cueva.learned import LearnedSeed, learned_stats
+    from cueva.metrics import rel_l1_field
+    from cueva.train_seed import DEFAULT
+    if not os.path.exists(DEFAULT):
+        return {"unavailable": "no trained seed network: run python -m cueva.train_seed"}
+    g.download()
+    ref = {n: g.interior(n).copy() for n in PRIM_NAMES}
+    m = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=1, c2p=2))
+    m.set_stream(stream.cuda_stream)
+    m.kh_init(**cfg.kh_kwargs())
+    m.upload()
+    net = LearnedSeed(device=device)
+    net.load(DEFAULT)
+    net.attach(m)
+    m.step(max(args.warmup, 3))
+    m.sync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    m.download()
+    errs = {n: rel_l1_field(n, m.interior(n), ref[n], ref) for n in PRIM_NAMES}
+    its, pts, fails = learned_stats(m)
+    m.close()
+    net.close()
+    return {"value": world * cfg.nx * cfg.ny * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "dtype": "f32 reconstruction + Riemann, f64 update / implicit E / con2prim",
+            "error_vs_fp64_after_steps": max(args.warmup, 3) + args.steps,
+            "rel_l1_vs_fp64": errs, "max_rel_l1_vs_fp64": max(errs.values()),
+            "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -261,10 +306,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed")
+    ap.add_argument("--c2p", type=int, default=1, help="1 Cardano (reference), 0 NR, 2 learned seed + Newton")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--grid", default=None, help="NXxNY override of the workload grid (profiling a small case)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed + learned-seed measurement")
     ap.add_argument("--mixed-study", action="store_true",
                     help="per-variable error and speed of mixed precision vs FP64 (2048x4096, MP7/MP9)")
     ap.add_argument("--study-steps", default="1,100,150,1000")
@@ -293,7 +340,13 @@ def main():
         pg = dist
     from cueva import Cueva
 
-    g = Cueva(device=local, pinned=True, **dict(cfg.solver_kwargs(), precision=args.precision))
+    g = Cueva(device=local, pinned=True, **dict(cfg.solver_kwargs(), precision=args.precision, c2p=args.c2p))
+    if args.c2p == 2:
+        from cueva.learned import LearnedSeed
+        from cueva.train_seed import DEFAULT
+        seed_net = LearnedSeed(device=local)
+        seed_net.load(DEFAULT)
+        seed_net.attach(g)
     # a dedicated (non-default) stream shared by the library and the CUDA events
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
@@ -328,6 +381,9 @@ def main():
     zones = cfg.nx * cfg.ny
     value = world * zones * args.steps / (ms_max * 1e-3)
     ms_per_step = ms_max / args.steps
+
+    # the mixed-precision + learned-seed form on the same workload and steps
+    mixed = None if args.no_mixed else run_mixed_learned(args, cfg, stream, g, local, world, pg)
 
     # end to end through the C-ABI with host buffers
     barrier()
@@ -385,7 +441,7 @@ def main():
                          "kernel": KERNELS[top], "kernels": kernels,
                          "note": f"{KERNELS[top]}: {bpu[top]:.0f} algorithmic B per unit x {units[top]} units "
                                  f"per launch / avg launch {kernels[KERNELS[top]]['avg_ms']:.3f} ms"},
-            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 2 * s * args.steps}
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 2 * s * args.steps, "mixed_learned": mixed}
     if rank == 0 and not args.no_cpu_baseline:
         r, cores, sample = cpu_port_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

@@ -176,8 +176,10 @@ int32_t cueva_mlp_train(cueva_mlp* mlp, const double* d_cons, const double* d_p,
  * n rows, for checking the backward kernels */
 int32_t cueva_mlp_gradients(cueva_mlp* mlp, const double* d_cons, const double* d_p, int32_t n, float* grads,
                             float* loss_out);
-/* network pressure seeds of n states (device out) */
-int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed);
+/* network pressure seeds of n states (device out): per thread in FP32
+ * (tensor_cores = 0) or warp-cooperative with bf16 tensor-core MMA and bf16
+ * activations (1, the form the fused step uses) */
+int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed, int32_t tensor_cores);
 /* batch con2prim for comparisons: method 1 Cardano, 2 network seed + Newton,
  * 3 Newton from d_seed; d_prev (5 x n) are the previous primitives the
  * Cardano path seeds from; d_iters (optional) gets the Newton iterations

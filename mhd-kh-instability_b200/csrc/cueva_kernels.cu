@@ -141,11 +141,14 @@ __global__ void k_electricvarint(const InstDesc* __restrict__ insts, int cur, in
 // prim[cur]; seeds v, rho, p are the prims in prim[cur]; result overwrites prim[cur]
 // The reference lets NaN states pass silently (its comparisons are false on
 // NaN); a non-finite recovered state is reported as ST_NONFINITE here.
-__device__ __forceinline__ uint32_t c2p_dispatch(const InstDesc& I, const C2PIn& in, C2POut& o) {
+// count == false: a lane that only keeps its warp converged (no counters);
+// full_warp: all 32 lanes of the warp make this call
+__device__ __forceinline__ uint32_t c2p_dispatch(const InstDesc& I, const C2PIn& in, C2POut& o, bool count = true,
+                                                 bool full_warp = false) {
   uint32_t st;
-  if (I.c2p == 1) st = c2p_cardano(in, I.gamma, I.eps1_c2p, o, I.counters);
+  if (I.c2p == 1) st = c2p_cardano(in, I.gamma, I.eps1_c2p, o, count ? I.counters : nullptr);
   else if (I.c2p == 0) st = c2p_nr(in, I.gamma, o);
-  else st = c2p_learned(in, I.gamma, I.eps1_c2p, I.mlp, o, I.counters);
+  else st = c2p_learned(in, I.gamma, I.eps1_c2p, I.mlp, o, I.counters, count, full_warp);
   if (!(isfinite(o.rho) && isfinite(o.p) && isfinite(o.vx) && isfinite(o.vy) && isfinite(o.vz))) st |= ST_NONFINITE;
   return st;
 }
@@ -426,9 +429,11 @@ struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
 
 // flux divergence + sources of point (i, j) (17_fluxandsource.f95:441-635)
 // and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
+// valid == false (EP_LAST only): the lane computes a copy of a real point so
+// that its warp reaches con2prim converged, and stores nothing
 template <int EP>
 __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
-                                                 const double (&qx)[NROLE], const Centre& cv) {
+                                                 const double (&qx)[NROLE], const Centre& cv, bool valid = true) {
   const int pitch = I.pitch;
   const long long fs = I.fstride;
   const double* __restrict__ prim = I.prim[sa.cur];
@@ -539,7 +544,8 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
       C2PIn in{Un[Q_D], Un[Q_TAU], Un[Q_SX], Un[Q_SY], Un[Q_SZ], Un[Q_EX], Un[Q_EY], Un[Q_EZ],
                Un[Q_BX], Un[Q_BY], Un[Q_BZ], vx, vy, vz, prim[P_RHO * fs + pc], prim[P_P * fs + pc]};
       C2POut o;
-      st |= c2p_dispatch(I, in, o);
+      st |= c2p_dispatch(I, in, o, valid, I.c2p == 2);   // k_xupd sends whole warps for c2p = 2
+      if (!valid) return 0u;
       double pv[NPRIM];
       pv[P_RHO] = o.rho; pv[P_P] = o.p; pv[P_VX] = o.vx; pv[P_VY] = o.vy; pv[P_VZ] = o.vz;
       pv[P_PSI] = Un[Q_PSI]; pv[P_PHI] = Un[Q_PHI];
@@ -623,12 +629,22 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
     const double d = fr - fl;
     qx[c] = ix2 != 0.0 ? d * ix2 : d / dlx;
   }
-  if (lane >= 1 && i <= ilast) {
-    // centre values: staged cell i is stencil point R of this lane's face
-    auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + lane + R]; };
+  const bool valid = lane >= 1 && i <= ilast;
+  // after the last stage every lane of the warp enters the update (lanes
+  // without a point repeat a real one and store nothing), so con2prim runs
+  // converged; earlier stages update the real points only
+  if (valid || (EP == EP_LAST && I.c2p == 2)) {
+    const int ii = valid ? i : (lane == 0 ? i0 + 1 : ilast);
+    const int ln = ii - i0;   // staged cell ii is stencil point R of lane ln's face
+    if (EP == EP_LAST && I.c2p == 2) {
+      // a lane without a point takes the divergence of the point it repeats
+#pragma unroll
+      for (int c = 0; c < NROLE; ++c) qx[c] = __shfl_sync(0xffffffffu, qx[c], ln);
+    }
+    auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + ln + R]; };
     const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
                     cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
-    stt |= update_point<EP>(I, sa, i, j, qx, cv);
+    stt |= update_point<EP>(I, sa, ii, j, qx, cv, valid);
   }
   if (stt) atomicOr(I.status, stt);
 }

@@ -54,10 +54,13 @@ struct MLPDevice {
   unsigned long long* stats;   // [0] Newton iterations, [1] points, [2] Cardano fall-backs
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU with the fast exponential and division (the network is defined by
+// this form; training and inference share it)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+__device__ __forceinline__ float sigmoid_fast(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 
-// raw (unnormalised) features of a conserved state (double arithmetic for
-// the cancellations, rounded to float at the end)
+// raw (unnormalised) features of a conserved state: the cancellations
+// (Ef, |Sf|, M, M/D - 1) in double, the logarithms in float
 __device__ __forceinline__ void c2p_features(double D, double tau, double Sx, double Sy, double Sz, double Ex,
                                              double Ey, double Ez, double Bx, double By, double Bz, float f[MLP_IN]) {
   const double S2 = Sx * Sx + Sy * Sy + Sz * Sz, B2 = Bx * Bx + By * By + Bz * Bz;
@@ -66,13 +69,13 @@ __device__ __forceinline__ void c2p_features(double D, double tau, double Sx, do
   const double sfm = sqrt(Sfx * Sfx + Sfy * Sfy + Sfz * Sfz);
   const double Ef = tau - 0.5 * (E2 + B2);
   const double M = sqrt(fmax((Ef - sfm) * (Ef + sfm), 0.0));
-  const double den = sqrt(S2 * B2);
-  f[0] = (float)log(D);
-  f[1] = (float)fmin(log(Ef / fmax(M, 1.0e-300)), 10.0);
-  f[2] = (float)log(fmax(M / D - 1.0, 1.0e-9));
-  f[3] = (float)log1p(B2 / D);
-  f[4] = (float)log1p(E2 / D);
-  f[5] = den > 0.0 ? (float)(SB / den) : 0.0f;
+  const float den = (float)(S2 * B2);
+  f[0] = logf((float)D);
+  f[1] = fminf(logf((float)(Ef / fmax(M, 1.0e-300))), 10.0f);
+  f[2] = logf((float)fmax(M / D - 1.0, 1.0e-9));
+  f[3] = log1pf((float)(B2 / D));
+  f[4] = log1pf((float)(E2 / D));
+  f[5] = den > 0.0f ? (float)SB * rsqrtf(den) : 0.0f;
 }
 
 // normalised log(p/D) predicted for one state (one thread, FP32 FMA)
@@ -113,7 +116,101 @@ __device__ __forceinline__ double mlp_pressure_seed(const MLPDevice& M, const C2
   float f[MLP_IN];
   c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
   const float y = mlp_forward(M, f) * M.sd_y + M.mu_y;
-  return in.D * exp((double)y);
+  return in.D * (double)__expf(y);
+}
+
+// ---- warp-cooperative inference on the tensor cores ------------------------
+// A converged warp evaluates the network for its 32 states with
+// mma.sync.m16n8k16 (bf16 in, FP32 accumulate): two 16-row tiles, 8
+// column tiles of 8 outputs per layer.  The accumulator fragment of two
+// adjacent column tiles is exactly the A fragment of the next layer's
+// 16-wide k block, so activations stay in registers (rounded to bf16).
+// Fragment layout (PTX ISA, m16n8k16): g = lane / 4, t = lane % 4;
+// A regs {0,1,2,3} = rows {g, g+8, g, g+8} x k pairs {2t, 2t, 2t+8, 2t+8};
+// B regs {0,1} = k pairs {2t, 2t+8} of column g; C = rows {g, g, g+8, g+8} x
+// columns {2t, 2t+1, 2t, 2t+1}.
+__device__ __forceinline__ unsigned pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const unsigned*>(&v);
+}
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ unsigned ld_pair(const __nv_bfloat16* p) { return *reinterpret_cast<const unsigned*>(p); }
+
+// hidden layer of one 16-row tile: out = silu(in W^T + b), K = 16 * KB
+template <int KB>
+__device__ __forceinline__ void warp_dense_silu(const unsigned (&ain)[KB][4], const __nv_bfloat16* W, const float* b,
+                                                int g, int t, unsigned (&aout)[4][4]) {
+#pragma unroll
+  for (int jt = 0; jt < 8; ++jt) {
+    const float b0 = b[8 * jt + 2 * t], b1 = b[8 * jt + 2 * t + 1];
+    float c[4] = {b0, b1, b0, b1};
+    const __nv_bfloat16* wrow = W + (8 * jt + g) * (16 * KB);
+#pragma unroll
+    for (int kb = 0; kb < KB; ++kb)
+      mma_bf16_16816(c, ain[kb], ld_pair(wrow + 16 * kb + 2 * t), ld_pair(wrow + 16 * kb + 2 * t + 8));
+    aout[jt >> 1][(jt & 1) ? 2 : 0] = pack_bf16x2(silu(c[0]), silu(c[1]));
+    aout[jt >> 1][(jt & 1) ? 3 : 1] = pack_bf16x2(silu(c[2]), silu(c[3]));
+  }
+}
+
+// normalised log(p/D) of the lane's state; all 32 lanes must be active
+__device__ __forceinline__ float mlp_forward_warp(const MLPDevice& M, const float f[MLP_IN]) {
+  __syncwarp();
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float x[MLP_IN];
+#pragma unroll
+  for (int k = 0; k < MLP_IN; ++k) x[k] = (f[k] - M.mu[k]) / M.sd[k];
+  float mine = 0.0f;
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt) {
+    // layer 1: A = features of rows 16 mt + g and + 8 (k < 6, zero padded to 16)
+    float lo[MLP_IN], hi[MLP_IN];
+#pragma unroll
+    for (int k = 0; k < MLP_IN; ++k) {
+      lo[k] = __shfl_sync(0xffffffffu, x[k], 16 * mt + g);
+      hi[k] = __shfl_sync(0xffffffffu, x[k], 16 * mt + g + 8);
+    }
+    const float l0 = (t == 0) ? lo[0] : (t == 1) ? lo[2] : (t == 2) ? lo[4] : 0.0f;
+    const float l1 = (t == 0) ? lo[1] : (t == 1) ? lo[3] : (t == 2) ? lo[5] : 0.0f;
+    const float h0 = (t == 0) ? hi[0] : (t == 1) ? hi[2] : (t == 2) ? hi[4] : 0.0f;
+    const float h1 = (t == 0) ? hi[1] : (t == 1) ? hi[3] : (t == 2) ? hi[5] : 0.0f;
+    const unsigned a1[1][4] = {{pack_bf16x2(l0, l1), pack_bf16x2(h0, h1), 0u, 0u}};
+    unsigned act[4][4], act2[4][4];
+    {
+      // W1 is [64][6]: its B fragment holds k = 2t, 2t+1 for t < 3, zeros above
+#pragma unroll
+      for (int jt = 0; jt < 8; ++jt) {
+        const float b0 = M.b1[8 * jt + 2 * t], b1 = M.b1[8 * jt + 2 * t + 1];
+        float c[4] = {b0, b1, b0, b1};
+        const unsigned w0 = (t < 3) ? ld_pair(M.W1 + (8 * jt + g) * MLP_IN + 2 * t) : 0u;
+        mma_bf16_16816(c, a1[0], w0, 0u);
+        act[jt >> 1][(jt & 1) ? 2 : 0] = pack_bf16x2(silu(c[0]), silu(c[1]));
+        act[jt >> 1][(jt & 1) ? 3 : 1] = pack_bf16x2(silu(c[2]), silu(c[3]));
+      }
+    }
+    warp_dense_silu<4>(act, M.W2, M.b2, g, t, act2);
+    warp_dense_silu<4>(act2, M.W3, M.b3, g, t, act);
+    // output layer: column 0 of an 8-wide tile holds W4
+    float c[4] = {M.b4, 0.0f, M.b4, 0.0f};
+#pragma unroll
+    for (int kb = 0; kb < 4; ++kb) {
+      const unsigned w0 = (g == 0) ? ld_pair(M.W4 + 16 * kb + 2 * t) : 0u;
+      const unsigned w1 = (g == 0) ? ld_pair(M.W4 + 16 * kb + 2 * t + 8) : 0u;
+      mma_bf16_16816(c, act[kb], w0, w1);
+    }
+    // y of row r sits in lane 4 (r % 8), element c0 (r < 8) or c2 (r >= 8)
+    const int r = lane - 16 * mt;
+    const float ylo = __shfl_sync(0xffffffffu, c[0], 4 * (r & 7));
+    const float yhi = __shfl_sync(0xffffffffu, c[2], 4 * (r & 7));
+    if (lane / 16 == mt) mine = (r < 8) ? ylo : yhi;
+  }
+  return mine;
 }
 
 // Newton-Raphson on f(p) from the seed p; returns the iterations used, or
@@ -149,28 +246,43 @@ __device__ __forceinline__ int c2p_newton(const C2PIn& in, double gamma, double 
   return it;
 }
 
+// the Cardano recovery as a call (keeps the learned path's code small)
+static __device__ __noinline__ uint32_t c2p_cardano_ool(const C2PIn& in, double gamma, double eps1, C2POut& o,
+                                                        unsigned long long* cnt) {
+  return c2p_cardano(in, gamma, eps1, o, cnt);
+}
+
 // c2p method 2: network seed + Newton; Cardano when the refinement fails or
-// no network is attached.  Out of line, so the network's 128 live FP32
-// activations do not raise the register allocation of the kernels that
-// merely contain this call.
+// no network is attached.  A converged warp runs the network on the tensor
+// cores; a partial warp evaluates it per thread.  Lanes with count == false
+// take part in the warp's network evaluation but not in the statistics or
+// the fix-up counters.  Out of line, so the network's registers do not
+// raise the allocation of the kernels that merely contain this call.
 static __device__ __noinline__ uint32_t c2p_learned(const C2PIn& in, double gamma, double eps1, const void* mlp,
-                                                C2POut& o, unsigned long long* cnt) {
-  if (!mlp) return c2p_cardano(in, gamma, eps1, o, cnt);
+                                                    C2POut& o, unsigned long long* cnt, bool count, bool full_warp) {
+  if (!mlp) return c2p_cardano(in, gamma, eps1, o, count ? cnt : nullptr);
   const MLPDevice& M = *static_cast<const MLPDevice*>(mlp);
-  const int it = c2p_newton(in, gamma, mlp_pressure_seed(M, in), o);
+  float f[MLP_IN];
+  c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
+  // full_warp: the caller guarantees that all 32 lanes make this call
+  if (full_warp) __syncwarp();
+  const unsigned mask = full_warp ? 0xffffffffu : __activemask();
+  const float yn = (mask == 0xffffffffu) ? mlp_forward_warp(M, f) : mlp_forward(M, f);
+  const double seed = in.D * (double)__expf(yn * M.sd_y + M.mu_y);
+  const int it = c2p_newton(in, gamma, seed, o);
   if (M.stats) {
     // one atomic per warp and counter
-    const unsigned mask = __activemask();
-    const unsigned its = __reduce_add_sync(mask, (unsigned)(it > 0 ? it : MLP_NR_MAXIT));
-    const unsigned nfail = __reduce_add_sync(mask, it > 0 ? 0u : 1u);
+    const unsigned its = __reduce_add_sync(mask, count ? (unsigned)(it > 0 ? it : MLP_NR_MAXIT) : 0u);
+    const unsigned pts = __reduce_add_sync(mask, count ? 1u : 0u);
+    const unsigned nfail = __reduce_add_sync(mask, (count && it <= 0) ? 1u : 0u);
     if ((threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) {
       atomicAdd(&M.stats[0], (unsigned long long)its);
-      atomicAdd(&M.stats[1], (unsigned long long)__popc(mask));
+      atomicAdd(&M.stats[1], (unsigned long long)pts);
       if (nfail) atomicAdd(&M.stats[2], (unsigned long long)nfail);
     }
   }
   if (it > 0) return 0u;
-  return c2p_cardano(in, gamma, eps1, o, cnt);
+  return c2p_cardano_ool(in, gamma, eps1, o, count ? cnt : nullptr);
 }
 
 }  // namespace cueva

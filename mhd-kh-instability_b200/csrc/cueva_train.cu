@@ -185,7 +185,7 @@ __global__ void k_loss(int B, const float* Y, const float* T, float* dY, float* 
 // dZ = dA * silu'(Z)
 __global__ void k_silu_back(long long n, const float* dA, const float* Z, float* dZ) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float z = Z[i], s = 1.0f / (1.0f + __expf(-z));
+    const float z = Z[i], s = sigmoid_fast(z);
     dZ[i] = dA[i] * (s * (1.0f + z * (1.0f - s)));
   }
 }
@@ -247,12 +247,19 @@ __global__ void k_c2p_batch(long long n, int method, double gamma, double eps1, 
   }
 }
 
-__global__ void k_predict(long long n, const MLPDevice* M, const double* cons, double* pseed) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    C2PIn in{cons[i], cons[n + i], cons[2 * n + i], cons[3 * n + i], cons[4 * n + i], cons[5 * n + i],
-             cons[6 * n + i], cons[7 * n + i], cons[8 * n + i], cons[9 * n + i], cons[10 * n + i],
-             0, 0, 0, 0, 0};
-    pseed[i] = mlp_pressure_seed(*M, in);
+// network seeds: per thread in FP32 (tensor == 0), or warp-cooperative on
+// the tensor cores (tensor == 1; every warp runs full, lanes past n repeat
+// state n-1 and store nothing)
+__global__ void k_predict(long long n, const MLPDevice* M, const double* cons, double* pseed, int tensor) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long nround = (n + 31) / 32 * 32;
+  for (long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; i0 < nround; i0 += stride) {
+    const long long i = i0 < n ? i0 : n - 1;
+    float f[MLP_IN];
+    c2p_features(cons[i], cons[n + i], cons[2 * n + i], cons[3 * n + i], cons[4 * n + i], cons[5 * n + i],
+                 cons[6 * n + i], cons[7 * n + i], cons[8 * n + i], cons[9 * n + i], cons[10 * n + i], f);
+    const float y = tensor ? mlp_forward_warp(*M, f) : mlp_forward(*M, f);
+    if (i0 < n) pseed[i] = cons[i] * (double)__expf(y * M->sd_y + M->mu_y);
   }
 }
 
@@ -565,11 +572,12 @@ int32_t cueva_mlp_gradients(cueva_mlp* M, const double* d_cons, const double* d_
   return rc;
 }
 
-int32_t cueva_mlp_predict(cueva_mlp* M, const double* d_cons, int64_t n, double* d_pseed) {
+int32_t cueva_mlp_predict(cueva_mlp* M, const double* d_cons, int64_t n, double* d_pseed, int32_t tensor_cores) {
   if (!M || n <= 0 || !d_cons || !d_pseed) return cueva_fail(CUEVA_ERR_ARG, "bad arguments");
   if (!M->normed) return cueva_fail(CUEVA_ERR_ARG, "the network has no normalisation");
   TRY(cudaSetDevice(M->dev));
-  k_predict<<<grid_for(n), 256>>>(n, M->d_dev, d_cons, d_pseed);
+  // whole warps: the grid covers n rounded up to 32 in multiples of the block
+  k_predict<<<grid_for((n + 31) / 32 * 32), 256>>>(n, M->d_dev, d_cons, d_pseed, tensor_cores ? 1 : 0);
   TRY(cudaGetLastError());
   TRY(cudaDeviceSynchronize());
   return CUEVA_OK;

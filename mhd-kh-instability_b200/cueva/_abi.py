@@ -96,7 +96,7 @@ def load(fma=False):
     L.cueva_mlp_fit_normalisation.argtypes = [vp, vp, vp, i64]
     L.cueva_mlp_train.argtypes = [vp, vp, vp, i64, i32, i32, ctypes.c_float, u64, f32p]
     L.cueva_mlp_gradients.argtypes = [vp, vp, vp, i32, f32p, f32p]
-    L.cueva_mlp_predict.argtypes = [vp, vp, i64, vp]
+    L.cueva_mlp_predict.argtypes = [vp, vp, i64, vp, i32]
     L.cueva_c2p_batch.argtypes = [i32, i32, vp, dbl, dbl, vp, vp, vp, i64, vp, vp]
     L.cueva_attach_mlp.argtypes = [vp, vp]
     L.cueva_learned_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]

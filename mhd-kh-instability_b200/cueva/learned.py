@@ -95,11 +95,13 @@ class LearnedSeed:
         return g, loss.value
 
     # ------------------------------------------------------------- inference
-    def predict(self, cons):
+    def predict(self, cons, tensor_cores=True):
+        """Pressure seeds: warp-cooperative bf16 tensor-core inference (the
+        form the fused step uses) or per-thread FP32."""
         import torch
         n = cons.shape[1]
         out = torch.empty(n, dtype=torch.float64, device=cons.device)
-        _abi.check(self.L, self.L.cueva_mlp_predict(self.h, _ptr(cons), n, _ptr(out)))
+        _abi.check(self.L, self.L.cueva_mlp_predict(self.h, _ptr(cons), n, _ptr(out), 1 if tensor_cores else 0))
         return out
 
     def c2p(self, method, cons, prev, seed=None, gamma=4.0 / 3.0, eps1=1e-6):

@@ -53,8 +53,10 @@ def features(cons):
     Ef = tau - 0.5 * (E2 + B2)
     M = np.sqrt(np.maximum((Ef - sfm) * (Ef + sfm), 0.0))
     den = np.sqrt(S2 * B2)
-    f = np.stack([np.log(D), np.minimum(np.log(Ef / np.maximum(M, 1e-300)), 10.0),
-                  np.log(np.maximum(M / D - 1.0, 1e-9)), np.log1p(B2 / D), np.log1p(E2 / D),
+    f32 = np.float32
+    f = np.stack([np.log(D.astype(f32)), np.minimum(np.log((Ef / np.maximum(M, 1e-300)).astype(f32)), 10.0),
+                  np.log(np.maximum(M / D - 1.0, 1e-9).astype(f32)), np.log1p((B2 / D).astype(f32)),
+                  np.log1p((E2 / D).astype(f32)),
                   np.where(den > 0, SB / np.where(den > 0, den, 1.0), 0.0)], axis=1)
     return f.astype(np.float32).astype(np.float64)
 

@@ -139,3 +139,20 @@ def test_ablation_inside_a_run(trained):
           f"{b[b > 0].mean():.2f} iterations")
     assert (a > 0).all() and (b > 0).all()
     g.close()
+
+
+def test_tensor_core_inference_matches_fp32(trained):
+    """The warp-cooperative bf16 MMA forward (bf16 activations) against the
+    per-thread FP32 forward of the same network: seeds agree to the bf16
+    activation rounding, far inside what the Newton refinement absorbs."""
+    import torch
+    from cueva.learned import synthetic_pairs
+    net = trained[0]
+    cons, prims = synthetic_pairs(100_003, seed=555)     # not a multiple of 32: a partial last warp
+    a = net.predict(cons, tensor_cores=True)
+    b = net.predict(cons, tensor_cores=False)
+    d = (torch.log(a) - torch.log(b)).abs()
+    print(f"log-seed difference tensor cores vs FP32: median {float(d.median()):.2e}, max {float(d.max()):.2e}")
+    assert float(d.median()) < 2e-2 and float(d.max()) < 0.5
+    e = (torch.log(a) - torch.log(prims[1])).abs()
+    assert float(e.median()) < 0.1
