@@ -299,6 +299,102 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
             "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}
 
 
+ENS_METRIC = "ensemble zone-updates/s: 64 KH instances batched (mixed + learned C2P) vs sequential plain FP64"
+
+
+def run_ensemble(args):
+    """The batched-ensemble workload: 64 KH instances (seed 2024) in one
+    CUDA-graph step per ensemble step, launch shape picked by the autotuner;
+    mixed precision + learned con2prim seed, against the same 64 instances
+    run one after another in plain FP64 (and the batched FP64 form)."""
+    import torch
+    from cueva import Cueva
+    from cueva.ensemble import Ensemble, kh_ensemble
+    from cueva.learned import LearnedSeed
+    from cueva.metrics import rel_l1_field
+    from cueva.train_seed import DEFAULT
+    insts = kh_ensemble(args.ens_n, seed=2024)
+    common = dict(order=4, flux_solver=7, rec_mp=0, intsum_reset=1)
+    zones = sum(i.nx * i.ny for i in insts)
+    warm, K = max(args.warmup, 3), args.steps
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def timed_ensemble(precision, c2p):
+        ens = Ensemble([i.solver_kwargs(**common, precision=precision, c2p=c2p) for i in insts])
+        ens.set_stream(stream.cuda_stream)
+        net = None
+        if c2p == 2:
+            net = LearnedSeed()
+            net.load(DEFAULT)
+            ens.attach(net)
+        for k, i in enumerate(insts):
+            ens.kh_init(k, **i.kh_kwargs())
+        tune = ens.autotune()
+        ens.step(warm)
+        ens.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ens.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ens.sync()
+        return ens, net, ms, tune
+
+    mixed, net, ms_mixed, tune_mixed = timed_ensemble(1, 2)
+    its, pts, fails = mixed.learned_stats()
+    fp64, _, ms_fp64, tune_fp64 = timed_ensemble(0, 1)
+    errs = []
+    for k in range(len(insts)):
+        ref = fp64.get_prims(k)
+        got = mixed.get_prims(k)
+        errs.append(max(rel_l1_field(n, got[n], ref[n], ref) for n in ("rho", "p", "vx", "vy", "By", "Ez")))
+    mixed.close()
+    fp64.close()
+    if net is not None:
+        net.close()
+    # the same instances one after another, plain FP64, one context each
+    ms_seq = 0.0
+    for i in insts:
+        g = Cueva(**i.solver_kwargs(**common))
+        g.set_stream(stream.cuda_stream)
+        g.kh_init(**i.kh_kwargs())
+        g.upload()
+        g.step(warm)
+        g.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_seq += e0.elapsed_time(e1)
+        g.close()
+
+    def rate(ms):
+        return zones * K / (ms * 1e-3)
+
+    sizes = {}
+    for i in insts:
+        sizes[f"{i.nx}x{i.ny}"] = sizes.get(f"{i.nx}x{i.ny}", 0) + 1
+    line = {"metric": ENS_METRIC, "value": rate(ms_mixed), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": warm,
+            "ms_per_step": ms_mixed / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 reconstruction + Riemann, f64 update / implicit E / con2prim (learned seed)",
+            "data": "synthetic KH ensemble (seed 2024)",
+            "config": {"workload": f"kh-ensemble-{len(insts)}", "instances": len(insts), "zones": zones,
+                       "grids": sizes, "solver": "MP5+HLLC", "imex": "SSP3(4,3,3), stage sums reset per stage"},
+            "autotune": {"rows": tune_mixed[0], "ctas_per_sm": tune_mixed[1], "ms_per_step": tune_mixed[2]},
+            "batched_fp64": {"value": rate(ms_fp64), "ms_per_step": ms_fp64 / K,
+                             "autotune": {"rows": tune_fp64[0], "ctas_per_sm": tune_fp64[1]}},
+            "sequential_fp64": {"value": rate(ms_seq), "ms_per_step": ms_seq / K},
+            "speedup_vs_sequential_fp64": ms_seq / ms_mixed,
+            "rel_l1_mixed_vs_fp64": {"median": float(sorted(errs)[len(errs) // 2]), "max": float(max(errs)),
+                                     "after_steps": warm + K},
+            "learned": {"newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -315,6 +411,8 @@ def main():
     ap.add_argument("--mixed-study", action="store_true",
                     help="per-variable error and speed of mixed precision vs FP64 (2048x4096, MP7/MP9)")
     ap.add_argument("--study-steps", default="1,100,150,1000")
+    ap.add_argument("--ensemble", action="store_true", help="the 64-instance batched KH ensemble workload")
+    ap.add_argument("--ens-n", type=int, default=64)
     args = ap.parse_args()
 
     from cueva.configs import C2
@@ -327,6 +425,8 @@ def main():
         return run_reference(args, cfg)
     if args.mixed_study:
         return mixed_study(args)
+    if args.ensemble:
+        return run_ensemble(args)
 
     import numpy as np
     import torch

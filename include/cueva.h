@@ -192,6 +192,36 @@ int32_t cueva_attach_mlp(cueva_ctx* ctx, const cueva_mlp* mlp);
 /* Newton iterations, points and Cardano fall-backs of the learned path so far */
 int32_t cueva_learned_stats(cueva_ctx* ctx, int64_t out3[3]);
 
+/* ---- ensembles ---------------------------------------------------------- */
+/* No counterpart in the reference (it runs one grid per process).  n
+ * independent grids -- each with its own size, sigma, boundaries, dt and c2p
+ * method, sharing order, flux_solver, rec_mp, precision, intsum_reset and
+ * device -- advanced together: each RK stage is one y-face and one x-face +
+ * update launch over the tiles of all instances, and a step is one CUDA
+ * graph.  Primitive blocks on the host are 14 x (imax+1) x (jmax+1) doubles,
+ * field-major, i fastest, in cueva_field order (rho .. q). */
+typedef struct cueva_ens cueva_ens;
+int32_t cueva_ens_create(const cueva_params* params, int32_t n, cueva_ens** out);
+int32_t cueva_ens_destroy(cueva_ens* ens);
+int32_t cueva_ens_set_stream(cueva_ens* ens, void* cuda_stream);
+int32_t cueva_ens_set_prims(cueva_ens* ens, int32_t k, const double* host_prims);
+int32_t cueva_ens_get_prims(cueva_ens* ens, int32_t k, double* host_prims);
+/* Kelvin-Helmholtz initial data for instance k (same conventions as cueva_kh_init) */
+int32_t cueva_ens_kh_init(cueva_ens* ens, int32_t k, double v0, double a, double amp, double width, double kpert,
+                          double phase, double bshear, double rho0, double p0);
+/* nsteps ensemble steps (prepares stage 1 first if the state changed) */
+int32_t cueva_ens_step(cueva_ens* ens, int32_t nsteps);
+/* synchronise; status_out (optional, n words) gets each instance's status bits */
+int32_t cueva_ens_sync(cueva_ens* ens, uint32_t* status_out);
+/* launch shape: tile height rows (8 or 4) and CTAs per SM of a persistent
+ * grid (0 = one tile per CTA) */
+int32_t cueva_ens_set_shape(cueva_ens* ens, int32_t rows, int32_t ctas_per_sm);
+/* times the candidate shapes on the current state, keeps the fastest and
+ * restores the state; reports the choice and its ms per step */
+int32_t cueva_ens_autotune(cueva_ens* ens, int32_t* rows, int32_t* ctas_per_sm, double* ms_per_step);
+int32_t cueva_ens_attach_mlp(cueva_ens* ens, const cueva_mlp* mlp);
+int32_t cueva_ens_learned_stats(cueva_ens* ens, int64_t out3[3]);
+
 /* ---- stage right-hand side without any device allocation -------------- */
 /* No counterpart in the reference.  Computes the same stage right-hand side
  * as cueva_flux_rhs ({hll,hllc}_flow_mpx 2D + fluxandsource), but on device

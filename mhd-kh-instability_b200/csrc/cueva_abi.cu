@@ -120,6 +120,98 @@ bool make_tableau(int order, Tableau& T) {
 
 }  // namespace
 
+namespace {
+
+int32_t validate_params(const cueva_params* p) {
+  if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
+  if (p->flux_solver != 5 && p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
+  if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
+  if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
+  if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
+    return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
+  if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
+  if (p->intsum_reset != 0 && p->intsum_reset != 1) return fail(CUEVA_ERR_ARG, "intsum_reset must be 0 or 1");
+  return CUEVA_OK;
+}
+
+// K_m storage: needed when a row r >= m+2 of the tableau uses column m
+int kslots(const Tableau& T, int (&kslot_of)[8]) {
+  int n = 0;
+  for (int m = 0; m < 8; ++m) kslot_of[m] = -1;
+  for (int m = 0; m < T.s; ++m) {
+    bool need = false;
+    for (int r = m + 2; r < T.s; ++r) need = need || T.Ab[r][m] != 0.0 || T.Abt[r][m] != 0.0;
+    if (need) kslot_of[m] = n++;
+  }
+  return n;
+}
+
+// geometry and device layout of one grid
+struct InstGeom {
+  int imax, jmax, nx, ny, pitch, fpitch;
+  long long fstride, ffs, nslab;
+  double delx, dely, delz, dt;
+};
+
+InstGeom inst_geom(const cueva_params* p, int nkslot) {
+  InstGeom G{};
+  G.imax = p->imax; G.jmax = p->jmax; G.nx = p->imax + 1; G.ny = p->jmax + 1;
+  G.pitch = (G.nx + 31) / 32 * 32;
+  G.fstride = (long long)G.pitch * G.ny;
+  G.delx = p->lx / (double)p->imax;
+  G.dely = p->ly / (double)p->jmax;
+  G.delz = p->lz / 1.0;
+  double mn = (G.dely < G.delx) ? G.dely : G.delx;
+  mn = (G.delz < mn) ? G.delz : mn;
+  G.dt = (p->dt > 0.0) ? p->dt : p->cfl * mn;
+  // interface flux scratch: x faces -1/2 .. imax+1/2 (imax+2 per row) on
+  // jmax+1 rows, y faces on jmax+2 rows of imax+1
+  G.fpitch = (G.nx + 1 + 31) / 32 * 32;
+  G.ffs = (long long)G.fpitch * (G.ny + 1);
+  const long long nfields = 2LL * NPRIM + 2LL * NAUX + 2LL * NSTAGE + 2LL * NCONS + (long long)nkslot * NRHS + NRHS;
+  G.nslab = nfields * G.fstride + 2LL * NFACE * G.ffs;
+  return G;
+}
+
+// instance descriptor over a slab of G.nslab doubles (tile ranges not set)
+void fill_desc(const cueva_params* p, const InstGeom& G, int nkslot, double* slab, uint32_t* status,
+               unsigned long long* counters, InstDesc& I) {
+  const long long fs = G.fstride;
+  double* q = slab;
+  I.prim[0] = q; q += NPRIM * fs; I.prim[1] = q; q += NPRIM * fs;
+  I.aux[0] = q; q += NAUX * fs; I.aux[1] = q; q += NAUX * fs;
+  I.stage[0] = q; q += NSTAGE * fs; I.stage[1] = q; q += NSTAGE * fs;
+  I.intsum = q; q += NCONS * fs;
+  I.finsum = q; q += NCONS * fs;
+  I.kbuf = q; q += (long long)nkslot * NRHS * fs;
+  I.rhs_out = q; q += NRHS * fs;
+  I.fx = q; q += NFACE * G.ffs;
+  I.fy = q; q += NFACE * G.ffs;
+  I.fpitch = G.fpitch; I.ffs = G.ffs;
+  I.status = status;
+  I.counters = counters;
+  I.mlp = nullptr;
+  I.imax = G.imax; I.jmax = G.jmax; I.pitch = G.pitch; I.fstride = fs;
+  I.bc_x = p->bc_x; I.bc_y = p->bc_y;
+  I.delx = G.delx; I.dely = G.dely; I.dt = G.dt; I.sigma = p->sigma; I.gamma = p->gamma;
+  auto inv_pow2 = [](double d) {
+    int e = 0;
+    return (std::frexp(d, &e) == 0.5 && std::isnormal(1.0 / d)) ? 1.0 / d : 0.0;
+  };
+  I.inv_delx_pow2 = inv_pow2(G.delx);
+  I.inv_dely_pow2 = inv_pow2(G.dely);
+  const double mn = (G.dely < G.delx) ? G.dely : G.delx;   // parameters.f95:329-334
+  const double cp = std::sqrt(mn / 1.0);
+  I.kappa_psi = 1.0 / (cp * cp);
+  I.kappa_phi = 1.0 / (cp * cp);
+  // the Fortran module variable eps1 keeps the value the flux routine stored last
+  I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
+  I.c2p = p->c2p;
+}
+
+}  // namespace
+
 struct cueva_ctx {
   cueva_params P{};
   Tableau T;
@@ -136,7 +228,7 @@ struct cueva_ctx {
   InstDesc h_inst{};
   int nkslot = 0;
   int kslot_of[8];        // slot of K_m (0-based m) or -1
-  int nb[2] = {0, 0};     // CTAs of the x-face + update and the y-face launches
+  StageShape shape;       // tile height, CTAs and tiles of the two stage launches
   int cur = 0, qin = 0;
   bool primed = false;
   double* bound[CUEVA_NFIELDS] = {};
@@ -189,10 +281,10 @@ int32_t read_status(cueva_ctx* c) {
   return CUEVA_OK;
 }
 
-StageArgs stage_args(const cueva_ctx* c, int l, int mode) {
+StageArgs stage_args_of(const Tableau& T, const int* kslot_of, int intsum_reset, int cur, int qin, int l,
+                        int mode) {
   StageArgs sa{};
-  const Tableau& T = c->T;
-  sa.l = l; sa.s = T.s; sa.cur = c->cur; sa.qin = c->qin; sa.mode = mode;
+  sa.l = l; sa.s = T.s; sa.cur = cur; sa.qin = qin; sa.mode = mode;
   sa.wb = T.wb[l - 1]; sa.wbt = T.wbt[l - 1];
   for (int m = 0; m < 8; ++m) { sa.kslot[m] = -1; sa.ab_next[m] = 0.0; sa.abt_next[m] = 0.0; }
   if (l < T.s) {
@@ -200,13 +292,34 @@ StageArgs stage_args(const cueva_ctx* c, int l, int mode) {
     sa.abt_diag_next = T.Abt[l][l];
   }
   sa.abt_diag_first = T.Abt[0][0];
-  for (int m = 1; m < l; ++m) sa.kslot[m - 1] = c->kslot_of[m - 1];
-  sa.store_k_slot = (l < T.s) ? c->kslot_of[l - 1] : -1;
+  for (int m = 1; m < l; ++m) sa.kslot[m - 1] = kslot_of[m - 1];
+  sa.store_k_slot = (l < T.s) ? kslot_of[l - 1] : -1;
   // the reference zeroes the stage sums once per step, so stage l+1 starts
   // from the sums of stage l; with intsum_reset every stage starts from zero
-  sa.need_intsum_load = (!c->P.intsum_reset && l >= 2 && l < T.s) ? 1 : 0;
-  sa.need_intsum_store = (!c->P.intsum_reset && l + 1 < T.s) ? 1 : 0;
+  sa.need_intsum_load = (!intsum_reset && l >= 2 && l < T.s) ? 1 : 0;
+  sa.need_intsum_store = (!intsum_reset && l + 1 < T.s) ? 1 : 0;
   return sa;
+}
+
+StageArgs stage_args(const cueva_ctx* c, int l, int mode) {
+  return stage_args_of(c->T, c->kslot_of, c->P.intsum_reset, c->cur, c->qin, l, mode);
+}
+
+// Kelvin-Helmholtz initial data at one node (reference orientation: x the
+// shear normal, y the flow direction; 03_init_var_primitive.f95:2297-2336)
+struct KHParams { double v0, a, amp, width, kpert, phase, bshear, rho0, p0; };
+void kh_point(const KHParams& k, double posx, double posy, double (&pv)[NPRIM]) {
+  const double vx = k.amp * std::sin(k.kpert * posy + k.phase) * std::exp(-(posx * posx) / k.width);
+  const double vy = k.v0 * std::tanh(posx / k.a);
+  const double vz = 0.0;
+  const double Bx = 0.0, By = k.bshear, Bz = 0.0;
+  pv[P_RHO] = k.rho0; pv[P_P] = k.p0;
+  pv[P_VX] = vx; pv[P_VY] = vy; pv[P_VZ] = vz;
+  pv[P_PSI] = 0.0; pv[P_PHI] = 0.0; pv[P_Q] = 0.0;
+  pv[P_BX] = Bx; pv[P_BY] = By; pv[P_BZ] = Bz;
+  pv[P_EX] = -(vy * Bz - vz * By);
+  pv[P_EY] = -(vz * Bx - vx * Bz);
+  pv[P_EZ] = -(vx * By - vy * Bx);
 }
 
 int32_t run_begin_step(cueva_ctx* c) {
@@ -218,7 +331,7 @@ int32_t run_begin_step(cueva_ctx* c) {
 int32_t enqueue_step(cueva_ctx* c) {
   for (int l = 1; l <= c->T.s; ++l) {
     const StageArgs sa = stage_args(c, l, 0);
-    CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1, sa));
+    CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1, sa));
     c->qin ^= 1;
   }
   c->cur ^= 1;
@@ -240,15 +353,7 @@ const char* cueva_last_error(void) { return g_err.c_str(); }
 int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   if (!p || !out) return fail(CUEVA_ERR_ARG, "null argument");
   *out = nullptr;
-  if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
-  if (p->flux_solver != 5 && p->flux_solver != 7)
-    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
-  if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
-  if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
-  if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
-    return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
-  if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
-  if (p->intsum_reset != 0 && p->intsum_reset != 1) return fail(CUEVA_ERR_ARG, "intsum_reset must be 0 or 1");
+  if (int32_t e = validate_params(p)) return e;
   cueva_ctx* c = new cueva_ctx();
   c->P = *p;
   if (!make_tableau(p->order, c->T)) { delete c; return fail(CUEVA_ERR_ARG, "unsupported IMEX order"); }
@@ -260,49 +365,15 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   if (p->device < 0 || p->device >= ndev) { delete c; return fail(CUEVA_ERR_ARG, "device ordinal out of range"); }
   c->dev = p->device;
   if (cudaSetDevice(c->dev) != cudaSuccess) { delete c; return fail(CUEVA_ERR_CUDA, "cudaSetDevice failed"); }
-  c->imax = p->imax; c->jmax = p->jmax; c->nx = p->imax + 1; c->ny = p->jmax + 1;
-  c->pitch = (c->nx + 31) / 32 * 32;
-  c->fstride = (long long)c->pitch * c->ny;
-  c->delx = p->lx / (double)p->imax;
-  c->dely = p->ly / (double)p->jmax;
-  c->delz = p->lz / 1.0;
-  {
-    const double a = c->delx, b = c->dely, z = c->delz;
-    double mn = (b < a) ? b : a;
-    mn = (z < mn) ? z : mn;
-    c->dt = (p->dt > 0.0) ? p->dt : p->cfl * mn;
-  }
-  // K_m storage: needed when a row r >= m+2 of the tableau uses column m
-  for (int m = 0; m < 8; ++m) c->kslot_of[m] = -1;
-  for (int m = 0; m < c->T.s; ++m) {
-    bool need = false;
-    for (int r = m + 2; r < c->T.s; ++r) need = need || c->T.Ab[r][m] != 0.0 || c->T.Abt[r][m] != 0.0;
-    if (need) c->kslot_of[m] = c->nkslot++;
-  }
-  const long long fs = c->fstride;
-  // interface flux scratch: x faces -1/2 .. imax+1/2 (imax+2 per row) on
-  // jmax+1 rows, y faces on jmax+2 rows of imax+1
-  const int fpitch = (c->nx + 1 + 31) / 32 * 32;
-  const long long ffs = (long long)fpitch * (c->ny + 1);
-  const long long nfields = 2LL * NPRIM + 2LL * NAUX + 2LL * NSTAGE + 2LL * NCONS + (long long)c->nkslot * NRHS + NRHS;
-  const long long nslab = nfields * fs + 2LL * NFACE * ffs;
-  if (cudaMalloc(&c->slab, (size_t)nslab * sizeof(double)) != cudaSuccess) {
+  c->nkslot = kslots(c->T, c->kslot_of);
+  const InstGeom G = inst_geom(p, c->nkslot);
+  c->imax = G.imax; c->jmax = G.jmax; c->nx = G.nx; c->ny = G.ny; c->pitch = G.pitch; c->fstride = G.fstride;
+  c->delx = G.delx; c->dely = G.dely; c->delz = G.delz; c->dt = G.dt;
+  if (cudaMalloc(&c->slab, (size_t)G.nslab * sizeof(double)) != cudaSuccess) {
     delete c; cudaGetLastError();
     return fail(CUEVA_ERR_CUDA, "cudaMalloc of the field slab failed");
   }
-  cudaMemset(c->slab, 0, (size_t)nslab * sizeof(double));
-  double* q = c->slab;
-  InstDesc& I = c->h_inst;
-  I.prim[0] = q; q += NPRIM * fs; I.prim[1] = q; q += NPRIM * fs;
-  I.aux[0] = q; q += NAUX * fs; I.aux[1] = q; q += NAUX * fs;
-  I.stage[0] = q; q += NSTAGE * fs; I.stage[1] = q; q += NSTAGE * fs;
-  I.intsum = q; q += NCONS * fs;
-  I.finsum = q; q += NCONS * fs;
-  I.kbuf = q; q += (long long)c->nkslot * NRHS * fs;
-  I.rhs_out = q; q += NRHS * fs;
-  I.fx = q; q += NFACE * ffs;
-  I.fy = q; q += NFACE * ffs;
-  I.fpitch = fpitch; I.ffs = ffs;
+  cudaMemset(c->slab, 0, (size_t)G.nslab * sizeof(double));
   if (cudaMalloc(&c->d_status, 4) != cudaSuccess || cudaMalloc(&c->d_counters, 3 * 8) != cudaSuccess ||
       cudaMalloc(&c->d_inst, sizeof(InstDesc)) != cudaSuccess) {
     cueva_ctx_destroy(c); cudaGetLastError();
@@ -310,30 +381,17 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   }
   cudaMemset(c->d_status, 0, 4);
   cudaMemset(c->d_counters, 0, 24);
-  I.status = c->d_status;
-  I.counters = c->d_counters;
-  I.mlp = nullptr;
-  I.imax = c->imax; I.jmax = c->jmax; I.pitch = c->pitch; I.fstride = fs;
-  I.bc_x = p->bc_x; I.bc_y = p->bc_y;
-  I.delx = c->delx; I.dely = c->dely; I.dt = c->dt; I.sigma = p->sigma; I.gamma = p->gamma;
-  auto inv_pow2 = [](double d) {
-    int e = 0;
-    return (std::frexp(d, &e) == 0.5 && std::isnormal(1.0 / d)) ? 1.0 / d : 0.0;
-  };
-  I.inv_delx_pow2 = inv_pow2(c->delx);
-  I.inv_dely_pow2 = inv_pow2(c->dely);
-  const double mn = (c->dely < c->delx) ? c->dely : c->delx;   // parameters.f95:329-334
-  const double cp = std::sqrt(mn / 1.0);
-  I.kappa_psi = 1.0 / (cp * cp);
-  I.kappa_phi = 1.0 / (cp * cp);
-  // the Fortran module variable eps1 keeps the value the flux routine stored last
-  I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
-  I.c2p = p->c2p;
+  InstDesc& I = c->h_inst;
+  fill_desc(p, G, c->nkslot, c->slab, c->d_status, c->d_counters, I);
   // x tiles: 31 points (32 faces) x FACE_ROWS rows; y tiles: 32 columns x
   // FACE_ROWS face rows of j = -1..jmax
-  I.block_count[LK_XUPD] = ((c->nx + 30) / 31) * ((c->ny + FACE_ROWS - 1) / FACE_ROWS);
-  I.block_count[LK_YFACE] = ((c->nx + 31) / 32) * ((c->ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
-  for (int k = 0; k < 2; ++k) { I.block_begin[k] = 0; c->nb[k] = I.block_count[k]; }
+  I.block_count[LK_XUPD] = xupd_tiles(c->imax, c->jmax, FACE_ROWS);
+  I.block_count[LK_YFACE] = yface_tiles(c->imax, c->jmax, FACE_ROWS);
+  c->shape.rows = FACE_ROWS;
+  for (int k = 0; k < 2; ++k) {
+    I.block_begin[k] = 0;
+    c->shape.grid[k] = c->shape.ntiles[k] = I.block_count[k];   // one tile per CTA
+  }
   if (prepare_stage(p->rec_mp, p->flux_solver, p->precision) != cudaSuccess ||
       cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -461,7 +519,7 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
   for (int n = 0; n < nsteps && rc == CUEVA_OK; ++n) {
     for (int l = 1; l <= c->T.s && rc == CUEVA_OK; ++l) {
       const StageArgs sa = stage_args(c, l, 0);
-      cudaError_t ce = launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1,
+      cudaError_t ce = launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1,
                                     sa, ev);
       if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[2]);
       if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
@@ -554,7 +612,7 @@ int32_t cueva_flux_rhs(cueva_ctx* c, int32_t l) {
     if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
   if (int32_t e = h2d(c, aux_f(c, c->cur, A_W), CUEVA_W, 1)) return e;
   const StageArgs sa = stage_args(c, l, 1);
-  CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->nb, c->stream, c->d_inst, 1, sa));
+  CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1, sa));
   c->primed = false;
   const int out[NRHS] = {CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
                          CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,
@@ -619,23 +677,13 @@ int32_t cueva_kh_init(cueva_ctx* c, double v0, double a, double amp, double widt
   if (int32_t e = check_ctx(c)) return e;
   for (int f = 0; f < NPRIM; ++f)
     if (!c->bound[CUEVA_RHO + f]) return fail(CUEVA_ERR_UNBOUND, "kh_init needs all 14 prim fields bound");
-  const double lx = c->P.lx, ly = c->P.ly;
+  const KHParams kh{v0, a, amp, width, kpert, phase, bshear, rho0, p0};
   for (int j = 0; j <= c->jmax; ++j)
     for (int i = 0; i <= c->imax; ++i) {
       const size_t k = (size_t)(i + 6) + (size_t)(j + 6) * (c->imax + 13);
-      const double posx = -0.5 * lx + i * c->delx;
-      const double posy = -0.5 * ly + j * c->dely;
-      const double vx = amp * std::sin(kpert * posy + phase) * std::exp(-(posx * posx) / width);
-      const double vy = v0 * std::tanh(posx / a);
-      const double vz = 0.0;
-      const double Bx = 0.0, By = bshear, Bz = 0.0;
-      c->bound[CUEVA_RHO][k] = rho0; c->bound[CUEVA_P][k] = p0;
-      c->bound[CUEVA_VX][k] = vx; c->bound[CUEVA_VY][k] = vy; c->bound[CUEVA_VZ][k] = vz;
-      c->bound[CUEVA_PSI][k] = 0.0; c->bound[CUEVA_PHI][k] = 0.0; c->bound[CUEVA_Q][k] = 0.0;
-      c->bound[CUEVA_BX][k] = Bx; c->bound[CUEVA_BY][k] = By; c->bound[CUEVA_BZ][k] = Bz;
-      c->bound[CUEVA_EX][k] = -(vy * Bz - vz * By);
-      c->bound[CUEVA_EY][k] = -(vz * Bx - vx * Bz);
-      c->bound[CUEVA_EZ][k] = -(vx * By - vy * Bx);
+      double pv[NPRIM];
+      kh_point(kh, -0.5 * c->P.lx + i * c->delx, -0.5 * c->P.ly + j * c->dely, pv);
+      for (int f = 0; f < NPRIM; ++f) c->bound[CUEVA_RHO + f][k] = pv[f];
     }
   return CUEVA_OK;
 }
@@ -717,9 +765,11 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
   }
   I.c2p = 1;
   I.block_begin[LK_XUPD] = I.block_begin[LK_YFACE] = 0;
-  I.block_count[LK_XUPD] = ((nx + 30) / 31) * ((ny + FACE_ROWS - 1) / FACE_ROWS);
-  I.block_count[LK_YFACE] = ((nx + 31) / 32) * ((ny + 1 + FACE_ROWS - 1) / FACE_ROWS);
-  const int nb[2] = {I.block_count[LK_XUPD], I.block_count[LK_YFACE]};
+  I.block_count[LK_XUPD] = xupd_tiles(p->imax, p->jmax, FACE_ROWS);
+  I.block_count[LK_YFACE] = yface_tiles(p->imax, p->jmax, FACE_ROWS);
+  StageShape sh;
+  sh.rows = FACE_ROWS;
+  for (int k = 0; k < 2; ++k) sh.grid[k] = sh.ntiles[k] = I.block_count[k];
   InstDesc* d_inst = (InstDesc*)(base + kNoallocHeader);
   CUDA_TRY(cudaMemsetAsync(base, 0, kNoallocHeader, st));
   CUDA_TRY(cudaMemcpyAsync(d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice, st));
@@ -727,7 +777,7 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
   sa.l = 1; sa.s = 1; sa.cur = 0; sa.qin = 0; sa.mode = 1;
   for (int m = 0; m < 8; ++m) sa.kslot[m] = -1;
   sa.store_k_slot = -1;
-  CUDA_TRY(launch_stage(p->rec_mp, p->flux_solver, p->precision, nb, st, d_inst, 1, sa));
+  CUDA_TRY(launch_stage(p->rec_mp, p->flux_solver, p->precision, sh, st, d_inst, 1, sa));
   if (status_bits) {
     uint32_t h = 0;
     CUDA_TRY(cudaMemcpyAsync(&h, base, 4, cudaMemcpyDeviceToHost, st));
@@ -739,6 +789,366 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
       return fail(CUEVA_ERR_PHYSICS, buf);
     }
   }
+  return CUEVA_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================
+// Ensembles: many independent grids advanced by the same launches.  Every
+// instance has its own slab and descriptor; the stage kernels map a tile
+// index to (instance, tile) through the descriptors' tile ranges, so one
+// y-face launch and one x-face + update launch per RK stage serve all
+// instances, and one CUDA graph holds a whole ensemble step.
+// =====================================================================
+struct cueva_ens {
+  int dev = 0;
+  int n = 0;
+  cueva_params P0{};                    // shared scheme: order, solver, rec_mp, precision, intsum_reset
+  Tableau T;
+  int nkslot = 0;
+  int kslot_of[8];
+  std::vector<cueva_params> P;
+  std::vector<InstGeom> G;
+  std::vector<InstDesc> I;
+  std::vector<double*> slab;
+  uint32_t* d_status = nullptr;          // one status word per instance
+  unsigned long long* d_counters = nullptr;
+  InstDesc* d_inst = nullptr;
+  cudaStream_t stream = nullptr, own_stream = nullptr;
+  StageShape shape;
+  int ctas_per_sm = 0;                   // 0: one tile per CTA
+  int cur = 0, qin = 0;
+  bool primed = false;
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  MLPDevice* d_mlp = nullptr;
+  unsigned long long* d_mlp_stats = nullptr;
+  long long max_points = 0;
+  int num_sms = 148;
+};
+
+namespace {
+
+void ens_destroy_graphs(cueva_ens* e) {
+  for (auto& row : e->graph)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// tile ranges for a tile height and the launch grid for a CTA count per SM
+int32_t ens_apply_shape(cueva_ens* e, int rows, int ctas_per_sm) {
+  int begin[2] = {0, 0};
+  for (int k = 0; k < e->n; ++k) {
+    InstDesc& I = e->I[k];
+    I.block_count[LK_XUPD] = xupd_tiles(I.imax, I.jmax, rows);
+    I.block_count[LK_YFACE] = yface_tiles(I.imax, I.jmax, rows);
+    for (int t = 0; t < 2; ++t) { I.block_begin[t] = begin[t]; begin[t] += I.block_count[t]; }
+  }
+  e->shape.rows = rows;
+  for (int t = 0; t < 2; ++t) {
+    e->shape.ntiles[t] = begin[t];
+    const long long persistent = (long long)ctas_per_sm * e->num_sms;
+    e->shape.grid[t] = (ctas_per_sm > 0 && persistent < begin[t]) ? (int)persistent : begin[t];
+  }
+  e->ctas_per_sm = ctas_per_sm;
+  ens_destroy_graphs(e);
+  CUDA_TRY(cudaMemcpyAsync(e->d_inst, e->I.data(), sizeof(InstDesc) * e->n, cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return CUEVA_OK;
+}
+
+int32_t ens_begin(cueva_ens* e) {
+  CUDA_TRY(launch_begin_step(e->max_points, e->stream, e->d_inst, e->n, e->cur, e->qin, e->T.Abt[0][0]));
+  e->primed = true;
+  return CUEVA_OK;
+}
+
+int32_t ens_enqueue_step(cueva_ens* e) {
+  for (int l = 1; l <= e->T.s; ++l) {
+    const StageArgs sa = stage_args_of(e->T, e->kslot_of, e->P0.intsum_reset, e->cur, e->qin, l, 0);
+    CUDA_TRY(launch_stage(e->P0.rec_mp, e->P0.flux_solver, e->P0.precision, e->shape, e->stream, e->d_inst, e->n, sa));
+    e->qin ^= 1;
+  }
+  e->cur ^= 1;
+  return CUEVA_OK;
+}
+
+int32_t ens_check(cueva_ens* e, int k) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  if (k < 0 || k >= e->n) return fail(CUEVA_ERR_ARG, "instance index out of range");
+  return CUEVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t cueva_ens_destroy(cueva_ens* e) {
+  if (!e) return CUEVA_OK;
+  cudaSetDevice(e->dev);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  ens_destroy_graphs(e);
+  for (double* s : e->slab)
+    if (s) cudaFree(s);
+  for (void* p : {(void*)e->d_status, (void*)e->d_counters, (void*)e->d_inst, (void*)e->d_mlp, (void*)e->d_mlp_stats})
+    if (p) cudaFree(p);
+  if (e->own_stream) cudaStreamDestroy(e->own_stream);
+  delete e;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_create(const cueva_params* params, int32_t n, cueva_ens** out) {
+  if (!params || !out || n <= 0) return fail(CUEVA_ERR_ARG, "null argument or empty ensemble");
+  *out = nullptr;
+  for (int k = 0; k < n; ++k) {
+    if (int32_t e = validate_params(&params[k]))
+      return fail(e, "instance " + std::to_string(k) + ": " + g_err);
+    const cueva_params& a = params[0];
+    const cueva_params& b = params[k];
+    if (b.order != a.order || b.flux_solver != a.flux_solver || b.rec_mp != a.rec_mp ||
+        b.precision != a.precision || b.intsum_reset != a.intsum_reset || b.device != a.device)
+      return fail(CUEVA_ERR_ARG, "instance " + std::to_string(k) +
+                                     ": order, flux_solver, rec_mp, precision, intsum_reset and device must agree");
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, "no CUDA device available");
+  }
+  if (params[0].device < 0 || params[0].device >= ndev) return fail(CUEVA_ERR_ARG, "device ordinal out of range");
+  CUDA_TRY(cudaSetDevice(params[0].device));
+  cueva_ens* e = new cueva_ens();
+  e->dev = params[0].device;
+  e->n = n;
+  e->P0 = params[0];
+  if (!make_tableau(e->P0.order, e->T)) { delete e; return fail(CUEVA_ERR_ARG, "unsupported IMEX order"); }
+  e->nkslot = kslots(e->T, e->kslot_of);
+  cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->dev);
+  e->P.assign(params, params + n);
+  e->I.resize(n);
+  e->slab.assign(n, nullptr);
+  cudaError_t ce = cudaMalloc(&e->d_status, sizeof(uint32_t) * n);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_counters, sizeof(unsigned long long) * 3 * n);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_inst, sizeof(InstDesc) * n);
+  if (ce == cudaSuccess) ce = cudaMemset(e->d_status, 0, sizeof(uint32_t) * n);
+  if (ce == cudaSuccess) ce = cudaMemset(e->d_counters, 0, sizeof(unsigned long long) * 3 * n);
+  for (int k = 0; k < n && ce == cudaSuccess; ++k) {
+    e->G.push_back(inst_geom(&params[k], e->nkslot));
+    ce = cudaMalloc(&e->slab[k], (size_t)e->G[k].nslab * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMemset(e->slab[k], 0, (size_t)e->G[k].nslab * sizeof(double));
+    if (ce == cudaSuccess) {
+      fill_desc(&params[k], e->G[k], e->nkslot, e->slab[k], e->d_status + k, e->d_counters + 3 * k, e->I[k]);
+      const long long pts = (long long)e->G[k].nx * e->G[k].ny;
+      if (pts > e->max_points) e->max_points = pts;
+    }
+  }
+  if (ce == cudaSuccess && prepare_stage(e->P0.rec_mp, e->P0.flux_solver, e->P0.precision) != cudaSuccess)
+    ce = cudaErrorInvalidValue;
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    cueva_ens_destroy(e);
+    cudaGetLastError();
+    return fail(CUEVA_ERR_CUDA, std::string("ensemble set-up: ") + cudaGetErrorString(ce));
+  }
+  e->stream = e->own_stream;
+  if (int32_t r = ens_apply_shape(e, FACE_ROWS, 0)) { cueva_ens_destroy(e); return r; }
+  *out = e;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_set_stream(cueva_ens* e, void* s) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  ens_destroy_graphs(e);
+  e->stream = s ? (cudaStream_t)s : e->own_stream;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_set_shape(cueva_ens* e, int32_t rows, int32_t ctas_per_sm) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  if ((rows != 4 && rows != 8) || ctas_per_sm < 0) return fail(CUEVA_ERR_ARG, "rows must be 4 or 8, ctas_per_sm >= 0");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  return ens_apply_shape(e, rows, ctas_per_sm);
+}
+
+int32_t cueva_ens_set_prims(cueva_ens* e, int32_t k, const double* host) {
+  if (int32_t r = ens_check(e, k)) return r;
+  if (!host) return fail(CUEVA_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  const InstGeom& G = e->G[k];
+  for (int f = 0; f < NPRIM; ++f)
+    CUDA_TRY(cudaMemcpy2DAsync(e->I[k].prim[e->cur] + (long long)f * G.fstride, (size_t)G.pitch * 8,
+                               host + (size_t)f * G.nx * G.ny, (size_t)G.nx * 8, (size_t)G.nx * 8, (size_t)G.ny,
+                               cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->primed = false;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_get_prims(cueva_ens* e, int32_t k, double* host) {
+  if (int32_t r = ens_check(e, k)) return r;
+  if (!host) return fail(CUEVA_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  const InstGeom& G = e->G[k];
+  for (int f = 0; f < NPRIM; ++f)
+    CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)f * G.nx * G.ny, (size_t)G.nx * 8,
+                               e->I[k].prim[e->cur] + (long long)f * G.fstride, (size_t)G.pitch * 8,
+                               (size_t)G.nx * 8, (size_t)G.ny, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_kh_init(cueva_ens* e, int32_t k, double v0, double a, double amp, double width, double kpert,
+                          double phase, double bshear, double rho0, double p0) {
+  if (int32_t r = ens_check(e, k)) return r;
+  const InstGeom& G = e->G[k];
+  const KHParams kh{v0, a, amp, width, kpert, phase, bshear, rho0, p0};
+  std::vector<double> h((size_t)NPRIM * G.nx * G.ny);
+  for (int j = 0; j <= G.jmax; ++j)
+    for (int i = 0; i <= G.imax; ++i) {
+      double pv[NPRIM];
+      kh_point(kh, -0.5 * e->P[k].lx + i * G.delx, -0.5 * e->P[k].ly + j * G.dely, pv);
+      for (int f = 0; f < NPRIM; ++f) h[(size_t)f * G.nx * G.ny + (size_t)j * G.nx + i] = pv[f];
+    }
+  return cueva_ens_set_prims(e, k, h.data());
+}
+
+int32_t cueva_ens_step(cueva_ens* e, int32_t nsteps) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  if (nsteps < 0) return fail(CUEVA_ERR_ARG, "nsteps < 0");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  if (!e->primed)
+    if (int32_t r = ens_begin(e)) return r;
+  for (int s = 0; s < nsteps; ++s) {
+    cudaGraphExec_t& g = e->graph[e->cur][e->qin];
+    if (!g) {
+      const int cur0 = e->cur, qin0 = e->qin;
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      int32_t r = ens_enqueue_step(e);
+      cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+      e->cur = cur0; e->qin = qin0;
+      if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+      if (ce != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&g, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    }
+    CUDA_TRY(cudaGraphLaunch(g, e->stream));
+    for (int l = 0; l < e->T.s; ++l) e->qin ^= 1;
+    e->cur ^= 1;
+  }
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_sync(cueva_ens* e, uint32_t* status_out) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  std::vector<uint32_t> st(e->n);
+  CUDA_TRY(cudaMemcpyAsync(st.data(), e->d_status, sizeof(uint32_t) * e->n, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (status_out) std::memcpy(status_out, st.data(), sizeof(uint32_t) * e->n);
+  for (int k = 0; k < e->n; ++k)
+    if (st[k]) {
+      char buf[128];
+      snprintf(buf, sizeof buf, "instance %d: kernel status 0x%x", k, st[k]);
+      return fail(CUEVA_ERR_PHYSICS, buf);
+    }
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_attach_mlp(cueva_ens* e, const cueva_mlp* mlp) {
+  if (!e || !mlp) return fail(CUEVA_ERR_ARG, "null argument");
+  if (mlp_device_of(mlp) != e->dev) return fail(CUEVA_ERR_ARG, "network and ensemble live on different devices");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  MLPDevice h;
+  if (int32_t r = mlp_device_image(mlp, &h)) return r;
+  if (!e->d_mlp) {
+    CUDA_TRY(cudaMalloc(&e->d_mlp, sizeof(MLPDevice)));
+    CUDA_TRY(cudaMalloc(&e->d_mlp_stats, 3 * sizeof(unsigned long long)));
+  }
+  h.stats = e->d_mlp_stats;
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaMemcpy(e->d_mlp, &h, sizeof(MLPDevice), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemset(e->d_mlp_stats, 0, 3 * sizeof(unsigned long long)));
+  for (auto& I : e->I) I.mlp = e->d_mlp;
+  CUDA_TRY(cudaMemcpy(e->d_inst, e->I.data(), sizeof(InstDesc) * e->n, cudaMemcpyHostToDevice));
+  return CUEVA_OK;
+}
+
+// Autotuner: times one ensemble step for each launch shape -- tile height
+// 8 or 4 rows, and one tile per CTA or a persistent grid of 1 or 2 (rows 8)
+// / 2 or 4 (rows 4) CTAs per SM -- on the ensemble's own state, keeps the
+// fastest and puts the state back.  Allocates a copy of the primitives.
+int32_t cueva_ens_autotune(cueva_ens* e, int32_t* rows_out, int32_t* ctas_out, double* ms_out) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  std::vector<double*> save(e->n, nullptr);
+  auto release = [&]() {
+    for (double* p : save)
+      if (p) cudaFree(p);
+  };
+  auto copy_prims = [&](bool to_save) -> cudaError_t {
+    for (int k = 0; k < e->n; ++k) {
+      const size_t bytes = (size_t)NPRIM * e->G[k].fstride * sizeof(double);
+      cudaError_t ce = to_save ? cudaMemcpyAsync(save[k], e->I[k].prim[e->cur], bytes, cudaMemcpyDeviceToDevice, e->stream)
+                               : cudaMemcpyAsync(e->I[k].prim[e->cur], save[k], bytes, cudaMemcpyDeviceToDevice, e->stream);
+      if (ce != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+  };
+  for (int k = 0; k < e->n; ++k)
+    if (cudaMalloc(&save[k], (size_t)NPRIM * e->G[k].fstride * sizeof(double)) != cudaSuccess) {
+      release(); cudaGetLastError();
+      return fail(CUEVA_ERR_CUDA, "autotune: no memory for the state copy");
+    }
+  if (copy_prims(true) != cudaSuccess) { release(); return fail(CUEVA_ERR_CUDA, "autotune: state copy failed"); }
+  const int cand[6][2] = {{8, 0}, {8, 2}, {8, 1}, {4, 0}, {4, 4}, {4, 2}};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  double best = 1e300;
+  int brow = FACE_ROWS, bctas = 0;
+  int32_t rc = CUEVA_OK;
+  const int cur0 = e->cur, qin0 = e->qin;
+  for (const auto& c : cand) {
+    e->cur = cur0; e->qin = qin0;
+    if ((rc = ens_apply_shape(e, c[0], c[1]))) break;
+    if (copy_prims(false) != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, "autotune: state restore failed"); break; }
+    e->primed = false;
+    if ((rc = cueva_ens_step(e, 1))) break;   // captures the graphs, warms the caches
+    cudaEventRecord(ev0, e->stream);
+    if ((rc = cueva_ens_step(e, 2))) break;
+    cudaEventRecord(ev1, e->stream);
+    if (cudaEventSynchronize(ev1) != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, "autotune: timing failed"); break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (ms / 2.0 < best) { best = ms / 2.0; brow = c[0]; bctas = c[1]; }
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  e->cur = cur0; e->qin = qin0;
+  if (!rc) rc = ens_apply_shape(e, brow, bctas);
+  if (!rc && copy_prims(false) != cudaSuccess) rc = fail(CUEVA_ERR_CUDA, "autotune: state restore failed");
+  if (!rc && cudaMemsetAsync(e->d_status, 0, sizeof(uint32_t) * e->n, e->stream) != cudaSuccess)
+    rc = fail(CUEVA_ERR_CUDA, "autotune: status reset failed");
+  cudaStreamSynchronize(e->stream);
+  release();
+  e->primed = false;
+  if (rc) return rc;
+  if (rows_out) *rows_out = brow;
+  if (ctas_out) *ctas_out = bctas;
+  if (ms_out) *ms_out = best;
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_learned_stats(cueva_ens* e, int64_t out3[3]) {
+  if (!e || !out3) return fail(CUEVA_ERR_ARG, "null argument");
+  unsigned long long h[3] = {0, 0, 0};
+  if (e->d_mlp_stats) {
+    CUDA_TRY(cudaMemcpyAsync(h, e->d_mlp_stats, sizeof h, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+  }
+  for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
   return CUEVA_OK;
 }
 

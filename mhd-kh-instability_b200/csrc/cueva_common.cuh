@@ -106,11 +106,24 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
   return i;
 }
 
-// launch geometry: 32 x FACE_ROWS threads per CTA for the face tiles
-// (x tiles update 31 points per row), 256 threads for the pointwise kernels
-constexpr int FACE_ROWS = 8;
+// launch geometry: 32 x ROWS threads per CTA for the face tiles (x tiles
+// update 31 points per row; ROWS is 8 or 4), 256 threads for the pointwise
+// kernels
+constexpr int FACE_ROWS = 8;   // default tile height
 constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
 constexpr int POINT_THREADS = 256;
 enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1 };
+
+// launch shape of one RK stage: tile height, CTAs per launch kind and the
+// tiles they loop over (grid == ntiles: one tile per CTA; smaller: persistent)
+struct StageShape {
+  int rows = FACE_ROWS;
+  int grid[2] = {0, 0};
+  int ntiles[2] = {0, 0};
+};
+
+// tiles of one instance for a tile height (x tiles: 31 points by rows)
+inline int xupd_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 30) / 31) * ((jmax + 1 + rows - 1) / rows); }
+inline int yface_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 31) / 32) * ((jmax + 2 + rows - 1) / rows); }
 
 }  // namespace cueva

@@ -204,19 +204,19 @@ __device__ __forceinline__ void prefetch_l2(const double* p, int n) {
 
 constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
 
-template <int RM, int SOLVER>
+template <int RM, int SOLVER, int ROWS>
 struct FaceGeom {
   static constexpr int R = MPR<RM>::R;
   static constexpr int NS = 2 * R + 2;                 // stencil points
   static constexpr int LONG = 32 + 2 * R + 1;          // staged cells along a 32-face segment
-  static constexpr int DEEP = FACE_ROWS + 2 * R + 1;   // staged rows across FACE_ROWS faces
+  static constexpr int DEEP = ROWS + 2 * R + 1;        // staged rows across ROWS faces
   static constexpr int NC = (SOLVER == 7) ? 4 : 3;     // coupled fields: v (+ rho for HLLC)
   // D = 0: normal [row][f][LONG], transverse [f][DEEP][32]
   // D = 1: normal [f][DEEP][32],  transverse [row][f][LONG]
-  static constexpr int NORMAL0 = FACE_ROWS * NF_FACE * LONG;
+  static constexpr int NORMAL0 = ROWS * NF_FACE * LONG;
   static constexpr int NORMAL1 = NF_FACE * DEEP * 32;
   static constexpr int TRANS0 = NC * DEEP * 32;
-  static constexpr int TRANS1 = FACE_ROWS * NC * LONG;
+  static constexpr int TRANS1 = ROWS * NC * LONG;
   static constexpr __host__ __device__ int normal(int D) { return D == 0 ? NORMAL0 : NORMAL1; }
   static constexpr size_t bytes(int D) {
     return sizeof(double) * (size_t)(D == 0 ? NORMAL0 + TRANS0 : NORMAL1 + TRANS1);
@@ -245,10 +245,10 @@ __device__ __forceinline__ const double* face_field(const double* prim, const do
 
 // issue the cp.async copies of one tile (first face i0, j0; last ilast, jlast);
 // cells reaching beyond the last face are not copied
-template <int RM, int SOLVER, int D>
+template <int RM, int SOLVER, int D, int ROWS>
 __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& sa, double* sn, double* st, int i0,
                                            int j0, int ilast, int jlast, int tid) {
-  using G = FaceGeom<RM, SOLVER>;
+  using G = FaceGeom<RM, SOLVER, ROWS>;
   constexpr int R = G::R, LONG = G::LONG, DEEP = G::DEEP, NC = G::NC;
   const int imax = I.imax, jmax = I.jmax, pitch = I.pitch, bcx = I.bc_x, bcy = I.bc_y;
   const long long fs = I.fstride;
@@ -258,7 +258,7 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
   const int ncell = ilast + R + 1 - (i0 - R) + 1;   // x cells i0-R .. ilast+R+1
   const int nrow = jlast + R + 1 - (j0 - R) + 1;    // y rows j0-R .. jlast+R+1
   // rows j0..jlast, cells along x: the normal stencils (D = 0) or the coupled ones (D = 1)
-  for (int e = tid; e < FACE_ROWS * LONG; e += 32 * FACE_ROWS) {
+  for (int e = tid; e < ROWS * LONG; e += 32 * ROWS) {
     const int r = e / LONG, c = e - r * LONG;
     if (j0 + r > jlast || c >= ncell) continue;
     const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
@@ -271,7 +271,7 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
     }
   }
   // columns i0..ilast, rows along y: the coupled stencils (D = 0) or the normal ones (D = 1)
-  for (int e = tid; e < DEEP * 32; e += 32 * FACE_ROWS) {
+  for (int e = tid; e < DEEP * 32; e += 32 * ROWS) {
     const int r = e >> 5, c = e & 31;
     if (r >= nrow || i0 + c > ilast) continue;
     const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
@@ -287,10 +287,10 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
 
 // flux of the face of (w, lane) from the staged tile (16_hll_flow_mpx.f95 /
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits
-template <int RM, int SOLVER, typename T, int D>
+template <int RM, int SOLVER, typename T, int D, int ROWS>
 __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
                                               T (&F)[NROLE]) {
-  using G = FaceGeom<RM, SOLVER>;
+  using G = FaceGeom<RM, SOLVER, ROWS>;
   constexpr int R = G::R, NS = G::NS;
   auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
   auto nrm = [&](int f, int q) -> T { return T(nrmd(f, q)); };
@@ -391,32 +391,40 @@ __device__ __forceinline__ const InstDesc& tile_inst(const InstDesc* __restrict_
   return insts[k];
 }
 
-// y faces: 32 columns x FACE_ROWS face rows j = j0-1+warp in [-1, jmax];
-// writes Fy(i, j+1/2) to the flux scratch
-template <int RM, int SOLVER, typename T>
-__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
-k_yface(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
-  using G = FaceGeom<RM, SOLVER>;
+// Tile loop: CTA b handles tiles b, b + gridDim.x, ... of the launch (ntiles
+// over all instances), so a grid of one CTA per tile and a persistent grid
+// of a few CTAs per SM run the same code.
+
+// y faces: 32 columns x ROWS face rows j = j0-1+warp in [-1, jmax]; writes
+// Fy(i, j+1/2) to the flux scratch
+template <int RM, int SOLVER, typename T, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS, 16 / ROWS)
+k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) {
+  using G = FaceGeom<RM, SOLVER, ROWS>;
   extern __shared__ double smem[];
-  int b = blockIdx.x;
-  const InstDesc& I = tile_inst(insts, ninst, LK_YFACE, b);
   const int lane = threadIdx.x, w = threadIdx.y;
-  const int bpr = (I.imax + 1 + 31) / 32;
-  const int i0 = (b % bpr) * 32, j0 = (b / bpr) * FACE_ROWS - 1;
-  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + FACE_ROWS - 1, I.jmax);
   double* sn = smem;
   double* st = smem + G::normal(1);
-  stage_tile<RM, SOLVER, 1>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
-  cp_async_wait_all();
-  __syncthreads();
-  const int i = i0 + lane, j = j0 + w;
-  if (i > ilast || j > jlast) return;
-  T F[NROLE];
-  const uint32_t stt = face_flux<RM, SOLVER, T, 1>(sn, st, w, lane, I.gamma, F);
-  const long long fo = (long long)(j + 1) * I.fpitch + i;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int b = tile;
+    const InstDesc& I = tile_inst(insts, ninst, LK_YFACE, b);
+    const int bpr = (I.imax + 1 + 31) / 32;
+    const int i0 = (b % bpr) * 32, j0 = (b / bpr) * ROWS - 1;
+    const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + ROWS - 1, I.jmax);
+    stage_tile<RM, SOLVER, 1, ROWS>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
+    cp_async_wait_all();
+    __syncthreads();
+    const int i = i0 + lane, j = j0 + w;
+    if (i <= ilast && j <= jlast) {
+      T F[NROLE];
+      const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, F);
+      const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
-  for (int c = 0; c < NROLE; ++c) I.fy[c * I.ffs + fo] = double(F[c]);
-  if (stt) atomicOr(I.status, stt);
+      for (int c = 0; c < NROLE; ++c) I.fy[c * I.ffs + fo] = double(F[c]);
+      if (stt) atomicOr(I.status, stt);
+    }
+    __syncthreads();   // the next tile's copies overwrite the staged values
+  }
 }
 
 // ------------------------------------------------- x faces + point update
@@ -560,22 +568,16 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
   return st;
 }
 
-template <int RM, int SOLVER, typename T, int EP>
-__global__ void __launch_bounds__(32 * FACE_ROWS, 2)
-k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
-  using G = FaceGeom<RM, SOLVER>;
+template <int RM, int SOLVER, typename T, int EP, int ROWS>
+__device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa, int b, double* sn, double* st) {
+  using G = FaceGeom<RM, SOLVER, ROWS>;
   constexpr int R = G::R, LONG = G::LONG;
-  extern __shared__ double smem[];
-  int b = blockIdx.x;
-  const InstDesc& I = tile_inst(insts, ninst, LK_XUPD, b);
   const int lane = threadIdx.x, w = threadIdx.y;
   // a tile updates 31 points per row: faces i0 .. i0+31 (i0 = first point - 1)
   const int bpr = (I.imax + 1 + 30) / 31;
-  const int i0 = (b % bpr) * 31 - 1, j0 = (b / bpr) * FACE_ROWS;
-  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + FACE_ROWS - 1, I.jmax);
-  double* sn = smem;
-  double* st = smem + G::normal(0);
-  stage_tile<RM, SOLVER, 0>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
+  const int i0 = (b % bpr) * 31 - 1, j0 = (b / bpr) * ROWS;
+  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + ROWS - 1, I.jmax);
+  stage_tile<RM, SOLVER, 0, ROWS>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
   if constexpr (EP != EP_RHS) {
     // the update's other inputs go to L2 while the faces are computed: per
     // row of the tile, the 6 aux and 9 time-n primitive fields, finsum and
@@ -587,7 +589,7 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
     for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
     const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;   // fields read at the point
     const int total = ncen * nr + NROLE * (nr + 1);
-    for (int e = w * 32 + lane; e < total && npt > 0; e += 32 * FACE_ROWS) {
+    for (int e = w * 32 + lane; e < total && npt > 0; e += 32 * ROWS) {
       if (e < ncen * nr) {
         const int r = e % nr;
         int f = e / nr;
@@ -613,12 +615,12 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   cp_async_wait_all();
   __syncthreads();
   const int i = i0 + lane, j = j0 + w;
-  if (j > jlast) return;   // whole warp
+  if (j > jlast) return;   // whole warp; the caller synchronises before the next tile
   T F[NROLE];
 #pragma unroll
   for (int c = 0; c < NROLE; ++c) F[c] = T(0);
   uint32_t stt = 0;
-  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0>(sn, st, w, lane, I.gamma, F);
+  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, F);
   // Fx(i-1/2) of point i is the face of lane-1
   const double dlx = I.delx, ix2 = I.inv_delx_pow2;
   double qx[NROLE];
@@ -649,45 +651,68 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, StageArgs sa) {
   if (stt) atomicOr(I.status, stt);
 }
 
+template <int RM, int SOLVER, typename T, int EP, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS, 16 / ROWS)
+k_xupd(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) {
+  using G = FaceGeom<RM, SOLVER, ROWS>;
+  extern __shared__ double smem[];
+  double* sn = smem;
+  double* st = smem + G::normal(0);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int b = tile;
+    const InstDesc& I = tile_inst(insts, ninst, LK_XUPD, b);
+    xupd_tile<RM, SOLVER, T, EP, ROWS>(I, sa, b, sn, st);
+    __syncthreads();   // the next tile's copies overwrite the staged values
+  }
+}
+
 // ---------------------------------------------------------------- launchers
-template <int RM, int SV, typename T>
-static void launch_tiles(const int (&nb)[2], cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
+template <int RM, int SV, typename T, int ROWS>
+static void launch_tiles(const StageShape& sh, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
                          cudaEvent_t* ev) {
-  using G = FaceGeom<RM, SV>;
-  const dim3 blk(32, FACE_ROWS);
+  using G = FaceGeom<RM, SV, ROWS>;
+  const dim3 blk(32, ROWS);
   if (ev) cudaEventRecord(ev[0], st);
-  k_yface<RM, SV, T><<<nb[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sa);
+  k_yface<RM, SV, T, ROWS><<<sh.grid[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sh.ntiles[LK_YFACE], sa);
   if (ev) cudaEventRecord(ev[1], st);
-  if (sa.mode == 1) k_xupd<RM, SV, T, EP_RHS><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
-  else if (sa.l < sa.s) k_xupd<RM, SV, T, EP_MID><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
-  else k_xupd<RM, SV, T, EP_LAST><<<nb[LK_XUPD], blk, G::bytes(0), st>>>(d, n, sa);
+  const int gx = sh.grid[LK_XUPD], nt = sh.ntiles[LK_XUPD];
+  if (sa.mode == 1) k_xupd<RM, SV, T, EP_RHS, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
+  else if (sa.l < sa.s) k_xupd<RM, SV, T, EP_MID, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
+  else k_xupd<RM, SV, T, EP_LAST, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
   if (ev) cudaEventRecord(ev[2], st);
 }
 
-template <int RM, int SV, typename T>
+template <int RM, int SV, typename T, int ROWS>
 static cudaError_t prepare_tiles() {
-  using G = FaceGeom<RM, SV>;
+  using G = FaceGeom<RM, SV, ROWS>;
   const int b0 = (int)G::bytes(0), b1 = (int)G::bytes(1);
-  cudaError_t e = cudaFuncSetAttribute(k_yface<RM, SV, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1);
+  cudaError_t e = cudaFuncSetAttribute(k_yface<RM, SV, T, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_RHS, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_MID>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_MID, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_LAST, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
   return e;
 }
 
 template <int RM, int SV>
-static void launch_rm_sv(int prec, const int (&nb)[2], cudaStream_t st, const InstDesc* d, int n,
+static void launch_rm_sv(int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                          const StageArgs& sa, cudaEvent_t* ev) {
-  if (prec == 0) launch_tiles<RM, SV, double>(nb, st, d, n, sa, ev);
-  else launch_tiles<RM, SV, float>(nb, st, d, n, sa, ev);
+  if (prec == 0) {
+    if (sh.rows == 4) launch_tiles<RM, SV, double, 4>(sh, st, d, n, sa, ev);
+    else launch_tiles<RM, SV, double, 8>(sh, st, d, n, sa, ev);
+  } else {
+    if (sh.rows == 4) launch_tiles<RM, SV, float, 4>(sh, st, d, n, sa, ev);
+    else launch_tiles<RM, SV, float, 8>(sh, st, d, n, sa, ev);
+  }
 }
 
 template <int RM, int SV>
 static cudaError_t prepare_rm_sv(int prec) {
-  return prec == 0 ? prepare_tiles<RM, SV, double>() : prepare_tiles<RM, SV, float>();
+  cudaError_t e = prec == 0 ? prepare_tiles<RM, SV, double, 8>() : prepare_tiles<RM, SV, float, 8>();
+  if (e == cudaSuccess) e = prec == 0 ? prepare_tiles<RM, SV, double, 4>() : prepare_tiles<RM, SV, float, 4>();
+  return e;
 }
 
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
@@ -702,15 +727,16 @@ cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
   }
 }
 
-cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[2], cudaStream_t st, const InstDesc* d,
+cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev) {
+  if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
   switch (rec_mp * 10 + (solver == 7 ? 1 : 0)) {
-    case 0: launch_rm_sv<0, 5>(prec, nb, st, d, n, sa, ev); break;
-    case 1: launch_rm_sv<0, 7>(prec, nb, st, d, n, sa, ev); break;
-    case 10: launch_rm_sv<1, 5>(prec, nb, st, d, n, sa, ev); break;
-    case 11: launch_rm_sv<1, 7>(prec, nb, st, d, n, sa, ev); break;
-    case 20: launch_rm_sv<2, 5>(prec, nb, st, d, n, sa, ev); break;
-    case 21: launch_rm_sv<2, 7>(prec, nb, st, d, n, sa, ev); break;
+    case 0: launch_rm_sv<0, 5>(prec, sh, st, d, n, sa, ev); break;
+    case 1: launch_rm_sv<0, 7>(prec, sh, st, d, n, sa, ev); break;
+    case 10: launch_rm_sv<1, 5>(prec, sh, st, d, n, sa, ev); break;
+    case 11: launch_rm_sv<1, 7>(prec, sh, st, d, n, sa, ev); break;
+    case 20: launch_rm_sv<2, 5>(prec, sh, st, d, n, sa, ev); break;
+    case 21: launch_rm_sv<2, 7>(prec, sh, st, d, n, sa, ev); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

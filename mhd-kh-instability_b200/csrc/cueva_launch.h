@@ -17,9 +17,9 @@ int mlp_device_of(const cueva_mlp* M);
 // sets the shared-memory limits of the stage kernels (call once per device
 // before the first launch or capture)
 cudaError_t prepare_stage(int rec_mp, int solver, int prec);
-// one RK stage: y faces, then x faces + update (nb = CTAs per launch kind);
-// with ev non-null, ev[0..2] are recorded before, between and after the launches
-cudaError_t launch_stage(int rec_mp, int solver, int prec, const int (&nb)[2], cudaStream_t st, const InstDesc* d,
+// one RK stage: y faces, then x faces + update; with ev non-null, ev[0..2]
+// are recorded before, between and after the launches
+cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev = nullptr);
 cudaError_t launch_begin_step(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
                               double abt11);

@@ -30,7 +30,10 @@ EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_s
            "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
            "cueva_mlp_destroy", "cueva_mlp_get_params", "cueva_mlp_set_params", "cueva_mlp_synthetic_pairs",
            "cueva_mlp_fit_normalisation", "cueva_mlp_train", "cueva_mlp_gradients", "cueva_mlp_predict",
-           "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats"]
+           "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats", "cueva_ens_create", "cueva_ens_destroy",
+           "cueva_ens_set_stream", "cueva_ens_set_prims", "cueva_ens_get_prims", "cueva_ens_kh_init",
+           "cueva_ens_step", "cueva_ens_sync", "cueva_ens_set_shape", "cueva_ens_autotune",
+           "cueva_ens_attach_mlp", "cueva_ens_learned_stats"]
 MLP_NPARAM, MLP_NNORM = 8833, 14
 
 
@@ -100,6 +103,18 @@ def load(fma=False):
     L.cueva_c2p_batch.argtypes = [i32, i32, vp, dbl, dbl, vp, vp, vp, i64, vp, vp]
     L.cueva_attach_mlp.argtypes = [vp, vp]
     L.cueva_learned_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.cueva_ens_create.argtypes = [ctypes.POINTER(Params), i32, ctypes.POINTER(vp)]
+    L.cueva_ens_destroy.argtypes = [vp]
+    L.cueva_ens_set_stream.argtypes = [vp, vp]
+    L.cueva_ens_set_prims.argtypes = [vp, i32, ctypes.POINTER(dbl)]
+    L.cueva_ens_get_prims.argtypes = [vp, i32, ctypes.POINTER(dbl)]
+    L.cueva_ens_kh_init.argtypes = [vp, i32] + [dbl] * 9
+    L.cueva_ens_step.argtypes = [vp, i32]
+    L.cueva_ens_sync.argtypes = [vp, ctypes.POINTER(u32)]
+    L.cueva_ens_set_shape.argtypes = [vp, i32, i32]
+    L.cueva_ens_autotune.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(dbl)]
+    L.cueva_ens_attach_mlp.argtypes = [vp, vp]
+    L.cueva_ens_learned_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.cueva_flux_rhs_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp, vp, i32, ctypes.c_int64, vp,
                                          ctypes.POINTER(u32)]
     _LIBS[key] = L
