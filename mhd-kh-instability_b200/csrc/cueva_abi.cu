@@ -124,8 +124,8 @@ namespace {
 
 int32_t validate_params(const cueva_params* p) {
   if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
-  if (p->flux_solver != 5 && p->flux_solver != 7)
-    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
+  if (p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
   if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
   if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
   if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
@@ -275,7 +275,7 @@ int32_t read_status(cueva_ctx* c) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st) {
     char buf[160];
-    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state)", st);
+    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed)", st);
     return fail(CUEVA_ERR_PHYSICS, buf);
   }
   return CUEVA_OK;
@@ -706,8 +706,8 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
                                double* rhs, int32_t pitch, int64_t fstride, void* stream, uint32_t* status_bits) {
   if (!p || !prim || !W || !stage || !rhs) return fail(CUEVA_ERR_ARG, "null argument");
   if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
-  if (p->flux_solver != 5 && p->flux_solver != 7)
-    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX) or 7 (HLLC+MPX)");
+  if (p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
   if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
   if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
     return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
@@ -727,7 +727,7 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
     void* base = nullptr;
     CUDA_TRY(cudaGetSymbolAddress(&base, g_noalloc_scratch));
     for (int rm = 0; rm < 3; ++rm)
-      for (int sv : {5, 7})
+      for (int sv : {5, 6, 7})
         for (int pr = 0; pr < 2; ++pr) CUDA_TRY(prepare_stage(rm, sv, pr));
     g_noalloc_base[p->device] = base;
   }

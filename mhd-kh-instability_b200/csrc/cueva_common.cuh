@@ -32,7 +32,8 @@ enum StatusBits : uint32_t {
   ST_SUPERLUMINAL = 2u,    // 12_varprimitive.f95:678,691 ; 12_varprimitive_nr.f95:217
   ST_HLLC_NOCONV = 4u,     // funciones.f95:240-245
   ST_HLLC_VSTAR = 8u,      // 16_hllc_flow_mpx.f95:4294,4605
-  ST_NONFINITE = 16u,
+  ST_NONFINITE = 16u,      // con2prim returned NaN / Inf
+  ST_HLLE_SPEED = 32u,     // 16_hlle_flow_mpx.f95:2796-2803, 2974-2981
 };
 
 // ---- per-instance descriptor (one grid of the ensemble) -------------------

@@ -1,77 +1,11 @@
-// cueva_kernels.cu -- sm_100a kernels of the CUEVA per-step hot path.
-//
-// One RK stage = two launches:
-//  k_yface  one thread per y interface (i, j+1/2), stencils staged in shared
-//           memory: MP5/7/9 reconstruction of the 20 y slots plus the x
-//           velocities at (i, j) that the reference's superluminal fix-up
-//           couples in, then the HLL / HLLC flux; 14 fluxes to a scratch slab;
-//  k_xupd   one thread per x interface (i+1/2, j), same staging, plus the
-//           y densities for the HLLC density fix-up chain; the x flux of the
-//           neighbour interface arrives by warp shuffle, so each thread then
-//           updates its point: flux divergence and sources
-//           (17_fluxandsource.f95:441-635) and a fused pointwise epilogue --
-//           sumfin, the next stage's sumint / varint / electricvarint /
-//           flowinit, or, after the last stage, varfin / electricfield,
-//           con2prim and the next step's startconvar.
-// The reference computes both faces of a point in one loop iteration
-// (16_hll_flow_mpx.f95:1358-1965); splitting the directions keeps one
-// direction's state per thread (register pressure, occupancy) at the cost of
-// the 14-double y-flux round trip through L2/HBM.
-#include <cuda_runtime.h>
-#include <math_constants.h>
-
-#include "cueva_common.cuh"
-#include "cueva_mp.cuh"
-#include "cueva_riemann.cuh"
-#include "cueva_point.cuh"
-#include "cueva_mlp.cuh"
+// cueva_kernels.cu -- pointwise kernels of the CUEVA hot path (begin of
+// step, routine mirrors) and the dispatch of the stage launches to the
+// per-solver translation units (cueva_stage_{hll,hllc,hlle}.cu; the stage
+// kernels themselves are described in cueva_stage.cuh).
+#include "cueva_launch.h"
+#include "cueva_stage.cuh"
 
 namespace cueva {
-
-// ------------------------------------------------------------------ helpers
-template <typename T>
-__device__ __forceinline__ T ldT(const double* p) { return T(__ldg(p)); }
-
-// begin-of-step work for one interior point: startconvar of the new prims,
-// stage-1 state Q_1 = U + dt*0 (cleanvarint zeroed intsum), its implicit E
-// and current J (06_conserved_var.f95, 10_varint.f95, 11_elecvarint.f95,
-// 14_flowinit.f95 for l = 1)
-__device__ __forceinline__ void begin_step_point(const InstDesc& I, double abt11, double* auxo, double* Qo,
-                                                 long long pc, const double* pv) {
-  const long long fs = I.fstride;
-  const Cons c = startconvar(pv[P_RHO], pv[P_P], pv[P_VX], pv[P_VY], pv[P_VZ], pv[P_EX], pv[P_EY], pv[P_EZ],
-                             pv[P_BX], pv[P_BY], pv[P_BZ], I.gamma);
-  auxo[A_D * fs + pc] = c.D;
-  auxo[A_TAU * fs + pc] = c.tau;
-  auxo[A_SX * fs + pc] = c.Sx;
-  auxo[A_SY * fs + pc] = c.Sy;
-  auxo[A_SZ * fs + pc] = c.Sz;
-  auxo[A_W * fs + pc] = c.W;
-  const double z = I.dt * 0.0;
-  const double Bx = pv[P_BX] + z, By = pv[P_BY] + z, Bz = pv[P_BZ] + z, q = pv[P_Q] + z;
-  double Ex, Ey, Ez;
-  implicit_e(abt11, I.sigma, I.dt, c.W, pv[P_VX], pv[P_VY], pv[P_VZ], Bx, By, Bz, pv[P_EX] + z, pv[P_EY] + z,
-             pv[P_EZ] + z, Ex, Ey, Ez);
-  double Jx, Jy, Jz;
-  current(I.sigma, c.W, pv[P_VX], pv[P_VY], pv[P_VZ], Ex, Ey, Ez, Bx, By, Bz, q, Jx, Jy, Jz);
-  Qo[Q_PSI * fs + pc] = pv[P_PSI] + z;
-  Qo[Q_PHI * fs + pc] = pv[P_PHI] + z;
-  Qo[Q_EX * fs + pc] = Ex;
-  Qo[Q_EY * fs + pc] = Ey;
-  Qo[Q_EZ * fs + pc] = Ez;
-  Qo[Q_BX * fs + pc] = Bx;
-  Qo[Q_BY * fs + pc] = By;
-  Qo[Q_BZ * fs + pc] = Bz;
-  Qo[Q_Q * fs + pc] = q;
-  Qo[Q_D * fs + pc] = c.D + z;
-  Qo[Q_TAU * fs + pc] = c.tau + z;
-  Qo[Q_SX * fs + pc] = c.Sx + z;
-  Qo[Q_SY * fs + pc] = c.Sy + z;
-  Qo[Q_SZ * fs + pc] = c.Sz + z;
-  Qo[Q_JX * fs + pc] = Jx;
-  Qo[Q_JY * fs + pc] = Jy;
-  Qo[Q_JZ * fs + pc] = Jz;
-}
 
 // ------------------------------------------------------------ prologue
 // startconvar + stage-1 state for the prims in prim[cur]
@@ -139,20 +73,6 @@ __global__ void k_electricvarint(const InstDesc* __restrict__ insts, int cur, in
 
 // con2prim with l_swap = 1: the evolved D, tau, S in aux[cur] and E, B in
 // prim[cur]; seeds v, rho, p are the prims in prim[cur]; result overwrites prim[cur]
-// The reference lets NaN states pass silently (its comparisons are false on
-// NaN); a non-finite recovered state is reported as ST_NONFINITE here.
-// count == false: a lane that only keeps its warp converged (no counters);
-// full_warp: all 32 lanes of the warp make this call
-__device__ __forceinline__ uint32_t c2p_dispatch(const InstDesc& I, const C2PIn& in, C2POut& o, bool count = true,
-                                                 bool full_warp = false) {
-  uint32_t st;
-  if (I.c2p == 1) st = c2p_cardano(in, I.gamma, I.eps1_c2p, o, count ? I.counters : nullptr);
-  else if (I.c2p == 0) st = c2p_nr(in, I.gamma, o);
-  else st = c2p_learned(in, I.gamma, I.eps1_c2p, I.mlp, o, I.counters, count, full_warp);
-  if (!(isfinite(o.rho) && isfinite(o.p) && isfinite(o.vx) && isfinite(o.vy) && isfinite(o.vz))) st |= ST_NONFINITE;
-  return st;
-}
-
 __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
   const InstDesc& I = insts[blockIdx.y];
   const int nx = I.imax + 1, ny = I.jmax + 1;
@@ -176,570 +96,24 @@ __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
   if (st) atomicOr(I.status, st);
 }
 
-// ------------------------------------------------------------ face tiles
-// A CTA covers 32 interfaces along the row times FACE_ROWS rows.  Every
-// value its stencils read is first copied into shared memory with cp.async
-// (all copies in flight at once, one wait), so the reconstruction and the
-// Riemann solve run from shared memory without global-load latency.
-//   x faces (D = 0): i = i0+lane, j = j0+warp;  y faces (D = 1): i = i0+lane,
-//   j = j0+warp; face "i" is the interface i+1/2 (x) or j+1/2 (y).
-// Staged regions:
-//   normal:     NF_FACE fields x FACE_ROWS rows x (32 + 2R + 1) cells along
-//               x (D = 0), or NF_FACE fields x (FACE_ROWS + 2R + 1) rows x 32
-//               columns (D = 1);
-//   transverse: the NC velocity (+ density) fields the fix-ups couple in,
-//               along the other direction through the face's cell.
-__device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-// L2 prefetch of the n doubles at p, widened to 16-byte boundaries (which
-// stay inside the 256-byte-aligned row the doubles belong to)
-__device__ __forceinline__ void prefetch_l2(const double* p, int n) {
-  const unsigned long long a = (unsigned long long)p & ~15ull;
-  const unsigned long long e = ((unsigned long long)(p + n) + 15ull) & ~15ull;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
-}
-
-constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
-
-template <int RM, int SOLVER, int ROWS>
-struct FaceGeom {
-  static constexpr int R = MPR<RM>::R;
-  static constexpr int NS = 2 * R + 2;                 // stencil points
-  static constexpr int LONG = 32 + 2 * R + 1;          // staged cells along a 32-face segment
-  static constexpr int DEEP = ROWS + 2 * R + 1;        // staged rows across ROWS faces
-  static constexpr int NC = (SOLVER == 7) ? 4 : 3;     // coupled fields: v (+ rho for HLLC)
-  // D = 0: normal [row][f][LONG], transverse [f][DEEP][32]
-  // D = 1: normal [f][DEEP][32],  transverse [row][f][LONG]
-  static constexpr int NORMAL0 = ROWS * NF_FACE * LONG;
-  static constexpr int NORMAL1 = NF_FACE * DEEP * 32;
-  static constexpr int TRANS0 = NC * DEEP * 32;
-  static constexpr int TRANS1 = ROWS * NC * LONG;
-  static constexpr __host__ __device__ int normal(int D) { return D == 0 ? NORMAL0 : NORMAL1; }
-  static constexpr size_t bytes(int D) {
-    return sizeof(double) * (size_t)(D == 0 ? NORMAL0 + TRANS0 : NORMAL1 + TRANS1);
-  }
-  // staged offset of field f at the face's stencil point q (normal) and of
-  // coupled field f at stencil point q through the face's cell (transverse)
-  template <int D> static __device__ __forceinline__ int nrm(int f, int q, int w, int lane) {
-    return D == 0 ? (w * NF_FACE + f) * LONG + lane + q : (f * DEEP + w + q) * 32 + lane;
-  }
-  template <int D> static __device__ __forceinline__ int trn(int f, int q, int w, int lane) {
-    return D == 0 ? (f * DEEP + w + q) * 32 + lane : (w * NC + f) * LONG + lane + q;
-  }
-};
-
-// staged field f: 0-4 primitive slots (vx, vy, vz, p, rho) of time n, 5-18
-// the stage's conserved psi..Sz, 19 the current along the normal
-template <int D>
-__device__ __forceinline__ const double* face_field(const double* prim, const double* Q, long long fs, int f) {
-  if (f < 5) {
-    const int pf = (f < 3) ? P_VX + f : (f == 3 ? P_P : P_RHO);
-    return prim + (long long)pf * fs;
-  }
-  const int qf = (f < 19) ? f - 5 : (D == 0 ? Q_JX : Q_JY);
-  return Q + (long long)qf * fs;
-}
-
-// issue the cp.async copies of one tile (first face i0, j0; last ilast, jlast);
-// cells reaching beyond the last face are not copied
-template <int RM, int SOLVER, int D, int ROWS>
-__device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& sa, double* sn, double* st, int i0,
-                                           int j0, int ilast, int jlast, int tid) {
-  using G = FaceGeom<RM, SOLVER, ROWS>;
-  constexpr int R = G::R, LONG = G::LONG, DEEP = G::DEEP, NC = G::NC;
-  const int imax = I.imax, jmax = I.jmax, pitch = I.pitch, bcx = I.bc_x, bcy = I.bc_y;
-  const long long fs = I.fstride;
-  const double* __restrict__ prim = I.prim[sa.cur];
-  const double* __restrict__ Q = I.stage[sa.qin];
-  auto cfield = [&](int c) -> const double* { return prim + (long long)(c < 3 ? P_VX + c : P_RHO) * fs; };
-  const int ncell = ilast + R + 1 - (i0 - R) + 1;   // x cells i0-R .. ilast+R+1
-  const int nrow = jlast + R + 1 - (j0 - R) + 1;    // y rows j0-R .. jlast+R+1
-  // rows j0..jlast, cells along x: the normal stencils (D = 0) or the coupled ones (D = 1)
-  for (int e = tid; e < ROWS * LONG; e += 32 * ROWS) {
-    const int r = e / LONG, c = e - r * LONG;
-    if (j0 + r > jlast || c >= ncell) continue;
-    const long long off = (long long)map_idx(j0 + r, jmax, bcy) * pitch + map_idx(i0 - R + c, imax, bcx);
-    if constexpr (D == 0) {
-#pragma unroll
-      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (r * NF_FACE + f) * LONG + c, face_field<D>(prim, Q, fs, f) + off);
-    } else {
-#pragma unroll
-      for (int f = 0; f < NC; ++f) cp_async8(st + (r * NC + f) * LONG + c, cfield(f) + off);
-    }
-  }
-  // columns i0..ilast, rows along y: the coupled stencils (D = 0) or the normal ones (D = 1)
-  for (int e = tid; e < DEEP * 32; e += 32 * ROWS) {
-    const int r = e >> 5, c = e & 31;
-    if (r >= nrow || i0 + c > ilast) continue;
-    const long long off = (long long)map_idx(j0 - R + r, jmax, bcy) * pitch + map_idx(i0 + c, imax, bcx);
-    if constexpr (D == 0) {
-#pragma unroll
-      for (int f = 0; f < NC; ++f) cp_async8(st + (f * DEEP + r) * 32 + c, cfield(f) + off);
-    } else {
-#pragma unroll
-      for (int f = 0; f < NF_FACE; ++f) cp_async8(sn + (f * DEEP + r) * 32 + c, face_field<D>(prim, Q, fs, f) + off);
-    }
-  }
-}
-
-// flux of the face of (w, lane) from the staged tile (16_hll_flow_mpx.f95 /
-// 16_hllc_flow_mpx.f95 for one interface); returns status bits
-template <int RM, int SOLVER, typename T, int D, int ROWS>
-__device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
-                                              T (&F)[NROLE]) {
-  using G = FaceGeom<RM, SOLVER, ROWS>;
-  constexpr int R = G::R, NS = G::NS;
-  auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
-  auto nrm = [&](int f, int q) -> T { return T(nrmd(f, q)); };
-  auto trn = [&](int f, int q) -> T { return T(st[G::template trn<D>(f, q, w, lane)]); };
-  auto rec = [&](int f, T& L, T& Rv) {
-    T u[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) u[q] = nrm(f, q);
-    const Pair<T> p = MPCall<RM, T>::template call<false>(u);
-    L = p.L; Rv = p.R;
-  };
-  auto recp = [&](int f, T& L, T& Rv) {
-    T u[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) u[q] = nrm(f, q);
-    const Pair<T> p = MPCall<RM, T>::template call<true>(u);
-    L = p.L; Rv = p.R;
-  };
-  auto rect = [&](int f, bool pos, T& L, T& Rv) {
-    T u[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) u[q] = trn(f, q);
-    const Pair<T> p = pos ? MPCall<RM, T>::template call<true>(u) : MPCall<RM, T>::template call<false>(u);
-    L = p.L; Rv = p.R;
-  };
-
-  uint32_t stt = 0;
-  Side<T> L, Rs;
-  // primitive slots of this direction (21-25 for x, 58-62 for y)
-  rec(0, L.vx, Rs.vx);
-  rec(1, L.vy, Rs.vy);
-  rec(2, L.vz, Rs.vz);
-  recp(3, L.p, Rs.p);
-  recp(4, L.rho, Rs.rho);
-  if constexpr (SOLVER == 5 || SOLVER == 7) {
-    // superluminal fall-back, 16_hll_flow_mpx.f95:1393-1462: the x and y
-    // reconstructions of the point fall back together if either is
-    // superluminal; left states take cell (i,j), right states cell i-1 (x)
-    // or j-1 (y), as in the reference
-    T ovx, ovy, ovz, wvx, wvy, wvz;
-    rect(0, false, ovx, wvx);
-    rect(1, false, ovy, wvy);
-    rect(2, false, ovz, wvz);
-    const T V2l = pw2(L.vx) + pw2(L.vy) + pw2(L.vz);
-    const T V2r = pw2(Rs.vx) + pw2(Rs.vy) + pw2(Rs.vz);
-    const T V2ol = pw2(ovx) + pw2(ovy) + pw2(ovz);
-    const T V2or = pw2(wvx) + pw2(wvy) + pw2(wvz);
-    if (V2l >= T(1) || V2r >= T(1) || V2ol >= T(1) || V2or >= T(1)) {
-      // cell (i, j) is stencil point R of the normal stencil; i-1 / j-1 is R-1
-      L.vx = nrm(0, R); L.vy = nrm(1, R); L.vz = nrm(2, R);
-      Rs.vx = nrm(0, R - 1); Rs.vy = nrm(1, R - 1); Rs.vz = nrm(2, R - 1);
-    }
-  }
-  if constexpr (SOLVER == 7) {
-    // density fix-up chain, 16_hllc_flow_mpx.f95:2663-2690: the first
-    // negative of (yL, yR, xL, xR) becomes 0.1 rho(i,j); an x side is only
-    // fixed when neither y side is negative
-    if (L.rho < T(0) || Rs.rho < T(0)) {
-      bool other_neg = false;
-      if (D == 0) {
-        T oL, oR;
-        rect(3, true, oL, oR);
-        other_neg = (oL < T(0)) || (oR < T(0));
-      }
-      if (!other_neg) {
-        const T r10 = T(nrmd(4, R) * 1.0e-1);
-        if (L.rho < T(0)) L.rho = r10;
-        else Rs.rho = r10;
-      }
-    }
-  }
-  rec(5 + Q_PSI, L.psi, Rs.psi);
-  rec(5 + Q_PHI, L.phi, Rs.phi);
-  rec(5 + Q_EX, L.Ex, Rs.Ex);
-  rec(5 + Q_EY, L.Ey, Rs.Ey);
-  rec(5 + Q_EZ, L.Ez, Rs.Ez);
-  rec(5 + Q_BX, L.Bx, Rs.Bx);
-  rec(5 + Q_BY, L.By, Rs.By);
-  rec(5 + Q_BZ, L.Bz, Rs.Bz);
-  rec(5 + Q_Q, L.q, Rs.q);
-  rec(5 + Q_D, L.D, Rs.D);
-  rec(5 + Q_TAU, L.tau, Rs.tau);
-  rec(5 + Q_SX, L.Sx, Rs.Sx);
-  rec(5 + Q_SY, L.Sy, Rs.Sy);
-  rec(5 + Q_SZ, L.Sz, Rs.Sz);
-  rec(19, L.J, Rs.J);
-  const T gamma = T(gamma_d);
-  if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, F);
-  else hllc_fluxes<D>(L, Rs, gamma, F, stt);
-  return stt;
-}
-
-__device__ __forceinline__ const InstDesc& tile_inst(const InstDesc* __restrict__ insts, int ninst, int kind, int& b) {
-  int k = 0;
-  for (int t = 1; t < ninst; ++t)
-    if (insts[t].block_begin[kind] <= b) k = t;
-  b -= insts[k].block_begin[kind];
-  return insts[k];
-}
-
-// Tile loop: CTA b handles tiles b, b + gridDim.x, ... of the launch (ntiles
-// over all instances), so a grid of one CTA per tile and a persistent grid
-// of a few CTAs per SM run the same code.
-
-// y faces: 32 columns x ROWS face rows j = j0-1+warp in [-1, jmax]; writes
-// Fy(i, j+1/2) to the flux scratch
-template <int RM, int SOLVER, typename T, int ROWS>
-__global__ void __launch_bounds__(32 * ROWS, 16 / ROWS)
-k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) {
-  using G = FaceGeom<RM, SOLVER, ROWS>;
-  extern __shared__ double smem[];
-  const int lane = threadIdx.x, w = threadIdx.y;
-  double* sn = smem;
-  double* st = smem + G::normal(1);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int b = tile;
-    const InstDesc& I = tile_inst(insts, ninst, LK_YFACE, b);
-    const int bpr = (I.imax + 1 + 31) / 32;
-    const int i0 = (b % bpr) * 32, j0 = (b / bpr) * ROWS - 1;
-    const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + ROWS - 1, I.jmax);
-    stage_tile<RM, SOLVER, 1, ROWS>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
-    cp_async_wait_all();
-    __syncthreads();
-    const int i = i0 + lane, j = j0 + w;
-    if (i <= ilast && j <= jlast) {
-      T F[NROLE];
-      const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, F);
-      const long long fo = (long long)(j + 1) * I.fpitch + i;
-#pragma unroll
-      for (int c = 0; c < NROLE; ++c) I.fy[c * I.ffs + fo] = double(F[c]);
-      if (stt) atomicOr(I.status, stt);
-    }
-    __syncthreads();   // the next tile's copies overwrite the staged values
-  }
-}
-
-// ------------------------------------------------- x faces + point update
-// EP selects the epilogue: EP_RHS stores the stage right-hand side only (the
-// routine mirror), EP_MID prepares stage l+1, EP_LAST finishes the step.
-enum Epilogue { EP_RHS = 0, EP_MID = 1, EP_LAST = 2 };
-
-// centre values of stage l (psi, phi, E, B, q) and time n (v) of a point
-struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
-
-// flux divergence + sources of point (i, j) (17_fluxandsource.f95:441-635)
-// and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
-// valid == false (EP_LAST only): the lane computes a copy of a real point so
-// that its warp reaches con2prim converged, and stores nothing
-template <int EP>
-__device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
-                                                 const double (&qx)[NROLE], const Centre& cv, bool valid = true) {
-  const int pitch = I.pitch;
-  const long long fs = I.fstride;
-  const double* __restrict__ prim = I.prim[sa.cur];
-  const double* __restrict__ aux = I.aux[sa.cur];
-  uint32_t st = 0;
-  const long long pc = (long long)j * pitch + i;
-  const long long fyo = (long long)(j + 1) * I.fpitch + i;      // Fy(i, j+1/2); Fy(i, j-1/2) at -fpitch
-  const double* __restrict__ fy = I.fy;
-  const double dly = I.dely, iy2 = I.inv_dely_pow2;
-  auto qy = [&](int r) {   // (dy)/dly
-    const double d = fy[r * I.ffs + fyo] - fy[r * I.ffs + fyo - I.fpitch];
-    return iy2 != 0.0 ? d * iy2 : d / dly;
-  };
-  auto qxf = [&](int r) { return qx[r]; };
-  const double q = cv.q, psi = cv.psi, phi = cv.phi, Ex = cv.Ex, Ey = cv.Ey, Ez = cv.Ez;
-  const double Bx = cv.Bx, By = cv.By, Bz = cv.Bz, vx = cv.vx, vy = cv.vy, vz = cv.vz;
-  const double W = aux[A_W * fs + pc];
-  double K[NRHS];
-  // 17_fluxandsource.f95:488-598; z differences are (X - X)/Delz = 0
-  // (-a)/d == -(a/d) exactly, so every term is -/+ the quotient of a difference
-  K[Q_PSI] = -qxf(R_PSI) - qy(R_PSI) + q - I.kappa_psi * psi;
-  K[Q_PHI] = -qxf(R_PHI) - qy(R_PHI) - I.kappa_phi * phi;
-  K[Q_BX] = -qy(R_BT2) + 0.0 - qxf(R_BN);
-  K[Q_BY] = qxf(R_BT1) - qy(R_BN);
-  K[Q_BZ] = -qxf(R_BT2) + qy(R_BT1);
-  K[Q_EX] = qy(R_ET2) - qxf(R_EN) - q * vx;
-  K[Q_EY] = 0.0 - qxf(R_ET1) - qy(R_EN) - q * vy;
-  K[Q_EZ] = qxf(R_ET2) - qy(R_ET1) - q * vz;
-  K[Q_Q] = -qxf(R_Q) - qy(R_Q);
-  K[Q_D] = -qxf(R_D) - qy(R_D);
-  K[Q_TAU] = -qxf(R_TAU) - qy(R_TAU);
-  K[Q_SX] = -qxf(R_SN) - qy(R_ST2);
-  K[Q_SY] = -qxf(R_ST1) - qy(R_SN);
-  K[Q_SZ] = -qxf(R_ST2) - qy(R_ST1);
-  stiff_source(I.sigma, W, vx, vy, vz, Ex, Ey, Ez, Bx, By, Bz, K[K_SEX], K[K_SEY], K[K_SEZ]);
-
-  if constexpr (EP == EP_RHS) {
-#pragma unroll
-    for (int c = 0; c < NRHS; ++c) I.rhs_out[c * fs + pc] = K[c];
-  } else {
-    // sumfin, 18_sumfin.f95:20-66
-    double fin[NCONS];
-#pragma unroll
-    for (int c = 0; c < NCONS; ++c) {
-      const double prev = (sa.l == 1) ? 0.0 : I.finsum[c * fs + pc];
-      if (c >= Q_EX && c <= Q_EZ) fin[c] = prev + (sa.wb * K[c] - sa.wbt * K[K_SEX + (c - Q_EX)]);
-      else fin[c] = prev + sa.wb * K[c];
-    }
-    // time-n conserved state U^n (prims for psi, phi, E, B, q; startconvar for D, tau, S)
-    double U[NCONS];
-    U[Q_PSI] = prim[P_PSI * fs + pc]; U[Q_PHI] = prim[P_PHI * fs + pc];
-    U[Q_EX] = prim[P_EX * fs + pc]; U[Q_EY] = prim[P_EY * fs + pc]; U[Q_EZ] = prim[P_EZ * fs + pc];
-    U[Q_BX] = prim[P_BX * fs + pc]; U[Q_BY] = prim[P_BY * fs + pc]; U[Q_BZ] = prim[P_BZ * fs + pc];
-    U[Q_Q] = prim[P_Q * fs + pc];
-    U[Q_D] = aux[A_D * fs + pc]; U[Q_TAU] = aux[A_TAU * fs + pc];
-    U[Q_SX] = aux[A_SX * fs + pc]; U[Q_SY] = aux[A_SY * fs + pc]; U[Q_SZ] = aux[A_SZ * fs + pc];
-    if constexpr (EP == EP_MID) {
-#pragma unroll
-      for (int c = 0; c < NCONS; ++c) I.finsum[c * fs + pc] = fin[c];
-      // sumint for stage l+1 (09_sumint.f95:18-67); intsum is zeroed only
-      // once per step (07_clean_var.f95), so it accumulates across stages
-      double acc[NCONS];
-#pragma unroll
-      for (int c = 0; c < NCONS; ++c) acc[c] = sa.need_intsum_load ? I.intsum[c * fs + pc] : 0.0;
-      for (int m = 1; m <= sa.l; ++m) {
-        const double ab = sa.ab_next[m - 1], abt = sa.abt_next[m - 1];
-        if (ab == 0.0 && abt == 0.0) continue;
-        const double* Km = (m < sa.l) ? I.kbuf + (long long)sa.kslot[m - 1] * NRHS * fs : nullptr;
-#pragma unroll
-        for (int c = 0; c < NCONS; ++c) {
-          const double F = Km ? Km[c * fs + pc] : K[c];
-          if (c >= Q_EX && c <= Q_EZ) {
-            const double S = Km ? Km[(K_SEX + c - Q_EX) * fs + pc] : K[K_SEX + c - Q_EX];
-            acc[c] = acc[c] + (ab * F - abt * S);
-          } else {
-            acc[c] = acc[c] + ab * F;
-          }
-        }
-      }
-      if (sa.need_intsum_store) {
-#pragma unroll
-        for (int c = 0; c < NCONS; ++c) I.intsum[c * fs + pc] = acc[c];
-      }
-      if (sa.store_k_slot >= 0) {
-        double* Ko = I.kbuf + (long long)sa.store_k_slot * NRHS * fs;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) Ko[c * fs + pc] = K[c];
-      }
-      // varint (10_varint.f95:23-63), electricvarint and flowinit of stage l+1
-      double Qn[NCONS];
-#pragma unroll
-      for (int c = 0; c < NCONS; ++c) Qn[c] = U[c] + I.dt * acc[c];
-      double Exn, Eyn, Ezn, Jx, Jy, Jz;
-      implicit_e(sa.abt_diag_next, I.sigma, I.dt, W, vx, vy, vz, Qn[Q_BX], Qn[Q_BY], Qn[Q_BZ], Qn[Q_EX],
-                 Qn[Q_EY], Qn[Q_EZ], Exn, Eyn, Ezn);
-      Qn[Q_EX] = Exn; Qn[Q_EY] = Eyn; Qn[Q_EZ] = Ezn;
-      current(I.sigma, W, vx, vy, vz, Exn, Eyn, Ezn, Qn[Q_BX], Qn[Q_BY], Qn[Q_BZ], Qn[Q_Q], Jx, Jy, Jz);
-      double* Qo = I.stage[1 - sa.qin];
-#pragma unroll
-      for (int c = 0; c < NCONS; ++c) Qo[c * fs + pc] = Qn[c];
-      Qo[Q_JX * fs + pc] = Jx; Qo[Q_JY * fs + pc] = Jy; Qo[Q_JZ * fs + pc] = Jz;
-    } else {
-      // varfin + electricfield (19_varfin.f95:39-51, 20_electricfield.f95:157-161)
-      double Un[NCONS];
-#pragma unroll
-      for (int c = 0; c < NCONS; ++c) Un[c] = U[c] + I.dt * fin[c];
-      // con2prim, l_swap = 1 (main_cueva_code.f95:312-326)
-      C2PIn in{Un[Q_D], Un[Q_TAU], Un[Q_SX], Un[Q_SY], Un[Q_SZ], Un[Q_EX], Un[Q_EY], Un[Q_EZ],
-               Un[Q_BX], Un[Q_BY], Un[Q_BZ], vx, vy, vz, prim[P_RHO * fs + pc], prim[P_P * fs + pc]};
-      C2POut o;
-      st |= c2p_dispatch(I, in, o, valid, I.c2p == 2);   // k_xupd sends whole warps for c2p = 2
-      if (!valid) return 0u;
-      double pv[NPRIM];
-      pv[P_RHO] = o.rho; pv[P_P] = o.p; pv[P_VX] = o.vx; pv[P_VY] = o.vy; pv[P_VZ] = o.vz;
-      pv[P_PSI] = Un[Q_PSI]; pv[P_PHI] = Un[Q_PHI];
-      pv[P_EX] = Un[Q_EX]; pv[P_EY] = Un[Q_EY]; pv[P_EZ] = Un[Q_EZ];
-      pv[P_BX] = Un[Q_BX]; pv[P_BY] = Un[Q_BY]; pv[P_BZ] = Un[Q_BZ]; pv[P_Q] = Un[Q_Q];
-      double* po = I.prim[1 - sa.cur];
-#pragma unroll
-      for (int c = 0; c < NPRIM; ++c) po[c * fs + pc] = pv[c];
-      begin_step_point(I, sa.abt_diag_first, I.aux[1 - sa.cur], I.stage[1 - sa.qin], pc, pv);
-    }
-  }
-  return st;
-}
-
-template <int RM, int SOLVER, typename T, int EP, int ROWS>
-__device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa, int b, double* sn, double* st) {
-  using G = FaceGeom<RM, SOLVER, ROWS>;
-  constexpr int R = G::R, LONG = G::LONG;
-  const int lane = threadIdx.x, w = threadIdx.y;
-  // a tile updates 31 points per row: faces i0 .. i0+31 (i0 = first point - 1)
-  const int bpr = (I.imax + 1 + 30) / 31;
-  const int i0 = (b % bpr) * 31 - 1, j0 = (b / bpr) * ROWS;
-  const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + ROWS - 1, I.jmax);
-  stage_tile<RM, SOLVER, 0, ROWS>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
-  if constexpr (EP != EP_RHS) {
-    // the update's other inputs go to L2 while the faces are computed: per
-    // row of the tile, the 6 aux and 9 time-n primitive fields, finsum and
-    // intsum when loaded, stored stage right-hand sides, and the y fluxes
-    const long long fs = I.fstride;
-    const int npt = ilast - i0, nr = jlast - j0 + 1;
-    const int nfin = (sa.l > 1) ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
-    int nk = 0;
-    for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
-    const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;   // fields read at the point
-    const int total = ncen * nr + NROLE * (nr + 1);
-    for (int e = w * 32 + lane; e < total && npt > 0; e += 32 * ROWS) {
-      if (e < ncen * nr) {
-        const int r = e % nr;
-        int f = e / nr;
-        const double* base;
-        if (f < NAUX) base = I.aux[sa.cur] + f * fs;
-        else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
-        else if ((f -= 9) < nfin) base = I.finsum + f * fs;
-        else if ((f -= nfin) < nint) base = I.intsum + f * fs;
-        else {
-          f -= nint;
-          int kk = f / NRHS, m = 1;
-          for (; m < sa.l; ++m)
-            if (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0) && kk-- == 0) break;
-          base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + f % NRHS) * fs;
-        }
-        prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
-      } else {
-        const int e2 = e - ncen * nr, r = e2 % (nr + 1), c = e2 / (nr + 1);
-        prefetch_l2(I.fy + c * I.ffs + (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
-      }
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int i = i0 + lane, j = j0 + w;
-  if (j > jlast) return;   // whole warp; the caller synchronises before the next tile
-  T F[NROLE];
-#pragma unroll
-  for (int c = 0; c < NROLE; ++c) F[c] = T(0);
-  uint32_t stt = 0;
-  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, F);
-  // Fx(i-1/2) of point i is the face of lane-1
-  const double dlx = I.delx, ix2 = I.inv_delx_pow2;
-  double qx[NROLE];
-#pragma unroll
-  for (int c = 0; c < NROLE; ++c) {
-    const double fr = double(F[c]);
-    const double fl = __shfl_up_sync(0xffffffffu, fr, 1);
-    const double d = fr - fl;
-    qx[c] = ix2 != 0.0 ? d * ix2 : d / dlx;
-  }
-  const bool valid = lane >= 1 && i <= ilast;
-  // after the last stage every lane of the warp enters the update (lanes
-  // without a point repeat a real one and store nothing), so con2prim runs
-  // converged; earlier stages update the real points only
-  if (valid || (EP == EP_LAST && I.c2p == 2)) {
-    const int ii = valid ? i : (lane == 0 ? i0 + 1 : ilast);
-    const int ln = ii - i0;   // staged cell ii is stencil point R of lane ln's face
-    if (EP == EP_LAST && I.c2p == 2) {
-      // a lane without a point takes the divergence of the point it repeats
-#pragma unroll
-      for (int c = 0; c < NROLE; ++c) qx[c] = __shfl_sync(0xffffffffu, qx[c], ln);
-    }
-    auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + ln + R]; };
-    const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
-                    cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
-    stt |= update_point<EP>(I, sa, ii, j, qx, cv, valid);
-  }
-  if (stt) atomicOr(I.status, stt);
-}
-
-template <int RM, int SOLVER, typename T, int EP, int ROWS>
-__global__ void __launch_bounds__(32 * ROWS, 16 / ROWS)
-k_xupd(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) {
-  using G = FaceGeom<RM, SOLVER, ROWS>;
-  extern __shared__ double smem[];
-  double* sn = smem;
-  double* st = smem + G::normal(0);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int b = tile;
-    const InstDesc& I = tile_inst(insts, ninst, LK_XUPD, b);
-    xupd_tile<RM, SOLVER, T, EP, ROWS>(I, sa, b, sn, st);
-    __syncthreads();   // the next tile's copies overwrite the staged values
-  }
-}
-
-// ---------------------------------------------------------------- launchers
-template <int RM, int SV, typename T, int ROWS>
-static void launch_tiles(const StageShape& sh, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
-                         cudaEvent_t* ev) {
-  using G = FaceGeom<RM, SV, ROWS>;
-  const dim3 blk(32, ROWS);
-  if (ev) cudaEventRecord(ev[0], st);
-  k_yface<RM, SV, T, ROWS><<<sh.grid[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sh.ntiles[LK_YFACE], sa);
-  if (ev) cudaEventRecord(ev[1], st);
-  const int gx = sh.grid[LK_XUPD], nt = sh.ntiles[LK_XUPD];
-  if (sa.mode == 1) k_xupd<RM, SV, T, EP_RHS, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
-  else if (sa.l < sa.s) k_xupd<RM, SV, T, EP_MID, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
-  else k_xupd<RM, SV, T, EP_LAST, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
-  if (ev) cudaEventRecord(ev[2], st);
-}
-
-template <int RM, int SV, typename T, int ROWS>
-static cudaError_t prepare_tiles() {
-  using G = FaceGeom<RM, SV, ROWS>;
-  const int b0 = (int)G::bytes(0), b1 = (int)G::bytes(1);
-  cudaError_t e = cudaFuncSetAttribute(k_yface<RM, SV, T, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b1);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_RHS, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_MID, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_LAST, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
-  return e;
-}
-
-template <int RM, int SV>
-static void launch_rm_sv(int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                         const StageArgs& sa, cudaEvent_t* ev) {
-  if (prec == 0) {
-    if (sh.rows == 4) launch_tiles<RM, SV, double, 4>(sh, st, d, n, sa, ev);
-    else launch_tiles<RM, SV, double, 8>(sh, st, d, n, sa, ev);
-  } else {
-    if (sh.rows == 4) launch_tiles<RM, SV, float, 4>(sh, st, d, n, sa, ev);
-    else launch_tiles<RM, SV, float, 8>(sh, st, d, n, sa, ev);
-  }
-}
-
-template <int RM, int SV>
-static cudaError_t prepare_rm_sv(int prec) {
-  cudaError_t e = prec == 0 ? prepare_tiles<RM, SV, double, 8>() : prepare_tiles<RM, SV, float, 8>();
-  if (e == cudaSuccess) e = prec == 0 ? prepare_tiles<RM, SV, double, 4>() : prepare_tiles<RM, SV, float, 4>();
-  return e;
-}
-
+// ------------------------------------------------------------- dispatch
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
-  switch (rec_mp * 10 + (solver == 7 ? 1 : 0)) {
-    case 0: return prepare_rm_sv<0, 5>(prec);
-    case 1: return prepare_rm_sv<0, 7>(prec);
-    case 10: return prepare_rm_sv<1, 5>(prec);
-    case 11: return prepare_rm_sv<1, 7>(prec);
-    case 20: return prepare_rm_sv<2, 5>(prec);
-    case 21: return prepare_rm_sv<2, 7>(prec);
+  switch (solver) {
+    case 5: return prepare_stage_hll(rec_mp, prec);
+    case 6: return prepare_stage_hlle(rec_mp, prec);
+    case 7: return prepare_stage_hllc(rec_mp, prec);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev) {
-  if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
-  switch (rec_mp * 10 + (solver == 7 ? 1 : 0)) {
-    case 0: launch_rm_sv<0, 5>(prec, sh, st, d, n, sa, ev); break;
-    case 1: launch_rm_sv<0, 7>(prec, sh, st, d, n, sa, ev); break;
-    case 10: launch_rm_sv<1, 5>(prec, sh, st, d, n, sa, ev); break;
-    case 11: launch_rm_sv<1, 7>(prec, sh, st, d, n, sa, ev); break;
-    case 20: launch_rm_sv<2, 5>(prec, sh, st, d, n, sa, ev); break;
-    case 21: launch_rm_sv<2, 7>(prec, sh, st, d, n, sa, ev); break;
+  switch (solver) {
+    case 5: return launch_stage_hll(rec_mp, prec, sh, st, d, n, sa, ev);
+    case 6: return launch_stage_hlle(rec_mp, prec, sh, st, d, n, sa, ev);
+    case 7: return launch_stage_hllc(rec_mp, prec, sh, st, d, n, sa, ev);
     default: return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
 }
 
 static dim3 point_grid(long long npts, int ninst) {
@@ -769,3 +143,4 @@ cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, 
 }
 
 }  // namespace cueva
+

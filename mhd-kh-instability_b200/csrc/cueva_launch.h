@@ -17,6 +17,16 @@ int mlp_device_of(const cueva_mlp* M);
 // sets the shared-memory limits of the stage kernels (call once per device
 // before the first launch or capture)
 cudaError_t prepare_stage(int rec_mp, int solver, int prec);
+// per-solver halves of prepare_stage / launch_stage (cueva_stage_*.cu)
+cudaError_t prepare_stage_hll(int rec_mp, int prec);
+cudaError_t prepare_stage_hllc(int rec_mp, int prec);
+cudaError_t prepare_stage_hlle(int rec_mp, int prec);
+cudaError_t launch_stage_hll(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
+                             const StageArgs& sa, cudaEvent_t* ev);
+cudaError_t launch_stage_hllc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
+                              const StageArgs& sa, cudaEvent_t* ev);
+cudaError_t launch_stage_hlle(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
+                              const StageArgs& sa, cudaEvent_t* ev);
 // one RK stage: y faces, then x faces + update; with ev non-null, ev[0..2]
 // are recorded before, between and after the launches
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,

@@ -1,8 +1,9 @@
 // cueva_riemann.cuh -- per-interface HLL / HLLC fluxes of the resistive RMHD
 // system, one direction at a time.
 //
-// Reference: 16_hll_flow_mpx.f95:1358-1965 (HLL) and
-// 16_hllc_flow_mpx.f95:2401-4618 (HLLC).  The Fortran writes the x and y
+// Reference: 16_hll_flow_mpx.f95:1358-1965 (HLL),
+// 16_hllc_flow_mpx.f95:2401-4618 (HLLC) and 16_hlle_flow_mpx.f95:2526-4614
+// (HLLE).  The Fortran writes the x and y
 // branches out separately; they are the same formulas under the cyclic map
 // (x,y,z) -> (y,z,x), so one direction template serves both.  Components are
 // addressed by role: n (normal), t1, t2 with (n,t1,t2) = (x,y,z) for the x
@@ -65,15 +66,27 @@ template <> struct Dir<1> {
   template <class S> static __device__ __forceinline__ auto vt2(const S& s) { return s.vx; }
 };
 
-// physical fluxes of one reconstructed side, 16_hll_flow_mpx.f95:1464-1733
-template <typename T> struct Phys { T FD, Ftau, FSn, FSt1, FSt2; };
+// physical fluxes of one reconstructed side, 16_hll_flow_mpx.f95:1464-1733;
+// h is the enthalpy density rho (1 + eps) + p
+template <typename T> struct Phys { T FD, Ftau, FSn, FSt1, FSt2, h; };
+
+// Lorentz factor of the HLL / HLLC routines, 1 / sqrt(1 - (vx^2 + vy^2 + vz^2))
+template <typename T>
+__device__ __forceinline__ T lorentz(const Side<T>& s) {
+  const T V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
+  return T(1.0) / sqrt(T(1.0) - V2);
+}
+// the HLLE routine subtracts the squares one at a time,
+// 1 / sqrt(1 - vx^2 - vy^2 - vz^2) (16_hlle_flow_mpx.f95:2289-2292)
+template <typename T>
+__device__ __forceinline__ T lorentz_hlle(const Side<T>& s) {
+  return T(1.0) / sqrt(T(1.0) - pw2(s.vx) - pw2(s.vy) - pw2(s.vz));
+}
 
 template <int D, typename T>
-__device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma) {
+__device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma, T W) {
   using X = Dir<D>;
   Phys<T> f;
-  const T V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
-  const T W = T(1.0) / sqrt(T(1.0) - V2);
   const T E2B2 = pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez) + pw2(s.Bx) + pw2(s.By) + pw2(s.Bz);
   const T eps = s.p / ((gamma - T(1.0)) * s.rho);
   const T h = s.rho * (T(1.0) + eps) + s.p;
@@ -87,7 +100,12 @@ __device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma) {
   f.FSt1 = -En * Et1 - Bn * Bt1 + hW2 * vn * vt1;
   if constexpr (D == 0) f.FSt2 = -En * Et2 - Bn * Bt2 + hW2 * vn * vt2;
   else                  f.FSt2 = -En * Et2 - Bn * Bt2 + hW2 * vt2 * vn;   // FSyx: vx before vy
+  f.h = h;
   return f;
+}
+template <int D, typename T>
+__device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma) {
+  return physical<D>(s, gamma, lorentz(s));
 }
 
 // fixed-speed (s1 = -1, s2 = +1) HLL combination
@@ -234,6 +252,122 @@ __device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, 
     st |= ST_HLLC_VSTAR;
 #pragma unroll
     for (int c = 0; c < NROLE; ++c) A[c] = T(NAN);
+  }
+}
+
+// HLLE variant, 16_hlle_flow_mpx.f95 (2D, :2526-4614).  psi, phi, E and B
+// keep the fixed-speed HLL fluxes (their star fluxes are the HLL ones,
+// :3489-3604; the flux choice :3881-4019 takes them in both branches); q, D,
+// tau and S use the bounds s1 = min(lambda-), s2 = max(lambda+) of the
+// relativistic sound speed (:2709-2826, the reference writes vn where the
+// textbook bound has vn^2 under the root), and D, tau, S receive the
+// HLLC-type contact of the same quadratic for v* (:3165-3420).  Flux choice
+// (:4021-4286): s1 >= 0 left physical flux, s1 <= 0 <= v* left star flux,
+// v* <= 0 <= s2 right star flux, s2 < 0 right physical flux.  No superluminal
+// or density fix-ups precede this solver.
+template <int D, typename T>
+__device__ __forceinline__ void hlle_bounds(const Side<T>& s, T h, T gamma, T& lm, T& lp) {
+  using X = Dir<D>;
+  const T vn = X::vn(s);
+  const T Cs = sqrt(gamma * s.p / (h));
+  const T V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
+  const T root = sqrt((T(1.0) - V2) * (T(1.0) - V2 * pw2(Cs) - vn * (T(1.0) - pw2(Cs))));
+  lp = (vn * (T(1.0) - pw2(Cs)) + Cs * root) / (T(1.0) - pw2(Cs) * V2);
+  lm = (vn * (T(1.0) - pw2(Cs)) - Cs * root) / (T(1.0) - pw2(Cs) * V2);
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st) {
+  using X = Dir<D>;
+  em_fluxes<D>(L, R, A);   // psi, phi, E, B; the charge flux is replaced below
+  const Phys<T> fl = physical<D>(L, gamma, lorentz_hlle(L)), fr = physical<D>(R, gamma, lorentz_hlle(R));
+  const T h = T(0.5);
+  // fixed-speed HLL states of E and B (the star E, B)
+  const T En_hll = h * (((X::En(R) + X::En(L)) + L.psi) - R.psi);
+  const T Et1_hll = h * (((X::Et1(R) + X::Et1(L)) + X::Bt2(L)) - X::Bt2(R));
+  const T Et2_hll = h * (((X::Et2(R) + X::Et2(L)) - X::Bt1(L)) + X::Bt1(R));
+  const T Bn_hll = h * (((X::Bn(R) + X::Bn(L)) + L.phi) - R.phi);
+  const T Bt1_hll = h * (((X::Bt1(R) + X::Bt1(L)) - X::Et2(L)) + X::Et2(R));
+  const T Bt2_hll = h * (((X::Bt2(R) + X::Bt2(L)) + X::Et1(L)) - X::Et1(R));
+  // wave bounds (:2796-2819: NaN stops the reference; |s| > 1 is clamped)
+  T lmL, lpL, lmR, lpR;
+  hlle_bounds<D>(R, fr.h, gamma, lmR, lpR);
+  hlle_bounds<D>(L, fl.h, gamma, lmL, lpL);
+  T s1 = fmin2(lmL, lmR), s2 = fmax2(lpL, lpR);
+  if (isnan(s1) || isnan(s2)) st |= ST_HLLE_SPEED;
+  const T eps2 = T(1.0e-9);
+  if (fabs(s1) > T(1.0)) s1 = fmax2(T(-1.0) + eps2, fmin2(T(1.0) - eps2, s1));
+  if (fabs(s2) > T(1.0)) s2 = fmax2(T(-1.0) + eps2, fmin2(T(1.0) - eps2, s2));
+  // fluid HLL states and HLLE fluxes with the bounds
+  const T D_hll = (s2 * R.D - s1 * L.D + fl.FD - fr.FD) / (s2 - s1);
+  const T tau_hll = (s2 * R.tau - s1 * L.tau + fl.Ftau - fr.Ftau) / (s2 - s1);
+  const T Sn_hll = (s2 * X::Sn(R) - s1 * X::Sn(L) + fl.FSn - fr.FSn) / (s2 - s1);
+  const T St1_hll = (s2 * X::St1(R) - s1 * X::St1(L) + fl.FSt1 - fr.FSt1) / (s2 - s1);
+  const T St2_hll = (s2 * X::St2(R) - s1 * X::St2(L) + fl.FSt2 - fr.FSt2) / (s2 - s1);
+  auto hlle = [&](T FL, T FR, T UL, T UR) { return (s2 * FL - s1 * FR + s1 * s2 * (UR - UL)) / (s2 - s1); };
+  const T q_f = hlle(L.J, R.J, L.q, R.q);
+  const T D_f = hlle(fl.FD, fr.FD, L.D, R.D);
+  const T tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+  const T Sn_f = hlle(fl.FSn, fr.FSn, X::Sn(L), X::Sn(R));
+  const T St1_f = hlle(fl.FSt1, fr.FSt1, X::St1(L), X::St1(R));
+  const T St2_f = hlle(fl.FSt2, fr.FSt2, X::St2(L), X::St2(R));
+  // contact speed of the HLLC quadratic, with the HLLE states and fluxes
+  const T ErotB_n = Bt2_hll * Et1_hll - Bt1_hll * Et2_hll;
+  const T ErotB_t1 = Bn_hll * Et2_hll - Bt2_hll * En_hll;
+  const T ErotB_t2 = Bt1_hll * En_hll - Bn_hll * Et1_hll;
+  const T E2_perp = pw2(Et1_hll) + pw2(Et2_hll);
+  const T B2_perp = pw2(Bt1_hll) + pw2(Bt2_hll);
+  T Exs, Eys, Ezs, Bxs, Bys, Bzs;
+  if constexpr (D == 0) { Exs = En_hll; Eys = Et1_hll; Ezs = Et2_hll; Bxs = Bn_hll; Bys = Bt1_hll; Bzs = Bt2_hll; }
+  else                  { Eys = En_hll; Ezs = Et1_hll; Exs = Et2_hll; Bys = Bn_hll; Bzs = Bt1_hll; Bxs = Bt2_hll; }
+  const T E2B2_str = T(0.5) * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+  const T a_hll = tau_f - ErotB_n;
+  const T b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
+  const T c_hll = Sn_hll - ErotB_n;
+  const T det_hll = pw2(b_hll) - T(4.0) * a_hll * c_hll;
+  const T q_root1 = -T(0.5) * (b_hll + fsgn1(b_hll) * fabs(sqrt(det_hll)));
+  T rt2 = c_hll / q_root1;
+  if (det_hll < T(0.0)) rt2 = c_hll / b_hll;
+  T V = hllc_vel(a_hll, -b_hll, c_hll, rt2, st);
+  if (fabs(V) <= T(1.0e-9)) V = T(0.0);
+  // star states (:3378-3420)
+  const T pstr = Sn_f + (pw2(En_hll) + pw2(Bn_hll)) - (tau_f - ErotB_n) * V;
+  const T SnR = (s2 * Sn_hll - tau_f * V) / (s2 - V);
+  const T SnL = (-s1 * Sn_hll + tau_f * V) / (V - s1);
+  const T St1R = (s2 * St1_hll - St1_f - ErotB_t1 * V - En_hll * Et1_hll - Bn_hll * Bt1_hll) / (s2 - V);
+  const T St1L = (-s1 * St1_hll + St1_f + ErotB_t1 * V + En_hll * Et1_hll + Bn_hll * Bt1_hll) / (V - s1);
+  const T St2R = (s2 * St2_hll - St2_f - ErotB_t2 * V - En_hll * Et2_hll - Bn_hll * Bt2_hll) / (s2 - V);
+  const T St2L = (-s1 * St2_hll + St2_f + ErotB_t2 * V + En_hll * Et2_hll + Bn_hll * Bt2_hll) / (V - s1);
+  const T tauR = (SnR - ErotB_n) / V - pstr + E2B2_str;
+  const T tauL = (SnL - ErotB_n) / V - pstr + E2B2_str;
+  const T DR = (s2 * D_hll - D_f) / (s2 - V);
+  const T DL = (-s1 * D_hll + D_f) / (V - s1);
+  // star fluxes (:3489-3604; v* == 0 keeps the HLLE fluxes)
+  T fDR = D_f, fDL = D_f, ftR = tau_f, ftL = tau_f, fSnR = Sn_f, fSnL = Sn_f, fS1R = St1_f, fS1L = St1_f,
+    fS2R = St2_f, fS2L = St2_f;
+  if (V != T(0.0)) {
+    fDR = D_f + s2 * (V - s1) * (DR - DL) / (s2 - s1);
+    fDL = D_f - s1 * (s2 - V) * (DR - DL) / (s2 - s1);
+    ftR = tau_f + s2 * (V - s1) * (tauR - tauL) / (s2 - s1);
+    ftL = tau_f - s1 * (s2 - V) * (tauR - tauL) / (s2 - s1);
+    fSnR = Sn_f + s2 * (V - s1) * (SnR - SnL) / (s2 - s1);
+    fSnL = Sn_f - s1 * (s2 - V) * (SnR - SnL) / (s2 - s1);
+    fS1R = St1_f + s2 * (V - s1) * (St1R - St1L) / (s2 - s1);
+    fS1L = St1_f - s1 * (s2 - V) * (St1R - St1L) / (s2 - s1);
+    fS2R = St2_f + s2 * (V - s1) * (St2R - St2L) / (s2 - s1);
+    fS2L = St2_f - s1 * (s2 - V) * (St2R - St2L) / (s2 - s1);
+  }
+  if (s1 >= T(0.0)) {
+    A[R_Q] = L.J; A[R_D] = fl.FD; A[R_TAU] = fl.Ftau; A[R_SN] = fl.FSn; A[R_ST1] = fl.FSt1; A[R_ST2] = fl.FSt2;
+  } else if (s1 <= T(0.0) && T(0.0) <= V) {
+    A[R_Q] = q_f; A[R_D] = fDL; A[R_TAU] = ftL; A[R_SN] = fSnL; A[R_ST1] = fS1L; A[R_ST2] = fS2L;
+  } else if (V <= T(0.0) && T(0.0) <= s2) {
+    A[R_Q] = q_f; A[R_D] = fDR; A[R_TAU] = ftR; A[R_SN] = fSnR; A[R_ST1] = fS1R; A[R_ST2] = fS2R;
+  } else if (s2 < T(0.0)) {
+    A[R_Q] = R.J; A[R_D] = fr.FD; A[R_TAU] = fr.Ftau; A[R_SN] = fr.FSn; A[R_ST1] = fr.FSt1; A[R_ST2] = fr.FSt2;
+  } else {   // the reference stops (:4284-4285, 4612-4613)
+    st |= ST_HLLC_VSTAR;
+    A[R_Q] = A[R_D] = A[R_TAU] = A[R_SN] = A[R_ST1] = A[R_ST2] = T(NAN);
   }
 }
 

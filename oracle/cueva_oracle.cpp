@@ -47,6 +47,7 @@ enum Status : int32_t {
   ST_HLLC_NOCONV = 4,     // funciones.f95:240-245
   ST_HLLC_VSTAR = 8,      // 16_hllc_flow_mpx.f95:4294,4605
   ST_NONFINITE = 16,
+  ST_HLLE_SPEED = 32,     // 16_hlle_flow_mpx.f95:2796-2803, 2974-2981
 };
 
 // ---------------------------------------------------------------- tableaux
@@ -1228,8 +1229,203 @@ struct Oracle {
 
   // HLLE is restated separately (16_hlle_flow_mpx.f95); until then the
   // solver id 6 is rejected at creation.
-  int32_t hlle_x(const Side&, const Side&, const PhysX&, const PhysX&, double*) { return ST_NONFINITE; }
-  int32_t hlle_y(const Side&, const Side&, const PhysX&, const PhysX&, double*) { return ST_NONFINITE; }
+  // ----------------------------------------- HLLE (16_hlle_flow_mpx.f95, 2D)
+  // EM fields, psi and phi take the fixed-speed HLL fluxes (s = -1, +1,
+  // :2526-2588, the star psi/phi fluxes are the HLL ones, :3489-3604); q, D,
+  // tau and S use the bounds sx1 = min(lambda-), sx2 = max(lambda+) from the
+  // relativistic sound speed (:2709-2826), and D, tau, S get the HLLC-type
+  // contact of the same quadratic for v* (:3165-3420).  Flux choice
+  // (:4021-4286): sx1 >= 0 left physical flux, sx1 <= 0 <= v* left star,
+  // v* <= 0 <= sx2 right star, sx2 < 0 right physical flux.
+  // Wave bounds of one side; vn is the normal velocity.  The reference
+  // writes vn (not vn^2) in the second factor under the root (:2722-2735).
+  void hlle_bounds(const Side& s, const PhysX& f, double vn, double& lm, double& lp) const {
+    const double Cs = std::sqrt(gamma * s.p / (f.h));
+    const double V2 = pw2(s.vx) + pw2(s.vy) + pw2(s.vz);
+    const double root = std::sqrt((1.0 - V2) * (1.0 - V2 * pw2(Cs) - vn * (1.0 - pw2(Cs))));
+    lp = (vn * (1.0 - pw2(Cs)) + Cs * root) / (1.0 - pw2(Cs) * V2);
+    lm = (vn * (1.0 - pw2(Cs)) - Cs * root) / (1.0 - pw2(Cs) * V2);
+  }
+  // sx1, sx2 with the NaN stop (:2796-2803) and the clamp to 1 - 1e-9 (:2805-2819)
+  static int32_t hlle_speeds(double lmL, double lmR, double lpL, double lpR, double& s1, double& s2) {
+    s1 = fmin2(lmL, lmR);
+    s2 = fmax2(lpL, lpR);
+    int32_t st = 0;
+    if (std::isnan(s1) || std::isnan(s2)) st |= ST_HLLE_SPEED;
+    const double eps2 = 1.0e-9;
+    if (std::fabs(s1) > 1.0) s1 = fmax2(-1.0 + eps2, fmin2(1.0 - eps2, s1));
+    if (std::fabs(s2) > 1.0) s2 = fmax2(-1.0 + eps2, fmin2(1.0 - eps2, s2));
+    return st;
+  }
+
+  int32_t hlle_x(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+    const double s1 = -1.0, s2 = 1.0;
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.psi - R.psi) / (s2 - s1);
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.Bz - R.Bz) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bym - R.Bym) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.phi - R.phi) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.Ezm - R.Ezm) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Ey - R.Ey) / (s2 - s1);
+    double lmL, lpL, lmR, lpR, sx1, sx2;
+    hlle_bounds(R, fr, R.vx, lmR, lpR);
+    hlle_bounds(L, fl, L.vx, lmL, lpL);
+    int32_t st = hlle_speeds(lmL, lmR, lpL, lpR, sx1, sx2);
+    const double DD_hll = (sx2 * R.D - sx1 * L.D + fl.FD - fr.FD) / (sx2 - sx1);
+    const double tau_hll = (sx2 * R.tau - sx1 * L.tau + fl.Ftau - fr.Ftau) / (sx2 - sx1);
+    const double Sx_hll = (sx2 * R.Sx - sx1 * L.Sx + fl.FSx - fr.FSx) / (sx2 - sx1);
+    const double Sy_hll = (sx2 * R.Sy - sx1 * L.Sy + fl.FSy - fr.FSy) / (sx2 - sx1);
+    const double Sz_hll = (sx2 * R.Sz - sx1 * L.Sz + fl.FSz - fr.FSz) / (sx2 - sx1);
+    auto hlle = [&](double FL, double FR, double UL, double UR) {
+      return (sx2 * FL - sx1 * FR + sx1 * sx2 * (UR - UL)) / (sx2 - sx1);
+    };
+    const double q_f = hlle(L.J, R.J, L.q, R.q);
+    const double DD_f = hlle(fl.FD, fr.FD, L.D, R.D);
+    const double tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+    const double Sx_f = hlle(fl.FSx, fr.FSx, L.Sx, R.Sx);
+    const double Sy_f = hlle(fl.FSy, fr.FSy, L.Sy, R.Sy);
+    const double Sz_f = hlle(fl.FSz, fr.FSz, L.Sz, R.Sz);
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Eys) + pw2(Ezs));
+    const double B2_perp = (pw2(Bys) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_x;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sx_f;
+    const double c_hll = Sx_hll - ErotB_x;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = 1.0e-6;   // double literal here, 16_hlle_flow_mpx.f95:3172
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sx_f + (pw2(Exs) + pw2(Bxs)) - (tau_f - ErotB_x) * V;
+    const double SxR = (sx2 * Sx_hll - tau_f * V) / (sx2 - V);
+    const double SxL = (-sx1 * Sx_hll + tau_f * V) / (V - sx1);
+    const double SyR = (sx2 * Sy_hll - Sy_f - ErotB_y * V - Exs * Eys - Bxs * Bys) / (sx2 - V);
+    const double SyL = (-sx1 * Sy_hll + Sy_f + ErotB_y * V + Exs * Eys + Bxs * Bys) / (V - sx1);
+    const double SzR = (sx2 * Sz_hll - Sz_f - ErotB_z * V - Exs * Ezs - Bxs * Bzs) / (sx2 - V);
+    const double SzL = (-sx1 * Sz_hll + Sz_f + ErotB_z * V + Exs * Ezs + Bxs * Bzs) / (V - sx1);
+    const double tauR = (SxR - ErotB_x) / V - pstr + E2B2_str;
+    const double tauL = (SxL - ErotB_x) / V - pstr + E2B2_str;
+    const double DR = (sx2 * DD_hll - DD_f) / (sx2 - V);
+    const double DL = (-sx1 * DD_hll + DD_f) / (V - sx1);
+    double fDR = DD_f, fDL = DD_f, ftR = tau_f, ftL = tau_f, fSxR = Sx_f, fSxL = Sx_f, fSyR = Sy_f, fSyL = Sy_f,
+           fSzR = Sz_f, fSzL = Sz_f;
+    if (V != 0.0) {
+      fDR = DD_f + sx2 * (V - sx1) * (DR - DL) / (sx2 - sx1);
+      fDL = DD_f - sx1 * (sx2 - V) * (DR - DL) / (sx2 - sx1);
+      ftR = tau_f + sx2 * (V - sx1) * (tauR - tauL) / (sx2 - sx1);
+      ftL = tau_f - sx1 * (sx2 - V) * (tauR - tauL) / (sx2 - sx1);
+      fSxR = Sx_f + sx2 * (V - sx1) * (SxR - SxL) / (sx2 - sx1);
+      fSxL = Sx_f - sx1 * (sx2 - V) * (SxR - SxL) / (sx2 - sx1);
+      fSyR = Sy_f + sx2 * (V - sx1) * (SyR - SyL) / (sx2 - sx1);
+      fSyL = Sy_f - sx1 * (sx2 - V) * (SyR - SyL) / (sx2 - sx1);
+      fSzR = Sz_f + sx2 * (V - sx1) * (SzR - SzL) / (sx2 - sx1);
+      fSzL = Sz_f - sx1 * (sx2 - V) * (SzR - SzL) / (sx2 - sx1);
+    }
+    // EM, psi, phi: HLL fluxes (out[0..15], set by the caller) in both v* branches
+    if (sx1 >= 0.0) {
+      out[16] = L.J; out[18] = fl.FD; out[20] = fl.Ftau; out[22] = fl.FSx; out[23] = fl.FSy; out[24] = fl.FSz;
+    } else if (sx1 <= 0.0 && 0.0 <= V) {
+      out[16] = q_f; out[18] = fDL; out[20] = ftL; out[22] = fSxL; out[23] = fSyL; out[24] = fSzL;
+    } else if (V <= 0.0 && 0.0 <= sx2) {
+      out[16] = q_f; out[18] = fDR; out[20] = ftR; out[22] = fSxR; out[23] = fSyR; out[24] = fSzR;
+    } else if (sx2 < 0.0) {
+      out[16] = R.J; out[18] = fr.FD; out[20] = fr.Ftau; out[22] = fr.FSx; out[23] = fr.FSy; out[24] = fr.FSz;
+    } else {   // the reference stops, :4284-4285
+      st |= ST_HLLC_VSTAR;
+      for (int c : {16, 18, 20, 22, 23, 24}) out[c] = NAN;
+    }
+    return st;
+  }
+
+  int32_t hlle_y(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+    const double s1 = -1.0, s2 = 1.0;
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.psi - R.psi) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bx - R.Bx) / (s2 - s1);
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.Bzm - R.Bzm) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.phi - R.phi) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Exm - R.Exm) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.Ez - R.Ez) / (s2 - s1);
+    double lmL, lpL, lmR, lpR, sy1, sy2;
+    hlle_bounds(R, fr, R.vy, lmR, lpR);
+    hlle_bounds(L, fl, L.vy, lmL, lpL);
+    int32_t st = hlle_speeds(lmL, lmR, lpL, lpR, sy1, sy2);
+    const double DD_hll = (sy2 * R.D - sy1 * L.D + fl.FD - fr.FD) / (sy2 - sy1);
+    const double tau_hll = (sy2 * R.tau - sy1 * L.tau + fl.Ftau - fr.Ftau) / (sy2 - sy1);
+    const double Sy_hll = (sy2 * R.Sy - sy1 * L.Sy + fl.FSy - fr.FSy) / (sy2 - sy1);
+    const double Sz_hll = (sy2 * R.Sz - sy1 * L.Sz + fl.FSz - fr.FSz) / (sy2 - sy1);
+    const double Sx_hll = (sy2 * R.Sx - sy1 * L.Sx + fl.FSx - fr.FSx) / (sy2 - sy1);
+    auto hlle = [&](double FL, double FR, double UL, double UR) {
+      return (sy2 * FL - sy1 * FR + sy1 * sy2 * (UR - UL)) / (sy2 - sy1);
+    };
+    const double q_f = hlle(L.J, R.J, L.q, R.q);
+    const double DD_f = hlle(fl.FD, fr.FD, L.D, R.D);
+    const double tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+    const double Sy_f = hlle(fl.FSy, fr.FSy, L.Sy, R.Sy);
+    const double Sz_f = hlle(fl.FSz, fr.FSz, L.Sz, R.Sz);
+    const double Sx_f = hlle(fl.FSx, fr.FSx, L.Sx, R.Sx);
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Exs) + pw2(Ezs));
+    const double B2_perp = (pw2(Bxs) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_y;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sy_f;
+    const double c_hll = Sy_hll - ErotB_y;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = 1.0e-6;
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sy_f + (pw2(Eys) + pw2(Bys)) - (tau_f - ErotB_y) * V;
+    const double SyR = (sy2 * Sy_hll - tau_f * V) / (sy2 - V);
+    const double SyL = (-sy1 * Sy_hll + tau_f * V) / (V - sy1);
+    const double SzR = (sy2 * Sz_hll - Sz_f - ErotB_z * V - Eys * Ezs - Bys * Bzs) / (sy2 - V);
+    const double SzL = (-sy1 * Sz_hll + Sz_f + ErotB_z * V + Eys * Ezs + Bys * Bzs) / (V - sy1);
+    const double SxR = (sy2 * Sx_hll - Sx_f - ErotB_x * V - Eys * Exs - Bys * Bxs) / (sy2 - V);
+    const double SxL = (-sy1 * Sx_hll + Sx_f + ErotB_x * V + Eys * Exs + Bys * Bxs) / (V - sy1);
+    const double tauR = (SyR - ErotB_y) / V - pstr + E2B2_str;
+    const double tauL = (SyL - ErotB_y) / V - pstr + E2B2_str;
+    const double DR = (sy2 * DD_hll - DD_f) / (sy2 - V);
+    const double DL = (-sy1 * DD_hll + DD_f) / (V - sy1);
+    double fDR = DD_f, fDL = DD_f, ftR = tau_f, ftL = tau_f, fSxR = Sx_f, fSxL = Sx_f, fSyR = Sy_f, fSyL = Sy_f,
+           fSzR = Sz_f, fSzL = Sz_f;
+    if (V != 0.0) {
+      fDR = DD_f + sy2 * (V - sy1) * (DR - DL) / (sy2 - sy1);
+      fDL = DD_f - sy1 * (sy2 - V) * (DR - DL) / (sy2 - sy1);
+      ftR = tau_f + sy2 * (V - sy1) * (tauR - tauL) / (sy2 - sy1);
+      ftL = tau_f - sy1 * (sy2 - V) * (tauR - tauL) / (sy2 - sy1);
+      fSxR = Sx_f + sy2 * (V - sy1) * (SxR - SxL) / (sy2 - sy1);
+      fSxL = Sx_f - sy1 * (sy2 - V) * (SxR - SxL) / (sy2 - sy1);
+      fSyR = Sy_f + sy2 * (V - sy1) * (SyR - SyL) / (sy2 - sy1);
+      fSyL = Sy_f - sy1 * (sy2 - V) * (SyR - SyL) / (sy2 - sy1);
+      fSzR = Sz_f + sy2 * (V - sy1) * (SzR - SzL) / (sy2 - sy1);
+      fSzL = Sz_f - sy1 * (sy2 - V) * (SzR - SzL) / (sy2 - sy1);
+    }
+    if (sy1 >= 0.0) {
+      out[17] = L.J; out[19] = fl.FD; out[21] = fl.Ftau; out[25] = fl.FSx; out[26] = fl.FSy; out[27] = fl.FSz;
+    } else if (sy1 <= 0.0 && 0.0 <= V) {
+      out[17] = q_f; out[19] = fDL; out[21] = ftL; out[25] = fSxL; out[26] = fSyL; out[27] = fSzL;
+    } else if (V <= 0.0 && 0.0 <= sy2) {
+      out[17] = q_f; out[19] = fDR; out[21] = ftR; out[25] = fSxR; out[26] = fSyR; out[27] = fSzR;
+    } else if (sy2 < 0.0) {
+      out[17] = R.J; out[19] = fr.FD; out[21] = fr.Ftau; out[25] = fr.FSx; out[26] = fr.FSy; out[27] = fr.FSz;
+    } else {   // the reference stops, :4612-4613
+      st |= ST_HLLC_VSTAR;
+      for (int c : {17, 19, 21, 25, 26, 27}) out[c] = NAN;
+    }
+    return st;
+  }
 
   // ---------------------------------------------- 17_fluxandsource.f95:441-635
   // z differences (X(i,j)-X(i,j))/Delz are kept as literal zeros.
@@ -1407,7 +1603,7 @@ extern "C" {
 
 void* oracle_create(const oracle_params* p) {
   if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
-  if (p->flux_solver != 5 && p->flux_solver != 7) return nullptr;
+  if (p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
   if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
   Tableau T;
   if (!make_tableau(p->order, T)) return nullptr;
