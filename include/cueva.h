@@ -262,6 +262,100 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* params, const double* prim, c
                                const double* stage, double* rhs, int32_t pitch, int64_t fstride, void* stream,
                                uint32_t* status_bits);
 
+/* ---- run diagnostics (22_writer.f95:821-1001, subroutine lector) ------- */
+/* Slots of a diagnostics record.  Slots 0..34 are the volume integrals
+ * sum(x * Delx * Dely) over the points 0..imax x 0..jmax that the writer
+ * prints to the Fortran units in brackets, with its expressions kept as
+ * written: B2 leaves Bx out, and in eint_r and efluid_r only the p term is
+ * multiplied by Delx * Dely.  D and tau are the conserved values of varfin
+ * (con2prim does not write them back), as at the writer's call
+ * (main_cueva_code.f95:332). */
+enum cueva_diag_slot {
+  CUEVA_DG_SUM_PSI = 0,   /* [80] psi */
+  CUEVA_DG_SUM_PHI,       /* [81] phi */
+  CUEVA_DG_SUM_EX,        /* [82] Ex^2 */
+  CUEVA_DG_SUM_EY,        /* [83] Ey^2 */
+  CUEVA_DG_SUM_EZ,        /* [84] Ez^2 */
+  CUEVA_DG_SUM_EXEY,      /* [85] Ex Ey */
+  CUEVA_DG_SUM_EXEZ,      /* [86] Ex Ez */
+  CUEVA_DG_SUM_EYEZ,      /* [87] Ey Ez */
+  CUEVA_DG_SUM_BX,        /* [88] Bx^2 */
+  CUEVA_DG_SUM_BY,        /* [90] By^2 */
+  CUEVA_DG_SUM_BZ,        /* [91] Bz^2 */
+  CUEVA_DG_SUM_BXBY,      /* [92] Bx By */
+  CUEVA_DG_SUM_BXBZ,      /* [93] Bx Bz */
+  CUEVA_DG_SUM_BYBZ,      /* [94] By Bz */
+  CUEVA_DG_SUM_VXVYVZ,    /* [95] v^2 */
+  CUEVA_DG_SUM_BXBYBZ,    /* [96] B^2 */
+  CUEVA_DG_SUM_VX,        /* [97] vx^2 */
+  CUEVA_DG_SUM_VY,        /* [98] vy^2 */
+  CUEVA_DG_SUM_VZ,        /* [99] vz^2 */
+  CUEVA_DG_SUM_VXVY,      /* [200] vx vy */
+  CUEVA_DG_SUM_VXVZ,      /* [201] vx vz */
+  CUEVA_DG_SUM_VYVZ,      /* [202] vy vz */
+  CUEVA_DG_SUM_Q,         /* [203] q */
+  CUEVA_DG_SUM_P,         /* [204] p */
+  CUEVA_DG_SUM_RHO,       /* [205] rho */
+  CUEVA_DG_EKIN_C,        /* [206] rho v^2 / 2 */
+  CUEVA_DG_EKIN_R,        /* [207] D (W - 1) */
+  CUEVA_DG_ETOT,          /* [208] tau */
+  CUEVA_DG_EFLUID_R,      /* [209] sum(rho h W^2 - p Delx Dely) */
+  CUEVA_DG_EMAG,          /* [210] (E^2 + By^2 + Bz^2) / 2 */
+  CUEVA_DG_EINT_C,        /* [211] rho eps */
+  CUEVA_DG_EINT_R,        /* [212] sum(W^2 (rho eps + p) - p Delx Dely) */
+  CUEVA_DG_LORENTZ,       /* [213] W */
+  CUEVA_DG_SUM_D,         /* [214] D */
+  CUEVA_DG_SUM_D_MED,     /* [215] D over i = floor(imax/4) .. floor(3 imax/4) */
+  CUEVA_DG_MAX_BX,        /* [216] max Bx / B0 */
+  CUEVA_DG_MAX_PHI,       /* [217] max phi */
+  CUEVA_DG_DELTA_REC,     /* [67] B0 r tanh(Delx/delta_rec) delta_rec / By(imed+1, jmed+1) */
+  CUEVA_DG_EZ_MED,        /* [68] Ez(imed, jmed), imed = floor(imax/2), jmed = floor(jmax/2) */
+  CUEVA_DG_BY_MED,        /* By(imed+1, jmed+1), the denominator of [67] */
+  /* Courant check (no counterpart in the reference, whose HLL-type fluxes use
+   * the light-speed bounds -1, +1 and a fixed Delt): never changes Delt */
+  CUEVA_DG_MAX_V,         /* max |v| */
+  CUEVA_DG_MAX_W,         /* max W */
+  CUEVA_DG_MAX_LAMBDA_X,  /* max |lambda| of the relativistic sound waves along x */
+  CUEVA_DG_MAX_LAMBDA_Y,  /* ... along y */
+  CUEVA_DG_COURANT,       /* Delt * max(max_lambda_x / Delx, max_lambda_y / Dely) */
+  CUEVA_NDIAG
+};
+
+typedef struct cueva_diag_record {
+  int64_t h;                /* step index h of the reference's time loop */
+  double t;                 /* t_advance after that step */
+  double v[CUEVA_NDIAG];
+} cueva_diag_record;
+
+typedef struct cueva_diag_config {
+  int32_t hglb;        /* a record after step h when h == 1 or mod(h, hglb) == 0 (22_writer.f95:821) */
+  int32_t capacity;    /* records kept on the device between cueva_diag_read calls */
+  double b0;           /* B0 (parameters.f95:131) */
+  double lr, ly;       /* Lr, Ly (parameters.f95:168,175) */
+  double delta_rec;    /* delta_rec (parameters.f95:206) */
+} cueva_diag_config;
+
+/* Step clock of the context: h = index of the last completed step and
+ * t = t_advance.  cueva_ctx_create starts at h = 0, t = 0 (hini = 1,
+ * main_cueva_code.f95:45); each step adds 1 to h and Delt to t
+ * (main_cueva_code.f95:161).  Set it when a run restarts from a backup. */
+int32_t cueva_set_clock(cueva_ctx* ctx, int64_t h, double t);
+int32_t cueva_get_clock(const cueva_ctx* ctx, int64_t* h, double* t);
+/* Enables (cfg non-null) or disables the records and empties the record
+ * buffer.  While enabled, cueva_step appends a record after each step whose
+ * h is 1 or a multiple of hglb (the last stage of such a step also stores
+ * varfin's D and tau for it). */
+int32_t cueva_diag_enable(cueva_ctx* ctx, const cueva_diag_config* cfg);
+/* Copies up to max_records of the records not yet read, oldest first, and
+ * marks them read; when more than capacity records were appended since the
+ * last read, the oldest were overwritten and are skipped.  *n_out = number
+ * copied.  Synchronises the context's stream. */
+int32_t cueva_diag_read(cueva_ctx* ctx, cueva_diag_record* out, int32_t max_records, int32_t* n_out);
+/* One record of the state now on the device, with h and t of the clock;
+ * D and tau here are startconvar's values of the current primitives.
+ * Needs a config from cueva_diag_enable for B0, Lr, Ly and delta_rec. */
+int32_t cueva_diag_now(cueva_ctx* ctx, cueva_diag_record* out);
+
 /* ---- synthetic input ------------------------------------------------- */
 /* Kelvin-Helmholtz initial data on the Fortran-layout prim arrays bound to
  * ctx (interior points; reference orientation: x = shear normal with copy

@@ -2,6 +2,7 @@
 // transfers, step orchestration with CUDA graphs, routine mirrors.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -235,6 +236,16 @@ struct cueva_ctx {
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   MLPDevice* d_mlp = nullptr;                 // attached learned seed (c2p = 2)
   unsigned long long* d_mlp_stats = nullptr;  // Newton iterations, points, fall-backs
+  // step clock (h, t_advance) and run diagnostics
+  long long h = 0;
+  double t = 0.0;
+  bool diag_on = false;
+  cueva_diag_config diag{};
+  double* d_diag_cons = nullptr;          // varfin D, tau (2 slabs) of record steps
+  double* d_diag_part = nullptr;          // per-CTA partial results
+  cueva_diag_record* d_diag_rec = nullptr;// ring of diag.capacity records
+  long long diag_written = 0, diag_read = 0;
+  cudaGraphExec_t graph_diag[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
 namespace {
@@ -328,9 +339,10 @@ int32_t run_begin_step(cueva_ctx* c) {
   return CUEVA_OK;
 }
 
-int32_t enqueue_step(cueva_ctx* c) {
+int32_t enqueue_step(cueva_ctx* c, double* diag_cons = nullptr) {
   for (int l = 1; l <= c->T.s; ++l) {
-    const StageArgs sa = stage_args(c, l, 0);
+    StageArgs sa = stage_args(c, l, 0);
+    if (l == c->T.s) sa.diag_cons = diag_cons;
     CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1, sa));
     c->qin ^= 1;
   }
@@ -342,6 +354,22 @@ void destroy_graphs(cueva_ctx* c) {
   for (auto& row : c->graph)
     for (auto& g : row)
       if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& row : c->graph_diag)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+bool diag_step(const cueva_ctx* c, long long h) {
+  return c->diag_on && (h == 1 || (c->diag.hglb > 0 && h % c->diag.hglb == 0));
+}
+
+void free_diag(cueva_ctx* c) {
+  if (c->d_diag_cons) cudaFree(c->d_diag_cons);
+  if (c->d_diag_part) cudaFree(c->d_diag_part);
+  if (c->d_diag_rec) cudaFree(c->d_diag_rec);
+  c->d_diag_cons = c->d_diag_part = nullptr;
+  c->d_diag_rec = nullptr;
+  c->diag_on = false;
 }
 
 }  // namespace
@@ -414,6 +442,7 @@ int32_t cueva_ctx_destroy(cueva_ctx* c) {
   if (c->d_inst) cudaFree(c->d_inst);
   if (c->d_mlp) cudaFree(c->d_mlp);
   if (c->d_mlp_stats) cudaFree(c->d_mlp_stats);
+  free_diag(c);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return CUEVA_OK;
@@ -481,13 +510,16 @@ int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {
   if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
   CUDA_TRY(cudaSetDevice(c->dev));
   for (int n = 0; n < nsteps; ++n) {
-    cudaGraphExec_t& g = c->graph[c->cur][c->qin];
+    // steps after which the writer reports (h == 1 or mod(h, hglb) == 0)
+    // run a graph whose last stage also keeps varfin's D and tau
+    const bool rec = diag_step(c, c->h + 1);
+    cudaGraphExec_t& g = rec ? c->graph_diag[c->cur][c->qin] : c->graph[c->cur][c->qin];
     if (!g) {
       // capture one step starting from this (cur, qin) parity
       const int cur0 = c->cur, qin0 = c->qin;
       cudaGraph_t graph = nullptr;
       CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int32_t e = enqueue_step(c);
+      int32_t e = enqueue_step(c, rec ? c->d_diag_cons : nullptr);
       cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
       if (e) { if (graph) cudaGraphDestroy(graph); return e; }
       if (ce != cudaSuccess) return fail(CUEVA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
@@ -499,6 +531,14 @@ int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {
     CUDA_TRY(cudaGraphLaunch(g, c->stream));
     for (int l = 0; l < c->T.s; ++l) c->qin ^= 1;
     c->cur ^= 1;
+    c->h += 1;
+    c->t = c->t + c->dt;
+    if (rec) {
+      cueva_diag_record* slot = c->d_diag_rec + (c->diag_written % c->diag.capacity);
+      CUDA_TRY(launch_diag(c->h_inst, c->cur, c->d_diag_cons, c->d_diag_cons + c->fstride, c->diag.b0,
+                           c->d_diag_part, c->h, c->t, slot, c->stream));
+      c->diag_written += 1;
+    }
   }
   return CUEVA_OK;
 }
@@ -532,6 +572,8 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
       c->qin ^= 1;
     }
     c->cur ^= 1;
+    c->h += 1;
+    c->t = c->t + c->dt;
   }
   for (auto& e : ev) cudaEventDestroy(e);
   if (rc) return rc;
@@ -559,6 +601,95 @@ int32_t cueva_counters(cueva_ctx* c, int64_t out3[3]) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
   return CUEVA_OK;
+}
+
+// ------------------------------------------------------------ run diagnostics
+int32_t cueva_set_clock(cueva_ctx* c, int64_t h, double t) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (h < 0) return fail(CUEVA_ERR_ARG, "step index h < 0");
+  c->h = h;
+  c->t = t;
+  return CUEVA_OK;
+}
+
+int32_t cueva_get_clock(const cueva_ctx* c, int64_t* h, double* t) {
+  if (!c) return fail(CUEVA_ERR_ARG, "null context");
+  if (h) *h = c->h;
+  if (t) *t = c->t;
+  return CUEVA_OK;
+}
+
+int32_t cueva_diag_enable(cueva_ctx* c, const cueva_diag_config* cfg) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  destroy_graphs(c);   // the record graphs hold the buffers' addresses
+  free_diag(c);
+  if (!cfg) return CUEVA_OK;
+  if (cfg->hglb < 1) return fail(CUEVA_ERR_ARG, "hglb must be >= 1");
+  if (cfg->capacity < 1) return fail(CUEVA_ERR_ARG, "capacity must be >= 1");
+  if (!(cfg->b0 != 0.0) || !(cfg->lr != 0.0) || !(cfg->delta_rec != 0.0))
+    return fail(CUEVA_ERR_ARG, "b0, lr and delta_rec must be non-zero");
+  const size_t part = (size_t)diag_blocks(c->imax, c->jmax) * diag_partials();
+  if (cudaMalloc(&c->d_diag_cons, 2 * (size_t)c->fstride * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_diag_part, part * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_diag_rec, ((size_t)cfg->capacity + 1) * sizeof(cueva_diag_record)) != cudaSuccess) {
+    cudaGetLastError();
+    free_diag(c);
+    return fail(CUEVA_ERR_CUDA, "cudaMalloc of the diagnostics buffers failed");
+  }
+  c->diag = *cfg;
+  c->diag_on = true;
+  c->diag_written = c->diag_read = 0;
+  return CUEVA_OK;
+}
+
+// writer unit 67 (22_writer.f95:1014-1019), evaluated on the host
+static void fill_delta_rec(const cueva_ctx* c, cueva_diag_record& r) {
+  const int jmed = c->jmax / 2;
+  const double posy = -(0.5 * c->diag.ly) + (double)(jmed + 1) * c->dely;
+  const double rr = std::sqrt(1.0 - (posy * posy) / (c->diag.lr * c->diag.lr));
+  r.v[CUEVA_DG_DELTA_REC] =
+      (((c->diag.b0 * rr) * std::tanh(c->delx / c->diag.delta_rec)) * c->diag.delta_rec) / r.v[CUEVA_DG_BY_MED];
+}
+
+int32_t cueva_diag_read(cueva_ctx* c, cueva_diag_record* out, int32_t max_records, int32_t* n_out) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!n_out || max_records < 0 || (max_records > 0 && !out)) return fail(CUEVA_ERR_ARG, "bad read arguments");
+  *n_out = 0;
+  if (!c->diag_on) return fail(CUEVA_ERR_ARG, "diagnostics are not enabled (cueva_diag_enable)");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  const long long cap = c->diag.capacity;
+  if (c->diag_written - c->diag_read > cap) c->diag_read = c->diag_written - cap;   // overwritten ones
+  const long long n = std::min<long long>(c->diag_written - c->diag_read, max_records);
+  for (long long k = 0; k < n;) {
+    const long long slot = (c->diag_read + k) % cap;
+    const long long run = std::min<long long>(n - k, cap - slot);
+    CUDA_TRY(cudaMemcpyAsync(out + k, c->d_diag_rec + slot, (size_t)run * sizeof(cueva_diag_record),
+                             cudaMemcpyDeviceToHost, c->stream));
+    k += run;
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (long long k = 0; k < n; ++k) fill_delta_rec(c, out[k]);
+  c->diag_read += n;
+  *n_out = (int32_t)n;
+  return read_status(c);
+}
+
+int32_t cueva_diag_now(cueva_ctx* c, cueva_diag_record* out) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!out) return fail(CUEVA_ERR_ARG, "null record");
+  if (!c->diag_on) return fail(CUEVA_ERR_ARG, "diagnostics are not enabled (cueva_diag_enable)");
+  if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  cueva_diag_record* slot = c->d_diag_rec + c->diag.capacity;
+  const double* a = c->h_inst.aux[c->cur];
+  CUDA_TRY(launch_diag(c->h_inst, c->cur, a + (long long)A_D * c->fstride, a + (long long)A_TAU * c->fstride,
+                       c->diag.b0, c->d_diag_part, c->h, c->t, slot, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(out, slot, sizeof(cueva_diag_record), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  fill_delta_rec(c, *out);
+  return read_status(c);
 }
 
 // ------------------------------------------------------------ routine mirrors

@@ -90,6 +90,7 @@ struct StageArgs {
   int need_intsum_load;  // stage l >= 2 and s >= 3: intsum_l is stored
   int need_intsum_store; // l + 1 < s
   int mode;            // 0 fused (next stage / final), 1 store rhs only
+  double* diag_cons;   // last stage: D and tau of varfin stored here (2 slabs) when non-null
 };
 
 // ---- small math helpers (Fortran semantics) ------------------------------

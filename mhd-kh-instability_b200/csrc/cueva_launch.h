@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <string>
 #include "cueva_common.cuh"
+#include "../../include/cueva.h"
 
 struct cueva_mlp;
 
@@ -37,4 +38,10 @@ cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* 
 cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int q,
                                   double abtll);
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);
+// run diagnostics of the prims in I.prim[cur] with the given D and tau slabs
+// (cueva_diag.cu): diag_blocks() rows of diag_partials() doubles of scratch
+int diag_blocks(int imax, int jmax);
+int diag_partials();
+cudaError_t launch_diag(const InstDesc& I, int cur, const double* D, const double* tau, double b0, double* part,
+                        long long h, double t, cueva_diag_record* rec, cudaStream_t st);
 }  // namespace cueva

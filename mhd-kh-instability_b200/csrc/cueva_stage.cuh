@@ -466,6 +466,8 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
       double Un[NCONS];
 #pragma unroll
       for (int c = 0; c < NCONS; ++c) Un[c] = U[c] + I.dt * fin[c];
+      // varfin's D and tau, which the run diagnostics read (con2prim does not write them back)
+      if (sa.diag_cons != nullptr && valid) { sa.diag_cons[pc] = Un[Q_D]; sa.diag_cons[fs + pc] = Un[Q_TAU]; }
       // con2prim, l_swap = 1 (main_cueva_code.f95:312-326)
       C2PIn in{Un[Q_D], Un[Q_TAU], Un[Q_SX], Un[Q_SY], Un[Q_SZ], Un[Q_EX], Un[Q_EY], Un[Q_EZ],
                Un[Q_BX], Un[Q_BY], Un[Q_BZ], vx, vy, vz, prim[P_RHO * fs + pc], prim[P_P * fs + pc]};

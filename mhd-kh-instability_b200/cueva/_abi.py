@@ -33,7 +33,8 @@ EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_s
            "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats", "cueva_ens_create", "cueva_ens_destroy",
            "cueva_ens_set_stream", "cueva_ens_set_prims", "cueva_ens_get_prims", "cueva_ens_kh_init",
            "cueva_ens_step", "cueva_ens_sync", "cueva_ens_set_shape", "cueva_ens_autotune",
-           "cueva_ens_attach_mlp", "cueva_ens_learned_stats"]
+           "cueva_ens_attach_mlp", "cueva_ens_learned_stats", "cueva_set_clock", "cueva_get_clock",
+           "cueva_diag_enable", "cueva_diag_read", "cueva_diag_now"]
 MLP_NPARAM, MLP_NNORM = 8833, 14
 
 
@@ -45,6 +46,28 @@ class Params(ctypes.Structure):
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double),
                 ("lz", ctypes.c_double), ("cfl", ctypes.c_double), ("sigma", ctypes.c_double),
                 ("gamma", ctypes.c_double), ("dt", ctypes.c_double)]
+
+
+# slots of cueva_diag_record.v (enum cueva_diag_slot); the writer's Fortran unit in brackets
+DIAG_SLOTS = ["sum_psi", "sum_phi", "sum_ex", "sum_ey", "sum_ez", "sum_exey", "sum_exez", "sum_eyez",
+              "sum_bx", "sum_by", "sum_bz", "sum_bxby", "sum_bxbz", "sum_bybz", "sum_vxvyvz", "sum_bxbybz",
+              "sum_vx", "sum_vy", "sum_vz", "sum_vxvy", "sum_vxvz", "sum_vyvz", "sum_q", "sum_p", "sum_rho",
+              "ekin_c", "ekin_r", "etot", "efluid_r", "emag", "eint_c", "eint_r", "lorentz", "sum_D",
+              "sum_D_med", "max_val_bx", "max_val_phi", "delta_rec_t", "Ez_med", "By_med",
+              "max_v", "max_W", "max_lambda_x", "max_lambda_y", "courant"]
+DIAG_UNITS = [80, 81, 82, 83, 84, 85, 86, 87, 88, 90, 91, 92, 93, 94, 95, 96, 97, 98, 99,
+              200, 201, 202, 203, 204, 205, 206, 207, 208, 209, 210, 211, 212, 213, 214, 215, 216, 217, 67, 68]
+NDIAG = len(DIAG_SLOTS)
+NDIAG_SUMS = 35
+
+
+class DiagRecord(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_int64), ("t", ctypes.c_double), ("v", ctypes.c_double * NDIAG)]
+
+
+class DiagConfig(ctypes.Structure):
+    _fields_ = [("hglb", ctypes.c_int32), ("capacity", ctypes.c_int32), ("b0", ctypes.c_double),
+                ("lr", ctypes.c_double), ("ly", ctypes.c_double), ("delta_rec", ctypes.c_double)]
 
 
 class CuevaError(RuntimeError):
@@ -115,6 +138,11 @@ def load(fma=False):
     L.cueva_ens_autotune.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(dbl)]
     L.cueva_ens_attach_mlp.argtypes = [vp, vp]
     L.cueva_ens_learned_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.cueva_set_clock.argtypes = [vp, i64, dbl]
+    L.cueva_get_clock.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(dbl)]
+    L.cueva_diag_enable.argtypes = [vp, ctypes.POINTER(DiagConfig)]
+    L.cueva_diag_read.argtypes = [vp, ctypes.POINTER(DiagRecord), i32, ctypes.POINTER(i32)]
+    L.cueva_diag_now.argtypes = [vp, ctypes.POINTER(DiagRecord)]
     L.cueva_flux_rhs_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp, vp, i32, ctypes.c_int64, vp,
                                          ctypes.POINTER(u32)]
     _LIBS[key] = L

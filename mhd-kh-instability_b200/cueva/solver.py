@@ -110,6 +110,52 @@ class Cueva:
     def set_stream(self, stream_ptr):
         _abi.check(self.L, self.L.cueva_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
 
+    # ------------------------------------------------------- clock and diagnostics
+    def set_clock(self, h, t):
+        """Step index h of the last completed step and t_advance (restarts)."""
+        _abi.check(self.L, self.L.cueva_set_clock(self.ctx, int(h), float(t)))
+
+    def clock(self):
+        h, t = ctypes.c_int64(), ctypes.c_double()
+        _abi.check(self.L, self.L.cueva_get_clock(self.ctx, ctypes.byref(h), ctypes.byref(t)))
+        return h.value, t.value
+
+    def diag_enable(self, hglb=1, capacity=1024, b0=0.1, lr=3.0, ly=None, delta_rec=None):
+        """Device-side records of the writer's diagnostics after every step h
+        with h == 1 or h % hglb == 0 (22_writer.f95:821-1019).  Defaults are
+        the reference's parameters.f95 values: B0 = 0.1, Lr = 3, Ly = the
+        context's y length, delta_rec = a_tm = S_l**(-1/3) * Lr with S_l = 1e3."""
+        if ly is None:
+            ly = self.params.ly
+        if delta_rec is None:
+            delta_rec = 1.0e3 ** (-1.0 / 3.0) * lr
+        self._diag_cfg = _abi.DiagConfig(int(hglb), int(capacity), b0, lr, ly, delta_rec)
+        _abi.check(self.L, self.L.cueva_diag_enable(self.ctx, ctypes.byref(self._diag_cfg)))
+
+    def diag_disable(self):
+        _abi.check(self.L, self.L.cueva_diag_enable(self.ctx, None))
+
+    @staticmethod
+    def _records_to_dict(recs):
+        out = {"h": np.array([r.h for r in recs], dtype=np.int64), "t": np.array([r.t for r in recs])}
+        vals = np.array([list(r.v) for r in recs]).reshape(len(recs), _abi.NDIAG)
+        for k, name in enumerate(_abi.DIAG_SLOTS):
+            out[name] = vals[:, k]
+        return out
+
+    def diagnostics(self, max_records=1 << 16):
+        """Records appended since the last call, as {slot name: array over records}."""
+        buf = (_abi.DiagRecord * max_records)()
+        n = ctypes.c_int32()
+        _abi.check(self.L, self.L.cueva_diag_read(self.ctx, buf, max_records, ctypes.byref(n)))
+        return self._records_to_dict(buf[:n.value])
+
+    def diag_now(self):
+        """One record of the current device state (D, tau from startconvar)."""
+        r = _abi.DiagRecord()
+        _abi.check(self.L, self.L.cueva_diag_now(self.ctx, ctypes.byref(r)))
+        return {k: v[0] for k, v in self._records_to_dict([r]).items()}
+
     # ------------------------------------------------------- routine mirrors
     def startconvar(self):
         _abi.check(self.L, self.L.cueva_startconvar(self.ctx))

@@ -45,6 +45,21 @@ module cueva_gpu
      real(c_double)     :: lx, ly, lz, cfl, sigma, gamma, dt
   end type cueva_params
 
+  ! run diagnostics (enum cueva_diag_slot; Fortran index = C slot + 1):
+  ! v(1:35) the lector sums in unit order 80..88, 90..99, 200..215,
+  ! v(36:37) max_val_bx, max_val_phi (216, 217), v(38) delta_rec_t (67),
+  ! v(39) Ez(imed,jmed) (68), v(40) By(imed+1,jmed+1), v(41:45) Courant check
+  integer(c_int32_t), parameter :: CUEVA_NDIAG = 45
+  type, bind(c) :: cueva_diag_record
+     integer(c_int64_t) :: h
+     real(c_double)     :: t
+     real(c_double)     :: v(CUEVA_NDIAG)
+  end type cueva_diag_record
+  type, bind(c) :: cueva_diag_config
+     integer(c_int32_t) :: hglb, capacity
+     real(c_double)     :: b0, lr, ly, delta_rec
+  end type cueva_diag_config
+
   interface
      integer(c_int32_t) function cueva_ctx_create(p, ctx) bind(c, name="cueva_ctx_create")
        import :: c_int32_t, c_ptr, cueva_params
@@ -109,6 +124,29 @@ module cueva_gpu
        import :: c_int32_t, c_ptr
        type(c_ptr), value :: ctx
      end function cueva_con2prim
+     integer(c_int32_t) function cueva_set_clock(ctx, h, t) bind(c, name="cueva_set_clock")
+       import :: c_int32_t, c_int64_t, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), value :: h
+       real(c_double), value :: t
+     end function cueva_set_clock
+     integer(c_int32_t) function cueva_diag_enable(ctx, cfg) bind(c, name="cueva_diag_enable")
+       import :: c_int32_t, c_ptr, cueva_diag_config
+       type(c_ptr), value :: ctx
+       type(cueva_diag_config), intent(in) :: cfg
+     end function cueva_diag_enable
+     integer(c_int32_t) function cueva_diag_read(ctx, out, max_records, n_out) bind(c, name="cueva_diag_read")
+       import :: c_int32_t, c_ptr, cueva_diag_record
+       type(c_ptr), value :: ctx
+       type(cueva_diag_record), intent(out) :: out(*)
+       integer(c_int32_t), value :: max_records
+       integer(c_int32_t), intent(out) :: n_out
+     end function cueva_diag_read
+     integer(c_int32_t) function cueva_diag_now(ctx, out) bind(c, name="cueva_diag_now")
+       import :: c_int32_t, c_ptr, cueva_diag_record
+       type(c_ptr), value :: ctx
+       type(cueva_diag_record), intent(out) :: out
+     end function cueva_diag_now
   end interface
 
 contains

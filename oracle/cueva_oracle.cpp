@@ -1592,6 +1592,109 @@ struct Oracle {
     }
     return status;
   }
+  // ------------------------------------- 22_writer.f95:821-1019 (lector, DIM == 2)
+  // The writer's sums in its own loop order (i outer, j inner), each term
+  // evaluated as written; abs[k] collects sum |term| of every sum (both
+  // terms of eint_r and efluid_r).  The writer also stores W, epsiln,
+  // enthpy, E2 and B2 into the module arrays; startconvar recomputes all of
+  // them before they are read again, so they stay local here.
+  void lector(double B0, double Lr, double Ly, double delta_rec, double* v, double* ab) {
+    const double *psi = a("psi"), *phi = a("phi"), *Ex = a("Ex"), *Ey = a("Ey"), *Ez = a("Ez");
+    const double *Bx = a("Bx"), *By = a("By"), *Bz = a("Bz"), *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz");
+    const double *q = a("q"), *p = a("p"), *rho = a("rho"), *D = a("D"), *tau = a("tau");
+    double s[35] = {0.0}, sa[35] = {0.0};
+    double mbx = -INFINITY, mphi = -INFINITY, mv = -INFINITY, mW = -INFINITY, mlx = -INFINITY, mly = -INFINITY;
+    auto add = [&](int k, double t) { s[k] = s[k] + t; sa[k] = sa[k] + std::fabs(t); };
+    const double dx = Delx, dy = Dely;
+    for (int i = 0; i <= imax; ++i)
+      for (int j = 0; j <= jmax; ++j) {
+        const size_t k = id(i, j);
+        add(0, psi[k] * dx * dy);
+        add(1, phi[k] * dx * dy);
+        add(2, pw2(Ex[k]) * dx * dy);
+        add(3, pw2(Ey[k]) * dx * dy);
+        add(4, pw2(Ez[k]) * dx * dy);
+        add(5, Ex[k] * Ey[k] * dx * dy);
+        add(6, Ex[k] * Ez[k] * dx * dy);
+        add(7, Ey[k] * Ez[k] * dx * dy);
+        add(8, pw2(Bx[k]) * dx * dy);
+        add(9, pw2(By[k]) * dx * dy);
+        add(10, pw2(Bz[k]) * dx * dy);
+        mbx = std::fmax(mbx, Bx[k] / B0);      // max_bx(i,j) = Bx / B0
+        mphi = std::fmax(mphi, phi[k]);
+        add(11, Bx[k] * By[k] * dx * dy);
+        add(12, Bx[k] * Bz[k] * dx * dy);
+        add(13, By[k] * Bz[k] * dx * dy);
+        add(15, (pw2(Bx[k]) + pw2(By[k]) + pw2(Bz[k])) * dx * dy);   // sum_bxbybz
+        add(14, (pw2(Vx[k]) + pw2(Vy[k]) + pw2(Vz[k])) * dx * dy);   // sum_vxvyvz
+        add(16, pw2(Vx[k]) * dx * dy);
+        add(17, pw2(Vy[k]) * dx * dy);
+        add(18, pw2(Vz[k]) * dx * dy);
+        add(19, Vx[k] * Vy[k] * dx * dy);
+        add(20, Vx[k] * Vz[k] * dx * dy);
+        add(21, Vy[k] * Vz[k] * dx * dy);
+        add(22, q[k] * dx * dy);
+        add(23, p[k] * dx * dy);
+        add(24, rho[k] * dx * dy);
+        add(33, D[k] * dx * dy);
+        const double eps = p[k] / ((gamma - 1.0) * rho[k]);
+        const double enth = rho[k] * (1.0 + eps) + p[k];
+        const double W = 1.0 / std::sqrt(1.0 - (pw2(Vx[k]) + pw2(Vy[k]) + pw2(Vz[k])));
+        const double E2 = pw2(Ex[k]) + pw2(Ey[k]) + pw2(Ez[k]);
+        const double B2 = pw2(By[k]) + pw2(Bz[k]);
+        add(25, 0.5 * rho[k] * (pw2(Vx[k]) + pw2(Vy[k]) + pw2(Vz[k])) * dx * dy);   // ekin_c
+        add(26, D[k] * (W - 1.0) * dx * dy);                                        // ekin_r
+        add(30, rho[k] * eps * dx * dy);                                            // eint_c
+        {  // eint_r = eint_r + W**2 * (rho*eps + p) - p * Delx * Dely
+          const double t1 = pw2(W) * (rho[k] * eps + p[k]), t2 = p[k] * dx * dy;
+          s[31] = s[31] + t1 - t2;
+          sa[31] = sa[31] + std::fabs(t1) + std::fabs(t2);
+        }
+        add(27, tau[k] * dx * dy);                                                  // etot
+        {  // efluid_r = efluid_r + enthpy * W**2 - p * Delx * Dely
+          const double t1 = enth * pw2(W), t2 = p[k] * dx * dy;
+          s[28] = s[28] + t1 - t2;
+          sa[28] = sa[28] + std::fabs(t1) + std::fabs(t2);
+        }
+        add(29, 0.5 * (E2 + B2) * dx * dy);                                         // emag (0.5 is exact in REAL*4)
+        add(32, W * dx * dy);                                                       // lorentz
+        // Courant check (no counterpart in the writer)
+        const double V2 = pw2(Vx[k]) + pw2(Vy[k]) + pw2(Vz[k]);
+        const double cs2 = gamma * p[k] / enth;
+        mv = std::fmax(mv, std::sqrt(V2));
+        mW = std::fmax(mW, W);
+        mlx = std::fmax(mlx, sound_lambda(Vx[k], V2, cs2));
+        mly = std::fmax(mly, sound_lambda(Vy[k], V2, cs2));
+      }
+    const int imed1 = (int)std::floor(0.25 * imax), imed2 = (int)std::floor(0.75 * imax);
+    for (int i = imed1; i <= imed2; ++i)
+      for (int j = 0; j <= jmax; ++j) add(34, D[id(i, j)] * dx * dy);
+    for (int k = 0; k < 35; ++k) { v[k] = s[k]; if (ab) ab[k] = sa[k]; }
+    v[35] = mbx;
+    v[36] = mphi;
+    const int imed = imax / 2, jmed = jmax / 2;    // floor(0.5d0*imax), floor(0.5d0*jmax)
+    const double posy = -0.5 * Ly + (jmed + 1) * Dely;
+    const double r = std::sqrt(1.0 - pw2(posy) / pw2(Lr));
+    const double by = a("By")[id(std::min(imed + 1, imax), std::min(jmed + 1, jmax))];
+    v[37] = B0 * r * std::tanh(Delx / delta_rec) * delta_rec / by;
+    v[38] = a("Ez")[id(imed, jmed)];
+    v[39] = by;
+    v[40] = mv;
+    v[41] = mW;
+    v[42] = mlx;
+    v[43] = mly;
+    v[44] = std::fmax(Delt * (mlx / Delx), Delt * (mly / Dely));
+  }
+  // largest |lambda| of the two relativistic sound waves along a direction
+  // with normal velocity vn (cs2 = gamma p / (rho h))
+  static double sound_lambda(double vn, double V2, double cs2) {
+    const double cs = std::sqrt(cs2);
+    const double root = std::sqrt((1.0 - V2) * (1.0 - V2 * cs2 - vn * vn * (1.0 - cs2)));
+    const double den = 1.0 - cs2 * V2;
+    const double lp = (vn * (1.0 - cs2) + cs * root) / den;
+    const double lm = (vn * (1.0 - cs2) - cs * root) / den;
+    return std::fmax(std::fabs(lp), std::fabs(lm));
+  }
 };
 
 const char* prim_names[OR_NPRIM] = {"rho", "p", "Vx", "Vy", "Vz", "psi", "phi", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "q"};
@@ -1707,6 +1810,12 @@ int32_t oracle_c2p_nr(const double* in, double gamma, double* out) {
   int32_t st = c2p_nr(i, gamma, o);
   out[0] = o.vx; out[1] = o.vy; out[2] = o.vz; out[3] = o.rho; out[4] = o.p; out[5] = o.W;
   return st;
+}
+void oracle_lector(void* h, double b0, double lr, double ly, double delta_rec, int32_t d_from_startconvar,
+                   double* out45, double* abs45) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (d_from_startconvar) o->startconvar();
+  o->lector(b0, lr, ly, delta_rec, out45, abs45);
 }
 int32_t oracle_tableau(int32_t order, double* wb8, double* wbt8, double* ab64, double* abt64) {
   Tableau T;

@@ -81,6 +81,14 @@ double  oracle_hllc_vel(double a, double b, double c, double rt);
 int32_t oracle_c2p_cardano(const double* in16, double gamma, double eps1, double* out6);
 int32_t oracle_c2p_nr(const double* in16, double gamma, double* out6);
 int32_t oracle_tableau(int32_t order, double* wb8, double* wbt8, double* ab64, double* abt64);
+/* run diagnostics of the writer, 22_writer.f95:821-1019 (lector, DIM == 2),
+ * on the current state in its loop order; 45 slots in the order of cueva.h's
+ * cueva_diag_slot.  d_from_startconvar != 0 first recomputes D and tau from
+ * the primitives (a step-boundary state); otherwise D and tau are varfin's
+ * values left by oracle_step, as at the writer's call.  abs45 (nullable)
+ * receives sum |term| of each of the 35 sums. */
+void    oracle_lector(void* h, double b0, double lr, double ly, double delta_rec, int32_t d_from_startconvar,
+                      double* out45, double* abs45);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,7 @@ def lib():
         L.oracle_tableau.restype = ctypes.c_int32
         L.oracle_tableau.argtypes = [dp, dp, dp, dp]
         L.oracle_tableau.argtypes = [ctypes.c_int32, dp, dp, dp, dp]
+        L.oracle_lector.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 4 + [ctypes.c_int32, dp, dp]
         _LIB = L
     return _LIB
 
@@ -139,6 +140,16 @@ class Oracle:
         c = (ctypes.c_int64 * 3)()
         lib().oracle_counters(self.h, c)
         return list(c)
+
+    def lector(self, b0=0.1, lr=3.0, ly=1.0, delta_rec=None, from_startconvar=False):
+        """Writer diagnostics (22_writer.f95:821-1019) of the current state:
+        (45 values in cueva_diag_slot order, sum |term| of the 35 sums)."""
+        if delta_rec is None:
+            delta_rec = 1.0e3 ** (-1.0 / 3.0) * lr
+        v = np.zeros(45)
+        ab = np.zeros(45)
+        lib().oracle_lector(self.h, b0, lr, ly, delta_rec, 1 if from_startconvar else 0, _dp(v), _dp(ab))
+        return v, ab
 
 
 def kh_init(imax, jmax, lx=2.0, ly=1.0, v0=0.5, a=0.01, amp=0.01, width=0.01, kpert=2 * np.pi,

@@ -80,3 +80,17 @@ def test_create_without_gpu_fails_loudly():
         assert rc == 0
     else:
         assert rc == 2 and "device" in msg
+
+
+def test_diag_record_table_matches_header():
+    """The Python slot table follows enum cueva_diag_slot, and its writer
+    units are the bracketed units of the header comments."""
+    from cueva import _abi
+    text = open(HEADER).read()
+    body = text[text.index("enum cueva_diag_slot {"):text.index("CUEVA_NDIAG\n")]
+    slots = re.findall(r"^\s*CUEVA_DG_(\w+)", body, re.M)
+    assert len(slots) == _abi.NDIAG == len(_abi.DIAG_SLOTS)
+    units = [int(u) for u in re.findall(r"/\* \[(\d+)\]", body)]
+    assert units == _abi.DIAG_UNITS
+    assert ctypes.sizeof(_abi.DiagRecord) == 16 + 8 * _abi.NDIAG
+    assert ctypes.sizeof(_abi.DiagConfig) == 8 + 4 * 8
