@@ -6,7 +6,7 @@
  * and write module arrays dimensioned (-6:imax+6, -6:jmax+6[, 1:kmax, 1:lmax])
  * (threevectors.f95:12-81, fourvectors.f95:12-170).  A Fortran caller keeps
  * those arrays and binds them here once with c_loc(array(-6,-6,1[,1]))
- * (see fortran/cueva_gpu.f90 and INTEGRATION.md); this library mirrors them on
+ * (see fortran/cueva_gpu.f90); this library mirrors them on
  * the GPU and replaces the routines listed next to each entry point.
  *
  * Conventions: every entry point returns 0 (CUEVA_OK) or a positive error
@@ -355,6 +355,34 @@ int32_t cueva_diag_read(cueva_ctx* ctx, cueva_diag_record* out, int32_t max_reco
  * D and tau here are startconvar's values of the current primitives.
  * Needs a config from cueva_diag_enable for B0, Lr, Ly and delta_rec. */
 int32_t cueva_diag_now(cueva_ctx* ctx, cueva_diag_record* out);
+
+/* ---- checkpoint / restart --------------------------------------------- */
+/* Binary checkpoint of the device state at a step boundary: the 14 carried
+ * primitives (all a step reads: startconvar rebuilds the rest) and the
+ * clock, with the grid, the writing configuration and a checksum in the
+ * header.  Loading needs a context of the same grid; it replaces the device
+ * state and the clock, prepares stage 1 like cueva_upload, and leaves the
+ * bound host arrays alone.  A run continued from a checkpoint is
+ * bit-identical to the uninterrupted run.  No counterpart in the reference
+ * (which restarts from its text backups, below). */
+int32_t cueva_checkpoint_save(cueva_ctx* ctx, const char* path);
+int32_t cueva_checkpoint_load(cueva_ctx* ctx, const char* path);
+/* The reference's backup text files all_variables_NNNN.dat: written by the
+ * writer every hloc steps (22_writer.f95:1134-1150), read by init_restart
+ * (03_restart_primitive.f95:51-57).  One list-directed record per point,
+ * i = -6..imax+6 outer, j = -6..jmax+6 inner, values psi phi Bx By Bz Vx Vy
+ * Vz Ex Ey Ez q rho p, ghosts included.  fields[CUEVA_RHO .. CUEVA_Q] are
+ * the 14 primitive host arrays in the Fortran layout (base = element
+ * (-6,-6)).  The reader follows list-directed input (separators, repeat
+ * counts, null values, slash, E/D/Q exponents and letter-less exponents such
+ * as 1.0-100, records spanning lines); the writer prints 17 significant
+ * digits, so a write-read round trip is exact, and like the reference it
+ * refuses to replace an existing file unless overwrite != 0.  nthreads <= 0
+ * uses every host core.  Host only: no GPU needed. */
+int32_t cueva_read_all_variables(const char* path, int32_t imax, int32_t jmax, double* const* fields,
+                                 int32_t nthreads);
+int32_t cueva_write_all_variables(const char* path, int32_t imax, int32_t jmax, const double* const* fields,
+                                  int32_t overwrite, int32_t nthreads);
 
 /* ---- synthetic input ------------------------------------------------- */
 /* Kelvin-Helmholtz initial data on the Fortran-layout prim arrays bound to

@@ -692,6 +692,94 @@ int32_t cueva_diag_now(cueva_ctx* c, cueva_diag_record* out) {
   return read_status(c);
 }
 
+// ------------------------------------------------------------ checkpoints
+struct CkHeader {
+  char magic[8];          // "CUEVACK1"
+  uint32_t version;       // 1
+  uint32_t header_bytes;  // sizeof(CkHeader)
+  int32_t imax, jmax, nfields, pad;
+  int64_t h;              // clock of the state
+  double t;
+  cueva_params params;    // configuration that wrote it (informational)
+  uint64_t checksum;      // FNV-1a over the payload's 64-bit words
+};
+
+static uint64_t ck_hash(const double* p, size_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t k = 0; k < n; ++k) {
+    uint64_t w;
+    std::memcpy(&w, p + k, 8);
+    h = (h ^ w) * 1099511628211ull;
+  }
+  return h;
+}
+
+int32_t cueva_checkpoint_save(cueva_ctx* c, const char* path) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!path) return fail(CUEVA_ERR_ARG, "null path");
+  if (!c->primed) return fail(CUEVA_ERR_UNBOUND, "no state on the device: cueva_upload(CUEVA_G_PRIMS) first");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  const size_t npt = (size_t)c->nx * c->ny;
+  std::vector<double> buf((size_t)NPRIM * npt);
+  for (int f = 0; f < NPRIM; ++f)
+    CUDA_TRY(cudaMemcpy2DAsync(buf.data() + f * npt, (size_t)c->nx * 8, prim_f(c, c->cur, f), (size_t)c->pitch * 8,
+                               (size_t)c->nx * 8, (size_t)c->ny, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (int32_t e = read_status(c)) return e;   // a non-physical state is not written
+  CkHeader hd{};
+  std::memcpy(hd.magic, "CUEVACK1", 8);
+  hd.version = 1;
+  hd.header_bytes = sizeof(CkHeader);
+  hd.imax = c->imax; hd.jmax = c->jmax; hd.nfields = NPRIM;
+  hd.h = c->h; hd.t = c->t;
+  hd.params = c->P;
+  hd.checksum = ck_hash(buf.data(), buf.size());
+  const std::string tmp = std::string(path) + ".partial";
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return fail(CUEVA_ERR_ARG, "cannot create " + tmp);
+  const bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1 && std::fwrite(buf.data(), 8, buf.size(), f) == buf.size();
+  if (std::fclose(f) != 0 || !ok || std::rename(tmp.c_str(), path) != 0) {
+    std::remove(tmp.c_str());
+    return fail(CUEVA_ERR_ARG, std::string("cannot write ") + path);
+  }
+  return CUEVA_OK;
+}
+
+int32_t cueva_checkpoint_load(cueva_ctx* c, const char* path) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (!path) return fail(CUEVA_ERR_ARG, "null path");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(CUEVA_ERR_ARG, std::string("cannot open ") + path);
+  CkHeader hd{};
+  if (std::fread(&hd, sizeof hd, 1, f) != 1 || std::memcmp(hd.magic, "CUEVACK1", 8) != 0 || hd.version != 1 ||
+      hd.header_bytes != sizeof(CkHeader) || hd.nfields != NPRIM) {
+    std::fclose(f);
+    return fail(CUEVA_ERR_ARG, std::string(path) + " is not a version-1 cueva checkpoint");
+  }
+  if (hd.imax != c->imax || hd.jmax != c->jmax) {
+    std::fclose(f);
+    return fail(CUEVA_ERR_ARG, "checkpoint grid " + std::to_string(hd.imax) + " x " + std::to_string(hd.jmax) +
+                                   " does not match the context's " + std::to_string(c->imax) + " x " +
+                                   std::to_string(c->jmax));
+  }
+  const size_t npt = (size_t)c->nx * c->ny;
+  std::vector<double> buf((size_t)NPRIM * npt);
+  const size_t got = std::fread(buf.data(), 8, buf.size(), f);
+  const bool extra = std::fgetc(f) != EOF;
+  std::fclose(f);
+  if (got != buf.size() || extra) return fail(CUEVA_ERR_ARG, std::string(path) + ": wrong payload size");
+  if (ck_hash(buf.data(), buf.size()) != hd.checksum) return fail(CUEVA_ERR_ARG, std::string(path) + ": checksum mismatch");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int k = 0; k < NPRIM; ++k)
+    CUDA_TRY(cudaMemcpy2DAsync(prim_f(c, c->cur, k), (size_t)c->pitch * 8, buf.data() + k * npt, (size_t)c->nx * 8,
+                               (size_t)c->nx * 8, (size_t)c->ny, cudaMemcpyHostToDevice, c->stream));
+  if (int32_t e = run_begin_step(c)) return e;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));   // buf is released on return
+  c->h = hd.h;
+  c->t = hd.t;
+  return CUEVA_OK;
+}
+
 // ------------------------------------------------------------ routine mirrors
 int32_t cueva_startconvar(cueva_ctx* c) {
   if (int32_t e = check_ctx(c)) return e;

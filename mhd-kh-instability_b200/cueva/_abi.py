@@ -34,7 +34,8 @@ EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_s
            "cueva_ens_set_stream", "cueva_ens_set_prims", "cueva_ens_get_prims", "cueva_ens_kh_init",
            "cueva_ens_step", "cueva_ens_sync", "cueva_ens_set_shape", "cueva_ens_autotune",
            "cueva_ens_attach_mlp", "cueva_ens_learned_stats", "cueva_set_clock", "cueva_get_clock",
-           "cueva_diag_enable", "cueva_diag_read", "cueva_diag_now"]
+           "cueva_diag_enable", "cueva_diag_read", "cueva_diag_now", "cueva_checkpoint_save",
+           "cueva_checkpoint_load", "cueva_read_all_variables", "cueva_write_all_variables"]
 MLP_NPARAM, MLP_NNORM = 8833, 14
 
 
@@ -143,6 +144,11 @@ def load(fma=False):
     L.cueva_diag_enable.argtypes = [vp, ctypes.POINTER(DiagConfig)]
     L.cueva_diag_read.argtypes = [vp, ctypes.POINTER(DiagRecord), i32, ctypes.POINTER(i32)]
     L.cueva_diag_now.argtypes = [vp, ctypes.POINTER(DiagRecord)]
+    L.cueva_checkpoint_save.argtypes = [vp, ctypes.c_char_p]
+    L.cueva_checkpoint_load.argtypes = [vp, ctypes.c_char_p]
+    dpp = ctypes.POINTER(ctypes.POINTER(dbl))
+    L.cueva_read_all_variables.argtypes = [ctypes.c_char_p, i32, i32, dpp, i32]
+    L.cueva_write_all_variables.argtypes = [ctypes.c_char_p, i32, i32, dpp, i32, i32]
     L.cueva_flux_rhs_noalloc.argtypes = [ctypes.POINTER(Params), vp, vp, vp, vp, i32, ctypes.c_int64, vp,
                                          ctypes.POINTER(u32)]
     _LIBS[key] = L
@@ -153,3 +159,15 @@ def check(L, rc):
     if rc != CUEVA_OK:
         raise CuevaError(rc, L.cueva_last_error().decode())
     return rc
+
+
+def field_table(arrays):
+    """ctypes table of pointers indexed by enum cueva_field for the 14
+    primitive arrays in `arrays` (name -> Fortran-layout float64 array)."""
+    tab = (ctypes.POINTER(ctypes.c_double) * len(PRIM_FIELDS))()
+    for k, n in enumerate(PRIM_FIELDS):
+        a = arrays[n]
+        if a.dtype != "float64" or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"{n}: a C-contiguous float64 array is required")
+        tab[k] = a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return tab

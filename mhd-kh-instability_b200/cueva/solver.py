@@ -156,6 +156,27 @@ class Cueva:
         _abi.check(self.L, self.L.cueva_diag_now(self.ctx, ctypes.byref(r)))
         return {k: v[0] for k, v in self._records_to_dict([r]).items()}
 
+    # ------------------------------------------------------- checkpoint / restart
+    def checkpoint_save(self, path):
+        """Binary checkpoint of the device state and the clock."""
+        _abi.check(self.L, self.L.cueva_checkpoint_save(self.ctx, str(path).encode()))
+
+    def checkpoint_load(self, path):
+        """Replaces the device state and the clock with a checkpoint of the same grid."""
+        _abi.check(self.L, self.L.cueva_checkpoint_load(self.ctx, str(path).encode()))
+
+    def write_all_variables(self, path, overwrite=False, nthreads=0):
+        """The bound host primitives (ghosts included) as the reference's
+        backup file all_variables_NNNN.dat (22_writer.f95:1134-1150)."""
+        write_all_variables(path, self.imax, self.jmax, {n: self.array(n) for n in _abi.PRIM_FIELDS},
+                            overwrite=overwrite, nthreads=nthreads, lib=self.L)
+
+    def read_all_variables(self, path, nthreads=0):
+        """Fills the bound host primitives from a backup file, as
+        init_restart does (03_restart_primitive.f95:51-57); upload() next."""
+        read_all_variables(path, self.imax, self.jmax, {n: self.array(n) for n in _abi.PRIM_FIELDS},
+                           nthreads=nthreads, lib=self.L)
+
     # ------------------------------------------------------- routine mirrors
     def startconvar(self):
         _abi.check(self.L, self.L.cueva_startconvar(self.ctx))
@@ -186,3 +207,21 @@ class Cueva:
             self.close()
         except Exception:
             pass
+
+
+def read_all_variables(path, imax, jmax, arrays=None, nthreads=0, lib=None):
+    """Reads a backup file into Fortran-layout arrays (shape (jmax+13,
+    imax+13), ghosts included); returns {primitive name: array}.  Host only."""
+    L = lib or _abi.load(False)
+    if arrays is None:
+        arrays = {n: np.zeros((jmax + 13, imax + 13)) for n in _abi.PRIM_FIELDS}
+    _abi.check(L, L.cueva_read_all_variables(str(path).encode(), int(imax), int(jmax), _abi.field_table(arrays),
+                                             int(nthreads)))
+    return arrays
+
+
+def write_all_variables(path, imax, jmax, arrays, overwrite=False, nthreads=0, lib=None):
+    """Writes Fortran-layout primitive arrays as a backup file.  Host only."""
+    L = lib or _abi.load(False)
+    _abi.check(L, L.cueva_write_all_variables(str(path).encode(), int(imax), int(jmax), _abi.field_table(arrays),
+                                              1 if overwrite else 0, int(nthreads)))

@@ -4,7 +4,7 @@
 ! or tested here; the C++ stand-in driver (host/cueva_driver.cpp) exercises
 ! the same calls on arrays with the Fortran layout.
 !
-! Use from the reference driver (see INTEGRATION.md):
+! Use from the reference driver:
 !   use cueva_gpu
 !   type(c_ptr) :: ctx
 !   call cueva_attach(ctx)                       ! after init_var_primitive
