@@ -40,6 +40,7 @@ extern "C" {
 #define CUEVA_ST_HLLC_VSTAR 8u      /* 16_hllc_flow_mpx.f95:4294,4605 */
 #define CUEVA_ST_NONFINITE 16u      /* con2prim returned NaN/Inf (the reference continues silently) */
 #define CUEVA_ST_HLLE_SPEED 32u     /* 16_hlle_flow_mpx.f95:2796-2803, 2974-2981 (NaN wave bounds) */
+#define CUEVA_ST_TC_TIMEOUT 64u     /* a bounded tensor-core (tcgen05) wait ran out; no reference counterpart */
 
 typedef struct cueva_ctx cueva_ctx;
 
@@ -178,8 +179,9 @@ int32_t cueva_mlp_train(cueva_mlp* mlp, const double* d_cons, const double* d_p,
 int32_t cueva_mlp_gradients(cueva_mlp* mlp, const double* d_cons, const double* d_p, int32_t n, float* grads,
                             float* loss_out);
 /* network pressure seeds of n states (device out): per thread in FP32
- * (tensor_cores = 0) or warp-cooperative with bf16 tensor-core MMA and bf16
- * activations (1, the form the fused step uses) */
+ * (tensor_cores = 0), warp-cooperative mma.sync with bf16 activations (1),
+ * or tcgen05 MMA on tiles of 128 states with the accumulator in tensor
+ * memory and bf16 activations (2, the form the step uses by default) */
 int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed, int32_t tensor_cores);
 /* batch con2prim for comparisons: method 1 Cardano, 2 network seed + Newton,
  * 3 Newton from d_seed; d_prev (5 x n) are the previous primitives the
@@ -190,6 +192,12 @@ int32_t cueva_c2p_batch(int32_t device, int32_t method, const cueva_mlp* mlp, do
                         int32_t* d_iters);
 /* copy a trained network into ctx; con2prim uses it when params.c2p == 2 */
 int32_t cueva_attach_mlp(cueva_ctx* ctx, const cueva_mlp* mlp);
+/* where the learned con2prim runs: 1 (set by cueva_attach_mlp) = a kernel of
+ * its own after the last RK stage, network on the tcgen05 tensor cores in
+ * tiles of 128 points, Newton in FP64, Cardano fall-back, then the next
+ * step's startconvar; 0 = inside the last stage's update with warp mma.sync
+ * inference (the earlier form, kept for comparison) */
+int32_t cueva_set_learned_kernel(cueva_ctx* ctx, int32_t mode);
 /* Newton iterations, points and Cardano fall-backs of the learned path so far */
 int32_t cueva_learned_stats(cueva_ctx* ctx, int64_t out3[3]);
 
@@ -221,6 +229,7 @@ int32_t cueva_ens_set_shape(cueva_ens* ens, int32_t rows, int32_t ctas_per_sm);
  * restores the state; reports the choice and its ms per step */
 int32_t cueva_ens_autotune(cueva_ens* ens, int32_t* rows, int32_t* ctas_per_sm, double* ms_per_step);
 int32_t cueva_ens_attach_mlp(cueva_ens* ens, const cueva_mlp* mlp);
+int32_t cueva_ens_set_learned_kernel(cueva_ens* ens, int32_t mode);   /* as cueva_set_learned_kernel */
 int32_t cueva_ens_learned_stats(cueva_ens* ens, int64_t out3[3]);
 
 /* ---- stage right-hand side without any device allocation -------------- */

@@ -209,6 +209,9 @@ void fill_desc(const cueva_params* p, const InstGeom& G, int nkslot, double* sla
   // the Fortran module variable eps1 keeps the value the flux routine stored last
   I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
   I.c2p = p->c2p;
+  I.c2p_tc = 0;
+  I.block_begin[LK_C2P] = 0;
+  I.block_count[LK_C2P] = c2p_tiles(G.imax, G.jmax);
 }
 
 }  // namespace
@@ -286,7 +289,7 @@ int32_t read_status(cueva_ctx* c) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st) {
     char buf[160];
-    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed)", st);
+    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed, 64 tensor-core wait)", st);
     return fail(CUEVA_ERR_PHYSICS, buf);
   }
   return CUEVA_OK;
@@ -339,6 +342,8 @@ int32_t run_begin_step(cueva_ctx* c) {
   return CUEVA_OK;
 }
 
+bool learned_tc(const InstDesc& I, const MLPDevice* d_mlp) { return I.c2p == 2 && I.c2p_tc && d_mlp; }
+
 int32_t enqueue_step(cueva_ctx* c, double* diag_cons = nullptr) {
   for (int l = 1; l <= c->T.s; ++l) {
     StageArgs sa = stage_args(c, l, 0);
@@ -346,6 +351,9 @@ int32_t enqueue_step(cueva_ctx* c, double* diag_cons = nullptr) {
     CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1, sa));
     c->qin ^= 1;
   }
+  if (learned_tc(c->h_inst, c->d_mlp))   // con2prim of the learned method and the next stage 1
+    CUDA_TRY(launch_c2p_step(c->stream, c->d_inst, 1, c->h_inst.block_count[LK_C2P], c->d_mlp, c->cur, c->qin,
+                             c->T.Abt[0][0]));
   c->cur ^= 1;
   return CUEVA_OK;
 }
@@ -570,6 +578,19 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
         launches_out[k] += 1;
       }
       c->qin ^= 1;
+    }
+    if (rc == CUEVA_OK && learned_tc(c->h_inst, c->d_mlp)) {
+      cudaError_t ce = cudaEventRecord(ev[0], c->stream);
+      if (ce == cudaSuccess)
+        ce = launch_c2p_step(c->stream, c->d_inst, 1, c->h_inst.block_count[LK_C2P], c->d_mlp, c->cur, c->qin,
+                             c->T.Abt[0][0]);
+      if (ce == cudaSuccess) ce = cudaEventRecord(ev[1], c->stream);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[1]);
+      if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      ms_out[2] += ms;
+      launches_out[2] += 1;
     }
     c->cur ^= 1;
     c->h += 1;
@@ -874,6 +895,19 @@ int32_t cueva_attach_mlp(cueva_ctx* c, const cueva_mlp* mlp) {
   CUDA_TRY(cudaMemcpy(c->d_mlp, &h, sizeof(MLPDevice), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemset(c->d_mlp_stats, 0, 3 * sizeof(unsigned long long)));
   c->h_inst.mlp = c->d_mlp;
+  c->h_inst.c2p_tc = 1;
+  destroy_graphs(c);   // the step gains the con2prim launch
+  CUDA_TRY(cudaMemcpy(c->d_inst, &c->h_inst, sizeof(InstDesc), cudaMemcpyHostToDevice));
+  return CUEVA_OK;
+}
+
+int32_t cueva_set_learned_kernel(cueva_ctx* c, int32_t mode) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (mode != 0 && mode != 1) return fail(CUEVA_ERR_ARG, "mode must be 0 (in the last stage) or 1 (tensor-core kernel)");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->h_inst.c2p_tc = mode;
+  destroy_graphs(c);
   CUDA_TRY(cudaMemcpy(c->d_inst, &c->h_inst, sizeof(InstDesc), cudaMemcpyHostToDevice));
   return CUEVA_OK;
 }
@@ -1044,6 +1078,7 @@ struct cueva_ens {
   unsigned long long* d_mlp_stats = nullptr;
   long long max_points = 0;
   int num_sms = 148;
+  int c2p_ntiles = 0;     // tiles of the learned con2prim launch over all instances
 };
 
 namespace {
@@ -1056,13 +1091,15 @@ void ens_destroy_graphs(cueva_ens* e) {
 
 // tile ranges for a tile height and the launch grid for a CTA count per SM
 int32_t ens_apply_shape(cueva_ens* e, int rows, int ctas_per_sm) {
-  int begin[2] = {0, 0};
+  int begin[3] = {0, 0, 0};
   for (int k = 0; k < e->n; ++k) {
     InstDesc& I = e->I[k];
     I.block_count[LK_XUPD] = xupd_tiles(I.imax, I.jmax, rows);
     I.block_count[LK_YFACE] = yface_tiles(I.imax, I.jmax, rows);
-    for (int t = 0; t < 2; ++t) { I.block_begin[t] = begin[t]; begin[t] += I.block_count[t]; }
+    I.block_count[LK_C2P] = c2p_tiles(I.imax, I.jmax);
+    for (int t = 0; t < 3; ++t) { I.block_begin[t] = begin[t]; begin[t] += I.block_count[t]; }
   }
+  e->c2p_ntiles = begin[LK_C2P];
   e->shape.rows = rows;
   for (int t = 0; t < 2; ++t) {
     e->shape.ntiles[t] = begin[t];
@@ -1088,6 +1125,10 @@ int32_t ens_enqueue_step(cueva_ens* e) {
     CUDA_TRY(launch_stage(e->P0.rec_mp, e->P0.flux_solver, e->P0.precision, e->shape, e->stream, e->d_inst, e->n, sa));
     e->qin ^= 1;
   }
+  bool any = false;
+  for (const auto& I : e->I) any = any || learned_tc(I, e->d_mlp);
+  if (any)   // one con2prim launch over the tiles of every instance with the learned method
+    CUDA_TRY(launch_c2p_step(e->stream, e->d_inst, e->n, e->c2p_ntiles, e->d_mlp, e->cur, e->qin, e->T.Abt[0][0]));
   e->cur ^= 1;
   return CUEVA_OK;
 }
@@ -1289,7 +1330,19 @@ int32_t cueva_ens_attach_mlp(cueva_ens* e, const cueva_mlp* mlp) {
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   CUDA_TRY(cudaMemcpy(e->d_mlp, &h, sizeof(MLPDevice), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemset(e->d_mlp_stats, 0, 3 * sizeof(unsigned long long)));
-  for (auto& I : e->I) I.mlp = e->d_mlp;
+  for (auto& I : e->I) { I.mlp = e->d_mlp; I.c2p_tc = 1; }
+  ens_destroy_graphs(e);   // the step gains the con2prim launch
+  CUDA_TRY(cudaMemcpy(e->d_inst, e->I.data(), sizeof(InstDesc) * e->n, cudaMemcpyHostToDevice));
+  return CUEVA_OK;
+}
+
+int32_t cueva_ens_set_learned_kernel(cueva_ens* e, int32_t mode) {
+  if (!e) return fail(CUEVA_ERR_ARG, "null ensemble");
+  if (mode != 0 && mode != 1) return fail(CUEVA_ERR_ARG, "mode must be 0 (in the last stage) or 1 (tensor-core kernel)");
+  CUDA_TRY(cudaSetDevice(e->dev));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  for (auto& I : e->I) I.c2p_tc = mode;
+  ens_destroy_graphs(e);
   CUDA_TRY(cudaMemcpy(e->d_inst, e->I.data(), sizeof(InstDesc) * e->n, cudaMemcpyHostToDevice));
   return CUEVA_OK;
 }

@@ -1,0 +1,151 @@
+// cueva_c2p.cu -- con2prim with the learned seed on the tcgen05 tensor cores,
+// as a kernel of its own after the last RK stage.
+//
+// With the learned method the last stage's update stops after varfin: it
+// stores the new psi, phi, E, B, q as primitives and the evolved D, tau, S
+// in the (consumed) final-sum slabs.  k_c2p_step then recovers rho, p, v in
+// tiles of 128 points -- network seed on the tensor cores (cueva_mlp_tc.cuh),
+// Newton-Raphson in FP64, the reference's Cardano recovery when Newton fails
+// -- and runs the next step's startconvar and stage-1 preparation, exactly
+// as the fused epilogue does for the other methods.  Keeping the network
+// out of the stencil kernel leaves that kernel's registers and occupancy
+// alone and lets the network run at tensor-core rate with its weights
+// staged once per CTA.
+#include "cueva_launch.h"
+#include "cueva_mlp_tc.cuh"
+#include "cueva_stage.cuh"
+
+namespace cueva {
+namespace {
+
+constexpr int C2P_CTAS_PER_SM = 4;
+
+// one point of the learned con2prim (all 128 threads of the CTA call it, in
+// step): seeds p from the network, refines it, falls back to Cardano
+struct LearnedOut {
+  C2POut o;
+  uint32_t st;
+  int it;
+};
+__device__ __forceinline__ bool learned_point(MLPShared& S, uint32_t& phase, const C2PIn& in, double gamma,
+                                              double eps1, unsigned long long* counters, bool count, LearnedOut& r) {
+  float f[MLP_IN];
+  c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
+  float y = 0.0f;
+  if (!mlp_tc_tile(S, phase, f, y)) return false;
+  const double seed = in.D * (double)__expf(y * S.sd_y + S.mu_y);
+  r.it = c2p_newton(in, gamma, seed, r.o);
+  r.st = 0u;
+  if (r.it <= 0) r.st = c2p_cardano_ool(in, gamma, eps1, r.o, count ? counters : nullptr);
+  if (!(isfinite(r.o.rho) && isfinite(r.o.p) && isfinite(r.o.vx) && isfinite(r.o.vy) && isfinite(r.o.vz)))
+    r.st |= ST_NONFINITE;
+  return true;
+}
+
+// Newton iterations, points and Cardano fall-backs: one atomic per warp and counter
+__device__ __forceinline__ void learned_stats(unsigned long long* stats, bool count, int it) {
+  if (!stats) return;
+  const unsigned its = __reduce_add_sync(0xffffffffu, count ? (unsigned)(it > 0 ? it : MLP_NR_MAXIT) : 0u);
+  const unsigned pts = __reduce_add_sync(0xffffffffu, count ? 1u : 0u);
+  const unsigned nfail = __reduce_add_sync(0xffffffffu, (count && it <= 0) ? 1u : 0u);
+  if ((threadIdx.x & 31) == 0) {
+    if (pts) { atomicAdd(&stats[0], (unsigned long long)its); atomicAdd(&stats[1], (unsigned long long)pts); }
+    if (nfail) atomicAdd(&stats[2], (unsigned long long)nfail);
+  }
+}
+
+// the tail of the step for the instances with the learned method: tiles of
+// 128 points over all instances (block ranges of launch kind LK_C2P)
+__global__ void __launch_bounds__(TC_ROWS, C2P_CTAS_PER_SM)
+k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPDevice* __restrict__ mlp, int cur,
+           int qout, double abt11) {
+  __shared__ MLPShared S;
+  mlp_tc_setup(S, *mlp);
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int b = tile;
+    const InstDesc& I = tile_inst(insts, ninst, LK_C2P, b);
+    if (!(I.c2p == 2 && I.c2p_tc)) continue;   // uniform over the CTA: a tile belongs to one instance
+    const int nx = I.imax + 1;
+    const long long npts = (long long)nx * (I.jmax + 1);
+    const long long p0 = (long long)b * TC_ROWS + threadIdx.x;
+    const bool valid = p0 < npts;
+    const long long p = valid ? p0 : npts - 1;   // rows past the end repeat the last point
+    const int i = int(p % nx), j = int(p / nx);
+    const long long fs = I.fstride, pc = (long long)j * I.pitch + i;
+    const double* un = I.finsum;        // varfin's D, tau, S in the slabs Q_D .. Q_SZ
+    const double* pold = I.prim[cur];
+    double* pn = I.prim[1 - cur];
+    const C2PIn in{un[Q_D * fs + pc], un[Q_TAU * fs + pc], un[Q_SX * fs + pc], un[Q_SY * fs + pc],
+                   un[Q_SZ * fs + pc], pn[P_EX * fs + pc], pn[P_EY * fs + pc], pn[P_EZ * fs + pc],
+                   pn[P_BX * fs + pc], pn[P_BY * fs + pc], pn[P_BZ * fs + pc], pold[P_VX * fs + pc],
+                   pold[P_VY * fs + pc], pold[P_VZ * fs + pc], pold[P_RHO * fs + pc], pold[P_P * fs + pc]};
+    LearnedOut r;
+    if (!learned_point(S, phase, in, I.gamma, I.eps1_c2p, I.counters, valid, r)) {
+      if (threadIdx.x == 0) atomicOr(I.status, ST_TC_TIMEOUT);
+      break;   // every thread of the CTA sees the same result
+    }
+    learned_stats(mlp->stats, valid, r.it);
+    const uint32_t st = __reduce_or_sync(0xffffffffu, valid ? r.st : 0u);
+    if (st && (threadIdx.x & 31) == 0) atomicOr(I.status, st);
+    if (valid) {
+      double pv[NPRIM];
+      pv[P_RHO] = r.o.rho; pv[P_P] = r.o.p; pv[P_VX] = r.o.vx; pv[P_VY] = r.o.vy; pv[P_VZ] = r.o.vz;
+      pn[P_RHO * fs + pc] = r.o.rho; pn[P_P * fs + pc] = r.o.p;
+      pn[P_VX * fs + pc] = r.o.vx; pn[P_VY * fs + pc] = r.o.vy; pn[P_VZ * fs + pc] = r.o.vz;
+#pragma unroll
+      for (int c = P_PSI; c < NPRIM; ++c) pv[c] = pn[c * fs + pc];
+      begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
+    }
+  }
+  mlp_tc_teardown(S, phase);
+}
+
+// network seeds of n states (SoA 11 x n conserved), tensor-core form
+__global__ void __launch_bounds__(TC_ROWS, C2P_CTAS_PER_SM)
+k_predict_tc(long long n, const MLPDevice* __restrict__ mlp, const double* __restrict__ cons,
+             double* __restrict__ pseed, uint32_t* __restrict__ err_status) {
+  __shared__ MLPShared S;
+  mlp_tc_setup(S, *mlp);
+  uint32_t phase = 0;
+  const long long ntiles = (n + TC_ROWS - 1) / TC_ROWS;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long i0 = tile * TC_ROWS + threadIdx.x;
+    const long long i = i0 < n ? i0 : n - 1;
+    float f[MLP_IN];
+    c2p_features(cons[i], cons[n + i], cons[2 * n + i], cons[3 * n + i], cons[4 * n + i], cons[5 * n + i],
+                 cons[6 * n + i], cons[7 * n + i], cons[8 * n + i], cons[9 * n + i], cons[10 * n + i], f);
+    float y = 0.0f;
+    if (!mlp_tc_tile(S, phase, f, y)) {
+      if (threadIdx.x == 0) atomicOr(err_status, ST_TC_TIMEOUT);
+      break;
+    }
+    if (i0 < n) pseed[i] = cons[i] * (double)__expf(y * S.sd_y + S.mu_y);
+  }
+  mlp_tc_teardown(S, phase);
+}
+
+int c2p_grid(long long ntiles) {
+  const long long g = (long long)C2P_CTAS_PER_SM * 148;
+  return (int)(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
+}
+
+}  // namespace
+
+int c2p_tiles(int imax, int jmax) {
+  return (int)(((long long)(imax + 1) * (jmax + 1) + TC_ROWS - 1) / TC_ROWS);
+}
+
+cudaError_t launch_c2p_step(cudaStream_t st, const InstDesc* d, int ninst, int ntiles, const MLPDevice* mlp, int cur,
+                            int qout, double abt11) {
+  k_c2p_step<<<c2p_grid(ntiles), TC_ROWS, 0, st>>>(d, ninst, ntiles, mlp, cur, qout, abt11);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_predict_tc(long long n, const MLPDevice* mlp, const double* cons, double* pseed,
+                              uint32_t* err_status, cudaStream_t st) {
+  k_predict_tc<<<c2p_grid((n + TC_ROWS - 1) / TC_ROWS), TC_ROWS, 0, st>>>(n, mlp, cons, pseed, err_status);
+  return cudaGetLastError();
+}
+
+}  // namespace cueva

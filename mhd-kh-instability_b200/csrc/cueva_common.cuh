@@ -34,6 +34,7 @@ enum StatusBits : uint32_t {
   ST_HLLC_VSTAR = 8u,      // 16_hllc_flow_mpx.f95:4294,4605
   ST_NONFINITE = 16u,      // con2prim returned NaN / Inf
   ST_HLLE_SPEED = 32u,     // 16_hlle_flow_mpx.f95:2796-2803, 2974-2981
+  ST_TC_TIMEOUT = 64u,     // a bounded tensor-core wait ran out (no reference counterpart)
 };
 
 // ---- per-instance descriptor (one grid of the ensemble) -------------------
@@ -63,15 +64,18 @@ struct InstDesc {
   double inv_delx_pow2, inv_dely_pow2;
   double eps1_c2p;     // value of the Fortran module variable eps1 when con2prim runs
   int c2p;             // 1 Cardano, 0 NR, 2 learned seed + Newton (Cardano fallback)
+  int c2p_tc;          // c2p 2 with a network: 1 = con2prim in k_c2p_step on the tcgen05 tensor
+                       // cores after the last stage, 0 = inside the last stage (warp mma.sync)
   // interface flux scratch: Fx(i+1/2, j) at fx[(j) * fpitch + (i + 1)],
   // Fy(i, j+1/2) at fy[(j + 1) * fpitch + i], NFACE fields each
   double* fx;
   double* fy;
   int fpitch;
   long long ffs;       // doubles per flux field
-  // work decomposition: CTAs of each launch kind (x faces + update, y faces)
-  int block_begin[2];
-  int block_count[2];
+  // work decomposition: tiles of each launch kind (x faces + update, y faces,
+  // learned con2prim)
+  int block_begin[3];
+  int block_count[3];
 };
 
 // ---- tableau data of one stage launch (by value, kernel parameter space) -----
@@ -114,7 +118,7 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
 constexpr int FACE_ROWS = 8;   // default tile height
 constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
 constexpr int POINT_THREADS = 256;
-enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1 };
+enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1, LK_C2P = 2 };
 
 // launch shape of one RK stage: tile height, CTAs per launch kind and the
 // tiles they loop over (grid == ntiles: one tile per CTA; smaller: persistent)

@@ -38,6 +38,14 @@ cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* 
 cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int q,
                                   double abtll);
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);
+// learned con2prim on the tcgen05 tensor cores after the last stage
+// (cueva_c2p.cu): tiles of 128 points per instance, and the launch over
+// ntiles tiles of all instances; network seeds of n SoA states
+int c2p_tiles(int imax, int jmax);
+cudaError_t launch_c2p_step(cudaStream_t st, const InstDesc* d, int ninst, int ntiles, const MLPDevice* mlp, int cur,
+                            int qout, double abt11);
+cudaError_t launch_predict_tc(long long n, const MLPDevice* mlp, const double* cons, double* pseed,
+                              uint32_t* err_status, cudaStream_t st);
 // run diagnostics of the prims in I.prim[cur] with the given D and tau slabs
 // (cueva_diag.cu): diag_blocks() rows of diag_partials() doubles of scratch
 int diag_blocks(int imax, int jmax);

@@ -468,6 +468,20 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
       for (int c = 0; c < NCONS; ++c) Un[c] = U[c] + I.dt * fin[c];
       // varfin's D and tau, which the run diagnostics read (con2prim does not write them back)
       if (sa.diag_cons != nullptr && valid) { sa.diag_cons[pc] = Un[Q_D]; sa.diag_cons[fs + pc] = Un[Q_TAU]; }
+      if (I.c2p == 2 && I.c2p_tc) {
+        // con2prim follows in k_c2p_step: the evolved D, tau, S go to the
+        // final-sum slabs (read above, not needed again this step), the
+        // fields varfin completes to the primitives of time n+1
+        if (!valid) return 0u;
+#pragma unroll
+        for (int c = Q_D; c <= Q_SZ; ++c) I.finsum[c * fs + pc] = Un[c];
+        double* po = I.prim[1 - sa.cur];
+        po[P_PSI * fs + pc] = Un[Q_PSI]; po[P_PHI * fs + pc] = Un[Q_PHI];
+        po[P_EX * fs + pc] = Un[Q_EX]; po[P_EY * fs + pc] = Un[Q_EY]; po[P_EZ * fs + pc] = Un[Q_EZ];
+        po[P_BX * fs + pc] = Un[Q_BX]; po[P_BY * fs + pc] = Un[Q_BY]; po[P_BZ * fs + pc] = Un[Q_BZ];
+        po[P_Q * fs + pc] = Un[Q_Q];
+        return st;
+      }
       // con2prim, l_swap = 1 (main_cueva_code.f95:312-326)
       C2PIn in{Un[Q_D], Un[Q_TAU], Un[Q_SX], Un[Q_SY], Un[Q_SZ], Un[Q_EX], Un[Q_EY], Un[Q_EZ],
                Un[Q_BX], Un[Q_BY], Un[Q_BZ], vx, vy, vz, prim[P_RHO * fs + pc], prim[P_P * fs + pc]};
@@ -555,10 +569,11 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
   // after the last stage every lane of the warp enters the update (lanes
   // without a point repeat a real one and store nothing), so con2prim runs
   // converged; earlier stages update the real points only
-  if (valid || (EP == EP_LAST && I.c2p == 2)) {
+  const bool warp_c2p = EP == EP_LAST && I.c2p == 2 && !I.c2p_tc;
+  if (valid || warp_c2p) {
     const int ii = valid ? i : (lane == 0 ? i0 + 1 : ilast);
     const int ln = ii - i0;   // staged cell ii is stencil point R of lane ln's face
-    if (EP == EP_LAST && I.c2p == 2) {
+    if (warp_c2p) {
       // a lane without a point takes the divergence of the point it repeats
 #pragma unroll
       for (int c = 0; c < NROLE; ++c) qx[c] = __shfl_sync(0xffffffffu, qx[c], ln);

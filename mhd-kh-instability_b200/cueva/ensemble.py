@@ -85,6 +85,11 @@ class Ensemble:
     def attach(self, net):
         _abi.check(self.L, self.L.cueva_ens_attach_mlp(self.h, net.h))
 
+    def set_learned_kernel(self, mode):
+        """Learned con2prim: 1 = tcgen05 kernel after the last stage
+        (default once attached), 0 = inside the last stage."""
+        _abi.check(self.L, self.L.cueva_ens_set_learned_kernel(self.h, int(mode)))
+
     def learned_stats(self):
         out = (ctypes.c_int64 * 3)()
         _abi.check(self.L, self.L.cueva_ens_learned_stats(self.h, out))

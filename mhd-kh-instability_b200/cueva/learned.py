@@ -96,12 +96,14 @@ class LearnedSeed:
 
     # ------------------------------------------------------------- inference
     def predict(self, cons, tensor_cores=True):
-        """Pressure seeds: warp-cooperative bf16 tensor-core inference (the
-        form the fused step uses) or per-thread FP32."""
+        """Pressure seeds: per-thread FP32 (tensor_cores = False / 0), warp
+        mma.sync with bf16 activations (True / 1) or tcgen05 tiles of 128
+        states (2, the form the step uses by default)."""
         import torch
         n = cons.shape[1]
         out = torch.empty(n, dtype=torch.float64, device=cons.device)
-        _abi.check(self.L, self.L.cueva_mlp_predict(self.h, _ptr(cons), n, _ptr(out), 1 if tensor_cores else 0))
+        mode = int(tensor_cores) if not isinstance(tensor_cores, bool) else (1 if tensor_cores else 0)
+        _abi.check(self.L, self.L.cueva_mlp_predict(self.h, _ptr(cons), n, _ptr(out), mode))
         return out
 
     def c2p(self, method, cons, prev, seed=None, gamma=4.0 / 3.0, eps1=1e-6):

@@ -110,6 +110,11 @@ class Cueva:
     def set_stream(self, stream_ptr):
         _abi.check(self.L, self.L.cueva_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
 
+    def set_learned_kernel(self, mode):
+        """Learned con2prim: 1 = tcgen05 kernel after the last stage (the
+        default once a network is attached), 0 = inside the last stage."""
+        _abi.check(self.L, self.L.cueva_set_learned_kernel(self.ctx, int(mode)))
+
     # ------------------------------------------------------- clock and diagnostics
     def set_clock(self, h, t):
         """Step index h of the last completed step and t_advance (restarts)."""

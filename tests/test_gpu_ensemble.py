@@ -69,3 +69,38 @@ def test_ensemble_rejects_mixed_schemes():
     inst = [dict(imax=64, jmax=32, sigma=1e3, order=4, flux_solver=7, intsum_reset=r) for r in (1, 0)]
     with pytest.raises(CuevaError):
         Ensemble(inst)
+
+
+def test_learned_ensemble_matches_single_runs():
+    """Instances with the learned con2prim (c2p = 2, network attached) next
+    to Cardano ones: the tcgen05 con2prim launch covers the learned
+    instances' tiles only, and every instance matches its single run to the
+    bit (same tiles of 128 points, same MMAs)."""
+    from cueva import Cueva
+    from cueva.ensemble import Ensemble
+    from cueva.learned import LearnedSeed, synthetic_pairs
+    cons, prims = synthetic_pairs(100_000, seed=99)
+    net = LearnedSeed(seed=5)
+    net.fit_normalisation(cons, prims)
+    net.train(cons, prims, steps=300, batch=4096, lr=2e-3)
+    c2ps = [2, 1, 2, 2]
+    ens = Ensemble([dict(imax=g["imax"], jmax=g["jmax"], sigma=g["sigma"], c2p=c, **COMMON)
+                    for g, c in zip(GRIDS, c2ps)])
+    for k, g in enumerate(GRIDS):
+        ens.kh_init(k, v0=g["v0"], a=0.05)
+    ens.attach(net)
+    ens.step(4)
+    ens.sync()
+    for k, (g, c) in enumerate(zip(GRIDS, c2ps)):
+        s = Cueva(g["imax"], g["jmax"], sigma=g["sigma"], c2p=c, **COMMON)
+        s.kh_init(v0=g["v0"], a=0.05)
+        s.upload()
+        net.attach(s)
+        s.step(4)
+        s.download()
+        got = ens.get_prims(k)
+        for n in PRIMS:
+            assert np.array_equal(got[n], s.interior(n)), (k, n)
+        s.close()
+    ens.close()
+    net.close()

@@ -156,3 +156,50 @@ def test_tensor_core_inference_matches_fp32(trained):
     assert float(d.median()) < 2e-2 and float(d.max()) < 0.5
     e = (torch.log(a) - torch.log(prims[1])).abs()
     assert float(e.median()) < 0.1
+
+
+def test_tcgen05_inference_matches_fp32(trained):
+    """The tcgen05 form (tiles of 128 states, accumulator in tensor memory,
+    SiLU through tanh.approx) against the per-thread FP32 forward and the
+    mma.sync form: the same network with bf16 activations, so the seeds
+    agree to the activation rounding."""
+    import torch
+    from cueva.learned import synthetic_pairs
+    net = trained[0]
+    cons, prims = synthetic_pairs(100_003, seed=556)     # a partial last tile
+    a = net.predict(cons, tensor_cores=2)
+    b = net.predict(cons, tensor_cores=0)
+    c = net.predict(cons, tensor_cores=1)
+    assert torch.isfinite(a).all()
+    d_fp32 = (torch.log(a) - torch.log(b)).abs()
+    d_warp = (torch.log(a) - torch.log(c)).abs()
+    print(f"tcgen05 log-seed difference: vs FP32 median {float(d_fp32.median()):.2e} max {float(d_fp32.max()):.2e}; "
+          f"vs mma.sync median {float(d_warp.median()):.2e} max {float(d_warp.max()):.2e}")
+    assert float(d_fp32.median()) < 2e-2 and float(d_fp32.max()) < 0.5
+    assert float(d_warp.median()) < 5e-3 and float(d_warp.max()) < 0.2
+
+
+@pytest.mark.parametrize("solver,order", [(7, 2), (5, 3)])
+def test_learned_kernel_modes_agree(trained, solver, order):
+    """The learned con2prim as a tcgen05 kernel after the last stage and
+    inside the last stage: both Newton roots to 1e-12, so the runs agree far
+    below the 1e-6 bar; both count every point once."""
+    from cueva import Cueva
+    from cueva.learned import learned_stats
+    net = trained[0]
+    kw = dict(order=order, flux_solver=solver, rec_mp=0, sigma=1e3, c2p=2)
+    runs = []
+    for mode in (1, 0):
+        g = Cueva(45, 38, **kw)   # ragged: partial tiles of 128 points
+        g.kh_init(v0=0.5, a=0.05)
+        g.upload()
+        net.attach(g)
+        g.set_learned_kernel(mode)
+        g.step(10)
+        g.download()
+        its, pts, fails = learned_stats(g)
+        assert pts == 10 * 46 * 39 and fails <= pts // 1000, (mode, pts, fails)
+        runs.append({n: g.interior(n).copy() for n in PRIMS})
+        g.close()
+    for n in PRIMS:
+        assert rel_l1_field(n, runs[0][n], runs[1][n], runs[1]) <= 1e-9, n
