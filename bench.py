@@ -267,12 +267,27 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
         return {"unavailable": "no trained seed network: run python -m cueva.train_seed"}
     g.download()
     ref = {n: g.interior(n).copy() for n in PRIM_NAMES}
+    net = LearnedSeed(device=device)
+    net.load(DEFAULT)
+    # one step from the initial state: mixed + learned, mixed + Cardano and FP64
+    one = {}
+    for prec, c2p in ((1, 2), (1, 1), (0, 1)):
+        o = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=prec, c2p=c2p))
+        o.set_stream(stream.cuda_stream)
+        o.kh_init(**cfg.kh_kwargs())
+        o.upload()
+        if c2p == 2:
+            net.attach(o)
+        o.step(1)
+        o.download()
+        one[(prec, c2p)] = {n: o.interior(n).copy() for n in PRIM_NAMES}
+        o.close()
+    one_err = {n: rel_l1_field(n, one[(1, 2)][n], one[(0, 1)][n], one[(0, 1)]) for n in PRIM_NAMES}
+    one_c2p = {n: rel_l1_field(n, one[(1, 2)][n], one[(1, 1)][n], one[(1, 1)]) for n in PRIM_NAMES}
     m = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=1, c2p=2))
     m.set_stream(stream.cuda_stream)
     m.kh_init(**cfg.kh_kwargs())
     m.upload()
-    net = LearnedSeed(device=device)
-    net.load(DEFAULT)
     net.attach(m)
     m.step(max(args.warmup, 3))
     m.sync()
@@ -290,10 +305,18 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     m.download()
     errs = {n: rel_l1_field(n, m.interior(n), ref[n], ref) for n in PRIM_NAMES}
     its, pts, fails = learned_stats(m)
+    prof_ms, prof_n = m.profile_steps(args.profile_steps) if args.profile_steps > 0 else ([0.0] * 3, [0] * 3)
     m.close()
     net.close()
+    nprof = max(args.profile_steps, 1)
     return {"value": world * cfg.nx * cfg.ny * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
             "dtype": "f32 reconstruction + Riemann, f64 update / implicit E / con2prim",
+            "con2prim": "network seed on the tcgen05 tensor cores (k_c2p_step), Newton in FP64, Cardano fall-back",
+            "kernel_ms_per_step": {"k_yface": prof_ms[0] / nprof, "k_xupd": prof_ms[1] / nprof,
+                                   "k_c2p_step": prof_ms[2] / nprof},
+            "rel_l1_learned_vs_cardano_one_step": one_c2p,
+            "max_rel_l1_learned_vs_cardano_one_step": max(one_c2p.values()),
+            "rel_l1_vs_fp64_one_step": one_err, "max_rel_l1_vs_fp64_one_step": max(one_err.values()),
             "error_vs_fp64_after_steps": max(args.warmup, 3) + args.steps,
             "rel_l1_vs_fp64": errs, "max_rel_l1_vs_fp64": max(errs.values()),
             "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}
