@@ -122,6 +122,10 @@ int32_t cueva_step(cueva_ctx* ctx, int32_t nsteps);
 int32_t cueva_sync(cueva_ctx* ctx);
 int32_t cueva_status(cueva_ctx* ctx, uint32_t* status_bits);
 int32_t cueva_counters(cueva_ctx* ctx, int64_t out3[3]);   /* contador_r, contador_p, contador_v */
+/* Status bits stay set (the reference stops at these sites) until cleared:
+ * after restoring a good state (cueva_upload or cueva_checkpoint_load) a
+ * caller that handles the error clears them and continues. */
+int32_t cueva_clear_status(cueva_ctx* ctx);
 /* nsteps steps launched one kernel at a time (no CUDA graph) with events
  * between the launches on the context stream; ms_out[k] receives the summed
  * device time of the y-face (k = 0) and the x-face + update (k = 1) kernels
@@ -181,7 +185,11 @@ int32_t cueva_mlp_gradients(cueva_mlp* mlp, const double* d_cons, const double* 
 /* network pressure seeds of n states (device out): per thread in FP32
  * (tensor_cores = 0), warp-cooperative mma.sync with bf16 activations (1),
  * or tcgen05 MMA on tiles of 128 states with the accumulator in tensor
- * memory and bf16 activations (2, the form the step uses by default) */
+ * memory and bf16 activations (2, the form the step uses by default).
+ * 3 is the self-test of the tcgen05 path's bounded waits: no MMA is issued,
+ * the first wait gives up after a short limit, every CTA frees its tensor
+ * memory, and the call returns CUEVA_ERR_PHYSICS (status 64) without
+ * writing seeds; the device stays usable. */
 int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed, int32_t tensor_cores);
 /* batch con2prim for comparisons: method 1 Cardano, 2 network seed + Newton,
  * 3 Newton from d_seed; d_prev (5 x n) are the previous primitives the

@@ -615,6 +615,14 @@ int32_t cueva_status(cueva_ctx* c, uint32_t* st) {
   return CUEVA_OK;
 }
 
+int32_t cueva_clear_status(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  CUDA_TRY(cudaMemsetAsync(c->d_status, 0, 4, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CUEVA_OK;
+}
+
 int32_t cueva_counters(cueva_ctx* c, int64_t out3[3]) {
   if (int32_t e = check_ctx(c)) return e;
   unsigned long long h[3];

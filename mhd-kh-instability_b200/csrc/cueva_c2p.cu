@@ -104,9 +104,9 @@ k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPD
 // network seeds of n states (SoA 11 x n conserved), tensor-core form
 __global__ void __launch_bounds__(TC_ROWS, C2P_CTAS_PER_SM)
 k_predict_tc(long long n, const MLPDevice* __restrict__ mlp, const double* __restrict__ cons,
-             double* __restrict__ pseed, uint32_t* __restrict__ err_status) {
+             double* __restrict__ pseed, uint32_t* __restrict__ err_status, uint32_t max_polls, uint32_t self_test) {
   __shared__ MLPShared S;
-  mlp_tc_setup(S, *mlp);
+  mlp_tc_setup(S, *mlp, max_polls, self_test);
   uint32_t phase = 0;
   const long long ntiles = (n + TC_ROWS - 1) / TC_ROWS;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -143,8 +143,11 @@ cudaError_t launch_c2p_step(cudaStream_t st, const InstDesc* d, int ninst, int n
 }
 
 cudaError_t launch_predict_tc(long long n, const MLPDevice* mlp, const double* cons, double* pseed,
-                              uint32_t* err_status, cudaStream_t st) {
-  k_predict_tc<<<c2p_grid((n + TC_ROWS - 1) / TC_ROWS), TC_ROWS, 0, st>>>(n, mlp, cons, pseed, err_status);
+                              uint32_t* err_status, cudaStream_t st, bool self_test) {
+  // the self-test bounds its waits tightly: the first one is meant to run out
+  k_predict_tc<<<c2p_grid((n + TC_ROWS - 1) / TC_ROWS), TC_ROWS, 0, st>>>(n, mlp, cons, pseed, err_status,
+                                                                          self_test ? 64u : TC_MAX_POLLS,
+                                                                          self_test ? 1u : 0u);
   return cudaGetLastError();
 }
 

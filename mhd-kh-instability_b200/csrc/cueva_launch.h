@@ -45,7 +45,7 @@ int c2p_tiles(int imax, int jmax);
 cudaError_t launch_c2p_step(cudaStream_t st, const InstDesc* d, int ninst, int ntiles, const MLPDevice* mlp, int cur,
                             int qout, double abt11);
 cudaError_t launch_predict_tc(long long n, const MLPDevice* mlp, const double* cons, double* pseed,
-                              uint32_t* err_status, cudaStream_t st);
+                              uint32_t* err_status, cudaStream_t st, bool self_test = false);
 // run diagnostics of the prims in I.prim[cur] with the given D and tau slabs
 // (cueva_diag.cu): diag_blocks() rows of diag_partials() doubles of scratch
 int diag_blocks(int imax, int jmax);

@@ -43,6 +43,8 @@ struct __align__(128) MLPShared {
   uint64_t bar;                    // MMA completion
   uint32_t taddr;                  // TMEM accumulator
   uint32_t fail;                   // a bounded wait ran out
+  uint32_t max_polls;              // bound of every mbarrier wait
+  uint32_t self_test;              // 1: issue no MMA, so the first wait runs out (tests the timeout path)
 };
 
 __device__ __forceinline__ float tanh_approx(float x) {
@@ -53,7 +55,8 @@ __device__ __forceinline__ float tanh_approx(float x) {
 
 // The CTA's set-up: network into shared memory (core-matrix layout), the
 // mbarrier, and (warp 0) the TMEM columns.  All threads call it.
-__device__ __forceinline__ void mlp_tc_setup(MLPShared& S, const MLPDevice& M) {
+__device__ __forceinline__ void mlp_tc_setup(MLPShared& S, const MLPDevice& M, uint32_t max_polls = TC_MAX_POLLS,
+                                             uint32_t self_test = 0) {
   const int t = threadIdx.x;
   // W2, W3: row n = output unit, 8 consecutive inputs = one 16-byte chunk
   for (int c = t; c < MLP_H * (MLP_H / 8); c += blockDim.x) {
@@ -80,6 +83,8 @@ __device__ __forceinline__ void mlp_tc_setup(MLPShared& S, const MLPDevice& M) {
   if (t == 0) {
     S.b4 = M.b4; S.mu_y = M.mu_y; S.sd_y = M.sd_y;
     S.fail = 0;
+    S.max_polls = max_polls;
+    S.self_test = self_test;
     umma::mbar_init(&S.bar, 1);
     umma::mbar_fence_init();
   }
@@ -94,7 +99,7 @@ __device__ __forceinline__ void mlp_tc_teardown(MLPShared& S, uint32_t phase) {
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
-  if (S.fail && threadIdx.x == 0) umma::mbar_wait(&S.bar, phase, TC_MAX_POLLS);   // MMAs still in flight
+  if (S.fail && threadIdx.x == 0) umma::mbar_wait(&S.bar, phase, S.max_polls);   // MMAs still in flight
   __syncthreads();
   if (threadIdx.x < 32) umma::tmem_dealloc(S.taddr, TC_TMEM_COLS);
 }
@@ -103,6 +108,7 @@ __device__ __forceinline__ void mlp_tc_teardown(MLPShared& S, uint32_t phase) {
 __device__ __forceinline__ void mlp_tc_issue(MLPShared& S, const uint8_t* A, const uint8_t* W, int nk,
                                              uint32_t idesc) {
   umma::fence_after_sync();
+  if (S.self_test) return;   // nothing will arrive on the barrier
   const uint32_t a0 = umma::smem_u32(A), w0 = umma::smem_u32(W);
   const uint32_t sbo = (uint32_t)nk * 256u;   // K * 16 bytes between 8-row groups
   for (int s = 0; s < nk; ++s)
@@ -114,7 +120,7 @@ __device__ __forceinline__ void mlp_tc_issue(MLPShared& S, const uint8_t* A, con
 // all threads: waits for the layer's MMAs; false (for every thread) if the
 // wait ran out
 __device__ __forceinline__ bool mlp_tc_wait(MLPShared& S, uint32_t& phase) {
-  if (!umma::mbar_wait(&S.bar, phase, TC_MAX_POLLS)) atomicOr(&S.fail, 1u);
+  if (!umma::mbar_wait(&S.bar, phase, S.max_polls)) atomicOr(&S.fail, 1u);
   __syncthreads();
   umma::fence_after_sync();
   if (S.fail) return false;   // phase keeps the parity of the commit still outstanding

@@ -576,13 +576,13 @@ int32_t cueva_mlp_predict(cueva_mlp* M, const double* d_cons, int64_t n, double*
   if (!M || n <= 0 || !d_cons || !d_pseed) return cueva_fail(CUEVA_ERR_ARG, "bad arguments");
   if (!M->normed) return cueva_fail(CUEVA_ERR_ARG, "the network has no normalisation");
   TRY(cudaSetDevice(M->dev));
-  if (tensor_cores < 0 || tensor_cores > 2) return cueva_fail(CUEVA_ERR_ARG, "tensor_cores must be 0, 1 or 2");
-  if (tensor_cores == 2) {
+  if (tensor_cores < 0 || tensor_cores > 3) return cueva_fail(CUEVA_ERR_ARG, "tensor_cores must be 0, 1, 2 or 3");
+  if (tensor_cores >= 2) {
     // tcgen05 tiles of 128 states; a bounded wait that runs out is reported
     uint32_t* d_err = nullptr;
     TRY(cudaMalloc(&d_err, sizeof(uint32_t)));
     cudaError_t e = cudaMemset(d_err, 0, sizeof(uint32_t));
-    if (e == cudaSuccess) e = launch_predict_tc(n, M->d_dev, d_cons, d_pseed, d_err, 0);
+    if (e == cudaSuccess) e = launch_predict_tc(n, M->d_dev, d_cons, d_pseed, d_err, 0, tensor_cores == 3);
     uint32_t herr = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&herr, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
     cudaFree(d_err);

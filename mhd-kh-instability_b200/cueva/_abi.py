@@ -36,7 +36,7 @@ EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_s
            "cueva_ens_attach_mlp", "cueva_ens_learned_stats", "cueva_set_clock", "cueva_get_clock",
            "cueva_diag_enable", "cueva_diag_read", "cueva_diag_now", "cueva_checkpoint_save",
            "cueva_checkpoint_load", "cueva_read_all_variables", "cueva_write_all_variables",
-           "cueva_set_learned_kernel", "cueva_ens_set_learned_kernel"]
+           "cueva_set_learned_kernel", "cueva_ens_set_learned_kernel", "cueva_clear_status"]
 MLP_NPARAM, MLP_NNORM = 8833, 14
 
 
@@ -146,6 +146,7 @@ def load(fma=False):
     L.cueva_diag_read.argtypes = [vp, ctypes.POINTER(DiagRecord), i32, ctypes.POINTER(i32)]
     L.cueva_diag_now.argtypes = [vp, ctypes.POINTER(DiagRecord)]
     L.cueva_set_learned_kernel.argtypes = [vp, i32]
+    L.cueva_clear_status.argtypes = [vp]
     L.cueva_ens_set_learned_kernel.argtypes = [vp, i32]
     L.cueva_checkpoint_save.argtypes = [vp, ctypes.c_char_p]
     L.cueva_checkpoint_load.argtypes = [vp, ctypes.c_char_p]

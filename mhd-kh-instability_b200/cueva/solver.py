@@ -94,6 +94,10 @@ class Cueva:
         _abi.check(self.L, self.L.cueva_status(self.ctx, ctypes.byref(s)))
         return s.value
 
+    def clear_status(self):
+        """Clears the sticky status bits after the caller handled them."""
+        _abi.check(self.L, self.L.cueva_clear_status(self.ctx))
+
     def counters(self):
         c = (ctypes.c_int64 * 3)()
         _abi.check(self.L, self.L.cueva_counters(self.ctx, c))

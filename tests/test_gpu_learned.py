@@ -203,3 +203,21 @@ def test_learned_kernel_modes_agree(trained, solver, order):
         g.close()
     for n in PRIMS:
         assert rel_l1_field(n, runs[0][n], runs[1][n], runs[1]) <= 1e-9, n
+
+
+def test_tcgen05_bounded_wait_reports_and_recovers(trained):
+    """The timeout path of the tensor-core waits: in the self-test mode no
+    MMA is issued, the bounded mbarrier wait runs out, the kernel frees its
+    tensor memory and the call reports status 64; the next call works."""
+    import torch
+    from cueva import CuevaError
+    from cueva.learned import synthetic_pairs
+    net = trained[0]
+    cons, _ = synthetic_pairs(10_000, seed=7)
+    with pytest.raises(CuevaError) as e:
+        net.predict(cons, tensor_cores=3)
+    assert e.value.code == 4 and "64" in str(e.value)
+    a = net.predict(cons, tensor_cores=2)
+    b = net.predict(cons, tensor_cores=0)
+    assert torch.isfinite(a).all()
+    assert float((torch.log(a) - torch.log(b)).abs().median()) < 2e-2

@@ -252,3 +252,22 @@ def test_seed_modes_agree_after_one_step(oracle_mod, solver):
     oracle_mod.set_libm_seed(0)
     for n in outs[0]:
         assert rel_l1(outs[0][n], outs[1][n]) <= 1e-14, n
+
+
+def test_c2p_status_codes(oracle_mod):
+    """Fault injection on the CPU: conserved states that the reference's
+    con2prim stops on raise the documented status bits instead (Cardano
+    `stop` sites = bit 1); the NR form returns non-finite values, which the
+    step's wrapper reports as bit 16."""
+    inp = np.zeros(16)
+    inp[[0, 1, 2, 14, 15]] = [1.0, 1.0, 5.0, 1.0, 1.0]          # |S| > tau: no physical state
+    st, out = oracle_mod.c2p(inp, method=1)
+    assert st & 1
+    st, out = oracle_mod.c2p(inp, method=0)
+    assert not np.all(np.isfinite(out))
+    inp[[1, 2]] = [-1.0, 0.0]                                     # negative energy
+    st, out = oracle_mod.c2p(inp, method=1)
+    assert st & 1
+    good = np.array([1.2, 2.0, 0.1, 0, 0, 0, 0, 0, 0, 0.1, 0, 0, 0, 0, 1, 1], dtype=float)
+    st, out = oracle_mod.c2p(good, method=1)
+    assert st == 0 and np.all(np.isfinite(out))
