@@ -111,11 +111,30 @@ __device__ __forceinline__ void cp_async8(double* sdst, const double* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 // L2 prefetch of the n doubles at p, widened to 16-byte boundaries (which
 // stay inside the 256-byte-aligned row the doubles belong to)
-__device__ __forceinline__ void prefetch_l2(const double* p, int n) {
+template <typename E>
+__device__ __forceinline__ void prefetch_l2(const E* p, int n) {
   const unsigned long long a = (unsigned long long)p & ~15ull;
   const unsigned long long e = ((unsigned long long)(p + n) + 15ull) & ~15ull;
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
 }
+
+// The y-flux scratch holds each flux in the type it is computed in: FP64,
+// or FP32 for the mixed-precision kernels (the update converts it to FP64
+// exactly as it would convert the register value, so the results are the
+// same and the scratch traffic halves).  Element e of field c of the slab
+// is at fy + c * ffs + e in units of that type.
+template <typename T>
+__device__ __forceinline__ void flux_store(double* fy, long long idx, T v) {
+  if constexpr (sizeof(T) == 8) fy[idx] = double(v);
+  else reinterpret_cast<float*>(fy)[idx] = float(v);
+}
+template <typename T>
+__device__ __forceinline__ double flux_load(const double* fy, long long idx) {
+  if constexpr (sizeof(T) == 8) return fy[idx];
+  else return double(reinterpret_cast<const float*>(fy)[idx]);
+}
+template <typename T>
+__device__ __forceinline__ const T* flux_base(const double* fy) { return reinterpret_cast<const T*>(fy); }
 
 constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
 
@@ -338,7 +357,7 @@ k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
       const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, F);
       const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
-      for (int c = 0; c < NROLE; ++c) I.fy[c * I.ffs + fo] = double(F[c]);
+      for (int c = 0; c < NROLE; ++c) flux_store<T>(I.fy, c * I.ffs + fo, F[c]);
       if (stt) atomicOr(I.status, stt);
     }
     __syncthreads();   // the next tile's copies overwrite the staged values
@@ -357,7 +376,7 @@ struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
 // and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
 // valid == false (EP_LAST only): the lane computes a copy of a real point so
 // that its warp reaches con2prim converged, and stores nothing
-template <int EP>
+template <int EP, typename T>
 __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
                                                  const double (&qx)[NROLE], const Centre& cv, bool valid = true) {
   const int pitch = I.pitch;
@@ -370,7 +389,7 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
   const double* __restrict__ fy = I.fy;
   const double dly = I.dely, iy2 = I.inv_dely_pow2;
   auto qy = [&](int r) {   // (dy)/dly
-    const double d = fy[r * I.ffs + fyo] - fy[r * I.ffs + fyo - I.fpitch];
+    const double d = flux_load<T>(fy, r * I.ffs + fyo) - flux_load<T>(fy, r * I.ffs + fyo - I.fpitch);
     return iy2 != 0.0 ? d * iy2 : d / dly;
   };
   auto qxf = [&](int r) { return qx[r]; };
@@ -542,7 +561,7 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
         prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
       } else {
         const int e2 = e - ncen * nr, r = e2 % (nr + 1), c = e2 / (nr + 1);
-        prefetch_l2(I.fy + c * I.ffs + (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
+        prefetch_l2(flux_base<T>(I.fy) + c * I.ffs + (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
       }
     }
   }
@@ -581,7 +600,7 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
     auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + ln + R]; };
     const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
                     cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
-    stt |= update_point<EP>(I, sa, ii, j, qx, cv, valid);
+    stt |= update_point<EP, T>(I, sa, ii, j, qx, cv, valid);
   }
   if (stt) atomicOr(I.status, stt);
 }
