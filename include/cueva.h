@@ -59,7 +59,9 @@ typedef struct cueva_params {
                            (07_clean_var.f95 via main_cueva_code.f95:184, the reference); 1: zeroed
                            before every stage (textbook IMEX-RK; the reference's SSP3(4,3,3) marked
                            "NO" in imex_scheme.f95:278 is only stable this way) */
-  int32_t pad;
+  int32_t primitive_rec;/* 1: reconstruct the primitives at the start of every step
+                           (primitive_rec of parameters.f95:26, 05_reconstruct.f95:525-746,
+                           main_cueva_code.f95:170-175); 0 (default): no reconstruction */
   double lx, ly, lz;    /* Longx, Longy, Longz (Delx = lx/imax, Dely = ly/jmax, Delz = lz) */
   double cfl, sigma, gamma;
   double dt;            /* <= 0 selects CFL*min(Delx,Dely,Delz) (parameters.f95:312) */
@@ -114,7 +116,8 @@ int32_t cueva_download(cueva_ctx* ctx, uint32_t groups);
 
 /* ---- the hot path ----------------------------------------------------- */
 /* nsteps executions of the body of the time loop, main_cueva_code.f95:53-328
- * (boundary, startconvar, cleanvarint, RK stages with sumint / varint /
+ * (boundary, recons_var_primitive when params.primitive_rec, startconvar,
+ * cleanvarint, RK stages with sumint / varint /
  * electricvarint / flowinit / {hll,hllc}_flow_mpx / fluxandsource / sumfin,
  * varfin, electricfield, varprimitivecardano or varprimitive_nr), on the
  * device-resident state.  Asynchronous on the context stream. */

@@ -133,6 +133,7 @@ int32_t validate_params(const cueva_params* p) {
     return fail(CUEVA_ERR_ARG, "bc_x, bc_y must be 0 (copy) or 1 (periodic)");
   if (p->precision != 0 && p->precision != 1) return fail(CUEVA_ERR_ARG, "precision must be 0 or 1");
   if (p->intsum_reset != 0 && p->intsum_reset != 1) return fail(CUEVA_ERR_ARG, "intsum_reset must be 0 or 1");
+  if (p->primitive_rec != 0 && p->primitive_rec != 1) return fail(CUEVA_ERR_ARG, "primitive_rec must be 0 or 1");
   return CUEVA_OK;
 }
 
@@ -210,6 +211,7 @@ void fill_desc(const cueva_params* p, const InstGeom& G, int nkslot, double* sla
   I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
   I.c2p = p->c2p;
   I.c2p_tc = 0;
+  I.primitive_rec = p->primitive_rec;
   I.block_begin[LK_C2P] = 0;
   I.block_count[LK_C2P] = c2p_tiles(G.imax, G.jmax);
 }
@@ -345,6 +347,10 @@ int32_t run_begin_step(cueva_ctx* c) {
 bool learned_tc(const InstDesc& I, const MLPDevice* d_mlp) { return I.c2p == 2 && I.c2p_tc && d_mlp; }
 
 int32_t enqueue_step(cueva_ctx* c, double* diag_cons = nullptr) {
+  if (c->P.primitive_rec) {   // main_cueva_code.f95:170-184: reconstruction, then startconvar and stage 1
+    CUDA_TRY(launch_recons_begin((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur, c->qin, c->T.Abt[0][0]));
+    c->cur ^= 1;
+  }
   for (int l = 1; l <= c->T.s; ++l) {
     StageArgs sa = stage_args(c, l, 0);
     if (l == c->T.s) sa.diag_cons = diag_cons;
@@ -538,7 +544,7 @@ int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {
     }
     CUDA_TRY(cudaGraphLaunch(g, c->stream));
     for (int l = 0; l < c->T.s; ++l) c->qin ^= 1;
-    c->cur ^= 1;
+    if (!c->P.primitive_rec) c->cur ^= 1;   // with the reconstruction the step flips the buffers twice
     c->h += 1;
     c->t = c->t + c->dt;
     if (rec) {
@@ -565,6 +571,19 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
     }
   int32_t rc = CUEVA_OK;
   for (int n = 0; n < nsteps && rc == CUEVA_OK; ++n) {
+    if (c->P.primitive_rec) {   // timed with the other kernels in ms_out[2]
+      cudaError_t ce = cudaEventRecord(ev[0], c->stream);
+      if (ce == cudaSuccess)
+        ce = launch_recons_begin((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur, c->qin, c->T.Abt[0][0]);
+      if (ce == cudaSuccess) ce = cudaEventRecord(ev[1], c->stream);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[1]);
+      if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      ms_out[2] += ms;
+      launches_out[2] += 1;
+      c->cur ^= 1;
+    }
     for (int l = 1; l <= c->T.s && rc == CUEVA_OK; ++l) {
       const StageArgs sa = stage_args(c, l, 0);
       cudaError_t ce = launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1,
@@ -1128,6 +1147,10 @@ int32_t ens_begin(cueva_ens* e) {
 }
 
 int32_t ens_enqueue_step(cueva_ens* e) {
+  if (e->P0.primitive_rec) {
+    CUDA_TRY(launch_recons_begin(e->max_points, e->stream, e->d_inst, e->n, e->cur, e->qin, e->T.Abt[0][0]));
+    e->cur ^= 1;
+  }
   for (int l = 1; l <= e->T.s; ++l) {
     const StageArgs sa = stage_args_of(e->T, e->kslot_of, e->P0.intsum_reset, e->cur, e->qin, l, 0);
     CUDA_TRY(launch_stage(e->P0.rec_mp, e->P0.flux_solver, e->P0.precision, e->shape, e->stream, e->d_inst, e->n, sa));
@@ -1174,9 +1197,11 @@ int32_t cueva_ens_create(const cueva_params* params, int32_t n, cueva_ens** out)
     const cueva_params& a = params[0];
     const cueva_params& b = params[k];
     if (b.order != a.order || b.flux_solver != a.flux_solver || b.rec_mp != a.rec_mp ||
-        b.precision != a.precision || b.intsum_reset != a.intsum_reset || b.device != a.device)
+        b.precision != a.precision || b.intsum_reset != a.intsum_reset || b.device != a.device ||
+        b.primitive_rec != a.primitive_rec)
       return fail(CUEVA_ERR_ARG, "instance " + std::to_string(k) +
-                                     ": order, flux_solver, rec_mp, precision, intsum_reset and device must agree");
+                                     ": order, flux_solver, rec_mp, precision, intsum_reset, primitive_rec and device "
+                                     "must agree");
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -1303,7 +1328,7 @@ int32_t cueva_ens_step(cueva_ens* e, int32_t nsteps) {
     }
     CUDA_TRY(cudaGraphLaunch(g, e->stream));
     for (int l = 0; l < e->T.s; ++l) e->qin ^= 1;
-    e->cur ^= 1;
+    if (!e->P0.primitive_rec) e->cur ^= 1;   // with the reconstruction the step flips the buffers twice
   }
   return CUEVA_OK;
 }

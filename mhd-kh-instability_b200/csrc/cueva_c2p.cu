@@ -95,7 +95,7 @@ k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPD
       pn[P_VX * fs + pc] = r.o.vx; pn[P_VY * fs + pc] = r.o.vy; pn[P_VZ * fs + pc] = r.o.vz;
 #pragma unroll
       for (int c = P_PSI; c < NPRIM; ++c) pv[c] = pn[c * fs + pc];
-      begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
+      if (!I.primitive_rec) begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
     }
   }
   mlp_tc_teardown(S, phase);

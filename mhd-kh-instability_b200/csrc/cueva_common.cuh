@@ -64,6 +64,8 @@ struct InstDesc {
   double inv_delx_pow2, inv_dely_pow2;
   double eps1_c2p;     // value of the Fortran module variable eps1 when con2prim runs
   int c2p;             // 1 Cardano, 0 NR, 2 learned seed + Newton (Cardano fallback)
+  int primitive_rec;   // 1: the step starts with the primitive reconstruction (k_recons_begin),
+                       // so the last stage does not prepare the next step's stage 1
   int c2p_tc;          // c2p 2 with a network: 1 = con2prim in k_c2p_step on the tcgen05 tensor
                        // cores after the last stage, 0 = inside the last stage (warp mma.sync)
   // interface flux scratch: Fx(i+1/2, j) at fx[(j) * fpitch + (i + 1)],

@@ -25,6 +25,43 @@ __global__ void k_begin_step(const InstDesc* __restrict__ insts, int ninst, int 
   (void)ninst;
 }
 
+// primitive reconstruction (05_reconstruct.f95:525-746, primitive_rec = 1):
+// per field, the monotonized-central slope along the grid diagonal
+// (limit = 2, funciones.f95:104-147), L = u + x and R = u - x with
+// x = slope / 2 (both faces of a point take the same slope arguments), and
+// the new value (R + L) / 2; ghost points by the boundary maps.  Reads
+// prim[cur], writes the reconstructed primitives to prim[1 - cur] and
+// prepares the step from them (startconvar, stage 1).
+__device__ __forceinline__ double limiter_mc(double ga, double gb) {
+  return 0.5 * (fsgn1(ga) + fsgn1(gb)) *
+         fmin2(fmin2(2.0 * fabs(ga), 2.0 * fabs(gb)), 0.5 * fabs(ga + gb));
+}
+
+__global__ void k_recons_begin(const InstDesc* __restrict__ insts, int cur, int qout, double abt11) {
+  const InstDesc& I = insts[blockIdx.y];
+  if (!I.primitive_rec) return;
+  const int nx = I.imax + 1, ny = I.jmax + 1;
+  const long long fs = I.fstride;
+  const double* u = I.prim[cur];
+  double* un = I.prim[1 - cur];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = int(t % nx), j = int(t / nx);
+    const long long pc = (long long)j * I.pitch + i;
+    const long long pm = (long long)map_idx(j - 1, I.jmax, I.bc_y) * I.pitch + map_idx(i - 1, I.imax, I.bc_x);
+    const long long pp = (long long)map_idx(j + 1, I.jmax, I.bc_y) * I.pitch + map_idx(i + 1, I.imax, I.bc_x);
+    double pv[NPRIM];
+#pragma unroll
+    for (int c = 0; c < NPRIM; ++c) {
+      const double m1 = u[c * fs + pm], m = u[c * fs + pc], p1 = u[c * fs + pp];
+      const double x = 0.5 * limiter_mc(p1 - m, m - m1);
+      pv[c] = 0.5 * ((m - x) + (m + x));
+      un[c * fs + pc] = pv[c];
+    }
+    begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
+  }
+}
+
 // ------------------------------------------------- routine mirrors (pointwise)
 // startconvar only (06_conserved_var.f95:79-140)
 __global__ void k_startconvar(const InstDesc* __restrict__ insts, int cur) {
@@ -135,6 +172,11 @@ cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* 
 cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int q,
                                   double abtll) {
   k_electricvarint<<<point_grid(npts, n), 256, 0, st>>>(d, cur, q, abtll);
+  return cudaGetLastError();
+}
+cudaError_t launch_recons_begin(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
+                                double abt11) {
+  k_recons_begin<<<point_grid(npts, n), 256, 0, st>>>(d, cur, qout, abt11);
   return cudaGetLastError();
 }
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur) {

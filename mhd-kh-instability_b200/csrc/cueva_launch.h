@@ -38,6 +38,10 @@ cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* 
 cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int q,
                                   double abtll);
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);
+// primitive reconstruction of prim[cur] into prim[1 - cur] + startconvar and
+// stage 1 of the reconstructed state (primitive_rec = 1)
+cudaError_t launch_recons_begin(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
+                                double abt11);
 // learned con2prim on the tcgen05 tensor cores after the last stage
 // (cueva_c2p.cu): tiles of 128 points per instance, and the launch over
 // ntiles tiles of all instances; network seeds of n SoA states

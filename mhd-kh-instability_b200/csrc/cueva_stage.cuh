@@ -515,7 +515,8 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
       double* po = I.prim[1 - sa.cur];
 #pragma unroll
       for (int c = 0; c < NPRIM; ++c) po[c * fs + pc] = pv[c];
-      begin_step_point(I, sa.abt_diag_first, I.aux[1 - sa.cur], I.stage[1 - sa.qin], pc, pv);
+      // with the primitive reconstruction the next step starts in k_recons_begin
+      if (!I.primitive_rec) begin_step_point(I, sa.abt_diag_first, I.aux[1 - sa.cur], I.stage[1 - sa.qin], pc, pv);
     }
   }
   return st;

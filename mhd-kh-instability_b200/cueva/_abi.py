@@ -44,7 +44,7 @@ class Params(ctypes.Structure):
     _fields_ = [("imax", ctypes.c_int32), ("jmax", ctypes.c_int32), ("order", ctypes.c_int32),
                 ("flux_solver", ctypes.c_int32), ("rec_mp", ctypes.c_int32), ("c2p", ctypes.c_int32),
                 ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("intsum_reset", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("device", ctypes.c_int32), ("intsum_reset", ctypes.c_int32), ("primitive_rec", ctypes.c_int32),
                 ("lx", ctypes.c_double), ("ly", ctypes.c_double),
                 ("lz", ctypes.c_double), ("cfl", ctypes.c_double), ("sigma", ctypes.c_double),
                 ("gamma", ctypes.c_double), ("dt", ctypes.c_double)]

@@ -22,15 +22,17 @@ class Ensemble:
     def __init__(self, instances, fma=False):
         """instances: list of keyword dicts as accepted by cueva.Cueva
         (imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, precision,
-        device, lx, ly, lz, cfl, sigma, gamma, dt, intsum_reset)."""
+        device, lx, ly, lz, cfl, sigma, gamma, dt, intsum_reset, primitive_rec)."""
         self.L = _abi.load(fma)
         defaults = dict(order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1, precision=0, device=0, lx=2.0,
-                        ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, intsum_reset=0)
+                        ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, intsum_reset=0,
+                        primitive_rec=0)
         self.instances = [dict(defaults, **kw) for kw in instances]
         arr = (_abi.Params * len(self.instances))()
         for k, d in enumerate(self.instances):
             arr[k] = _abi.Params(d["imax"], d["jmax"], d["order"], d["flux_solver"], d["rec_mp"], d["c2p"],
-                                 d["bc_x"], d["bc_y"], d["precision"], d["device"], d["intsum_reset"], 0, d["lx"],
+                                 d["bc_x"], d["bc_y"], d["precision"], d["device"], d["intsum_reset"],
+                                 d["primitive_rec"], d["lx"],
                                  d["ly"], d["lz"], d["cfl"], d["sigma"], d["gamma"], d["dt"])
         self._params = arr
         h = ctypes.c_void_p()

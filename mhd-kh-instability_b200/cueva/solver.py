@@ -20,11 +20,11 @@ from . import _abi
 class Cueva:
     def __init__(self, imax, jmax, order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1, precision=0,
                  device=0, lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, fma=False,
-                 pinned=False, intsum_reset=0):
+                 pinned=False, intsum_reset=0, primitive_rec=0):
         self.L = _abi.load(fma)
         self.imax, self.jmax = int(imax), int(jmax)
         self.params = _abi.Params(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, precision, device,
-                                  intsum_reset, 0, lx, ly, lz, cfl, sigma, gamma, dt)
+                                  intsum_reset, primitive_rec, lx, ly, lz, cfl, sigma, gamma, dt)
         h = ctypes.c_void_p()
         _abi.check(self.L, self.L.cueva_ctx_create(ctypes.byref(self.params), ctypes.byref(h)))
         self.ctx = h

@@ -41,7 +41,7 @@ module cueva_gpu
 
   type, bind(c) :: cueva_params
      integer(c_int32_t) :: imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y
-     integer(c_int32_t) :: precision, device, intsum_reset, pad
+     integer(c_int32_t) :: precision, device, intsum_reset, primitive_rec
      real(c_double)     :: lx, ly, lz, cfl, sigma, gamma, dt
   end type cueva_params
 
@@ -164,7 +164,8 @@ contains
     prm%bc_x = 0; prm%bc_y = 1                   ! BOUND 6: x copy, y periodic
     if (BOUND == 1) prm%bc_y = 0                 ! copy / copy
     if (BOUND == 2) prm%bc_x = 1                 ! periodic / periodic
-    prm%precision = 0; prm%device = 0; prm%intsum_reset = 0; prm%pad = 0
+    prm%precision = 0; prm%device = 0; prm%intsum_reset = 0
+    prm%primitive_rec = primitive_rec           ! parameters.f95:26
     prm%lx = Longx; prm%ly = Longy; prm%lz = Longz; prm%cfl = CFL
     prm%sigma = sigma; prm%gamma = gamma; prm%dt = Delt
     ierr = cueva_ctx_create(prm, ctx)

@@ -61,6 +61,7 @@ const Key kKeys[] = {
     {"restart_file", "all_variables.dat", "backup file read when RESTART = 1"},
     {"precision", "0", "0 FP64, 1 FP32 reconstruction and Riemann solves"},
     {"intsum_reset", "0", "1 zeroes the stage sums before every stage"},
+    {"primitive_rec", "0", "1 reconstructs the primitives at the start of every step (05_reconstruct.f95)"},
     {"device", "0", "CUDA device ordinal"},
     {"kh_v0", "0.5", "shear velocity"},
     {"kh_a", "0.01", "shear width"},
@@ -203,6 +204,7 @@ int main(int argc, char** argv) {
   p.flux_solver = C.integer("flux_solver"); p.rec_mp = C.integer("rec_mp"); p.c2p = C.integer("conserved_to_primitive");
   p.bc_x = bc_x; p.bc_y = bc_y; p.precision = C.integer("precision"); p.device = C.integer("device");
   p.intsum_reset = C.integer("intsum_reset");
+  p.primitive_rec = C.integer("primitive_rec");
   p.lx = C.num("Longx"); p.ly = C.num("Longy"); p.lz = C.num("Longz"); p.cfl = C.num("CFL");
   p.sigma = C.num("sigma"); p.gamma = C.num("gamma"); p.dt = C.num("Delt");
 

@@ -149,6 +149,11 @@ bool make_tableau(int order, Tableau& T) {
 // u, up, um are indexed -6..n+6 (pointer offset +6).  posfix selects the
 // p/rho positivity fix of mp5.f95:177-262 (applied to slots 24,25 / 61,62).
 
+// slope limiter of the primitive reconstruction, limit = 2 (monotonized
+// central), funciones.f95:104-147
+inline double limiter_mc(double ga, double gb) {
+  return 0.5 * (fsign(1.0, ga) + fsign(1.0, gb)) * fmin3(2.0 * std::fabs(ga), 2.0 * std::fabs(gb), 0.5 * std::fabs(ga + gb));
+}
 inline double DMM(double x, double y) {  // funciones.f95:148-162
   return 0.5 * (fsign(1.0, x) + fsign(1.0, y)) * fmin2(std::fabs(x), std::fabs(y));
 }
@@ -1555,9 +1560,37 @@ struct Oracle {
     for (const char* s : n) fill_ghosts(a(s));
   }
 
+  // ------------------------- 05_reconstruct.f95:525-746 (primitive_rec = 1, DIM == 2)
+  // MC-limited slopes along the grid diagonal (i-1,j-1), (i,j), (i+1,j+1),
+  // (i+2,j+2): L(i,j) = u + slope/2, R(i+1,j+1) = u(i+1,j+1) - slope'/2, and
+  // the new value is the mean of R and L of the point.  Both faces of a
+  // point take the same limiter arguments, so the mean equals u up to the
+  // rounding of (u - x) + (u + x); the reference does exactly this.
+  void recons_var_primitive() {
+    const char* n[] = {"psi", "phi", "Bx", "By", "Bz", "Ex", "Ey", "Ez", "Vx", "Vy", "Vz", "q", "p", "rho"};
+    std::vector<double> L(ng, 0.0), R(ng, 0.0);
+    for (const char* f : n) {
+      double* u = a(f);
+#pragma omp parallel for schedule(static)
+      for (int j = -2; j <= jmax; ++j)
+        for (int i = -2; i <= imax; ++i) {
+          const double um1 = u[id(i - 1, j - 1)], m = u[id(i, j)], p1 = u[id(i + 1, j + 1)], p2 = u[id(i + 2, j + 2)];
+          L[id(i, j)] = m + 0.5 * limiter_mc(p1 - m, m - um1);
+          R[id(i + 1, j + 1)] = p1 - 0.5 * limiter_mc(p2 - p1, p1 - m);
+        }
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j <= jmax; ++j)
+        for (int i = 0; i <= imax; ++i) u[id(i, j)] = 0.5 * (R[id(i, j)] + L[id(i, j)]);
+    }
+  }
+
   // main_cueva_code.f95:53-328 stages part
   void begin_step() {
     boundary_prims();   // :53
+    if (P.primitive_rec) {   // :170-175
+      recons_var_primitive();
+      boundary_prims();
+    }
     startconvar();      // :181
     cleanvarint();      // :184
   }
@@ -1708,6 +1741,7 @@ void* oracle_create(const oracle_params* p) {
   if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
   if (p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
   if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
+  if (p->primitive_rec < 0 || p->primitive_rec > 1) return nullptr;
   Tableau T;
   if (!make_tableau(p->order, T)) return nullptr;
   return new Oracle(*p);

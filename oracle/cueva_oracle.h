@@ -35,6 +35,8 @@ typedef struct oracle_params {
   int32_t bc_x, bc_y;      /* 0 copy, 1 periodic (04_boundary.f95 BOUND 1/2/6) */
   int32_t intsum_reset;    /* 0: intsum zeroed once per step (07_clean_var.f95, main_cueva_code.f95:184),
                               as the reference; 1: zeroed before every stage (textbook IMEX-RK) */
+  int32_t primitive_rec;   /* 1: reconstruct the primitives at the start of every step
+                              (05_reconstruct.f95, main_cueva_code.f95:170-175) */
   double lx, ly, lz;       /* Longx, Longy, Longz */
   double cfl, sigma, gamma;
   double dt;               /* <= 0: CFL*min(Delx,Dely,Delz) (parameters.f95:312) */

@@ -19,7 +19,7 @@ class OracleParams(ctypes.Structure):
     _fields_ = [("imax", ctypes.c_int32), ("jmax", ctypes.c_int32), ("order", ctypes.c_int32),
                 ("flux_solver", ctypes.c_int32), ("rec_mp", ctypes.c_int32), ("c2p", ctypes.c_int32),
                 ("bc_x", ctypes.c_int32), ("bc_y", ctypes.c_int32), ("intsum_reset", ctypes.c_int32),
-                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+                ("primitive_rec", ctypes.c_int32), ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
                 ("cfl", ctypes.c_double), ("sigma", ctypes.c_double), ("gamma", ctypes.c_double),
                 ("dt", ctypes.c_double)]
 
@@ -94,9 +94,10 @@ class Oracle:
     """One CUEVA run on the host: prims in, prims out, internal arrays by name."""
 
     def __init__(self, imax, jmax, order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1,
-                 lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, intsum_reset=0):
+                 lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3, gamma=4.0 / 3.0, dt=0.0, intsum_reset=0,
+                 primitive_rec=0):
         self.imax, self.jmax = imax, jmax
-        self.p = OracleParams(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, intsum_reset,
+        self.p = OracleParams(imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y, intsum_reset, primitive_rec,
                               lx, ly, lz, cfl, sigma, gamma, dt)
         self.h = lib().oracle_create(ctypes.byref(self.p))
         if not self.h:

@@ -52,7 +52,7 @@ def _create(**kw):
     from cueva import _abi
     L = cueva.load(False)
     base = dict(imax=64, jmax=32, order=2, flux_solver=5, rec_mp=0, c2p=1, bc_x=0, bc_y=1, precision=0,
-                device=0, intsum_reset=0, pad=0, lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3,
+                device=0, intsum_reset=0, primitive_rec=0, lx=2.0, ly=1.0, lz=1.0, cfl=0.25, sigma=1e3,
                 gamma=4.0 / 3.0, dt=0.0)
     base.update(kw)
     p = _abi.Params(**base)
@@ -67,7 +67,7 @@ def _create(**kw):
 @pytest.mark.parametrize("kw,frag", [
     (dict(imax=4), "imax"), (dict(flux_solver=3), "flux_solver"), (dict(rec_mp=5), "rec_mp"),
     (dict(c2p=7), "c2p"), (dict(bc_x=2), "bc_x"), (dict(order=7), "order"), (dict(precision=3), "precision"),
-    (dict(intsum_reset=2), "intsum_reset")])
+    (dict(intsum_reset=2), "intsum_reset"), (dict(primitive_rec=3), "primitive_rec")])
 def test_bad_configuration_rejected(kw, frag):
     rc, msg = _create(**kw)
     assert rc == 1 and frag.split("_")[0] in msg.lower().replace(" ", "_")

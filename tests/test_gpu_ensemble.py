@@ -104,3 +104,25 @@ def test_learned_ensemble_matches_single_runs():
         s.close()
     ens.close()
     net.close()
+
+
+def test_primitive_reconstruction_ensemble_matches_single_runs():
+    from cueva import Cueva
+    from cueva.ensemble import Ensemble
+    common = dict(COMMON, primitive_rec=1)
+    ens = Ensemble([dict(imax=g["imax"], jmax=g["jmax"], sigma=g["sigma"], **common) for g in GRIDS])
+    for k, g in enumerate(GRIDS):
+        ens.kh_init(k, v0=g["v0"], a=0.05)
+    ens.step(4)
+    ens.sync()
+    for k, g in enumerate(GRIDS):
+        s = Cueva(g["imax"], g["jmax"], sigma=g["sigma"], **common)
+        s.kh_init(v0=g["v0"], a=0.05)
+        s.upload()
+        s.step(4)
+        s.download()
+        got = ens.get_prims(k)
+        for n in PRIMS:
+            assert np.array_equal(got[n], s.interior(n)), (k, n)
+        s.close()
+    ens.close()

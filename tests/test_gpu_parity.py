@@ -178,3 +178,26 @@ def test_ssp433_reference_breakdown_reproduced(oracle_mod, solver):
     else:
         pytest.fail("oracle did not break down")
     g.close()
+
+
+@pytest.mark.parametrize("solver,order,rec,bc_x,grid", [(7, 2, 0, 0, (64, 32)), (5, 3, 1, 0, (64, 32)),
+                                                        (6, 2, 2, 1, (45, 38))])
+def test_steps_primitive_reconstruction(oracle_mod, solver, order, rec, bc_x, grid):
+    """primitive_rec = 1: every step starts with the diagonal MC
+    reconstruction of the primitives (05_reconstruct.f95:525-746) in
+    k_recons_begin; 1 step <= 1e-12, 200 steps <= 1e-9 against the oracle."""
+    imax, jmax = grid
+    g, o = _pair(oracle_mod, imax, jmax, False, order=order, flux_solver=solver, rec_mp=rec, sigma=1e3,
+                 bc_x=bc_x, primitive_rec=1)
+    g.kh_init(v0=0.5, a=0.05)
+    o.set_prims(g.prims())
+    g.upload()
+    for steps, bar in ((1, 1e-12), (199, 1e-9)):
+        g.step(steps)
+        g.download()
+        assert o.step(steps) == 0
+        ref = o.get_prims()
+        for n in PRIMS:
+            err = rel_l1_field(n, g.interior(n), ref[n], ref)
+            assert err <= bar, (steps, n, err)
+    g.close()

@@ -271,3 +271,28 @@ def test_c2p_status_codes(oracle_mod):
     good = np.array([1.2, 2.0, 0.1, 0, 0, 0, 0, 0, 0, 0.1, 0, 0, 0, 0, 1, 1], dtype=float)
     st, out = oracle_mod.c2p(good, method=1)
     assert st == 0 and np.all(np.isfinite(out))
+
+
+def test_primitive_reconstruction_is_identity_to_rounding(oracle_mod):
+    """05_reconstruct.f95 (primitive_rec = 1) takes the same limiter
+    arguments for the R and L values of a point, so (R + L)/2 returns the
+    value up to the rounding of (u - x) + (u + x): a uniform state stays
+    exact, a KH state changes by a few ulp."""
+    pr = oracle_mod.kh_init(32, 16, v0=0.5, a=0.05)
+    runs = {}
+    for r in (0, 1):
+        o = oracle_mod.Oracle(32, 16, order=2, flux_solver=7, primitive_rec=r)
+        o.set_prims(pr)
+        assert o.step(1) == 0
+        runs[r] = o.get_prims()
+    for n in runs[0]:
+        a, b = runs[0][n], runs[1][n]
+        scale = max(float(np.abs(a).max()), 1e-300)
+        assert float(np.abs(a - b).max()) <= 1e-14 * scale, n
+    u = {n: np.full_like(v, 0.25 if n in ("rho", "p") else 0.0) for n, v in pr.items()}
+    o = oracle_mod.Oracle(32, 16, order=2, flux_solver=5, primitive_rec=1)
+    o.set_prims(u)
+    assert o.step(1) == 0
+    out = o.get_prims()
+    for n in u:
+        assert np.array_equal(out[n], u[n]), n
