@@ -56,6 +56,28 @@ __device__ __forceinline__ void learned_stats(unsigned long long* stats, bool co
 
 // the tail of the step for the instances with the learned method: tiles of
 // 128 points over all instances (block ranges of launch kind LK_C2P)
+// L2 prefetch of the inputs of tile b of instance I (the 19 fields the
+// tile reads; its 128 points cover at most two row segments per field)
+__device__ __forceinline__ void c2p_prefetch(const InstDesc& I, int b, int cur) {
+  const int t = threadIdx.x;
+  if (t >= 2 * 19) return;
+  const int nx = I.imax + 1;
+  const long long npts = (long long)nx * (I.jmax + 1);
+  const long long p0 = (long long)b * TC_ROWS;
+  if (p0 >= npts) return;
+  const long long p1 = (p0 + TC_ROWS < npts ? p0 + TC_ROWS : npts) - 1;   // last point of the tile
+  const int f = t >> 1, seg = t & 1;
+  const int j0 = int(p0 / nx), i0 = int(p0 % nx), j1 = int(p1 / nx), i1 = int(p1 % nx);
+  if (seg == 1 && j1 == j0) return;
+  const int row = seg ? j1 : j0, ia = seg ? 0 : i0, ib = (seg || j1 == j0) ? i1 : nx - 1;
+  const long long fs = I.fstride;
+  const double* base;
+  if (f < 5) base = I.finsum + (long long)(Q_D + f) * fs;                   // varfin's D, tau, S
+  else if (f < 14) base = I.prim[1 - cur] + (long long)(P_PSI + f - 5) * fs; // psi .. q of time n+1
+  else base = I.prim[cur] + (long long)(f - 14) * fs;                       // rho, p, v seeds
+  prefetch_l2(base + (long long)row * I.pitch + ia, ib - ia + 1);
+}
+
 __global__ void __launch_bounds__(TC_ROWS, C2P_CTAS_PER_SM)
 k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPDevice* __restrict__ mlp, int cur,
            int qout, double abt11) {
@@ -66,6 +88,11 @@ k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPD
     int b = tile;
     const InstDesc& I = tile_inst(insts, ninst, LK_C2P, b);
     if (!(I.c2p == 2 && I.c2p_tc)) continue;   // uniform over the CTA: a tile belongs to one instance
+    if (tile + (int)gridDim.x < ntiles) {       // the next tile's inputs go to L2 meanwhile
+      int bn = tile + (int)gridDim.x;
+      const InstDesc& In = tile_inst(insts, ninst, LK_C2P, bn);
+      if (In.c2p == 2 && In.c2p_tc) c2p_prefetch(In, bn, cur);
+    }
     const int nx = I.imax + 1;
     const long long npts = (long long)nx * (I.jmax + 1);
     const long long p0 = (long long)b * TC_ROWS + threadIdx.x;
