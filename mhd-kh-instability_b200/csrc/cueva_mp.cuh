@@ -25,8 +25,17 @@ __device__ __forceinline__ T DM4(T w, T xx, T y, T z) {  // funciones.f95:165-18
          fmin2(fmin2(fmin2(fabs(w), fabs(xx)), fabs(y)), fabs(z));
 }
 
-// stencil radius of the unlimited interface formula
+// stencil radius of the unlimited interface formula; RM = 3 is the
+// second-order MC reconstruction of the MCL flux routines (radius 1)
 template <int RM> struct MPR { static constexpr int R = RM + 2; };
+template <> struct MPR<3> { static constexpr int R = 1; };
+
+// monotonized-central slope (mcl with slop = 2, funciones.f95:56-95)
+template <typename T>
+__device__ __forceinline__ T mc_slope(T fa, T fb) {
+  return T(0.5) * (fsgn1(fa) + fsgn1(fb)) *
+         fmin2(fmin2(T(2.0) * fabs(fa), T(2.0) * fabs(fb)), T(0.5) * fabs(fa + fb));
+}
 
 // unlimited left value at k+1/2 (SH97 eq. 2.1 / 2.31) around register index C
 template <int RM, int C, typename T, int N>
@@ -181,6 +190,17 @@ template <typename T> struct MPCall<2, T> {
   template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[10]) {
     return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9])
                : pair(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9]);
+  }
+};
+
+// second-order MC pair of 16_hll_flow_mcl.f95:565-1112 (FAC = 0.5, no
+// positivity fix): u holds cells i-1 .. i+2
+template <typename T> struct MPCall<3, T> {
+  template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[4]) {
+    Pair<T> p;
+    p.L = u[1] + T(0.5) * mc_slope(u[2] - u[1], u[1] - u[0]);
+    p.R = u[2] - T(0.5) * mc_slope(u[3] - u[2], u[2] - u[1]);
+    return p;
   }
 };
 

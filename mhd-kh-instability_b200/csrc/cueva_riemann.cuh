@@ -140,6 +140,39 @@ __device__ __forceinline__ void hll_fluxes(const Side<T>& L, const Side<T>& R, T
   A[R_ST2] = hll(fl.FSt2, fr.FSt2, X::St2(L), X::St2(R));
 }
 
+// HLL of the second-order MCL routine, 16_hll_flow_mcl.f95:1014-1396 (Sp = 1):
+// the fluxes of the MPX HLL with W = 1 / sqrt(1 - vx^2 - vy^2 - vz^2), the
+// normal current computed from each side's reconstructed state,
+//   J_n = sigma W (E_n + (B_t2 v_t1 - B_t1 v_t2) - (E.v) v_n) + q v_n,
+// and the "_m" values of E_t2 and B_t1 (-u + slope, which is not the
+// negated side value) in the roles R_BT1 and R_ET2
+template <int D, typename T>
+__device__ __forceinline__ void mcl_fluxes(const Side<T>& L, const Side<T>& R, const T (&m_et2)[2],
+                                           const T (&m_bt1)[2], T gamma, T sigma, T* A) {
+  using X = Dir<D>;
+  A[R_PSI] = hll(X::En(L), X::En(R), L.psi, R.psi);
+  A[R_PHI] = hll(X::Bn(L), X::Bn(R), L.phi, R.phi);
+  A[R_BN] = hll(L.phi, R.phi, X::Bn(L), X::Bn(R));
+  A[R_BT1] = -hll(m_et2[0], m_et2[1], X::Bt1(L), X::Bt1(R));
+  A[R_BT2] = hll(X::Et1(L), X::Et1(R), X::Bt2(L), X::Bt2(R));
+  A[R_EN] = hll(L.psi, R.psi, X::En(L), X::En(R));
+  A[R_ET1] = hll(X::Bt2(L), X::Bt2(R), X::Et1(L), X::Et1(R));
+  A[R_ET2] = -hll(m_bt1[0], m_bt1[1], X::Et2(L), X::Et2(R));
+  const T WL = lorentz_hlle(L), WR = lorentz_hlle(R);
+  auto jn = [&](const Side<T>& s, T W) {
+    const T vrotB = X::Bt2(s) * X::vt1(s) - X::Bt1(s) * X::vt2(s);
+    const T Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+    return sigma * W * (X::En(s) + vrotB - Edotv * X::vn(s)) + s.q * X::vn(s);
+  };
+  A[R_Q] = hll(jn(L, WL), jn(R, WR), L.q, R.q);
+  const Phys<T> fl = physical<D>(L, gamma, WL), fr = physical<D>(R, gamma, WR);
+  A[R_D] = hll(fl.FD, fr.FD, L.D, R.D);
+  A[R_TAU] = hll(fl.Ftau, fr.Ftau, L.tau, R.tau);
+  A[R_SN] = hll(fl.FSn, fr.FSn, X::Sn(L), X::Sn(R));
+  A[R_ST1] = hll(fl.FSt1, fr.FSt1, X::St1(L), X::St1(R));
+  A[R_ST2] = hll(fl.FSt2, fr.FSt2, X::St2(L), X::St2(R));
+}
+
 // get_hllc_vel, funciones.f95:188-259: Newton on a v^2 - b v + c = 0 in
 // [-1,1].  The Fortran's first f evaluation reads the local v before it is
 // assigned (line 229); this evaluates it at the seed oldv, like the oracle.

@@ -225,7 +225,7 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits
 template <int RM, int SOLVER, typename T, int D, int ROWS>
 __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
-                                              T (&F)[NROLE]) {
+                                              double sigma_d, T (&F)[NROLE]) {
   using G = FaceGeom<RM, SOLVER, ROWS>;
   constexpr int R = G::R, NS = G::NS;
   auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
@@ -255,6 +255,44 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
 
   uint32_t stt = 0;
   Side<T> L, Rs;
+  if constexpr (SOLVER == 2) {
+    // HLL with the second-order MC reconstruction, 16_hll_flow_mcl.f95:565-1396
+    // (x and y faces of a point are the same formulas in the direction roles)
+    static_assert(RM == 3, "the MCL fluxes use the MC reconstruction");
+    T m_et2[2], m_bt1[2];   // "_m" values (-u + slope) of E_t2 and B_t1, left and right
+    auto recm = [&](int f, T& Lv, T& Rv, T* m) {
+      T u[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) u[q] = nrm(f, q);
+      const T sl = T(0.5) * mc_slope(u[2] - u[1], u[1] - u[0]);
+      const T sr = T(0.5) * mc_slope(u[3] - u[2], u[2] - u[1]);
+      Lv = u[1] + sl;
+      Rv = u[2] - sr;
+      if (m) { m[0] = -u[1] + sl; m[1] = -u[2] - sr; }
+    };
+    constexpr int fEt2 = 5 + (D == 0 ? Q_EZ : Q_EX), fBt1 = 5 + (D == 0 ? Q_BY : Q_BZ);
+    recm(0, L.vx, Rs.vx, nullptr);
+    recm(1, L.vy, Rs.vy, nullptr);
+    recm(2, L.vz, Rs.vz, nullptr);
+    recm(3, L.p, Rs.p, nullptr);
+    recm(4, L.rho, Rs.rho, nullptr);
+    recm(5 + Q_PSI, L.psi, Rs.psi, nullptr);
+    recm(5 + Q_PHI, L.phi, Rs.phi, nullptr);
+    recm(5 + Q_EX, L.Ex, Rs.Ex, fEt2 == 5 + Q_EX ? m_et2 : nullptr);
+    recm(5 + Q_EY, L.Ey, Rs.Ey, nullptr);
+    recm(5 + Q_EZ, L.Ez, Rs.Ez, fEt2 == 5 + Q_EZ ? m_et2 : nullptr);
+    recm(5 + Q_BX, L.Bx, Rs.Bx, nullptr);
+    recm(5 + Q_BY, L.By, Rs.By, fBt1 == 5 + Q_BY ? m_bt1 : nullptr);
+    recm(5 + Q_BZ, L.Bz, Rs.Bz, fBt1 == 5 + Q_BZ ? m_bt1 : nullptr);
+    recm(5 + Q_Q, L.q, Rs.q, nullptr);
+    recm(5 + Q_D, L.D, Rs.D, nullptr);
+    recm(5 + Q_TAU, L.tau, Rs.tau, nullptr);
+    recm(5 + Q_SX, L.Sx, Rs.Sx, nullptr);
+    recm(5 + Q_SY, L.Sy, Rs.Sy, nullptr);
+    recm(5 + Q_SZ, L.Sz, Rs.Sz, nullptr);
+    mcl_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F);
+    return stt;
+  }
   // primitive slots of this direction (21-25 for x, 58-62 for y)
   rec(0, L.vx, Rs.vx);
   rec(1, L.vy, Rs.vy);
@@ -316,7 +354,7 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
   const T gamma = T(gamma_d);
   if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, F);
   else if constexpr (SOLVER == 6) hlle_fluxes<D>(L, Rs, gamma, F, stt);
-  else hllc_fluxes<D>(L, Rs, gamma, F, stt);
+  else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, F, stt);
   return stt;
 }
 
@@ -354,7 +392,7 @@ k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
     const int i = i0 + lane, j = j0 + w;
     if (i <= ilast && j <= jlast) {
       T F[NROLE];
-      const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, F);
+      const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
       const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
       for (int c = 0; c < NROLE; ++c) flux_store<T>(I.fy, c * I.ffs + fo, F[c]);
@@ -574,7 +612,7 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
 #pragma unroll
   for (int c = 0; c < NROLE; ++c) F[c] = T(0);
   uint32_t stt = 0;
-  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, F);
+  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
   // Fx(i-1/2) of point i is the face of lane-1
   const double dlx = I.delx, ix2 = I.inv_delx_pow2;
   double qx[NROLE];
@@ -675,22 +713,30 @@ template <int SV>
 cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                                 const StageArgs& sa, cudaEvent_t* ev) {
   if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
-  switch (rec_mp) {
-    case 0: launch_rm_sv<0, SV>(prec, sh, st, d, n, sa, ev); break;
-    case 1: launch_rm_sv<1, SV>(prec, sh, st, d, n, sa, ev); break;
-    case 2: launch_rm_sv<2, SV>(prec, sh, st, d, n, sa, ev); break;
-    default: return cudaErrorInvalidValue;
+  if constexpr (SV == 2) {   // the MCL routine has its own reconstruction; rec_mp does not apply
+    launch_rm_sv<3, SV>(prec, sh, st, d, n, sa, ev);
+  } else {
+    switch (rec_mp) {
+      case 0: launch_rm_sv<0, SV>(prec, sh, st, d, n, sa, ev); break;
+      case 1: launch_rm_sv<1, SV>(prec, sh, st, d, n, sa, ev); break;
+      case 2: launch_rm_sv<2, SV>(prec, sh, st, d, n, sa, ev); break;
+      default: return cudaErrorInvalidValue;
+    }
   }
   return cudaGetLastError();
 }
 
 template <int SV>
 cudaError_t prepare_stage_solver(int rec_mp, int prec) {
-  switch (rec_mp) {
-    case 0: return prepare_rm_sv<0, SV>(prec);
-    case 1: return prepare_rm_sv<1, SV>(prec);
-    case 2: return prepare_rm_sv<2, SV>(prec);
-    default: return cudaErrorInvalidValue;
+  if constexpr (SV == 2) {
+    return prepare_rm_sv<3, SV>(prec);
+  } else {
+    switch (rec_mp) {
+      case 0: return prepare_rm_sv<0, SV>(prec);
+      case 1: return prepare_rm_sv<1, SV>(prec);
+      case 2: return prepare_rm_sv<2, SV>(prec);
+      default: return cudaErrorInvalidValue;
+    }
   }
 }
 

@@ -585,7 +585,9 @@ struct Oracle {
     kappa_phi = 1.0 / pw2(cp_phi);
     gamma = p.gamma; sigma = p.sigma;
     // value the module variable eps1 holds when con2prim runs (set last by the flux routine)
-    eps1_c2p = (p.flux_solver == 7) ? (double)1.0e-6f : 1.0e-6;
+    // (the MCL routine of flux_solver 2 never sets it: the zero-initialised
+    // module variable; only the superluminal seed clamp reads it)
+    eps1_c2p = (p.flux_solver == 7) ? (double)1.0e-6f : (p.flux_solver == 2 ? 0.0 : 1.0e-6);
     make_tableau(p.order, T);
     lmax = T.s;
     const char* names[] = {
@@ -805,7 +807,55 @@ struct Oracle {
     }
   }
 
+  // --------------------- second-order MC reconstruction (16_hll_flow_mcl.f95:565-1112)
+  // face i+1/2 of a line: L = u(i) + FAC mcl(u(i+1)-u(i), u(i)-u(i-1)),
+  // R = u(i+1) - FAC mcl(u(i+2)-u(i+1), u(i+1)-u(i)) with FAC = FAC_SR = 0.5
+  // (parameters.f95:42-43) and mcl the monotonized-central slope (slop = 2,
+  // funciones.f95:56-95).  The "_m" values of E and B keep the slope's sign
+  // and negate only the cell value: L_m = -u(i) + FAC mcl(...),
+  // R_m = -u(i+1) - FAC mcl(...) (:655-667, :708-735), which is not -L / -R.
+  void mcl_line(int n, const double* u, bool negate, double* L, double* R) {
+    for (int i = -1; i <= n + 1; ++i) {
+      const double um1 = u[i - 1 + 6], u0 = u[i + 6], u1 = u[i + 1 + 6], u2 = u[i + 2 + 6];
+      const double sl = 0.5 * limiter_mc(u1 - u0, u0 - um1);
+      const double sr = 0.5 * limiter_mc(u2 - u1, u1 - u0);
+      L[i + 6] = negate ? -u0 + sl : u0 + sl;
+      R[i + 6] = negate ? -u1 - sr : u1 - sr;
+    }
+  }
+  void reconstruct_mcl() {
+    XL.assign(X_N, std::vector<double>(ng, 0.0)); XR.assign(X_N, std::vector<double>(ng, 0.0));
+    YL.assign(Y_N, std::vector<double>(ng, 0.0)); YR.assign(Y_N, std::vector<double>(ng, 0.0));
+#pragma omp parallel
+    {
+      std::vector<double> u(imax + 13), L(imax + 13), R(imax + 13);
+#pragma omp for schedule(static)
+      for (int jj = -1; jj <= jmax + 1; ++jj)
+        for (int s = 0; s < X_JX; ++s) {
+          const double* src; double sg;
+          slot_src(s, true, src, sg);
+          for (int i = -6; i <= imax + 6; ++i) u[i + 6] = src[id(i, jj)];
+          mcl_line(imax, u.data(), sg < 0, L.data(), R.data());
+          for (int i = -1; i <= imax + 1; ++i) { XL[s][id(i, jj)] = L[i + 6]; XR[s][id(i, jj)] = R[i + 6]; }
+        }
+    }
+#pragma omp parallel
+    {
+      std::vector<double> u(jmax + 13), L(jmax + 13), R(jmax + 13);
+#pragma omp for schedule(static)
+      for (int ii = -1; ii <= imax + 1; ++ii)
+        for (int s = 0; s < Y_JY; ++s) {
+          const double* src; double sg;
+          slot_src(s, false, src, sg);
+          for (int j = -6; j <= jmax + 6; ++j) u[j + 6] = src[id(ii, j)];
+          mcl_line(jmax, u.data(), sg < 0, L.data(), R.data());
+          for (int j = -1; j <= jmax + 1; ++j) { YL[s][id(ii, j)] = L[j + 6]; YR[s][id(ii, j)] = R[j + 6]; }
+        }
+    }
+  }
+
   void reconstruct() {
+    if (P.flux_solver == 2) { reconstruct_mcl(); return; }
     const int rec = P.rec_mp;
     XL.assign(X_N, std::vector<double>(ng, 0.0)); XR.assign(X_N, std::vector<double>(ng, 0.0));
     YL.assign(Y_N, std::vector<double>(ng, 0.0)); YR.assign(Y_N, std::vector<double>(ng, 0.0));
@@ -907,6 +957,55 @@ struct Oracle {
     return (s2 * FL - s1 * FR + s1 * s2 * (UR - UL)) / (s2 - s1);
   }
 
+  // HLL fluxes of the MC-reconstructed states (16_hll_flow_mcl.f95:1014-1396):
+  // the same arrays as the MPX routines, with W = 1/sqrt(1 - vx^2 - vy^2 - vz^2)
+  // (:900-905), the current J computed from the reconstructed states of
+  // each side instead of reconstructed (:1026-1042), and the "_m" values in
+  // the fluxes EzlaxBy, ExlaxBz, BylaxEz, BzlaxEx
+  void mcl_fluxes(const Side& xl, const Side& xr, const Side& yl, const Side& yr, double* out) {
+    PhysX fxl = physx(xl), fxr = physx(xr), fyl = physy(yl), fyr = physy(yr);
+    hlle_w(fxl, xl); hlle_w(fxr, xr); hlle_w(fyl, yl); hlle_w(fyr, yr);
+    fxl = physx_w(xl, fxl.W); fxr = physx_w(xr, fxr.W); fyl = physy_w(yl, fyl.W); fyr = physy_w(yr, fyr.W);
+    auto jx = [&](const Side& s, double W) {
+      const double vrotB = s.Bz * s.vy - s.By * s.vz;
+      const double Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+      return sigma * W * (s.Ex + vrotB - Edotv * s.vx) + s.q * s.vx;
+    };
+    auto jy = [&](const Side& s, double W) {
+      const double vrotB = s.Bx * s.vz - s.Bz * s.vx;
+      const double Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+      return sigma * W * (s.Ey + vrotB - Edotv * s.vy) + s.q * s.vy;
+    };
+    out[0] = hllf(xl.Ex, xr.Ex, xl.psi, xr.psi);                 // Exlaxpsi
+    out[1] = hllf(yl.Ey, yr.Ey, yl.psi, yr.psi);                 // Eylaxpsi
+    out[2] = hllf(xl.Bx, xr.Bx, xl.phi, xr.phi);                 // Bxlaxphi
+    out[3] = hllf(yl.By, yr.By, yl.phi, yr.phi);                 // Bylaxphi
+    out[4] = hllf(xl.phi, xr.phi, xl.Bx, xr.Bx);                 // philaxBx
+    out[5] = hllf(yl.Ez, yr.Ez, yl.Bx, yr.Bx);                   // EzlaxBx
+    out[6] = -hllf(xl.Ezm, xr.Ezm, xl.By, xr.By);                // EzlaxBy
+    out[7] = hllf(yl.phi, yr.phi, yl.By, yr.By);                 // philaxBy
+    out[8] = hllf(xl.Ey, xr.Ey, xl.Bz, xr.Bz);                   // EylaxBz
+    out[9] = -hllf(yl.Exm, yr.Exm, yl.Bz, yr.Bz);                // ExlaxBz
+    out[10] = hllf(xl.psi, xr.psi, xl.Ex, xr.Ex);                // psilaxEx
+    out[11] = -hllf(yl.Bzm, yr.Bzm, yl.Ex, yr.Ex);               // BzlaxEx
+    out[12] = hllf(xl.Bz, xr.Bz, xl.Ey, xr.Ey);                  // BzlaxEy
+    out[13] = hllf(yl.psi, yr.psi, yl.Ey, yr.Ey);                // psilaxEy
+    out[14] = -hllf(xl.Bym, xr.Bym, xl.Ez, xr.Ez);               // BylaxEz
+    out[15] = hllf(yl.Bx, yr.Bx, yl.Ez, yr.Ez);                  // BxlaxEz
+    out[16] = hllf(jx(xl, fxl.W), jx(xr, fxr.W), xl.q, xr.q);    // Jxlax
+    out[17] = hllf(jy(yl, fyl.W), jy(yr, fyr.W), yl.q, yr.q);    // Jylax
+    out[18] = hllf(fxl.FD, fxr.FD, xl.D, xr.D);
+    out[19] = hllf(fyl.FD, fyr.FD, yl.D, yr.D);
+    out[20] = hllf(fxl.Ftau, fxr.Ftau, xl.tau, xr.tau);
+    out[21] = hllf(fyl.Ftau, fyr.Ftau, yl.tau, yr.tau);
+    out[22] = hllf(fxl.FSx, fxr.FSx, xl.Sx, xr.Sx);
+    out[23] = hllf(fxl.FSy, fxr.FSy, xl.Sy, xr.Sy);
+    out[24] = hllf(fxl.FSz, fxr.FSz, xl.Sz, xr.Sz);
+    out[25] = hllf(fyl.FSx, fyr.FSx, yl.Sx, yr.Sx);
+    out[26] = hllf(fyl.FSy, fyr.FSy, yl.Sy, yr.Sy);
+    out[27] = hllf(fyl.FSz, fyr.FSz, yl.Sz, yr.Sz);
+  }
+
   // ------------------------------------------- Riemann loop (2D, i=-1..imax, j=-1..jmax)
   void riemann() {
     const int solver = P.flux_solver;
@@ -945,6 +1044,12 @@ struct Oracle {
           };
           if (V2xl >= 1.0 || V2xr >= 1.0) fallback();
           if (V2yl >= 1.0 || V2yr >= 1.0) fallback();
+        }
+        if (solver == 2) {   // 16_hll_flow_mcl.f95:1014-1396 (const_sp = 0: Sp = 1, SLC = 0)
+          double out[28];
+          mcl_fluxes(xl, xr, yl, yr, out);
+          for (int c = 0; c < 28; ++c) o[c][k] = out[c];
+          continue;
         }
         if (solver == 7) {
           // density fix-up chain, 16_hllc_flow_mpx.f95:2663-2690
@@ -1739,7 +1844,7 @@ extern "C" {
 
 void* oracle_create(const oracle_params* p) {
   if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
-  if (p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
+  if (p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
   if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
   if (p->primitive_rec < 0 || p->primitive_rec > 1) return nullptr;
   Tableau T;

@@ -134,7 +134,8 @@ def test_tableaux_consistent(oracle_mod):
         assert np.all(np.triu(abt[:s, :s], 1) == 0)             # implicit part lower (DIRK)
 
 
-@pytest.mark.parametrize("solver,order,rec", [(5, 2, 0), (7, 4, 0), (7, 2, 1), (5, 3, 2), (6, 2, 0), (6, 4, 2)])
+@pytest.mark.parametrize("solver,order,rec", [(5, 2, 0), (7, 4, 0), (7, 2, 1), (5, 3, 2), (6, 2, 0), (6, 4, 2), (2, 2, 0),
+                                              (2, 4, 0)])
 def test_uniform_state_stays_uniform(oracle_mod, solver, order, rec):
     imax, jmax = 20, 12
     o = oracle_mod.Oracle(imax, jmax, order=order, flux_solver=solver, rec_mp=rec, bc_x=0, bc_y=1, sigma=1e3)
@@ -296,3 +297,19 @@ def test_primitive_reconstruction_is_identity_to_rounding(oracle_mod):
     out = o.get_prims()
     for n in u:
         assert np.array_equal(out[n], u[n]), n
+
+
+def test_mcl_reconstruction_second_order(oracle_mod):
+    """The MC reconstruction of flux_solver 2 (16_hll_flow_mcl.f95) is exact
+    on linear data away from extrema, and its "_m" values negate only the
+    cell value: -u + slope, not -(u + slope)."""
+    pr = oracle_mod.kh_init(24, 12, v0=0.0, a=0.05, amp=0.0)
+    ramp = np.add.outer(0.01 * np.arange(13), 0.02 * np.arange(25)) + 1.0   # linear in i and j
+    pr = {n: (ramp.copy() if n in ("rho", "p") else np.zeros_like(ramp)) for n in pr}
+    o = oracle_mod.Oracle(24, 12, order=1, flux_solver=2, bc_x=0, bc_y=0, sigma=1.0)
+    o.set_prims(pr)
+    assert o.run_stages(1) == 0
+    # the x flux of D at interior faces is 0.5 (FD_L + FD_R) - 0.5 (D_R - D_L) with v = 0:
+    # -(D_R - D_L)/2 with the exact face values, i.e. 0 for continuous linear data
+    fd = o.named("FDxlax", 1)
+    assert np.allclose(fd[2:-2, 2:-3], 0.0, atol=1e-14)
