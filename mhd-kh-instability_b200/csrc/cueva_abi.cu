@@ -125,8 +125,10 @@ namespace {
 
 int32_t validate_params(const cueva_params* p) {
   if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
-  if (p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7)
-    return fail(CUEVA_ERR_ARG, "flux_solver must be 2 (HLL+MC), 5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
+  if (p->flux_solver != 1 && p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 &&
+      p->flux_solver != 7)
+    return fail(CUEVA_ERR_ARG,
+                "flux_solver must be 1 (Lax+MC), 2 (HLL+MC), 5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
   if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
   if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
   if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))
@@ -208,8 +210,8 @@ void fill_desc(const cueva_params* p, const InstGeom& G, int nkslot, double* sla
   I.kappa_psi = 1.0 / (cp * cp);
   I.kappa_phi = 1.0 / (cp * cp);
   // the Fortran module variable eps1 keeps the value the flux routine stored last
-  // (the MCL routine of flux_solver 2 never sets it: zero-initialised)
-  I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : (p->flux_solver == 2 ? 0.0 : 1.0e-6);
+  // (the Lax and MCL routines of flux_solver 1 and 2 never set it: zero-initialised)
+  I.eps1_c2p = (p->flux_solver == 7) ? (double)1.0e-6f : (p->flux_solver <= 2 ? 0.0 : 1.0e-6);
   I.c2p = p->c2p;
   I.c2p_tc = 0;
   I.primitive_rec = p->primitive_rec;

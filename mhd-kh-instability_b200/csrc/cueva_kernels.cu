@@ -136,6 +136,7 @@ __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
 // ------------------------------------------------------------- dispatch
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
   switch (solver) {
+    case 1: return prepare_stage_lax(rec_mp, prec);
     case 2: return prepare_stage_mcl(rec_mp, prec);
     case 5: return prepare_stage_hll(rec_mp, prec);
     case 6: return prepare_stage_hlle(rec_mp, prec);
@@ -147,6 +148,7 @@ cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev) {
   switch (solver) {
+    case 1: return launch_stage_lax(rec_mp, prec, sh, st, d, n, sa, ev);
     case 2: return launch_stage_mcl(rec_mp, prec, sh, st, d, n, sa, ev);
     case 5: return launch_stage_hll(rec_mp, prec, sh, st, d, n, sa, ev);
     case 6: return launch_stage_hlle(rec_mp, prec, sh, st, d, n, sa, ev);

@@ -19,10 +19,13 @@ int mlp_device_of(const cueva_mlp* M);
 // before the first launch or capture)
 cudaError_t prepare_stage(int rec_mp, int solver, int prec);
 // per-solver halves of prepare_stage / launch_stage (cueva_stage_*.cu)
+cudaError_t prepare_stage_lax(int rec_mp, int prec);
 cudaError_t prepare_stage_hll(int rec_mp, int prec);
 cudaError_t prepare_stage_mcl(int rec_mp, int prec);
 cudaError_t prepare_stage_hllc(int rec_mp, int prec);
 cudaError_t prepare_stage_hlle(int rec_mp, int prec);
+cudaError_t launch_stage_lax(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
+                             const StageArgs& sa, cudaEvent_t* ev);
 cudaError_t launch_stage_hll(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                              const StageArgs& sa, cudaEvent_t* ev);
 cudaError_t launch_stage_mcl(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,

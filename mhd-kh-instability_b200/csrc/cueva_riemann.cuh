@@ -173,6 +173,51 @@ __device__ __forceinline__ void mcl_fluxes(const Side<T>& L, const Side<T>& R, c
   A[R_ST2] = hll(fl.FSt2, fr.FSt2, X::St2(L), X::St2(R));
 }
 
+// Lax-Friedrichs cell pairs, 15_lax_flow.f95:749-918 (Sp = 1, const_sp = 0):
+// role r transports U with the cell flux F; the face combines p = F + U and
+// m = F - U of the cells around it.  The fluid fluxes are flowinit's
+// (14_flowinit.f95:258-360): stage E, B, D, S and the time-n v, p and
+// hW2 = enthpy W^2, EB = |E|^2 + |B|^2 (each summed x, y, z on its own).
+// R_BT1 / R_ET2 carry the reference's sign-flipped cells -E_t2 + B_t1 and
+// -B_t1 + E_t2 (EzlaxBy, BylaxEz in x; ExlaxBz, BzlaxEx in y).
+template <int D, typename T>
+__device__ __forceinline__ void lax_pair(int r, const Side<T>& s, T hW2, T EB, T& F, T& U) {
+  using X = Dir<D>;
+  switch (r) {
+    case R_PSI: F = X::En(s); U = s.psi; break;
+    case R_PHI: F = X::Bn(s); U = s.phi; break;
+    case R_BN: F = s.phi; U = X::Bn(s); break;
+    case R_BT1: F = -X::Et2(s); U = X::Bt1(s); break;
+    case R_BT2: F = X::Et1(s); U = X::Bt2(s); break;
+    case R_EN: F = s.psi; U = X::En(s); break;
+    case R_ET1: F = X::Bt2(s); U = X::Et1(s); break;
+    case R_ET2: F = -X::Bt1(s); U = X::Et2(s); break;
+    case R_Q: F = s.J; U = s.q; break;
+    case R_D: F = s.D * X::vn(s); U = s.D; break;
+    case R_TAU: F = (X::Bt2(s) * X::Et1(s) - X::Bt1(s) * X::Et2(s)) + hW2 * X::vn(s); U = s.tau; break;
+    case R_SN:
+      F = -pw2(X::En(s)) - pw2(X::Bn(s)) + hW2 * pw2(X::vn(s)) + T(0.5) * EB + s.p;
+      U = X::Sn(s);
+      break;
+    case R_ST1: F = -X::En(s) * X::Et1(s) - X::Bn(s) * X::Bt1(s) + hW2 * X::vn(s) * X::vt1(s); U = X::St1(s); break;
+    default:   // R_ST2; FSyx multiplies vx before vy
+      if constexpr (D == 0) F = -X::En(s) * X::Et2(s) - X::Bn(s) * X::Bt2(s) + hW2 * X::vn(s) * X::vt2(s);
+      else                  F = -X::En(s) * X::Et2(s) - X::Bn(s) * X::Bt2(s) + hW2 * X::vt2(s) * X::vn(s);
+      U = X::St2(s);
+      break;
+  }
+}
+// enthpy W^2 and |E|^2 + |B|^2 of a cell, with startconvar's W and enthalpy
+// (06_conserved_var.f95:86-133)
+template <typename T>
+__device__ __forceinline__ void lax_cell_scalars(const Side<T>& s, T gamma, T& hW2, T& EB) {
+  const T W = lorentz(s);
+  const T eps = s.p / ((gamma - T(1.0)) * s.rho);
+  const T h = s.rho * (T(1.0) + eps) + s.p;
+  hW2 = h * pw2(W);
+  EB = (pw2(s.Ex) + pw2(s.Ey) + pw2(s.Ez)) + (pw2(s.Bx) + pw2(s.By) + pw2(s.Bz));
+}
+
 // get_hllc_vel, funciones.f95:188-259: Newton on a v^2 - b v + c = 0 in
 // [-1,1].  The Fortran's first f evaluation reads the local v before it is
 // assigned (line 229); this evaluates it at the seed oldv, like the oracle.

@@ -1,5 +1,5 @@
 // cueva_stage.cuh -- the two stage kernels of the CUEVA hot path (templates),
-// shared by the per-solver translation units cueva_stage_{hll,hllc,hlle}.cu
+// shared by the per-solver translation units cueva_stage_{lax,mcl,hll,hllc,hlle}.cu
 // and by the pointwise kernels of cueva_kernels.cu.
 //
 // One RK stage = two launches:
@@ -255,6 +255,44 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
 
   uint32_t stt = 0;
   Side<T> L, Rs;
+  if constexpr (SOLVER == 1) {
+    // Lax-Friedrichs with MC slopes, 15_lax_flow.f95:920-1457: for stencil
+    // cells 0..3 (the face lies between 1 and 2)
+    //   L = p1 + FAC mcl(p2 - p1, p1 - p0),  R = m2 - FAC mcl(p3 - p2, p2 - p1),
+    // both with the slopes of p, and the face flux 0.5 (L + R), negated for
+    // the sign-flipped roles R_BT1 and R_ET2
+    static_assert(RM == 3, "the Lax fluxes use the MC slopes");
+    const T gamma = T(gamma_d);
+    auto cell = [&](int q) {
+      Side<T> s;
+      s.vx = nrm(0, q); s.vy = nrm(1, q); s.vz = nrm(2, q); s.p = nrm(3, q); s.rho = nrm(4, q);
+      s.psi = nrm(5 + Q_PSI, q); s.phi = nrm(5 + Q_PHI, q);
+      s.Ex = nrm(5 + Q_EX, q); s.Ey = nrm(5 + Q_EY, q); s.Ez = nrm(5 + Q_EZ, q);
+      s.Bx = nrm(5 + Q_BX, q); s.By = nrm(5 + Q_BY, q); s.Bz = nrm(5 + Q_BZ, q);
+      s.q = nrm(5 + Q_Q, q); s.D = nrm(5 + Q_D, q); s.tau = nrm(5 + Q_TAU, q);
+      s.Sx = nrm(5 + Q_SX, q); s.Sy = nrm(5 + Q_SY, q); s.Sz = nrm(5 + Q_SZ, q);
+      s.J = nrm(19, q);
+      return s;
+    };
+    T hW2[NS], EB[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) lax_cell_scalars(cell(q), gamma, hW2[q], EB[q]);
+#pragma unroll
+    for (int r = 0; r < NROLE; ++r) {
+      T p[NS], m2 = T(0);
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        T f, u;
+        lax_pair<D>(r, cell(q), hW2[q], EB[q], f, u);
+        p[q] = f + u;
+        if (q == 2) m2 = f - u;
+      }
+      const T Lf = p[1] + T(0.5) * mc_slope(p[2] - p[1], p[1] - p[0]);
+      const T Rf = m2 - T(0.5) * mc_slope(p[3] - p[2], p[2] - p[1]);
+      F[r] = (r == R_BT1 || r == R_ET2) ? -(T(0.5) * (Lf + Rf)) : T(0.5) * (Lf + Rf);
+    }
+    return stt;
+  }
   if constexpr (SOLVER == 2) {
     // HLL with the second-order MC reconstruction, 16_hll_flow_mcl.f95:565-1396
     // (x and y faces of a point are the same formulas in the direction roles)
@@ -713,7 +751,7 @@ template <int SV>
 cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                                 const StageArgs& sa, cudaEvent_t* ev) {
   if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
-  if constexpr (SV == 2) {   // the MCL routine has its own reconstruction; rec_mp does not apply
+  if constexpr (SV == 1 || SV == 2) {   // the Lax and MCL routines use MC slopes; rec_mp does not apply
     launch_rm_sv<3, SV>(prec, sh, st, d, n, sa, ev);
   } else {
     switch (rec_mp) {
@@ -728,7 +766,7 @@ cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cuda
 
 template <int SV>
 cudaError_t prepare_stage_solver(int rec_mp, int prec) {
-  if constexpr (SV == 2) {
+  if constexpr (SV == 1 || SV == 2) {
     return prepare_rm_sv<3, SV>(prec);
   } else {
     switch (rec_mp) {

@@ -585,9 +585,10 @@ struct Oracle {
     kappa_phi = 1.0 / pw2(cp_phi);
     gamma = p.gamma; sigma = p.sigma;
     // value the module variable eps1 holds when con2prim runs (set last by the flux routine)
-    // (the MCL routine of flux_solver 2 never sets it: the zero-initialised
-    // module variable; only the superluminal seed clamp reads it)
-    eps1_c2p = (p.flux_solver == 7) ? (double)1.0e-6f : (p.flux_solver == 2 ? 0.0 : 1.0e-6);
+    // (the Lax routine of flux_solver 1 and the MCL routine of flux_solver 2
+    // never set it: the zero-initialised module variable; only the
+    // superluminal seed clamp reads it)
+    eps1_c2p = (p.flux_solver == 7) ? (double)1.0e-6f : (p.flux_solver <= 2 ? 0.0 : 1.0e-6);
     make_tableau(p.order, T);
     lmax = T.s;
     const char* names[] = {
@@ -854,7 +855,99 @@ struct Oracle {
     }
   }
 
+  // ------------- Lax-Friedrichs flux with MC slopes (flux_solver 1), 15_lax_flow.f95:733-1457
+  // Every cell (ghosts included) carries the pair p = F + Sp U, m = F - Sp U
+  // of each flux F and the conserved variable U it transports, with Sp = 1
+  // (const_sp = 0, parameters.f95:274).  Face i+1/2 of a line:
+  //   L = p(i)   + FAC mcl(p(i+1) - p(i),   p(i)   - p(i-1))
+  //   R = m(i+1) - FAC mcl(p(i+2) - p(i+1), p(i+1) - p(i))      (slopes of p on both sides)
+  //   F(i+1/2) = 0.5 (L + R), negated for EzlaxBy, ExlaxBz, BzlaxEx, BylaxEz,
+  // whose cell flux is written with the opposite sign (-Ez + By, ...).
+  // F of the fluid comes from flowinit (14_flowinit.f95:258-360): stage
+  // E, B, D, S with the time-n v, W, enthpy and p, computed on the interior
+  // and copied to the ghosts by boundary_flux_conserved; the current F is
+  // the stage J of flowinit.
+  void lax_flow() {
+    double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *W = a("W"), *h = a("enthpy"), *p = a("p");
+    double *Ex = a("Exint"), *Ey = a("Eyint"), *Ez = a("Ezint"), *Bx = a("Bxint"), *By = a("Byint"),
+           *Bz = a("Bzint"), *DD = a("DDint");
+    enum { FDX, FDY, FTX, FTY, FSXX, FSXY, FSXZ, FSYX, FSYY, FSYZ, NCF };
+    std::vector<std::vector<double>> cf(NCF, std::vector<double>(ng, 0.0));
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j <= jmax; ++j)
+      for (int i = 0; i <= imax; ++i) {
+        const size_t k = id(i, j);
+        const double E2 = pw2(Ex[k]) + pw2(Ey[k]) + pw2(Ez[k]);
+        const double B2 = pw2(Bx[k]) + pw2(By[k]) + pw2(Bz[k]);
+        const double hW2 = h[k] * pw2(W[k]);
+        cf[FDX][k] = DD[k] * Vx[k];
+        cf[FDY][k] = DD[k] * Vy[k];
+        cf[FTX][k] = (Bz[k] * Ey[k] - By[k] * Ez[k]) + hW2 * Vx[k];
+        cf[FTY][k] = (Bx[k] * Ez[k] - Bz[k] * Ex[k]) + hW2 * Vy[k];
+        cf[FSXX][k] = -pw2(Ex[k]) - pw2(Bx[k]) + hW2 * pw2(Vx[k]) + 0.5 * (E2 + B2) + p[k];
+        cf[FSXY][k] = -Ex[k] * Ey[k] - Bx[k] * By[k] + hW2 * Vx[k] * Vy[k];
+        cf[FSXZ][k] = -Ex[k] * Ez[k] - Bx[k] * Bz[k] + hW2 * Vx[k] * Vz[k];
+        cf[FSYX][k] = -Ex[k] * Ey[k] - Bx[k] * By[k] + hW2 * Vx[k] * Vy[k];
+        cf[FSYY][k] = -pw2(Ey[k]) - pw2(By[k]) + hW2 * pw2(Vy[k]) + 0.5 * (E2 + B2) + p[k];
+        cf[FSYZ][k] = -Ey[k] * Ez[k] - By[k] * Bz[k] + hW2 * Vy[k] * Vz[k];
+      }
+    for (auto& f : cf) fill_ghosts(f.data());
+    struct Pairing { const double* F; bool negF; const double* U; bool ydir; bool negface; };
+    const double *psi = a("psiint"), *phi = a("phiint"), *q = a("qint"), *tau = a("tauint");
+    const double *Sx = a("Sxint"), *Sy = a("Syint"), *Sz = a("Szint");
+    const Pairing pr[28] = {
+        {Ex, false, psi, false, false},              // Exlaxpsi
+        {Ey, false, psi, true, false},               // Eylaxpsi
+        {Bx, false, phi, false, false},              // Bxlaxphi
+        {By, false, phi, true, false},               // Bylaxphi
+        {phi, false, Bx, false, false},              // philaxBx
+        {Ez, false, Bx, true, false},                // EzlaxBx
+        {Ez, true, By, false, true},                 // EzlaxBy
+        {phi, false, By, true, false},               // philaxBy
+        {Ey, false, Bz, false, false},               // EylaxBz
+        {Ex, true, Bz, true, true},                  // ExlaxBz
+        {psi, false, Ex, false, false},              // psilaxEx
+        {Bz, true, Ex, true, true},                  // BzlaxEx
+        {Bz, false, Ey, false, false},               // BzlaxEy
+        {psi, false, Ey, true, false},               // psilaxEy
+        {By, true, Ez, false, true},                 // BylaxEz
+        {Bx, false, Ez, true, false},                // BxlaxEz
+        {a("Jxint"), false, q, false, false},        // Jxlax
+        {a("Jyint"), false, q, true, false},         // Jylax
+        {cf[FDX].data(), false, DD, false, false},   // FDxlax
+        {cf[FDY].data(), false, DD, true, false},    // FDylax
+        {cf[FTX].data(), false, tau, false, false},  // Ftauxlax
+        {cf[FTY].data(), false, tau, true, false},   // Ftauylax
+        {cf[FSXX].data(), false, Sx, false, false},  // FSxxlax
+        {cf[FSXY].data(), false, Sy, false, false},  // FSxylax
+        {cf[FSXZ].data(), false, Sz, false, false},  // FSxzlax
+        {cf[FSYX].data(), false, Sx, true, false},   // FSyxlax
+        {cf[FSYY].data(), false, Sy, true, false},   // FSyylax
+        {cf[FSYZ].data(), false, Sz, true, false}};  // FSyzlax
+    const char* on[] = {"Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "EzlaxBx", "EzlaxBy",
+                        "philaxBy", "EylaxBz", "ExlaxBz", "psilaxEx", "BzlaxEx", "BzlaxEy", "psilaxEy",
+                        "BylaxEz", "BxlaxEz", "Jxlax", "Jylax", "FDxlax", "FDylax", "Ftauxlax", "Ftauylax",
+                        "FSxxlax", "FSxylax", "FSxzlax", "FSyxlax", "FSyylax", "FSyzlax"};
+    const double Sp = 1.0;
+    for (int c = 0; c < 28; ++c) {
+      const Pairing& P2 = pr[c];
+      double* o = a(on[c]);
+      auto pv = [&](size_t k) { return (P2.negF ? -P2.F[k] : P2.F[k]) + Sp * P2.U[k]; };
+      auto mv = [&](size_t k) { return (P2.negF ? -P2.F[k] : P2.F[k]) - Sp * P2.U[k]; };
+#pragma omp parallel for schedule(static)
+      for (int j = -1; j <= jmax; ++j)
+        for (int i = -1; i <= imax; ++i) {
+          auto at = [&](int s) { return P2.ydir ? id(i, j + s) : id(i + s, j); };
+          const double pm1 = pv(at(-1)), p0 = pv(at(0)), p1 = pv(at(1)), p2 = pv(at(2));
+          const double L = p0 + 0.5 * limiter_mc(p1 - p0, p0 - pm1);
+          const double R = mv(at(1)) - 0.5 * limiter_mc(p2 - p1, p1 - p0);
+          o[id(i, j)] = P2.negface ? -(0.5 * (L + R)) : 0.5 * (L + R);
+        }
+    }
+  }
+
   void reconstruct() {
+    if (P.flux_solver == 1) return;   // lax_flow works on the cell pairs directly
     if (P.flux_solver == 2) { reconstruct_mcl(); return; }
     const int rec = P.rec_mp;
     XL.assign(X_N, std::vector<double>(ng, 0.0)); XR.assign(X_N, std::vector<double>(ng, 0.0));
@@ -1009,6 +1102,7 @@ struct Oracle {
   // ------------------------------------------- Riemann loop (2D, i=-1..imax, j=-1..jmax)
   void riemann() {
     const int solver = P.flux_solver;
+    if (solver == 1) { lax_flow(); return; }
     double *Vx = a("Vx"), *Vy = a("Vy"), *Vz = a("Vz"), *rho = a("rho");
     double* o[28];
     const char* on[] = {"Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "EzlaxBx", "EzlaxBy",
@@ -1844,7 +1938,7 @@ extern "C" {
 
 void* oracle_create(const oracle_params* p) {
   if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
-  if (p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
+  if (p->flux_solver != 1 && p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
   if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
   if (p->primitive_rec < 0 || p->primitive_rec > 1) return nullptr;
   Tableau T;

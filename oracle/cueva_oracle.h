@@ -29,8 +29,8 @@ extern "C" {
 typedef struct oracle_params {
   int32_t imax, jmax;      /* grid points 0..imax x 0..jmax (parameters.f95:110-111) */
   int32_t order;           /* IMEX tableau: 1,2,3,4,5,6,8 (imex_scheme.f95) */
-  int32_t flux_solver;     /* 2 HLL+MC (16_hll_flow_mcl.f95), 5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX
-                              (main_cueva_code.f95:263-273) */
+  int32_t flux_solver;     /* 1 Lax-Friedrichs+MC (15_lax_flow.f95), 2 HLL+MC (16_hll_flow_mcl.f95),
+                              5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX (main_cueva_code.f95:247-273) */
   int32_t rec_mp;          /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
   int32_t c2p;             /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37) */
   int32_t bc_x, bc_y;      /* 0 copy, 1 periodic (04_boundary.f95 BOUND 1/2/6) */

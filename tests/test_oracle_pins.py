@@ -135,7 +135,7 @@ def test_tableaux_consistent(oracle_mod):
 
 
 @pytest.mark.parametrize("solver,order,rec", [(5, 2, 0), (7, 4, 0), (7, 2, 1), (5, 3, 2), (6, 2, 0), (6, 4, 2), (2, 2, 0),
-                                              (2, 4, 0)])
+                                              (2, 4, 0), (1, 2, 0), (1, 4, 0)])
 def test_uniform_state_stays_uniform(oracle_mod, solver, order, rec):
     imax, jmax = 20, 12
     o = oracle_mod.Oracle(imax, jmax, order=order, flux_solver=solver, rec_mp=rec, bc_x=0, bc_y=1, sigma=1e3)
@@ -313,3 +313,24 @@ def test_mcl_reconstruction_second_order(oracle_mod):
     # -(D_R - D_L)/2 with the exact face values, i.e. 0 for continuous linear data
     fd = o.named("FDxlax", 1)
     assert np.allclose(fd[2:-2, 2:-3], 0.0, atol=1e-14)
+
+
+def test_lax_right_state_takes_the_slopes_of_p(oracle_mod):
+    """flux_solver 1 (15_lax_flow.f95:920-1457): each cell carries
+    p = F + U and m = F - U, and the right state of a face is
+    m(i+1) - FAC mcl(p(i+2) - p(i+1), p(i+1) - p(i)) -- the slopes of p,
+    not of m.  With v = 0 the D flux F = D vx vanishes, so on data linear in
+    the cell index (step a) the face flux is 0.5 (D + a/2 - D - 3a/2) = -a/2,
+    where slopes of m would give 0."""
+    imax, jmax = 24, 12
+    pr = oracle_mod.kh_init(imax, jmax, v0=0.0, a=0.05, amp=0.0)
+    ramp = np.add.outer(0.01 * np.arange(jmax + 1), 0.02 * np.arange(imax + 1)) + 1.0
+    pr = {n: (ramp.copy() if n in ("rho", "p") else np.zeros_like(ramp)) for n in pr}
+    o = oracle_mod.Oracle(imax, jmax, order=1, flux_solver=1, bc_x=0, bc_y=0, sigma=1.0)
+    o.set_prims(pr)
+    assert o.run_stages(1) == 0
+    fdx, fdy = o.named("FDxlax", 1), o.named("FDylax", 1)
+    assert np.allclose(fdx[:, 1:-2], -0.01, rtol=0, atol=1e-14)
+    assert np.allclose(fdy[1:-2, :], -0.005, rtol=0, atol=1e-14)
+    # the charge flux pairs J with q: both vanish here
+    assert np.all(o.named("Jxlax", 1) == 0.0)
