@@ -49,9 +49,10 @@ typedef struct cueva_ctx cueva_ctx;
 typedef struct cueva_params {
   int32_t imax, jmax;   /* grid points 0..imax x 0..jmax (parameters.f95:110-111), both >= 6 */
   int32_t order;        /* IMEX tableau (parameters.f95:10): 1, 2 SSP2(2,2,2), 3 SSP2(3,3,2), 4 SSP3(4,3,3), 5, 6, 8 */
-  int32_t flux_solver;  /* 1 Lax-Friedrichs with MC slopes (15_lax_flow.f95), 2 HLL with the second-order
-                           MC reconstruction (16_hll_flow_mcl.f95) -- rec_mp does not apply to 1 and 2 --,
-                           5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX (main_cueva_code.f95:247-273) */
+  int32_t flux_solver;  /* 1 Lax-Friedrichs with MC slopes (15_lax_flow.f95); 2 HLL, 3 HLLE, 4 HLLC with
+                           the second-order MC reconstruction (16_hll/hlle/hllc_flow_mcl.f95) -- rec_mp
+                           does not apply to 1-4 --; 5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX
+                           (main_cueva_code.f95:247-273) */
   int32_t rec_mp;       /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
   int32_t c2p;          /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37), 2 learned seed + Newton */
   int32_t bc_x, bc_y;   /* per-axis ghost rule: 0 copy, 1 periodic (BOUND 1 / 2 / 6 of 04_boundary.f95) */

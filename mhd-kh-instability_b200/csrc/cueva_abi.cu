@@ -125,10 +125,9 @@ namespace {
 
 int32_t validate_params(const cueva_params* p) {
   if (p->imax < 6 || p->jmax < 6) return fail(CUEVA_ERR_ARG, "imax and jmax must be >= 6 (6 ghost cells)");
-  if (p->flux_solver != 1 && p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 &&
-      p->flux_solver != 7)
-    return fail(CUEVA_ERR_ARG,
-                "flux_solver must be 1 (Lax+MC), 2 (HLL+MC), 5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
+  if (p->flux_solver < 1 || p->flux_solver > 7)
+    return fail(CUEVA_ERR_ARG, "flux_solver must be 1 (Lax+MC), 2 (HLL+MC), 3 (HLLE+MC), 4 (HLLC+MC), "
+                               "5 (HLL+MPX), 6 (HLLE+MPX) or 7 (HLLC+MPX)");
   if (p->rec_mp < 0 || p->rec_mp > 2) return fail(CUEVA_ERR_ARG, "rec_mp must be 0, 1 or 2");
   if (p->c2p < 0 || p->c2p > 2) return fail(CUEVA_ERR_ARG, "c2p must be 0, 1 or 2");
   if ((p->bc_x != 0 && p->bc_x != 1) || (p->bc_y != 0 && p->bc_y != 1))

@@ -138,6 +138,8 @@ cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
   switch (solver) {
     case 1: return prepare_stage_lax(rec_mp, prec);
     case 2: return prepare_stage_mcl(rec_mp, prec);
+    case 3: return prepare_stage_hllemc(rec_mp, prec);
+    case 4: return prepare_stage_hllcmc(rec_mp, prec);
     case 5: return prepare_stage_hll(rec_mp, prec);
     case 6: return prepare_stage_hlle(rec_mp, prec);
     case 7: return prepare_stage_hllc(rec_mp, prec);
@@ -150,6 +152,8 @@ cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh,
   switch (solver) {
     case 1: return launch_stage_lax(rec_mp, prec, sh, st, d, n, sa, ev);
     case 2: return launch_stage_mcl(rec_mp, prec, sh, st, d, n, sa, ev);
+    case 3: return launch_stage_hllemc(rec_mp, prec, sh, st, d, n, sa, ev);
+    case 4: return launch_stage_hllcmc(rec_mp, prec, sh, st, d, n, sa, ev);
     case 5: return launch_stage_hll(rec_mp, prec, sh, st, d, n, sa, ev);
     case 6: return launch_stage_hlle(rec_mp, prec, sh, st, d, n, sa, ev);
     case 7: return launch_stage_hllc(rec_mp, prec, sh, st, d, n, sa, ev);

@@ -22,6 +22,8 @@ cudaError_t prepare_stage(int rec_mp, int solver, int prec);
 cudaError_t prepare_stage_lax(int rec_mp, int prec);
 cudaError_t prepare_stage_hll(int rec_mp, int prec);
 cudaError_t prepare_stage_mcl(int rec_mp, int prec);
+cudaError_t prepare_stage_hllemc(int rec_mp, int prec);
+cudaError_t prepare_stage_hllcmc(int rec_mp, int prec);
 cudaError_t prepare_stage_hllc(int rec_mp, int prec);
 cudaError_t prepare_stage_hlle(int rec_mp, int prec);
 cudaError_t launch_stage_lax(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
@@ -30,6 +32,10 @@ cudaError_t launch_stage_hll(int rec_mp, int prec, const StageShape& sh, cudaStr
                              const StageArgs& sa, cudaEvent_t* ev);
 cudaError_t launch_stage_mcl(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                              const StageArgs& sa, cudaEvent_t* ev);
+cudaError_t launch_stage_hllemc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
+                                int n, const StageArgs& sa, cudaEvent_t* ev);
+cudaError_t launch_stage_hllcmc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
+                                int n, const StageArgs& sa, cudaEvent_t* ev);
 cudaError_t launch_stage_hllc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                               const StageArgs& sa, cudaEvent_t* ev);
 cudaError_t launch_stage_hlle(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,

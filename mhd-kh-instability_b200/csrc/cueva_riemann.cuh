@@ -449,4 +449,213 @@ __device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, 
   }
 }
 
+// HLLC of the MC family, 16_hllc_flow_mcl.f95 (2D :1751-4056): the HLLC of
+// hllc_fluxes (same HLL states, star states and flux choice, s = -1, +1) on
+// the MC sides -- the "_m" values of E_t2 and B_t1 in the HLL states and
+// fluxes, the current of each side, W = 1 / sqrt(1 - vx^2 - vy^2 - vz^2) --
+// with |v*| <= 1e-6 taken as 0 (:2580-2600; the MPX routine uses 1e-9).
+template <int D, typename T>
+__device__ __forceinline__ void hllcmc_fluxes(const Side<T>& L, const Side<T>& R, const T (&m_et2)[2],
+                                              const T (&m_bt1)[2], T gamma, T sigma, T* A, uint32_t& st) {
+  using X = Dir<D>;
+  mcl_fluxes<D>(L, R, m_et2, m_bt1, gamma, sigma, A);   // fixed-speed HLL fluxes of every role
+  const Phys<T> fl = physical<D>(L, gamma, lorentz_hlle(L)), fr = physical<D>(R, gamma, lorentz_hlle(R));
+  const T h = T(0.5);
+  const T psi_hll = h * (((R.psi + L.psi) + X::En(L)) - X::En(R));
+  const T phi_hll = h * (((R.phi + L.phi) + X::Bn(L)) - X::Bn(R));
+  const T En_hll = h * (((X::En(R) + X::En(L)) + L.psi) - R.psi);
+  const T Et1_hll = h * (((X::Et1(R) + X::Et1(L)) + X::Bt2(L)) - X::Bt2(R));
+  const T Et2_hll = h * (((X::Et2(R) + X::Et2(L)) + m_bt1[0]) - m_bt1[1]);
+  const T Bn_hll = h * (((X::Bn(R) + X::Bn(L)) + L.phi) - R.phi);
+  const T Bt1_hll = h * (((X::Bt1(R) + X::Bt1(L)) + m_et2[0]) - m_et2[1]);
+  const T Bt2_hll = h * (((X::Bt2(R) + X::Bt2(L)) + X::Et1(L)) - X::Et1(R));
+  const T D_hll = h * (((R.D + L.D) + fl.FD) - fr.FD);
+  const T tau_hll = h * (((R.tau + L.tau) + fl.Ftau) - fr.Ftau);
+  const T Sn_hll = h * (((X::Sn(R) + X::Sn(L)) + fl.FSn) - fr.FSn);
+  const T St1_hll = h * (((X::St1(R) + X::St1(L)) + fl.FSt1) - fr.FSt1);
+  const T St2_hll = h * (((X::St2(R) + X::St2(L)) + fl.FSt2) - fr.FSt2);
+  const T psi_f = A[R_PSI], phi_f = A[R_PHI], En_f = A[R_EN], Bn_f = A[R_BN];
+  const T D_f = A[R_D], tau_f = A[R_TAU], Sn_f = A[R_SN], St1_f = A[R_ST1], St2_f = A[R_ST2];
+  const T ErotB_n = Bt2_hll * Et1_hll - Bt1_hll * Et2_hll;
+  const T ErotB_t1 = Bn_hll * Et2_hll - Bt2_hll * En_hll;
+  const T ErotB_t2 = Bt1_hll * En_hll - Bn_hll * Et1_hll;
+  const T E2_perp = pw2(Et1_hll) + pw2(Et2_hll);
+  const T B2_perp = pw2(Bt1_hll) + pw2(Bt2_hll);
+  T Exs, Eys, Ezs, Bxs, Bys, Bzs;
+  if constexpr (D == 0) { Exs = En_hll; Eys = Et1_hll; Ezs = Et2_hll; Bxs = Bn_hll; Bys = Bt1_hll; Bzs = Bt2_hll; }
+  else                  { Eys = En_hll; Ezs = Et1_hll; Exs = Et2_hll; Bys = Bn_hll; Bzs = Bt1_hll; Bxs = Bt2_hll; }
+  const T E2B2_str = T(0.5) * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+  const T a_hll = tau_f - ErotB_n;
+  const T b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
+  const T c_hll = Sn_hll - ErotB_n;
+  const T det_hll = pw2(b_hll) - T(4.0) * a_hll * c_hll;
+  const T q_root1 = -T(0.5) * (b_hll + fsgn1(b_hll) * fabs(sqrt(det_hll)));
+  T rt2 = c_hll / q_root1;
+  if (det_hll < T(0.0)) rt2 = c_hll / b_hll;
+  T V = hllc_vel(a_hll, -b_hll, c_hll, rt2, st);
+  if (fabs(V) <= T(1.0e-6)) V = T(0.0);
+  const T pstr = Sn_f + (pw2(En_hll) + pw2(Bn_hll)) - (tau_f - ErotB_n) * V;
+  const T omV = T(1.0) - V, opV = V + T(1.0);
+  const T psiR = (psi_hll - V * En_f) / omV, psiL = (psi_hll + V * En_f) / opV;
+  const T phiR = (phi_hll - V * Bn_f) / omV, phiL = (phi_hll + V * Bn_f) / opV;
+  const T SnR = (Sn_hll - tau_f * V) / omV, SnL = (Sn_hll + tau_f * V) / opV;
+  const T St1R = (St1_hll - St1_f - ErotB_t1 * V - En_hll * Et1_hll - Bn_hll * Bt1_hll) / omV;
+  const T St1L = (St1_hll + St1_f + ErotB_t1 * V + En_hll * Et1_hll + Bn_hll * Bt1_hll) / opV;
+  const T St2R = (St2_hll - St2_f - ErotB_t2 * V - En_hll * Et2_hll - Bn_hll * Bt2_hll) / omV;
+  const T St2L = (St2_hll + St2_f + ErotB_t2 * V + En_hll * Et2_hll + Bn_hll * Bt2_hll) / opV;
+  const T tauR = (SnR - ErotB_n) / V - pstr + E2B2_str;
+  const T tauL = (SnL - ErotB_n) / V - pstr + E2B2_str;
+  const T DR = (D_hll - D_f) / omV, DL = (D_hll + D_f) / opV;
+  // flux choice (:3530-3620): v* > 0 left star flux, v* < 0 right star flux,
+  // v* == 0 the HLL fluxes; E, B and q keep the HLL fluxes throughout
+  if (V > T(0.0)) {
+    A[R_PSI] = psi_f + (omV * (psiR - psiL)) * h;
+    A[R_PHI] = phi_f + (omV * (phiR - phiL)) * h;
+    A[R_D] = D_f + omV * (DR - DL) * h;
+    A[R_TAU] = tau_f + omV * (tauR - tauL) * h;
+    A[R_SN] = Sn_f + omV * (SnR - SnL) * h;
+    A[R_ST1] = St1_f + omV * (St1R - St1L) * h;
+    A[R_ST2] = St2_f + omV * (St2R - St2L) * h;
+  } else if (V < T(0.0)) {
+    A[R_PSI] = psi_f + (opV * (psiR - psiL)) * h;
+    A[R_PHI] = phi_f + (opV * (phiR - phiL)) * h;
+    A[R_D] = D_f + opV * (DR - DL) * h;
+    A[R_TAU] = tau_f + opV * (tauR - tauL) * h;
+    A[R_SN] = Sn_f + opV * (SnR - SnL) * h;
+    A[R_ST1] = St1_f + opV * (St1R - St1L) * h;
+    A[R_ST2] = St2_f + opV * (St2R - St2L) * h;
+  } else if (!(V == T(0.0))) {
+    st |= ST_HLLC_VSTAR;
+#pragma unroll
+    for (int c = 0; c < NROLE; ++c) A[c] = T(NAN);
+  }
+}
+
+// HLLE of the MC family, 16_hlle_flow_mcl.f95 (2D :1638-4345), on the MC
+// reconstruction with the "_m" values of E_t2 and B_t1 and the current
+// of each side (as mcl_fluxes).  Bounds and the v* quadratic are the
+// MPX HLLE's; the star states and fluxes differ (:2911-3150):
+//   S_n*  = (s S_n,hll - F(S_n)_hll +- (p* - B_n*^2 - E_n*^2 - (E*xB*)_n v*)) / (s - v*)
+//   tau*  = (s tau_hll - F(tau)_hll +- ((p* - |E*|^2/2 - |B*|^2/2) v* + (E*xB*)_n)) / (s - v*)
+//   F*    = F(side) + s (U* - U(side)),   s = s1 (left) or s2 (right);
+// the EM fluxes for v* != 0 are those of the star state (psi: E_n*,
+// E_n: psi*, E_t1: B_t2*, E_t2: -B_t1*, B_n: phi*, B_t1: -E_t2*,
+// B_t2: E_t1*), for v* == 0 the fixed-speed HLL ones; the current flux is
+// the HLLE one in both star regions.  Flux choice (:3236-4343): s1 > 0
+// left physical flux, s1 <= 0 <= v* left star, v* < 0 <= s2 right star,
+// s2 < 0 right physical flux.  A NaN v* leaves the reference's EM arrays
+// unset (and its fluid choice stops the run); both are reported as
+// ST_HLLC_VSTAR with NaN fluxes here.
+template <int D, typename T>
+__device__ __forceinline__ void hllemc_fluxes(const Side<T>& L, const Side<T>& R, const T (&m_et2)[2],
+                                              const T (&m_bt1)[2], T gamma, T sigma, T* A, uint32_t& st) {
+  using X = Dir<D>;
+  const T h = T(0.5);
+  // fixed-speed HLL states (the star E, B, psi, phi)
+  const T psi_hll = h * (((R.psi + L.psi) + X::En(L)) - X::En(R));
+  const T phi_hll = h * (((R.phi + L.phi) + X::Bn(L)) - X::Bn(R));
+  const T En_hll = h * (((X::En(R) + X::En(L)) + L.psi) - R.psi);
+  const T Et1_hll = h * (((X::Et1(R) + X::Et1(L)) + X::Bt2(L)) - X::Bt2(R));
+  const T Et2_hll = h * (((X::Et2(R) + X::Et2(L)) + m_bt1[0]) - m_bt1[1]);
+  const T Bn_hll = h * (((X::Bn(R) + X::Bn(L)) + L.phi) - R.phi);
+  const T Bt1_hll = h * (((X::Bt1(R) + X::Bt1(L)) + m_et2[0]) - m_et2[1]);
+  const T Bt2_hll = h * (((X::Bt2(R) + X::Bt2(L)) + X::Et1(L)) - X::Et1(R));
+  const T WL = lorentz_hlle(L), WR = lorentz_hlle(R);
+  const Phys<T> fl = physical<D>(L, gamma, WL), fr = physical<D>(R, gamma, WR);
+  auto jn = [&](const Side<T>& s, T W) {
+    const T vrotB = X::Bt2(s) * X::vt1(s) - X::Bt1(s) * X::vt2(s);
+    const T Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+    return sigma * W * (X::En(s) + vrotB - Edotv * X::vn(s)) + s.q * X::vn(s);
+  };
+  const T JL = jn(L, WL), JR = jn(R, WR);
+  T lmL, lpL, lmR, lpR;
+  hlle_bounds<D>(R, fr.h, gamma, lmR, lpR);
+  hlle_bounds<D>(L, fl.h, gamma, lmL, lpL);
+  T s1 = fmin2(lmL, lmR), s2 = fmax2(lpL, lpR);
+  if (isnan(s1) || isnan(s2)) st |= ST_HLLE_SPEED;
+  const T eps2 = T(1.0e-9);
+  if (fabs(s1) > T(1.0)) s1 = fmax2(T(-1.0) + eps2, fmin2(T(1.0) - eps2, s1));
+  if (fabs(s2) > T(1.0)) s2 = fmax2(T(-1.0) + eps2, fmin2(T(1.0) - eps2, s2));
+  const T D_hll = (s2 * R.D - s1 * L.D + fl.FD - fr.FD) / (s2 - s1);
+  const T tau_hll = (s2 * R.tau - s1 * L.tau + fl.Ftau - fr.Ftau) / (s2 - s1);
+  const T Sn_hll = (s2 * X::Sn(R) - s1 * X::Sn(L) + fl.FSn - fr.FSn) / (s2 - s1);
+  const T St1_hll = (s2 * X::St1(R) - s1 * X::St1(L) + fl.FSt1 - fr.FSt1) / (s2 - s1);
+  const T St2_hll = (s2 * X::St2(R) - s1 * X::St2(L) + fl.FSt2 - fr.FSt2) / (s2 - s1);
+  auto hlle = [&](T FL, T FR, T UL, T UR) { return (s2 * FL - s1 * FR + s1 * s2 * (UR - UL)) / (s2 - s1); };
+  const T q_f = hlle(JL, JR, L.q, R.q);
+  const T D_f = hlle(fl.FD, fr.FD, L.D, R.D);
+  const T tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+  const T Sn_f = hlle(fl.FSn, fr.FSn, X::Sn(L), X::Sn(R));
+  const T St1_f = hlle(fl.FSt1, fr.FSt1, X::St1(L), X::St1(R));
+  const T St2_f = hlle(fl.FSt2, fr.FSt2, X::St2(L), X::St2(R));
+  const T ErotB_n = Bt2_hll * Et1_hll - Bt1_hll * Et2_hll;
+  const T ErotB_t1 = Bn_hll * Et2_hll - Bt2_hll * En_hll;
+  const T ErotB_t2 = Bt1_hll * En_hll - Bn_hll * Et1_hll;
+  const T E2_perp = pw2(Et1_hll) + pw2(Et2_hll);
+  const T B2_perp = pw2(Bt1_hll) + pw2(Bt2_hll);
+  T Exs, Eys, Ezs, Bxs, Bys, Bzs;
+  if constexpr (D == 0) { Exs = En_hll; Eys = Et1_hll; Ezs = Et2_hll; Bxs = Bn_hll; Bys = Bt1_hll; Bzs = Bt2_hll; }
+  else                  { Eys = En_hll; Ezs = Et1_hll; Exs = Et2_hll; Bys = Bn_hll; Bzs = Bt1_hll; Bxs = Bt2_hll; }
+  const T E2B2_str = T(0.5) * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+  const T a_hll = tau_f - ErotB_n;
+  const T b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
+  const T c_hll = Sn_hll - ErotB_n;
+  const T det_hll = pw2(b_hll) - T(4.0) * a_hll * c_hll;
+  const T q_root1 = -T(0.5) * (b_hll + fsgn1(b_hll) * fabs(sqrt(det_hll)));
+  T rt2 = c_hll / q_root1;
+  if (det_hll < T(0.0)) rt2 = c_hll / b_hll;
+  T V = hllc_vel(a_hll, -b_hll, c_hll, rt2, st);
+  if (fabs(V) <= T(1.0e-9)) V = T(0.0);
+  // star states
+  const T pstr = Sn_f + (pw2(En_hll) + pw2(Bn_hll)) - (tau_f - ErotB_n) * V;
+  const T SnR = (s2 * Sn_hll - Sn_f + pstr - pw2(Bn_hll) - pw2(En_hll) - ErotB_n * V) / (s2 - V);
+  const T SnL = (-s1 * Sn_hll + Sn_f - pstr + pw2(Bn_hll) + pw2(En_hll) + ErotB_n * V) / (V - s1);
+  const T St1R = (s2 * St1_hll - St1_f - ErotB_t1 * V - En_hll * Et1_hll - Bn_hll * Bt1_hll) / (s2 - V);
+  const T St1L = (-s1 * St1_hll + St1_f + ErotB_t1 * V + En_hll * Et1_hll + Bn_hll * Bt1_hll) / (V - s1);
+  const T St2R = (s2 * St2_hll - St2_f - ErotB_t2 * V - En_hll * Et2_hll - Bn_hll * Bt2_hll) / (s2 - V);
+  const T St2L = (-s1 * St2_hll + St2_f + ErotB_t2 * V + En_hll * Et2_hll + Bn_hll * Bt2_hll) / (V - s1);
+  const T tauR = (s2 * tau_hll - tau_f + (pstr - E2B2_str) * V + ErotB_n) / (s2 - V);
+  const T tauL = (-s1 * tau_hll + tau_f - (pstr - E2B2_str) * V - ErotB_n) / (V - s1);
+  const T DR = (s2 * D_hll - D_f) / (s2 - V);
+  const T DL = (-s1 * D_hll + D_f) / (V - s1);
+  // star fluxes
+  T fDR = D_f, fDL = D_f, ftR = tau_f, ftL = tau_f, fSnR = Sn_f, fSnL = Sn_f, fS1R = St1_f, fS1L = St1_f,
+    fS2R = St2_f, fS2L = St2_f;
+  if (V == T(0.0)) {
+    A[R_PSI] = hll(X::En(L), X::En(R), L.psi, R.psi);
+    A[R_PHI] = hll(X::Bn(L), X::Bn(R), L.phi, R.phi);
+    A[R_BN] = hll(L.phi, R.phi, X::Bn(L), X::Bn(R));
+    A[R_BT1] = -hll(m_et2[0], m_et2[1], X::Bt1(L), X::Bt1(R));
+    A[R_BT2] = hll(X::Et1(L), X::Et1(R), X::Bt2(L), X::Bt2(R));
+    A[R_EN] = hll(L.psi, R.psi, X::En(L), X::En(R));
+    A[R_ET1] = hll(X::Bt2(L), X::Bt2(R), X::Et1(L), X::Et1(R));
+    A[R_ET2] = -hll(m_bt1[0], m_bt1[1], X::Et2(L), X::Et2(R));
+  } else if (V == V) {
+    // flux of the star state; R_BT1 / R_ET2 hold -F(B_t1) = E_t2*, -F(E_t2) = B_t1*
+    A[R_PSI] = En_hll; A[R_PHI] = Bn_hll; A[R_BN] = phi_hll; A[R_BT1] = Et2_hll;
+    A[R_BT2] = Et1_hll; A[R_EN] = psi_hll; A[R_ET1] = Bt2_hll; A[R_ET2] = Bt1_hll;
+    fDR = fr.FD + s2 * (DR - R.D);                 fDL = fl.FD + s1 * (DL - L.D);
+    ftR = fr.Ftau + s2 * (tauR - R.tau);           ftL = fl.Ftau + s1 * (tauL - L.tau);
+    fSnR = fr.FSn + s2 * (SnR - X::Sn(R));         fSnL = fl.FSn + s1 * (SnL - X::Sn(L));
+    fS1R = fr.FSt1 + s2 * (St1R - X::St1(R));      fS1L = fl.FSt1 + s1 * (St1L - X::St1(L));
+    fS2R = fr.FSt2 + s2 * (St2R - X::St2(R));      fS2L = fl.FSt2 + s1 * (St2L - X::St2(L));
+  } else {
+    st |= ST_HLLC_VSTAR;
+#pragma unroll
+    for (int c = R_PSI; c <= R_ET2; ++c) A[c] = T(NAN);
+  }
+  if (s1 > T(0.0)) {
+    A[R_Q] = JL; A[R_D] = fl.FD; A[R_TAU] = fl.Ftau; A[R_SN] = fl.FSn; A[R_ST1] = fl.FSt1; A[R_ST2] = fl.FSt2;
+  } else if (s1 <= T(0.0) && T(0.0) <= V) {
+    A[R_Q] = q_f; A[R_D] = fDL; A[R_TAU] = ftL; A[R_SN] = fSnL; A[R_ST1] = fS1L; A[R_ST2] = fS2L;
+  } else if (V < T(0.0) && T(0.0) <= s2) {
+    A[R_Q] = q_f; A[R_D] = fDR; A[R_TAU] = ftR; A[R_SN] = fSnR; A[R_ST1] = fS1R; A[R_ST2] = fS2R;
+  } else if (s2 < T(0.0)) {
+    A[R_Q] = JR; A[R_D] = fr.FD; A[R_TAU] = fr.Ftau; A[R_SN] = fr.FSn; A[R_ST1] = fr.FSt1; A[R_ST2] = fr.FSt2;
+  } else {   // the reference stops
+    st |= ST_HLLC_VSTAR;
+    A[R_Q] = A[R_D] = A[R_TAU] = A[R_SN] = A[R_ST1] = A[R_ST2] = T(NAN);
+  }
+}
+
 }  // namespace cueva

@@ -1,5 +1,5 @@
 // cueva_stage.cuh -- the two stage kernels of the CUEVA hot path (templates),
-// shared by the per-solver translation units cueva_stage_{lax,mcl,hll,hllc,hlle}.cu
+// shared by the per-solver translation units cueva_stage_{lax,mcl,hllemc,hllcmc,hll,hllc,hlle}.cu
 // and by the pointwise kernels of cueva_kernels.cu.
 //
 // One RK stage = two launches:
@@ -293,9 +293,11 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     }
     return stt;
   }
-  if constexpr (SOLVER == 2) {
-    // HLL with the second-order MC reconstruction, 16_hll_flow_mcl.f95:565-1396
-    // (x and y faces of a point are the same formulas in the direction roles)
+  if constexpr (SOLVER >= 2 && SOLVER <= 4) {
+    // HLL (16_hll_flow_mcl.f95:565-1396), HLLE (16_hlle_flow_mcl.f95:1647-4345)
+    // or HLLC (16_hllc_flow_mcl.f95:1760-4056) with the second-order MC
+    // reconstruction (x and y faces of a point are the same formulas in the
+    // direction roles)
     static_assert(RM == 3, "the MCL fluxes use the MC reconstruction");
     T m_et2[2], m_bt1[2];   // "_m" values (-u + slope) of E_t2 and B_t1, left and right
     auto recm = [&](int f, T& Lv, T& Rv, T* m) {
@@ -328,7 +330,9 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     recm(5 + Q_SX, L.Sx, Rs.Sx, nullptr);
     recm(5 + Q_SY, L.Sy, Rs.Sy, nullptr);
     recm(5 + Q_SZ, L.Sz, Rs.Sz, nullptr);
-    mcl_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F);
+    if constexpr (SOLVER == 2) mcl_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F);
+    else if constexpr (SOLVER == 3) hllemc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F, stt);
+    else hllcmc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F, stt);
     return stt;
   }
   // primitive slots of this direction (21-25 for x, 58-62 for y)
@@ -751,7 +755,7 @@ template <int SV>
 cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                                 const StageArgs& sa, cudaEvent_t* ev) {
   if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
-  if constexpr (SV == 1 || SV == 2) {   // the Lax and MCL routines use MC slopes; rec_mp does not apply
+  if constexpr (SV >= 1 && SV <= 4) {   // the MC family uses MC slopes; rec_mp does not apply
     launch_rm_sv<3, SV>(prec, sh, st, d, n, sa, ev);
   } else {
     switch (rec_mp) {
@@ -766,7 +770,7 @@ cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cuda
 
 template <int SV>
 cudaError_t prepare_stage_solver(int rec_mp, int prec) {
-  if constexpr (SV == 1 || SV == 2) {
+  if constexpr (SV >= 1 && SV <= 4) {
     return prepare_rm_sv<3, SV>(prec);
   } else {
     switch (rec_mp) {

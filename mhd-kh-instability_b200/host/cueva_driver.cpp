@@ -42,7 +42,7 @@ const Key kKeys[] = {
     {"imax", "256", "grid points 0..imax along x (parameters.f95:110)"},
     {"jmax", "128", "grid points 0..jmax along y (parameters.f95:111)"},
     {"order", "2", "IMEX tableau: 1, 2 SSP2(2,2,2), 3 SSP2(3,3,2), 4 SSP3(4,3,3), 5, 6, 8"},
-    {"flux_solver", "5", "1 Lax-Friedrichs with MC slopes, 2 HLL with MC reconstruction, 5 HLL, 6 HLLE, 7 HLLC (MPX reconstruction)"},
+    {"flux_solver", "5", "1 Lax-Friedrichs with MC slopes, 2 HLL / 3 HLLE / 4 HLLC with MC reconstruction, 5 HLL, 6 HLLE, 7 HLLC (MPX reconstruction)"},
     {"rec_mp", "0", "0 MP5, 1 MP7, 2 MP9"},
     {"conserved_to_primitive", "1", "1 Cardano, 0 Newton-Raphson"},
     {"BOUND", "6", "1 copy/copy, 2 periodic/periodic, 6 x copy / y periodic (04_boundary.f95)"},

@@ -948,7 +948,7 @@ struct Oracle {
 
   void reconstruct() {
     if (P.flux_solver == 1) return;   // lax_flow works on the cell pairs directly
-    if (P.flux_solver == 2) { reconstruct_mcl(); return; }
+    if (P.flux_solver >= 2 && P.flux_solver <= 4) { reconstruct_mcl(); return; }
     const int rec = P.rec_mp;
     XL.assign(X_N, std::vector<double>(ng, 0.0)); XR.assign(X_N, std::vector<double>(ng, 0.0));
     YL.assign(Y_N, std::vector<double>(ng, 0.0)); YR.assign(Y_N, std::vector<double>(ng, 0.0));
@@ -1145,6 +1145,16 @@ struct Oracle {
           for (int c = 0; c < 28; ++c) o[c][k] = out[c];
           continue;
         }
+        if (solver == 3) {   // 16_hlle_flow_mcl.f95:1647-4345
+          PhysX fxl = physx(xl), fxr = physx(xr), fyl = physy(yl), fyr = physy(yr);
+          hlle_w(fxl, xl); hlle_w(fxr, xr); hlle_w(fyl, yl); hlle_w(fyr, yr);
+          fxl = physx_w(xl, fxl.W); fxr = physx_w(xr, fxr.W); fyl = physy_w(yl, fyl.W); fyr = physy_w(yr, fyr.W);
+          double out[28];
+          st_acc |= hllemc_x(xl, xr, fxl, fxr, side_jx(xl, fxl.W), side_jx(xr, fxr.W), out);
+          st_acc |= hllemc_y(yl, yr, fyl, fyr, side_jy(yl, fyl.W), side_jy(yr, fyr.W), out);
+          for (int c = 0; c < 28; ++c) o[c][k] = out[c];
+          continue;
+        }
         if (solver == 7) {
           // density fix-up chain, 16_hllc_flow_mpx.f95:2663-2690
           if (yl.rho < 0.0) yl.rho = rho[k] * 1.0e-1;
@@ -1153,8 +1163,12 @@ struct Oracle {
           else if (xr.rho < 0.0) xr.rho = rho[k] * 1.0e-1;
         }
         PhysX fxl = physx(xl), fxr = physx(xr), fyl = physy(yl), fyr = physy(yr);
-        if (solver == 6) { hlle_w(fxl, xl); hlle_w(fxr, xr); hlle_w(fyl, yl); hlle_w(fyr, yr);
+        if (solver == 6 || solver == 4) { hlle_w(fxl, xl); hlle_w(fxr, xr); hlle_w(fyl, yl); hlle_w(fyr, yr);
           fxl = physx_w(xl, fxl.W); fxr = physx_w(xr, fxr.W); fyl = physy_w(yl, fyl.W); fyr = physy_w(yr, fyr.W); }
+        if (solver == 4) {   // 16_hllc_flow_mcl.f95: the current of each side's MC state
+          xl.J = side_jx(xl, fxl.W); xr.J = side_jx(xr, fxr.W);
+          yl.J = side_jy(yl, fyl.W); yr.J = side_jy(yr, fyr.W);
+        }
         double out[28];
         // EM + charge fluxes are HLL for every solver (HLLC star EM fluxes equal the HLL ones)
         out[0] = hllf(xl.Ex, xr.Ex, xl.psi, xr.psi);                 // Exlaxpsi
@@ -1189,6 +1203,9 @@ struct Oracle {
         } else if (solver == 7) {
           st_acc |= hllc_x(xl, xr, fxl, fxr, out);
           st_acc |= hllc_y(yl, yr, fyl, fyr, out);
+        } else if (solver == 4) {   // 16_hllc_flow_mcl.f95:2580-2600: |v*| <= 1e-6 counts as 0
+          st_acc |= hllc_x(xl, xr, fxl, fxr, out, 1.0e-6);
+          st_acc |= hllc_y(yl, yr, fyl, fyr, out, 1.0e-6);
         } else {
           st_acc |= hlle_x(xl, xr, fxl, fxr, out);
           st_acc |= hlle_y(yl, yr, fyl, fyr, out);
@@ -1222,9 +1239,14 @@ struct Oracle {
   }
 
   // ----------------------------------------- HLLC, x direction
+  // The HLLC of the MC family (16_hllc_flow_mcl.f95, flux_solver 4, 2D
+  // :1751-4056) has the same HLL states, star states and flux choice on the
+  // MC sides (the "_m" values in Ez / By, the current of each side, W from
+  // 1 - vx^2 - vy^2 - vz^2) and zeroes |v*| <= 1e-6 (vzero) instead of 1e-9.
   // 16_hllc_flow_mpx.f95:2816-3100 (HLL states/fluxes), 3184-3335 (v*),
   // 3485-3520 (star states), 3592-3740 (star fluxes), 3908-4300 (selection)
-  int32_t hllc_x(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+  int32_t hllc_x(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out,
+                  double vzero = 1.0e-9) {
     int32_t st = 0;
     const double s1 = -1.0, s2 = 1.0;
     const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ex - R.Ex) / (s2 - s1);
@@ -1271,7 +1293,7 @@ struct Oracle {
     if (det_hll < 0.0) rt2 = c_hll / b_hll;
     double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
     const double eps1 = 1.0e-6;  // 16_hllc_flow_mpx.f95:3217
-    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    if (std::fabs(V) <= vzero) V = 0.0;
     else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
     const double pstr = Sx_f + (pw2(Exs) + pw2(Bxs)) - (tau_f - ErotB_x) * V;
     const double psiR = (s2 * psi_hll - V * Ex_f) / (s2 - V);
@@ -1329,7 +1351,8 @@ struct Oracle {
 
   // ----------------------------------------- HLLC, y direction
   // 16_hllc_flow_mpx.f95:2960-3100, 3340-3475, 3522-3570, 3742-3905, 4305-4610
-  int32_t hllc_y(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out) {
+  int32_t hllc_y(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double* out,
+                  double vzero = 1.0e-9) {
     int32_t st = 0;
     const double s1 = -1.0, s2 = 1.0;
     const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ey - R.Ey) / (s2 - s1);
@@ -1375,7 +1398,7 @@ struct Oracle {
     if (det_hll < 0.0) rt2 = c_hll / b_hll;
     double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
     const double eps1 = (double)1.0e-6f;  // single-precision literal, 16_hllc_flow_mpx.f95:3354
-    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    if (std::fabs(V) <= vzero) V = 0.0;
     else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
     const double pstr = Sy_f + (pw2(Eys) + pw2(Bys)) - (tau_f - ErotB_y) * V;
     const double psiR = (s2 * psi_hll - V * Ey_f) / (s2 - V);
@@ -1431,8 +1454,6 @@ struct Oracle {
     return st;
   }
 
-  // HLLE is restated separately (16_hlle_flow_mpx.f95); until then the
-  // solver id 6 is rejected at creation.
   // ----------------------------------------- HLLE (16_hlle_flow_mpx.f95, 2D)
   // EM fields, psi and phi take the fixed-speed HLL fluxes (s = -1, +1,
   // :2526-2588, the star psi/phi fluxes are the HLL ones, :3489-3604); q, D,
@@ -1459,6 +1480,224 @@ struct Oracle {
     const double eps2 = 1.0e-9;
     if (std::fabs(s1) > 1.0) s1 = fmax2(-1.0 + eps2, fmin2(1.0 - eps2, s1));
     if (std::fabs(s2) > 1.0) s2 = fmax2(-1.0 + eps2, fmin2(1.0 - eps2, s2));
+    return st;
+  }
+
+  // ------------------- HLLE with the MC reconstruction (16_hlle_flow_mcl.f95, 2D, :1638-4345)
+  // Sides come from the MC reconstruction (the "_m" values of Ez / By in x,
+  // Ex / Bz in y), W from 1 - vx^2 - vy^2 - vz^2 and the current J from each
+  // side's state, as in the HLL routine of the family.  The averaged states
+  // the routine also forms (p_L, rho_L, enthpy_L, ...) feed only its
+  // diagnostics prints.  Wave bounds and the v* quadratic are those of the
+  // MPX HLLE; the star states and fluxes differ (:2911-3029 for x):
+  //   S_n* = (s S_n,hll - F(S_n)_hll +- (p* - B_n*^2 - E_n*^2 - (E*xB*)_n v*)) / (s - v*),
+  //   tau* = (s tau_hll - F(tau)_hll +- ((p* - |E*B*|^2/2) v* + (E*xB*)_n)) / (s - v*),
+  //   F*   = F(side) + s (U* - U(side))            (s = sx1 left, sx2 right),
+  // and for v* != 0 the EM fluxes are the fluxes of the star state
+  // (psi: E_n*, E_n: psi*, E_t1: B_t2*, E_t2: -B_t1*, ...), for v* == 0 the
+  // fixed-speed HLL fluxes (:3042-3150).  Flux choice (:3236-4343): sx1 > 0
+  // left physical flux, sx1 <= 0 <= v* left star, v* < 0 <= sx2 right star,
+  // sx2 < 0 right physical flux.  A NaN v* leaves the reference's EM arrays
+  // unset; it is reported here with NaN fluxes.
+  double side_jx(const Side& s, double W) const {
+    const double vrotB = s.Bz * s.vy - s.By * s.vz;
+    const double Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+    return sigma * W * (s.Ex + vrotB - Edotv * s.vx) + s.q * s.vx;
+  }
+  double side_jy(const Side& s, double W) const {
+    const double vrotB = s.Bx * s.vz - s.Bz * s.vx;
+    const double Edotv = s.Ex * s.vx + s.Ey * s.vy + s.Ez * s.vz;
+    return sigma * W * (s.Ey + vrotB - Edotv * s.vy) + s.q * s.vy;
+  }
+  int32_t hllemc_x(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double JL, double JR,
+                   double* out) {
+    const double s1 = -1.0, s2 = 1.0;
+    const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ex - R.Ex) / (s2 - s1);
+    const double phi_hll = (s2 * R.phi - s1 * L.phi + L.Bx - R.Bx) / (s2 - s1);
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.psi - R.psi) / (s2 - s1);
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.Bz - R.Bz) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bym - R.Bym) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.phi - R.phi) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.Ezm - R.Ezm) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Ey - R.Ey) / (s2 - s1);
+    double lmL, lpL, lmR, lpR, sx1, sx2;
+    hlle_bounds(R, fr, R.vx, lmR, lpR);
+    hlle_bounds(L, fl, L.vx, lmL, lpL);
+    int32_t st = hlle_speeds(lmL, lmR, lpL, lpR, sx1, sx2);
+    const double DD_hll = (sx2 * R.D - sx1 * L.D + fl.FD - fr.FD) / (sx2 - sx1);
+    const double tau_hll = (sx2 * R.tau - sx1 * L.tau + fl.Ftau - fr.Ftau) / (sx2 - sx1);
+    const double Sx_hll = (sx2 * R.Sx - sx1 * L.Sx + fl.FSx - fr.FSx) / (sx2 - sx1);
+    const double Sy_hll = (sx2 * R.Sy - sx1 * L.Sy + fl.FSy - fr.FSy) / (sx2 - sx1);
+    const double Sz_hll = (sx2 * R.Sz - sx1 * L.Sz + fl.FSz - fr.FSz) / (sx2 - sx1);
+    auto hlle = [&](double FL, double FR, double UL, double UR) {
+      return (sx2 * FL - sx1 * FR + sx1 * sx2 * (UR - UL)) / (sx2 - sx1);
+    };
+    const double q_f = hlle(JL, JR, L.q, R.q);
+    const double DD_f = hlle(fl.FD, fr.FD, L.D, R.D);
+    const double tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+    const double Sx_f = hlle(fl.FSx, fr.FSx, L.Sx, R.Sx);
+    const double Sy_f = hlle(fl.FSy, fr.FSy, L.Sy, R.Sy);
+    const double Sz_f = hlle(fl.FSz, fr.FSz, L.Sz, R.Sz);
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Eys) + pw2(Ezs));
+    const double B2_perp = (pw2(Bys) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_x;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sx_f;
+    const double c_hll = Sx_hll - ErotB_x;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = 1.0e-6;
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sx_f + (pw2(Exs) + pw2(Bxs)) - (tau_f - ErotB_x) * V;
+    const double SxR = (sx2 * Sx_hll - Sx_f + pstr - pw2(Bxs) - pw2(Exs) - ErotB_x * V) / (sx2 - V);
+    const double SxL = (-sx1 * Sx_hll + Sx_f - pstr + pw2(Bxs) + pw2(Exs) + ErotB_x * V) / (V - sx1);
+    const double SyR = (sx2 * Sy_hll - Sy_f - ErotB_y * V - Exs * Eys - Bxs * Bys) / (sx2 - V);
+    const double SyL = (-sx1 * Sy_hll + Sy_f + ErotB_y * V + Exs * Eys + Bxs * Bys) / (V - sx1);
+    const double SzR = (sx2 * Sz_hll - Sz_f - ErotB_z * V - Exs * Ezs - Bxs * Bzs) / (sx2 - V);
+    const double SzL = (-sx1 * Sz_hll + Sz_f + ErotB_z * V + Exs * Ezs + Bxs * Bzs) / (V - sx1);
+    const double tauR = (sx2 * tau_hll - tau_f + (pstr - E2B2_str) * V + ErotB_x) / (sx2 - V);
+    const double tauL = (-sx1 * tau_hll + tau_f - (pstr - E2B2_str) * V - ErotB_x) / (V - sx1);
+    const double DR = (sx2 * DD_hll - DD_f) / (sx2 - V);
+    const double DL = (-sx1 * DD_hll + DD_f) / (V - sx1);
+    double fpsi, fphi, fEx, fEy, fEz, fBx, fBy, fBz;
+    double fDR = DD_f, fDL = DD_f, ftR = tau_f, ftL = tau_f, fSxR = Sx_f, fSxL = Sx_f, fSyR = Sy_f, fSyL = Sy_f,
+           fSzR = Sz_f, fSzL = Sz_f;
+    if (V == 0.0) {
+      fpsi = hllf(L.Ex, R.Ex, L.psi, R.psi); fphi = hllf(L.Bx, R.Bx, L.phi, R.phi);
+      fBx = hllf(L.phi, R.phi, L.Bx, R.Bx); fBy = hllf(L.Ezm, R.Ezm, L.By, R.By);
+      fBz = hllf(L.Ey, R.Ey, L.Bz, R.Bz); fEx = hllf(L.psi, R.psi, L.Ex, R.Ex);
+      fEy = hllf(L.Bz, R.Bz, L.Ey, R.Ey); fEz = hllf(L.Bym, R.Bym, L.Ez, R.Ez);
+    } else {
+      fpsi = Exs; fphi = Bxs; fEx = psi_hll; fEy = Bzs; fEz = -Bys; fBx = phi_hll; fBy = -Ezs; fBz = Eys;
+      fDR = fr.FD + sx2 * (DR - R.D);        fDL = fl.FD + sx1 * (DL - L.D);
+      ftR = fr.Ftau + sx2 * (tauR - R.tau);  ftL = fl.Ftau + sx1 * (tauL - L.tau);
+      fSxR = fr.FSx + sx2 * (SxR - R.Sx);    fSxL = fl.FSx + sx1 * (SxL - L.Sx);
+      fSyR = fr.FSy + sx2 * (SyR - R.Sy);    fSyL = fl.FSy + sx1 * (SyL - L.Sy);
+      fSzR = fr.FSz + sx2 * (SzR - R.Sz);    fSzL = fl.FSz + sx1 * (SzL - L.Sz);
+    }
+    if (0.0 <= V || V < 0.0) {   // both star sides carry the same EM fluxes
+      out[0] = fpsi; out[2] = fphi; out[4] = fBx; out[6] = -fBy; out[8] = fBz; out[10] = fEx; out[12] = fEy;
+      out[14] = -fEz;
+    } else {
+      st |= ST_HLLC_VSTAR;
+      for (int c : {0, 2, 4, 6, 8, 10, 12, 14}) out[c] = NAN;
+    }
+    if (sx1 > 0.0) {
+      out[16] = JL; out[18] = fl.FD; out[20] = fl.Ftau; out[22] = fl.FSx; out[23] = fl.FSy; out[24] = fl.FSz;
+    } else if (sx1 <= 0.0 && 0.0 <= V) {
+      out[16] = q_f; out[18] = fDL; out[20] = ftL; out[22] = fSxL; out[23] = fSyL; out[24] = fSzL;
+    } else if (V < 0.0 && 0.0 <= sx2) {
+      out[16] = q_f; out[18] = fDR; out[20] = ftR; out[22] = fSxR; out[23] = fSyR; out[24] = fSzR;
+    } else if (sx2 < 0.0) {
+      out[16] = JR; out[18] = fr.FD; out[20] = fr.Ftau; out[22] = fr.FSx; out[23] = fr.FSy; out[24] = fr.FSz;
+    } else {   // the reference stops
+      st |= ST_HLLC_VSTAR;
+      for (int c : {16, 18, 20, 22, 23, 24}) out[c] = NAN;
+    }
+    return st;
+  }
+  // y faces (16_hlle_flow_mcl.f95 y branches): physy's FSx, FSy, FSz are FSyx, FSyy, FSyz
+  int32_t hllemc_y(const Side& L, const Side& R, const PhysX& fl, const PhysX& fr, double JL, double JR,
+                   double* out) {
+    const double s1 = -1.0, s2 = 1.0;
+    const double psi_hll = (s2 * R.psi - s1 * L.psi + L.Ey - R.Ey) / (s2 - s1);
+    const double phi_hll = (s2 * R.phi - s1 * L.phi + L.By - R.By) / (s2 - s1);
+    const double Ey_hll = (s2 * R.Ey - s1 * L.Ey + L.psi - R.psi) / (s2 - s1);
+    const double Ez_hll = (s2 * R.Ez - s1 * L.Ez + L.Bx - R.Bx) / (s2 - s1);
+    const double Ex_hll = (s2 * R.Ex - s1 * L.Ex + L.Bzm - R.Bzm) / (s2 - s1);
+    const double By_hll = (s2 * R.By - s1 * L.By + L.phi - R.phi) / (s2 - s1);
+    const double Bz_hll = (s2 * R.Bz - s1 * L.Bz + L.Exm - R.Exm) / (s2 - s1);
+    const double Bx_hll = (s2 * R.Bx - s1 * L.Bx + L.Ez - R.Ez) / (s2 - s1);
+    double lmL, lpL, lmR, lpR, sy1, sy2;
+    hlle_bounds(R, fr, R.vy, lmR, lpR);
+    hlle_bounds(L, fl, L.vy, lmL, lpL);
+    int32_t st = hlle_speeds(lmL, lmR, lpL, lpR, sy1, sy2);
+    const double DD_hll = (sy2 * R.D - sy1 * L.D + fl.FD - fr.FD) / (sy2 - sy1);
+    const double tau_hll = (sy2 * R.tau - sy1 * L.tau + fl.Ftau - fr.Ftau) / (sy2 - sy1);
+    const double Sy_hll = (sy2 * R.Sy - sy1 * L.Sy + fl.FSy - fr.FSy) / (sy2 - sy1);
+    const double Sz_hll = (sy2 * R.Sz - sy1 * L.Sz + fl.FSz - fr.FSz) / (sy2 - sy1);
+    const double Sx_hll = (sy2 * R.Sx - sy1 * L.Sx + fl.FSx - fr.FSx) / (sy2 - sy1);
+    auto hlle = [&](double FL, double FR, double UL, double UR) {
+      return (sy2 * FL - sy1 * FR + sy1 * sy2 * (UR - UL)) / (sy2 - sy1);
+    };
+    const double q_f = hlle(JL, JR, L.q, R.q);
+    const double DD_f = hlle(fl.FD, fr.FD, L.D, R.D);
+    const double tau_f = hlle(fl.Ftau, fr.Ftau, L.tau, R.tau);
+    const double Sy_f = hlle(fl.FSy, fr.FSy, L.Sy, R.Sy);
+    const double Sz_f = hlle(fl.FSz, fr.FSz, L.Sz, R.Sz);
+    const double Sx_f = hlle(fl.FSx, fr.FSx, L.Sx, R.Sx);
+    const double Exs = Ex_hll, Eys = Ey_hll, Ezs = Ez_hll, Bxs = Bx_hll, Bys = By_hll, Bzs = Bz_hll;
+    const double ErotB_x = (Bzs * Eys - Bys * Ezs);
+    const double ErotB_y = (Bxs * Ezs - Bzs * Exs);
+    const double ErotB_z = (Bys * Exs - Bxs * Eys);
+    const double E2_perp = (pw2(Exs) + pw2(Ezs));
+    const double B2_perp = (pw2(Bxs) + pw2(Bzs));
+    const double E2B2_str = 0.5 * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
+    const double a_hll = tau_f - ErotB_y;
+    const double b_hll = E2_perp + B2_perp - tau_hll - Sy_f;
+    const double c_hll = Sy_hll - ErotB_y;
+    const double det_hll = pw2(b_hll) - 4.0 * a_hll * c_hll;
+    const double q_root1 = -0.5 * (b_hll + fsign(1.0, b_hll) * std::fabs(std::sqrt(det_hll)));
+    double rt2 = c_hll / q_root1;
+    if (det_hll < 0.0) rt2 = c_hll / b_hll;
+    double V = get_hllc_vel(a_hll, -b_hll, c_hll, rt2, &st);
+    const double eps1 = 1.0e-6;
+    if (std::fabs(V) <= 1.0e-9) V = 0.0;
+    else if (std::fabs(V) > 1.0) V = fmax2(-1.0 + eps1, fmin2(1.0 - eps1, V));
+    const double pstr = Sy_f + (pw2(Eys) + pw2(Bys)) - (tau_f - ErotB_y) * V;
+    const double SyR = (sy2 * Sy_hll - Sy_f + pstr - pw2(Bys) - pw2(Eys) - ErotB_y * V) / (sy2 - V);
+    const double SyL = (-sy1 * Sy_hll + Sy_f - pstr + pw2(Bys) + pw2(Eys) + ErotB_y * V) / (V - sy1);
+    const double SzR = (sy2 * Sz_hll - Sz_f - ErotB_z * V - Eys * Ezs - Bys * Bzs) / (sy2 - V);
+    const double SzL = (-sy1 * Sz_hll + Sz_f + ErotB_z * V + Eys * Ezs + Bys * Bzs) / (V - sy1);
+    const double SxR = (sy2 * Sx_hll - Sx_f - ErotB_x * V - Eys * Exs - Bys * Bxs) / (sy2 - V);
+    const double SxL = (-sy1 * Sx_hll + Sx_f + ErotB_x * V + Eys * Exs + Bys * Bxs) / (V - sy1);
+    const double tauR = (sy2 * tau_hll - tau_f + (pstr - E2B2_str) * V + ErotB_y) / (sy2 - V);
+    const double tauL = (-sy1 * tau_hll + tau_f - (pstr - E2B2_str) * V - ErotB_y) / (V - sy1);
+    const double DR = (sy2 * DD_hll - DD_f) / (sy2 - V);
+    const double DL = (-sy1 * DD_hll + DD_f) / (V - sy1);
+    double fpsi, fphi, fEx, fEy, fEz, fBx, fBy, fBz;
+    double fDR = DD_f, fDL = DD_f, ftR = tau_f, ftL = tau_f, fSxR = Sx_f, fSxL = Sx_f, fSyR = Sy_f, fSyL = Sy_f,
+           fSzR = Sz_f, fSzL = Sz_f;
+    if (V == 0.0) {
+      fpsi = hllf(L.Ey, R.Ey, L.psi, R.psi); fphi = hllf(L.By, R.By, L.phi, R.phi);
+      fBy = hllf(L.phi, R.phi, L.By, R.By); fBz = hllf(L.Exm, R.Exm, L.Bz, R.Bz);
+      fBx = hllf(L.Ez, R.Ez, L.Bx, R.Bx); fEy = hllf(L.psi, R.psi, L.Ey, R.Ey);
+      fEz = hllf(L.Bx, R.Bx, L.Ez, R.Ez); fEx = hllf(L.Bzm, R.Bzm, L.Ex, R.Ex);
+    } else {
+      fpsi = Eys; fphi = Bys; fEx = -Bzs; fEy = psi_hll; fEz = Bxs; fBx = Ezs; fBy = phi_hll; fBz = -Exs;
+      fDR = fr.FD + sy2 * (DR - R.D);        fDL = fl.FD + sy1 * (DL - L.D);
+      ftR = fr.Ftau + sy2 * (tauR - R.tau);  ftL = fl.Ftau + sy1 * (tauL - L.tau);
+      fSxR = fr.FSx + sy2 * (SxR - R.Sx);    fSxL = fl.FSx + sy1 * (SxL - L.Sx);
+      fSyR = fr.FSy + sy2 * (SyR - R.Sy);    fSyL = fl.FSy + sy1 * (SyL - L.Sy);
+      fSzR = fr.FSz + sy2 * (SzR - R.Sz);    fSzL = fl.FSz + sy1 * (SzL - L.Sz);
+    }
+    if (0.0 <= V || V < 0.0) {
+      out[1] = fpsi; out[3] = fphi; out[5] = fBx; out[7] = fBy; out[9] = -fBz; out[11] = -fEx; out[13] = fEy;
+      out[15] = fEz;
+    } else {
+      st |= ST_HLLC_VSTAR;
+      for (int c : {1, 3, 5, 7, 9, 11, 13, 15}) out[c] = NAN;
+    }
+    if (sy1 > 0.0) {
+      out[17] = JL; out[19] = fl.FD; out[21] = fl.Ftau; out[25] = fl.FSx; out[26] = fl.FSy; out[27] = fl.FSz;
+    } else if (sy1 <= 0.0 && 0.0 <= V) {
+      out[17] = q_f; out[19] = fDL; out[21] = ftL; out[25] = fSxL; out[26] = fSyL; out[27] = fSzL;
+    } else if (V < 0.0 && 0.0 <= sy2) {
+      out[17] = q_f; out[19] = fDR; out[21] = ftR; out[25] = fSxR; out[26] = fSyR; out[27] = fSzR;
+    } else if (sy2 < 0.0) {
+      out[17] = JR; out[19] = fr.FD; out[21] = fr.Ftau; out[25] = fr.FSx; out[26] = fr.FSy; out[27] = fr.FSz;
+    } else {
+      st |= ST_HLLC_VSTAR;
+      for (int c : {17, 19, 21, 25, 26, 27}) out[c] = NAN;
+    }
     return st;
   }
 
@@ -1938,7 +2177,7 @@ extern "C" {
 
 void* oracle_create(const oracle_params* p) {
   if (!p || p->imax < 6 || p->jmax < 6) return nullptr;
-  if (p->flux_solver != 1 && p->flux_solver != 2 && p->flux_solver != 5 && p->flux_solver != 6 && p->flux_solver != 7) return nullptr;
+  if (p->flux_solver < 1 || p->flux_solver > 7) return nullptr;   // main_cueva_code.f95:247-279
   if (p->rec_mp < 0 || p->rec_mp > 2) return nullptr;
   if (p->primitive_rec < 0 || p->primitive_rec > 1) return nullptr;
   Tableau T;

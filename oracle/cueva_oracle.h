@@ -30,6 +30,7 @@ typedef struct oracle_params {
   int32_t imax, jmax;      /* grid points 0..imax x 0..jmax (parameters.f95:110-111) */
   int32_t order;           /* IMEX tableau: 1,2,3,4,5,6,8 (imex_scheme.f95) */
   int32_t flux_solver;     /* 1 Lax-Friedrichs+MC (15_lax_flow.f95), 2 HLL+MC (16_hll_flow_mcl.f95),
+                              3 HLLE+MC (16_hlle_flow_mcl.f95), 4 HLLC+MC (16_hllc_flow_mcl.f95),
                               5 HLL+MPX, 6 HLLE+MPX, 7 HLLC+MPX (main_cueva_code.f95:247-273) */
   int32_t rec_mp;          /* 0 MP5, 1 MP7, 2 MP9 (parameters.f95:33) */
   int32_t c2p;             /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37) */

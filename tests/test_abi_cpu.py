@@ -65,7 +65,7 @@ def _create(**kw):
 
 
 @pytest.mark.parametrize("kw,frag", [
-    (dict(imax=4), "imax"), (dict(flux_solver=3), "flux_solver"), (dict(rec_mp=5), "rec_mp"),
+    (dict(imax=4), "imax"), (dict(flux_solver=8), "flux_solver"), (dict(rec_mp=5), "rec_mp"),
     (dict(c2p=7), "c2p"), (dict(bc_x=2), "bc_x"), (dict(order=7), "order"), (dict(precision=3), "precision"),
     (dict(intsum_reset=2), "intsum_reset"), (dict(primitive_rec=3), "primitive_rec")])
 def test_bad_configuration_rejected(kw, frag):

@@ -44,7 +44,7 @@ def _kh(g, o, v0=0.5, sigma_kw=None):
     return pr
 
 
-@pytest.mark.parametrize("solver,rec", [(5, 0), (7, 0), (5, 1), (5, 2), (7, 2), (6, 0), (6, 1), (6, 2), (2, 0), (1, 0)])
+@pytest.mark.parametrize("solver,rec", [(5, 0), (7, 0), (5, 1), (5, 2), (7, 2), (6, 0), (6, 1), (6, 2), (2, 0), (1, 0), (3, 0), (4, 0)])
 def test_flux_rhs_stage1_exact(oracle_mod, solver, rec):
     """hll/hllc_flow_mpx + fluxandsource of stage 1, bit-identical in the default build."""
     imax, jmax = 64, 32
@@ -89,7 +89,8 @@ def test_flux_rhs_stage1_both_builds(oracle_mod, fma):
 
 STEP_CASES = [  # (flux_solver, order, rec_mp, intsum_reset); shear width 0.05 resolves on 64 x 32
     (5, 2, 0, 0), (7, 2, 0, 0), (7, 3, 0, 0), (7, 4, 0, 1), (5, 2, 1, 0), (7, 2, 2, 0), (6, 2, 0, 0), (6, 4, 1, 1),
-    (2, 2, 0, 0), (2, 4, 0, 1), (1, 2, 0, 0), (1, 3, 0, 1)]
+    (2, 2, 0, 0), (2, 4, 0, 1), (1, 2, 0, 0), (1, 3, 0, 1), (3, 2, 0, 0), (3, 4, 0, 1),
+    (4, 2, 0, 0), (4, 4, 0, 1)]
 
 
 @pytest.mark.parametrize("fma", [False, True])
@@ -136,6 +137,10 @@ def test_steps_vs_oracle(oracle_mod, fma, solver, order, rec, reset):
     (37, 50, 2, 0, 1),
     (45, 38, 1, 0, 0),    # Lax-Friedrichs with MC slopes
     (37, 50, 1, 0, 1),
+    (45, 38, 3, 0, 0),    # HLLE with the MC reconstruction
+    (37, 50, 3, 0, 1),
+    (45, 38, 4, 0, 0),    # HLLC with the MC reconstruction
+    (37, 50, 4, 0, 1),
 ])
 def test_steps_ragged_grids(oracle_mod, imax, jmax, solver, rec, bc_x):
     """Partial CTA tiles, non-power-of-two spacings (true divisions in the

@@ -135,7 +135,8 @@ def test_tableaux_consistent(oracle_mod):
 
 
 @pytest.mark.parametrize("solver,order,rec", [(5, 2, 0), (7, 4, 0), (7, 2, 1), (5, 3, 2), (6, 2, 0), (6, 4, 2), (2, 2, 0),
-                                              (2, 4, 0), (1, 2, 0), (1, 4, 0)])
+                                              (2, 4, 0), (1, 2, 0), (1, 4, 0), (3, 2, 0),
+                                              (3, 4, 0), (4, 2, 0), (4, 4, 0)])
 def test_uniform_state_stays_uniform(oracle_mod, solver, order, rec):
     imax, jmax = 20, 12
     o = oracle_mod.Oracle(imax, jmax, order=order, flux_solver=solver, rec_mp=rec, bc_x=0, bc_y=1, sigma=1e3)
