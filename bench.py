@@ -80,12 +80,19 @@ class ClockSampler:
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.n0 = 0
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once the sampler reports: a short
+            # region would otherwise end before nvidia-smi's first line
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.n0 = len(self.samples)
         except (OSError, ValueError):
             self.proc = None
         return self
@@ -98,6 +105,11 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc is not None:
+            # one more line after the region, so a region shorter than the
+            # sampling period still has a sample at its end
+            n1, t0 = len(self.samples), time.time()
+            while len(self.samples) <= n1 and time.time() - t0 < 2.0 and self.proc.poll() is None:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -107,14 +119,15 @@ class ClockSampler:
             self.thread.join(timeout=2)
 
     def summary(self):
-        if not self.samples:
+        region = self.samples[self.n0:] or self.samples
+        if not region:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
-        mx = max((float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()), default=None)
+        sm = sorted(float(s[1]) for s in region if s[1].replace(".", "").isdigit())
+        mx = max((float(s[2]) for s in region if s[2].replace(".", "").isdigit()), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        reasons = sorted({names[k] for s in region for k in range(4) if s[5 + k].lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(region)}
 
 
 def dist_env():

@@ -211,3 +211,35 @@ def test_steps_primitive_reconstruction(oracle_mod, solver, order, rec, bc_x, gr
             err = rel_l1_field(n, g.interior(n), ref[n], ref)
             assert err <= bar, (steps, n, err)
     g.close()
+
+
+@pytest.mark.parametrize("solver", [1, 2, 3, 4, 5, 6, 7])
+def test_mixed_precision_close_to_fp64_oracle(oracle_mod, solver):
+    """precision = 1 (FP32 reconstruction and Riemann solve, FP64 elsewhere)
+    for every flux routine: after 1 and 20 steps of the KH layer the
+    primitives stay within a small relative L1 of the FP64 oracle -- the
+    FP32 rounding of the face fluxes, not a different scheme -- and the run
+    raises no status.  Measured on the B200: worst variable 4.5e-6 .. 7.2e-6
+    after 1 step, 7.9e-6 .. 1.9e-4 after 20 (Bx, which starts at zero, and
+    the velocities across the shear layer grow the rounding fastest)."""
+    imax, jmax = 64, 32
+    g, o = _pair(oracle_mod, imax, jmax, False, order=2, flux_solver=solver, rec_mp=0, sigma=1e3, precision=1)
+    g.kh_init(v0=0.5, a=0.05)
+    o.set_prims(g.prims())
+    g.upload()
+    worst = {}
+    for steps, bar in ((1, 2e-5), (19, 1e-3)):
+        g.step(steps)
+        g.download()
+        assert o.step(steps) == 0
+        assert g.status() == 0
+        ref = o.get_prims()
+        for n in PRIMS:
+            got = g.interior(n)
+            assert np.all(np.isfinite(got)), n
+            err = rel_l1_field(n, got, ref[n], ref)
+            worst[(steps, n)] = err
+            assert err <= bar, (steps, n, err)
+    print(f"solver {solver}: worst 1-step {max(v for (s, _), v in worst.items() if s == 1):.2e}, "
+          f"20-step {max(v for (s, _), v in worst.items() if s == 19):.2e}")
+    g.close()
