@@ -89,6 +89,15 @@ enum cueva_field {
   CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
   CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,
   CUEVA_SXFLUX, CUEVA_SYFLUX, CUEVA_SZFLUX, CUEVA_EXASTSOUR, CUEVA_EYASTSOUR, CUEVA_EZASTSOUR,
+  /* stage interface fluxes, (.., 1:lmax) arrays of fourvectors.f95: the outputs of the
+   * flux routines (15_lax_flow.f95, 16_*_flow_mcl.f95, 16_*_flow_mpx.f95) that
+   * 17_fluxandsource.f95 reads.  X(i,j) of an x array is the flux through i+1/2, of a y
+   * array the flux through j+1/2 */
+  CUEVA_EXLAXPSI, CUEVA_EYLAXPSI, CUEVA_BXLAXPHI, CUEVA_BYLAXPHI, CUEVA_PHILAXBX, CUEVA_EZLAXBX,
+  CUEVA_EZLAXBY, CUEVA_PHILAXBY, CUEVA_EYLAXBZ, CUEVA_EXLAXBZ, CUEVA_PSILAXEX, CUEVA_BZLAXEX,
+  CUEVA_BZLAXEY, CUEVA_PSILAXEY, CUEVA_BYLAXEZ, CUEVA_BXLAXEZ, CUEVA_JXLAX, CUEVA_JYLAX,
+  CUEVA_FDXLAX, CUEVA_FDYLAX, CUEVA_FTAUXLAX, CUEVA_FTAUYLAX, CUEVA_FSXXLAX, CUEVA_FSXYLAX,
+  CUEVA_FSXZLAX, CUEVA_FSYXLAX, CUEVA_FSYYLAX, CUEVA_FSYZLAX,
   CUEVA_NFIELDS
 };
 
@@ -147,10 +156,23 @@ int32_t cueva_startconvar(cueva_ctx* ctx);
  * flowinit, 14_flowinit.f95:280-302: Exast(l), Bxint(l).., qint(l), W, V ->
  * Exint(l).., Jxint(l).. */
 int32_t cueva_electricvarint(cueva_ctx* ctx, int32_t l);
-/* {hll,hllc}_flow_mpx 2D + fluxandsource for stage l:
+/* the flux routine selected by flux_solver (main_cueva_code.f95:247-279) +
+ * fluxandsource for stage l:
  * psiint(l)..Szint(l), Exint(l).., Jxint(l).., V, p, rho, W ->
  * psiflux(l)..Szflux(l), Exastsour(l).. */
 int32_t cueva_flux_rhs(cueva_ctx* ctx, int32_t l);
+/* The same split at the reference's routine boundary.  cueva_flux_flow is the
+ * flux routine alone (lax_flow, hll_flow, hlle_flow, hllc_flow, hll_flow_mpx,
+ * hlle_flow_mpx or hllc_flow_mpx by flux_solver): same inputs as
+ * cueva_flux_rhs -> the 28 interface flux arrays of stage l (Exlaxpsi(l) ..
+ * FSyzlax(l)), each on the faces 17_fluxandsource.f95 reads: x arrays at
+ * i = -1..imax, j = 0..jmax, y arrays at i = 0..imax, j = -1..jmax (the rest
+ * of the arrays is left as it was).  cueva_fluxandsource is
+ * 17_fluxandsource.f95:433-699: those fluxes, psiint(l)..Szint(l), Exint(l)..,
+ * V, W -> psiflux(l)..Szflux(l), Exastsour(l)..  The two calls in a row give
+ * the result of cueva_flux_rhs bit for bit. */
+int32_t cueva_flux_flow(cueva_ctx* ctx, int32_t l);
+int32_t cueva_fluxandsource(cueva_ctx* ctx, int32_t l);
 /* varprimitivecardano / varprimitive_nr with l_swap = 1: D, tau, S, E, B and
  * the seeds V, rho, p -> V, rho, p */
 int32_t cueva_con2prim(cueva_ctx* ctx);

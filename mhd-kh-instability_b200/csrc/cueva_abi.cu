@@ -892,6 +892,110 @@ int32_t cueva_flux_rhs(cueva_ctx* c, int32_t l) {
   return read_status(c);
 }
 
+// ---------------------------------------- routine mirrors of the flux step
+namespace {
+// bound array of field f, stage l, element (i, j) (Fortran indices)
+double* host_at(cueva_ctx* c, int field, int l, int i, int j) {
+  return c->bound[field] + (size_t)(l - 1) * host_field_elems(c) + (size_t)(i + 6) +
+         (size_t)(j + 6) * (size_t)(c->imax + 13);
+}
+// interface flux fields by role (order of enum Role), x and y faces
+const int kFaceX[NFACE] = {CUEVA_EXLAXPSI, CUEVA_BXLAXPHI, CUEVA_PHILAXBX, CUEVA_EZLAXBY, CUEVA_EYLAXBZ,
+                           CUEVA_PSILAXEX, CUEVA_BZLAXEY, CUEVA_BYLAXEZ, CUEVA_JXLAX, CUEVA_FDXLAX,
+                           CUEVA_FTAUXLAX, CUEVA_FSXXLAX, CUEVA_FSXYLAX, CUEVA_FSXZLAX};
+const int kFaceY[NFACE] = {CUEVA_EYLAXPSI, CUEVA_BYLAXPHI, CUEVA_PHILAXBY, CUEVA_EXLAXBZ, CUEVA_EZLAXBX,
+                           CUEVA_PSILAXEY, CUEVA_BXLAXEZ, CUEVA_BZLAXEX, CUEVA_JYLAX, CUEVA_FDYLAX,
+                           CUEVA_FTAUYLAX, CUEVA_FSYYLAX, CUEVA_FSYZLAX, CUEVA_FSYXLAX};
+
+int32_t check_faces_bound(cueva_ctx* c) {
+  for (int r = 0; r < NFACE; ++r)
+    for (int f : {kFaceX[r], kFaceY[r]})
+      if (!c->bound[f]) return fail(CUEVA_ERR_UNBOUND, "field " + std::to_string(f) + " not bound");
+  return CUEVA_OK;
+}
+
+// the stage inputs shared by cueva_flux_rhs, cueva_flux_flow, cueva_fluxandsource
+int32_t upload_stage_inputs(cueva_ctx* c, int l) {
+  const int q = c->qin;
+  const int in[NSTAGE] = {CUEVA_PSIINT, CUEVA_PHIINT, CUEVA_EXINT, CUEVA_EYINT, CUEVA_EZINT, CUEVA_BXINT,
+                          CUEVA_BYINT, CUEVA_BZINT, CUEVA_QINT, CUEVA_DDINT, CUEVA_TAUINT, CUEVA_SXINT,
+                          CUEVA_SYINT, CUEVA_SZINT, CUEVA_JXINT, CUEVA_JYINT, CUEVA_JZINT};
+  for (int k = 0; k < NSTAGE; ++k)
+    if (int32_t e = h2d(c, stage_f(c, q, k), in[k], l)) return e;
+  for (int f : {P_VX, P_VY, P_VZ, P_P, P_RHO})
+    if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
+  return h2d(c, aux_f(c, c->cur, A_W), CUEVA_W, 1);
+}
+int32_t download_rhs(cueva_ctx* c, int l) {
+  const int out[NRHS] = {CUEVA_PSIFLUX, CUEVA_PHIFLUX, CUEVA_EXASTFLUX, CUEVA_EYASTFLUX, CUEVA_EZASTFLUX,
+                         CUEVA_BXFLUX, CUEVA_BYFLUX, CUEVA_BZFLUX, CUEVA_QFLUX, CUEVA_DFLUX, CUEVA_TAUFLUX,
+                         CUEVA_SXFLUX, CUEVA_SYFLUX, CUEVA_SZFLUX, CUEVA_EXASTSOUR, CUEVA_EYASTSOUR,
+                         CUEVA_EZASTSOUR};
+  for (int k = 0; k < NRHS; ++k)
+    if (int32_t e = d2h(c, c->h_inst.rhs_out + (long long)k * c->fstride, out[k], l)) return e;
+  return CUEVA_OK;
+}
+}  // namespace
+
+int32_t cueva_flux_flow(cueva_ctx* c, int32_t l) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (l < 1 || l > c->T.s) return fail(CUEVA_ERR_ARG, "stage index out of range");
+  if (int32_t e = check_faces_bound(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  if (int32_t e = upload_stage_inputs(c, l)) return e;
+  const StageArgs sa = stage_args(c, l, 2);
+  CUDA_TRY(launch_stage(c->P.rec_mp, c->P.flux_solver, c->P.precision, c->shape, c->stream, c->d_inst, 1, sa));
+  c->primed = false;
+  const InstDesc& I = c->h_inst;
+  const size_t hp = (size_t)(c->imax + 13) * 8;
+  // x faces i = -1..imax of rows 0..jmax: fx[j * fpitch + (i + 1)]
+  for (int r = 0; r < NFACE; ++r)
+    CUDA_TRY(cudaMemcpy2DAsync(host_at(c, kFaceX[r], l, -1, 0), hp, I.fx + r * I.ffs, (size_t)I.fpitch * 8,
+                               (size_t)(c->imax + 2) * 8, (size_t)(c->jmax + 1), cudaMemcpyDeviceToHost,
+                               c->stream));
+  // y faces j = -1..jmax of columns 0..imax: fy[(j + 1) * fpitch + i], FP32 in the mixed kernels
+  if (c->P.precision == 0) {
+    for (int r = 0; r < NFACE; ++r)
+      CUDA_TRY(cudaMemcpy2DAsync(host_at(c, kFaceY[r], l, 0, -1), hp, I.fy + r * I.ffs, (size_t)I.fpitch * 8,
+                                 (size_t)(c->imax + 1) * 8, (size_t)(c->jmax + 2), cudaMemcpyDeviceToHost,
+                                 c->stream));
+  } else {
+    std::vector<float> tmp((size_t)NFACE * (size_t)I.ffs);
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), I.fy, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < NFACE; ++r)
+      for (int j = -1; j <= c->jmax; ++j) {
+        double* dst = host_at(c, kFaceY[r], l, 0, j);
+        const float* src = tmp.data() + (size_t)r * I.ffs + (size_t)(j + 1) * I.fpitch;
+        for (int i = 0; i <= c->imax; ++i) dst[i] = double(src[i]);
+      }
+  }
+  return read_status(c);
+}
+
+int32_t cueva_fluxandsource(cueva_ctx* c, int32_t l) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (l < 1 || l > c->T.s) return fail(CUEVA_ERR_ARG, "stage index out of range");
+  if (int32_t e = check_faces_bound(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  if (int32_t e = upload_stage_inputs(c, l)) return e;
+  const InstDesc& I = c->h_inst;
+  const size_t hp = (size_t)(c->imax + 13) * 8;
+  for (int r = 0; r < NFACE; ++r) {
+    CUDA_TRY(cudaMemcpy2DAsync(I.fx + r * I.ffs, (size_t)I.fpitch * 8, host_at(c, kFaceX[r], l, -1, 0), hp,
+                               (size_t)(c->imax + 2) * 8, (size_t)(c->jmax + 1), cudaMemcpyHostToDevice,
+                               c->stream));
+    CUDA_TRY(cudaMemcpy2DAsync(I.fy + r * I.ffs, (size_t)I.fpitch * 8, host_at(c, kFaceY[r], l, 0, -1), hp,
+                               (size_t)(c->imax + 1) * 8, (size_t)(c->jmax + 2), cudaMemcpyHostToDevice,
+                               c->stream));
+  }
+  const StageArgs sa = stage_args(c, l, 1);
+  CUDA_TRY(launch_fluxandsource((long long)c->nx * c->ny, c->stream, c->d_inst, 1, sa));
+  c->primed = false;
+  if (int32_t e = download_rhs(c, l)) return e;
+  return read_status(c);
+}
+
 int32_t cueva_con2prim(cueva_ctx* c) {
   if (int32_t e = check_ctx(c)) return e;
   CUDA_TRY(cudaSetDevice(c->dev));

@@ -95,7 +95,7 @@ struct StageArgs {
   int store_k_slot;    // slot to store K_l, -1 if not needed
   int need_intsum_load;  // stage l >= 2 and s >= 3: intsum_l is stored
   int need_intsum_store; // l + 1 < s
-  int mode;            // 0 fused (next stage / final), 1 store rhs only
+  int mode;            // 0 fused (next stage / final), 1 store rhs only, 2 also the x-face fluxes (I.fx)
   double* diag_cons;   // last stage: D and tau of varfin stored here (2 slabs) when non-null
 };
 

@@ -108,6 +108,34 @@ __global__ void k_electricvarint(const InstDesc* __restrict__ insts, int cur, in
   }
 }
 
+// 17_fluxandsource.f95:433-699 on stored interface fluxes (the routine
+// mirror cueva_fluxandsource): Fx(i+1/2, j) in I.fx and Fy(i, j+1/2) in I.fy,
+// both FP64; the x differences are formed as in k_xupd, the rest is the same
+// update_point, so the result equals the fused stage's right-hand side
+__global__ void k_fluxandsource(const InstDesc* __restrict__ insts, StageArgs sa) {
+  const InstDesc& I = insts[blockIdx.y];
+  const int nx = I.imax + 1, ny = I.jmax + 1;
+  const long long fs = I.fstride;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = int(t % nx), j = int(t / nx);
+    const long long pc = (long long)j * I.pitch + i, fo = (long long)j * I.fpitch + i + 1;
+    double qx[NROLE];
+#pragma unroll
+    for (int c = 0; c < NROLE; ++c) {
+      const double d = I.fx[c * I.ffs + fo] - I.fx[c * I.ffs + fo - 1];
+      qx[c] = I.inv_delx_pow2 != 0.0 ? d * I.inv_delx_pow2 : d / I.delx;
+    }
+    const double* Q = I.stage[sa.qin];
+    const double* pv = I.prim[sa.cur];
+    const Centre cv{Q[Q_Q * fs + pc], Q[Q_PSI * fs + pc], Q[Q_PHI * fs + pc], Q[Q_EX * fs + pc],
+                    Q[Q_EY * fs + pc], Q[Q_EZ * fs + pc], Q[Q_BX * fs + pc], Q[Q_BY * fs + pc],
+                    Q[Q_BZ * fs + pc], pv[P_VX * fs + pc], pv[P_VY * fs + pc], pv[P_VZ * fs + pc]};
+    const uint32_t st = update_point<EP_RHS, double>(I, sa, i, j, qx, cv);
+    if (st) atomicOr(I.status, st);
+  }
+}
+
 // con2prim with l_swap = 1: the evolved D, tau, S in aux[cur] and E, B in
 // prim[cur]; seeds v, rho, p are the prims in prim[cur]; result overwrites prim[cur]
 __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
@@ -185,6 +213,10 @@ cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDes
 cudaError_t launch_recons_begin(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
                                 double abt11) {
   k_recons_begin<<<point_grid(npts, n), 256, 0, st>>>(d, cur, qout, abt11);
+  return cudaGetLastError();
+}
+cudaError_t launch_fluxandsource(long long npts, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa) {
+  k_fluxandsource<<<point_grid(npts, n), 256, 0, st>>>(d, sa);
   return cudaGetLastError();
 }
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur) {

@@ -655,6 +655,14 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
   for (int c = 0; c < NROLE; ++c) F[c] = T(0);
   uint32_t stt = 0;
   if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
+  if constexpr (EP == EP_RHS) {
+    // the routine mirror of the flux routine (mode 2) also stores the x-face
+    // fluxes; a face on a tile seam is stored by the tile of its right point
+    if (sa.mode == 2 && i <= ilast && (lane >= 1 || i == -1)) {
+#pragma unroll
+      for (int c = 0; c < NROLE; ++c) I.fx[c * I.ffs + (long long)j * I.fpitch + (i + 1)] = double(F[c]);
+    }
+  }
   // Fx(i-1/2) of point i is the face of lane-1
   const double dlx = I.delx, ix2 = I.inv_delx_pow2;
   double qx[NROLE];
@@ -711,7 +719,7 @@ static void launch_tiles(const StageShape& sh, cudaStream_t st, const InstDesc* 
   k_yface<RM, SV, T, ROWS><<<sh.grid[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sh.ntiles[LK_YFACE], sa);
   if (ev) cudaEventRecord(ev[1], st);
   const int gx = sh.grid[LK_XUPD], nt = sh.ntiles[LK_XUPD];
-  if (sa.mode == 1) k_xupd<RM, SV, T, EP_RHS, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
+  if (sa.mode >= 1) k_xupd<RM, SV, T, EP_RHS, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
   else if (sa.l < sa.s) k_xupd<RM, SV, T, EP_MID, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
   else k_xupd<RM, SV, T, EP_LAST, ROWS><<<gx, blk, G::bytes(0), st>>>(d, n, nt, sa);
   if (ev) cudaEventRecord(ev[2], st);

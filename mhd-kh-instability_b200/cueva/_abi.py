@@ -20,14 +20,22 @@ STAGE_FIELDS = ["psiint", "phiint", "Exint", "Eyint", "Ezint", "Bxint", "Byint",
                 "tauint", "Sxint", "Syint", "Szint", "Jxint", "Jyint", "Jzint", "Exast", "Eyast", "Ezast"]
 RHS_FIELDS = ["psiflux", "phiflux", "Exastflux", "Eyastflux", "Ezastflux", "Bxflux", "Byflux", "Bzflux",
               "qflux", "Dflux", "tauflux", "Sxflux", "Syflux", "Szflux", "Exastsour", "Eyastsour", "Ezastsour"]
-FIELDS = PRIM_FIELDS + CONS_FIELDS + STAGE_FIELDS + RHS_FIELDS
+# stage interface fluxes (the flux routines' outputs read by 17_fluxandsource.f95)
+FACE_FIELDS = ["Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "EzlaxBx", "EzlaxBy", "philaxBy",
+               "EylaxBz", "ExlaxBz", "psilaxEx", "BzlaxEx", "BzlaxEy", "psilaxEy", "BylaxEz", "BxlaxEz", "Jxlax",
+               "Jylax", "FDxlax", "FDylax", "Ftauxlax", "Ftauylax", "FSxxlax", "FSxylax", "FSxzlax", "FSyxlax",
+               "FSyylax", "FSyzlax"]
+# x-face arrays (flux through i+1/2); the others are y faces (j+1/2)
+FACE_X = {"Exlaxpsi", "Bxlaxphi", "philaxBx", "EzlaxBy", "EylaxBz", "psilaxEx", "BzlaxEy", "BylaxEz", "Jxlax",
+          "FDxlax", "Ftauxlax", "FSxxlax", "FSxylax", "FSxzlax"}
+FIELDS = PRIM_FIELDS + CONS_FIELDS + STAGE_FIELDS + RHS_FIELDS + FACE_FIELDS
 FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
-PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS)
+PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS) | set(FACE_FIELDS)
 
 EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
            "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
            "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
-           "cueva_electricvarint", "cueva_flux_rhs", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
+           "cueva_electricvarint", "cueva_flux_rhs", "cueva_flux_flow", "cueva_fluxandsource", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
            "cueva_mlp_destroy", "cueva_mlp_get_params", "cueva_mlp_set_params", "cueva_mlp_synthetic_pairs",
            "cueva_mlp_fit_normalisation", "cueva_mlp_train", "cueva_mlp_gradients", "cueva_mlp_predict",
            "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats", "cueva_ens_create", "cueva_ens_destroy",
@@ -112,6 +120,8 @@ def load(fma=False):
     L.cueva_startconvar.argtypes = [vp]
     L.cueva_electricvarint.argtypes = [vp, i32]
     L.cueva_flux_rhs.argtypes = [vp, i32]
+    L.cueva_flux_flow.argtypes = [vp, i32]
+    L.cueva_fluxandsource.argtypes = [vp, i32]
     L.cueva_con2prim.argtypes = [vp]
     L.cueva_kh_init.argtypes = [vp] + [dbl] * 9
     L.cueva_profile_steps.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(i32)]

@@ -6,7 +6,8 @@ arrays -- each field is dimensioned (-6:imax+6, -6:jmax+6) column-major
 (fourvectors.f95:12-170) -- binds them to a context, and exposes the
 routines the way main_cueva_code.f95 calls them: ``step`` replaces the body
 of the time loop (main_cueva_code.f95:53-328), and ``startconvar``,
-``electricvarint``, ``flux_rhs``, ``con2prim`` mirror the single routines.
+``electricvarint``, ``flux_flow``, ``fluxandsource`` (or both at once,
+``flux_rhs``), ``con2prim`` mirror the single routines.
 In numpy terms a field is an array of shape (jmax+13, imax+13) (C order,
 i fastest) and ``interior(name)`` is its [6:jmax+7, 6:imax+7] view.
 """
@@ -199,6 +200,28 @@ class Cueva:
         for n in _abi.RHS_FIELDS:
             self.array(n)
         _abi.check(self.L, self.L.cueva_flux_rhs(self.ctx, int(l)))
+
+    def flux_flow(self, l):
+        """The flux routine alone (lax_flow / hll*_flow / hll*_flow_mpx by
+        flux_solver): fills the 28 interface flux arrays of stage l on the
+        faces fluxandsource reads (see ``faces``)."""
+        for n in _abi.FACE_FIELDS:
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_flux_flow(self.ctx, int(l)))
+
+    def fluxandsource(self, l):
+        """17_fluxandsource.f95 on the bound interface flux arrays of stage l."""
+        for n in _abi.FACE_FIELDS + _abi.RHS_FIELDS:
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_fluxandsource(self.ctx, int(l)))
+
+    def faces(self, name, l):
+        """View of an interface flux array on the faces the divergence reads:
+        x arrays at i = -1..imax, j = 0..jmax; y arrays at i = 0..imax, j = -1..jmax."""
+        a = self.array(name)[l - 1]
+        if name in _abi.FACE_X:
+            return a[6:self.jmax + 7, 5:self.imax + 7]
+        return a[5:self.jmax + 7, 6:self.imax + 7]
 
     def con2prim(self):
         _abi.check(self.L, self.L.cueva_con2prim(self.ctx))

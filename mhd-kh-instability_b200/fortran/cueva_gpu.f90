@@ -38,6 +38,17 @@ module cueva_gpu
   integer(c_int32_t), parameter :: CUEVA_TAUFLUX = 50, CUEVA_SXFLUX = 51, CUEVA_SYFLUX = 52
   integer(c_int32_t), parameter :: CUEVA_SZFLUX = 53, CUEVA_EXASTSOUR = 54, CUEVA_EYASTSOUR = 55
   integer(c_int32_t), parameter :: CUEVA_EZASTSOUR = 56
+  ! stage interface fluxes (outputs of the flux routines, fourvectors.f95)
+  integer(c_int32_t), parameter :: CUEVA_EXLAXPSI = 57, CUEVA_EYLAXPSI = 58, CUEVA_BXLAXPHI = 59
+  integer(c_int32_t), parameter :: CUEVA_BYLAXPHI = 60, CUEVA_PHILAXBX = 61, CUEVA_EZLAXBX = 62
+  integer(c_int32_t), parameter :: CUEVA_EZLAXBY = 63, CUEVA_PHILAXBY = 64, CUEVA_EYLAXBZ = 65
+  integer(c_int32_t), parameter :: CUEVA_EXLAXBZ = 66, CUEVA_PSILAXEX = 67, CUEVA_BZLAXEX = 68
+  integer(c_int32_t), parameter :: CUEVA_BZLAXEY = 69, CUEVA_PSILAXEY = 70, CUEVA_BYLAXEZ = 71
+  integer(c_int32_t), parameter :: CUEVA_BXLAXEZ = 72, CUEVA_JXLAX = 73, CUEVA_JYLAX = 74
+  integer(c_int32_t), parameter :: CUEVA_FDXLAX = 75, CUEVA_FDYLAX = 76, CUEVA_FTAUXLAX = 77
+  integer(c_int32_t), parameter :: CUEVA_FTAUYLAX = 78, CUEVA_FSXXLAX = 79, CUEVA_FSXYLAX = 80
+  integer(c_int32_t), parameter :: CUEVA_FSXZLAX = 81, CUEVA_FSYXLAX = 82, CUEVA_FSYYLAX = 83
+  integer(c_int32_t), parameter :: CUEVA_FSYZLAX = 84
 
   type, bind(c) :: cueva_params
      integer(c_int32_t) :: imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y
@@ -120,6 +131,16 @@ module cueva_gpu
        type(c_ptr), value :: ctx
        integer(c_int32_t), value :: l
      end function cueva_flux_rhs
+     integer(c_int32_t) function cueva_flux_flow(ctx, l) bind(c, name="cueva_flux_flow")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: l
+     end function cueva_flux_flow
+     integer(c_int32_t) function cueva_fluxandsource(ctx, l) bind(c, name="cueva_fluxandsource")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: l
+     end function cueva_fluxandsource
      integer(c_int32_t) function cueva_con2prim(ctx) bind(c, name="cueva_con2prim")
        import :: c_int32_t, c_ptr
        type(c_ptr), value :: ctx

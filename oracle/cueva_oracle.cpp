@@ -2235,6 +2235,20 @@ int32_t oracle_get_named(void* h, const char* name, int32_t l, double* out) {
     for (int i = 0; i <= o->imax; ++i) out[(size_t)i + (size_t)j * (o->imax + 1)] = src[o->id(i, j)];
   return 0;
 }
+// the whole ghosted array (-6..imax+6) x (-6..jmax+6), i fastest
+int32_t oracle_get_named_full(void* h, const char* name, int32_t l, double* out) {
+  Oracle* o = static_cast<Oracle*>(h);
+  const double* src = nullptr;
+  auto it = o->A.find(name);
+  if (it != o->A.end()) src = it->second.data();
+  else if (l >= 1 && l <= o->lmax) {
+    auto jt = o->K[l - 1].find(name);
+    if (jt != o->K[l - 1].end()) src = jt->second.data();
+  }
+  if (!src) return -1;
+  std::copy(src, src + o->ng, out);
+  return 0;
+}
 void oracle_counters(void* h, int64_t* out3) {
   Oracle* o = static_cast<Oracle*>(h);
   for (int c = 0; c < 3; ++c) out3[c] = o->counters[c];

@@ -67,6 +67,8 @@ int32_t oracle_run_stages(void* h, int32_t upto);
 /* interior copy of a named internal array ("psiflux", "Exastsour", "Exlaxpsi",
  * "Exint", "Jxint", "D", "tau", ...); l selects the stage for per-stage arrays */
 int32_t oracle_get_named(void* h, const char* name, int32_t l, double* out);
+/* the whole ghosted array, (jmax+13) x (imax+13), element (i, j) at (i+6) + (j+6)*(imax+13) */
+int32_t oracle_get_named_full(void* h, const char* name, int32_t l, double* out);
 void    oracle_counters(void* h, int64_t* out3);
 
 /* KH initial data in the reference orientation (x_ref = BASELINE y, copy;

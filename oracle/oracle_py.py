@@ -54,6 +54,8 @@ def lib():
         L.oracle_run_stages.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.oracle_get_named.restype = ctypes.c_int32
         L.oracle_get_named.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, dp]
+        L.oracle_get_named_full.restype = ctypes.c_int32
+        L.oracle_get_named_full.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, dp]
         L.oracle_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         L.oracle_kh_init.argtypes = [ctypes.c_int32, ctypes.c_int32] + [ctypes.c_double] * 11 + \
             [ctypes.POINTER(dp)]
@@ -134,6 +136,13 @@ class Oracle:
     def named(self, name, l=1):
         out = np.empty(self.shape)
         if lib().oracle_get_named(self.h, name.encode(), int(l), _dp(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def named_full(self, name, l=1):
+        """The whole ghosted array, shape (jmax+13, imax+13): element (i, j) at [j+6, i+6]."""
+        out = np.empty((self.jmax + 13, self.imax + 13))
+        if lib().oracle_get_named_full(self.h, name.encode(), int(l), _dp(out)) != 0:
             raise KeyError(name)
         return out
 

@@ -40,6 +40,15 @@ def test_python_field_table_matches_header():
     assert [e.lower() for e in enum] == [f.lower() for f in _abi.FIELDS]
 
 
+def test_fortran_module_field_ids_match_header():
+    """fortran/cueva_gpu.f90 names every field id of enum cueva_field with
+    the same value (the Fortran side binds its arrays by these numbers)."""
+    text = open(os.path.join(ROOT, "mhd-kh-instability_b200", "fortran", "cueva_gpu.f90")).read()
+    ids = {m.group(1).upper(): int(m.group(2)) for m in re.finditer(r"CUEVA_(\w+)\s*=\s*(\d+)", text)}
+    for k, name in enumerate(_field_enum()):
+        assert ids.get(name.upper()) == k, (name, ids.get(name.upper()), k)
+
+
 def test_params_struct_layout():
     from cueva import _abi
     # 12 int32 then 7 doubles, as declared in cueva.h

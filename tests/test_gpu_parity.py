@@ -243,3 +243,36 @@ def test_mixed_precision_close_to_fp64_oracle(oracle_mod, solver):
     print(f"solver {solver}: worst 1-step {max(v for (s, _), v in worst.items() if s == 1):.2e}, "
           f"20-step {max(v for (s, _), v in worst.items() if s == 19):.2e}")
     g.close()
+
+
+@pytest.mark.parametrize("solver,rec", [(1, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 1), (7, 2)])
+def test_flux_routine_mirror_interface_fluxes_exact(oracle_mod, solver, rec):
+    """cueva_flux_flow is the flux routine alone: its 28 interface flux arrays
+    (Exlaxpsi .. FSyzlax) equal the oracle's bit for bit on the faces
+    17_fluxandsource.f95 reads, and cueva_fluxandsource on them gives the
+    right-hand side of cueva_flux_rhs bit for bit."""
+    from cueva import _abi
+    imax, jmax = 45, 38   # ragged tiles and non-power-of-two spacings
+    g, o = _pair(oracle_mod, imax, jmax, False, order=2, flux_solver=solver, rec_mp=rec, sigma=1e3)
+    _kh(g, o)
+    o.run_stages(1)
+    for n, on in STAGE_MAP.items():
+        g.set_interior(n, o.named(on), l=1)
+    for n in PRIMS:
+        g.set_interior(n, o.get_prims()[n])
+    g.set_interior("W", o.named("W"))
+    g.flux_flow(1)
+    for n in _abi.FACE_FIELDS:
+        ref = o.named_full(n)
+        ref = ref[6:jmax + 7, 5:imax + 7] if n in _abi.FACE_X else ref[5:jmax + 7, 6:imax + 7]
+        got = g.faces(n, 1)
+        assert got.shape == ref.shape
+        nbad = int((got != ref).sum())
+        assert nbad == 0, f"{n}: {nbad} of {got.size} faces differ"
+    g.fluxandsource(1)
+    split = {n: g.interior(n, 1).copy() for n in RHS}
+    g.flux_rhs(1)
+    for n in RHS:
+        assert np.array_equal(split[n], g.interior(n, 1)), n
+        assert np.array_equal(split[n], o.named(n, 1)), n
+    g.close()
