@@ -98,6 +98,10 @@ enum cueva_field {
   CUEVA_BZLAXEY, CUEVA_PSILAXEY, CUEVA_BYLAXEZ, CUEVA_BXLAXEZ, CUEVA_JXLAX, CUEVA_JYLAX,
   CUEVA_FDXLAX, CUEVA_FDYLAX, CUEVA_FTAUXLAX, CUEVA_FTAUYLAX, CUEVA_FSXXLAX, CUEVA_FSXYLAX,
   CUEVA_FSXZLAX, CUEVA_FSYXLAX, CUEVA_FSYYLAX, CUEVA_FSYZLAX,
+  /* final stage sums (threevectors.f95), the increments of varfin / electricfield */
+  CUEVA_PSIFINSUM, CUEVA_PHIFINSUM, CUEVA_BXFINSUM, CUEVA_BYFINSUM, CUEVA_BZFINSUM, CUEVA_EXFINSUM,
+  CUEVA_EYFINSUM, CUEVA_EZFINSUM, CUEVA_QFINSUM, CUEVA_DFINSUM, CUEVA_TAUFINSUM, CUEVA_SXFINSUM,
+  CUEVA_SYFINSUM, CUEVA_SZFINSUM,
   CUEVA_NFIELDS
 };
 
@@ -173,6 +177,12 @@ int32_t cueva_flux_rhs(cueva_ctx* ctx, int32_t l);
  * the result of cueva_flux_rhs bit for bit. */
 int32_t cueva_flux_flow(cueva_ctx* ctx, int32_t l);
 int32_t cueva_fluxandsource(cueva_ctx* ctx, int32_t l);
+/* varfin (19_varfin.f95:16-54): psi, phi, B, q, D, tau, S += Delt * their
+ * final sums; electricfield (20_electricfield.f95:153-167, IMEX):
+ * E += Delt * Exfinsum.. (the same update the fused step applies after its
+ * last stage) */
+int32_t cueva_varfin(cueva_ctx* ctx);
+int32_t cueva_electricfield(cueva_ctx* ctx);
 /* varprimitivecardano / varprimitive_nr with l_swap = 1: D, tau, S, E, B and
  * the seeds V, rho, p -> V, rho, p */
 int32_t cueva_con2prim(cueva_ctx* ctx);

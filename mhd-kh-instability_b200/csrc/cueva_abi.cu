@@ -996,6 +996,55 @@ int32_t cueva_fluxandsource(cueva_ctx* c, int32_t l) {
   return read_status(c);
 }
 
+namespace {
+// varfin / electricfield: the bound final sums and fields of the Q slots in
+// mask go up, U += Delt * finsum on the device, the fields come back
+int32_t add_finsum(cueva_ctx* c, uint32_t mask) {
+  CUDA_TRY(cudaSetDevice(c->dev));
+  struct Slot { int q, fin, field; double* dev; };
+  const InstDesc& I = c->h_inst;
+  const long long fs = c->fstride;
+  const Slot slots[NCONS] = {
+      {Q_PSI, CUEVA_PSIFINSUM, CUEVA_PSI, prim_f(c, c->cur, P_PSI)},
+      {Q_PHI, CUEVA_PHIFINSUM, CUEVA_PHI, prim_f(c, c->cur, P_PHI)},
+      {Q_EX, CUEVA_EXFINSUM, CUEVA_EX, prim_f(c, c->cur, P_EX)},
+      {Q_EY, CUEVA_EYFINSUM, CUEVA_EY, prim_f(c, c->cur, P_EY)},
+      {Q_EZ, CUEVA_EZFINSUM, CUEVA_EZ, prim_f(c, c->cur, P_EZ)},
+      {Q_BX, CUEVA_BXFINSUM, CUEVA_BX, prim_f(c, c->cur, P_BX)},
+      {Q_BY, CUEVA_BYFINSUM, CUEVA_BY, prim_f(c, c->cur, P_BY)},
+      {Q_BZ, CUEVA_BZFINSUM, CUEVA_BZ, prim_f(c, c->cur, P_BZ)},
+      {Q_Q, CUEVA_QFINSUM, CUEVA_Q, prim_f(c, c->cur, P_Q)},
+      {Q_D, CUEVA_DFINSUM, CUEVA_D, aux_f(c, c->cur, A_D)},
+      {Q_TAU, CUEVA_TAUFINSUM, CUEVA_TAU, aux_f(c, c->cur, A_TAU)},
+      {Q_SX, CUEVA_SXFINSUM, CUEVA_SX, aux_f(c, c->cur, A_SX)},
+      {Q_SY, CUEVA_SYFINSUM, CUEVA_SY, aux_f(c, c->cur, A_SY)},
+      {Q_SZ, CUEVA_SZFINSUM, CUEVA_SZ, aux_f(c, c->cur, A_SZ)}};
+  for (const Slot& s : slots) {
+    if (!(mask >> s.q & 1u)) continue;
+    if (int32_t e = h2d(c, I.finsum + s.q * fs, s.fin, 1)) return e;
+    if (int32_t e = h2d(c, s.dev, s.field, 1)) return e;
+  }
+  CUDA_TRY(launch_add_finsum((long long)c->nx * c->ny, c->stream, c->d_inst, 1, c->cur, mask));
+  c->primed = false;
+  for (const Slot& s : slots)
+    if (mask >> s.q & 1u)
+      if (int32_t e = d2h(c, s.dev, s.field, 1)) return e;
+  return read_status(c);
+}
+}  // namespace
+
+int32_t cueva_varfin(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  uint32_t mask = 0;
+  for (int q : {Q_PSI, Q_PHI, Q_BX, Q_BY, Q_BZ, Q_Q, Q_D, Q_TAU, Q_SX, Q_SY, Q_SZ}) mask |= 1u << q;
+  return add_finsum(c, mask);
+}
+
+int32_t cueva_electricfield(cueva_ctx* c) {
+  if (int32_t e = check_ctx(c)) return e;
+  return add_finsum(c, (1u << Q_EX) | (1u << Q_EY) | (1u << Q_EZ));
+}
+
 int32_t cueva_con2prim(cueva_ctx* c) {
   if (int32_t e = check_ctx(c)) return e;
   CUDA_TRY(cudaSetDevice(c->dev));

@@ -136,6 +136,29 @@ __global__ void k_fluxandsource(const InstDesc* __restrict__ insts, StageArgs sa
   }
 }
 
+// varfin / electricfield (19_varfin.f95:16-54, 20_electricfield.f95:153-167):
+// U += dt * finsum for the conserved slots of mask (bit Q_*), U being the
+// carried primitive (psi, phi, E, B, q) or the time-n conserved (D, tau, S)
+__global__ void k_add_finsum(const InstDesc* __restrict__ insts, int cur, uint32_t mask) {
+  const InstDesc& I = insts[blockIdx.y];
+  const int nx = I.imax + 1, ny = I.jmax + 1;
+  const long long fs = I.fstride;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * ny;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = int(t % nx), j = int(t / nx);
+    const long long pc = (long long)j * I.pitch + i;
+#pragma unroll
+    for (int c = 0; c < NCONS; ++c) {
+      if (!(mask >> c & 1u)) continue;
+      double* u = (c < Q_D) ? I.prim[cur] + (long long)(c == Q_PSI ? P_PSI : c == Q_PHI ? P_PHI
+                                                          : c <= Q_EZ ? P_EX + (c - Q_EX)
+                                                          : c <= Q_BZ ? P_BX + (c - Q_BX) : P_Q) * fs
+                            : I.aux[cur] + (long long)(A_D + (c - Q_D)) * fs;
+      u[pc] = u[pc] + I.dt * I.finsum[c * fs + pc];
+    }
+  }
+}
+
 // con2prim with l_swap = 1: the evolved D, tau, S in aux[cur] and E, B in
 // prim[cur]; seeds v, rho, p are the prims in prim[cur]; result overwrites prim[cur]
 __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
@@ -217,6 +240,10 @@ cudaError_t launch_recons_begin(long long npts, cudaStream_t st, const InstDesc*
 }
 cudaError_t launch_fluxandsource(long long npts, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa) {
   k_fluxandsource<<<point_grid(npts, n), 256, 0, st>>>(d, sa);
+  return cudaGetLastError();
+}
+cudaError_t launch_add_finsum(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, uint32_t mask) {
+  k_add_finsum<<<point_grid(npts, n), 256, 0, st>>>(d, cur, mask);
   return cudaGetLastError();
 }
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur) {

@@ -50,6 +50,8 @@ cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* 
 cudaError_t launch_electricvarint(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int q,
                                   double abtll);
 cudaError_t launch_con2prim(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);
+// varfin / electricfield: U += dt * finsum for the conserved slots in mask (bit Q_*)
+cudaError_t launch_add_finsum(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, uint32_t mask);
 // 17_fluxandsource.f95 on the stored interface fluxes I.fx / I.fy (FP64): rhs_out of stage sa.l
 cudaError_t launch_fluxandsource(long long npts, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa);
 // primitive reconstruction of prim[cur] into prim[1 - cur] + startconvar and

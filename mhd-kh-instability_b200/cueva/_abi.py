@@ -28,14 +28,17 @@ FACE_FIELDS = ["Exlaxpsi", "Eylaxpsi", "Bxlaxphi", "Bylaxphi", "philaxBx", "Ezla
 # x-face arrays (flux through i+1/2); the others are y faces (j+1/2)
 FACE_X = {"Exlaxpsi", "Bxlaxphi", "philaxBx", "EzlaxBy", "EylaxBz", "psilaxEx", "BzlaxEy", "BylaxEz", "Jxlax",
           "FDxlax", "Ftauxlax", "FSxxlax", "FSxylax", "FSxzlax"}
-FIELDS = PRIM_FIELDS + CONS_FIELDS + STAGE_FIELDS + RHS_FIELDS + FACE_FIELDS
+# final stage sums (increments of varfin / electricfield)
+FINSUM_FIELDS = ["psifinsum", "phifinsum", "Bxfinsum", "Byfinsum", "Bzfinsum", "Exfinsum", "Eyfinsum", "Ezfinsum",
+                 "qfinsum", "Dfinsum", "taufinsum", "Sxfinsum", "Syfinsum", "Szfinsum"]
+FIELDS = PRIM_FIELDS + CONS_FIELDS + STAGE_FIELDS + RHS_FIELDS + FACE_FIELDS + FINSUM_FIELDS
 FIELD_ID = {n: k for k, n in enumerate(FIELDS)}
 PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS) | set(FACE_FIELDS)
 
 EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
            "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
            "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
-           "cueva_electricvarint", "cueva_flux_rhs", "cueva_flux_flow", "cueva_fluxandsource", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
+           "cueva_electricvarint", "cueva_flux_rhs", "cueva_flux_flow", "cueva_fluxandsource", "cueva_varfin", "cueva_electricfield", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
            "cueva_mlp_destroy", "cueva_mlp_get_params", "cueva_mlp_set_params", "cueva_mlp_synthetic_pairs",
            "cueva_mlp_fit_normalisation", "cueva_mlp_train", "cueva_mlp_gradients", "cueva_mlp_predict",
            "cueva_c2p_batch", "cueva_attach_mlp", "cueva_learned_stats", "cueva_ens_create", "cueva_ens_destroy",
@@ -122,6 +125,8 @@ def load(fma=False):
     L.cueva_flux_rhs.argtypes = [vp, i32]
     L.cueva_flux_flow.argtypes = [vp, i32]
     L.cueva_fluxandsource.argtypes = [vp, i32]
+    L.cueva_varfin.argtypes = [vp]
+    L.cueva_electricfield.argtypes = [vp]
     L.cueva_con2prim.argtypes = [vp]
     L.cueva_kh_init.argtypes = [vp] + [dbl] * 9
     L.cueva_profile_steps.argtypes = [vp, i32, ctypes.POINTER(dbl), ctypes.POINTER(i32)]

@@ -7,7 +7,8 @@ arrays -- each field is dimensioned (-6:imax+6, -6:jmax+6) column-major
 routines the way main_cueva_code.f95 calls them: ``step`` replaces the body
 of the time loop (main_cueva_code.f95:53-328), and ``startconvar``,
 ``electricvarint``, ``flux_flow``, ``fluxandsource`` (or both at once,
-``flux_rhs``), ``con2prim`` mirror the single routines.
+``flux_rhs``), ``varfin``, ``electricfield``, ``con2prim`` mirror the single
+routines.
 In numpy terms a field is an array of shape (jmax+13, imax+13) (C order,
 i fastest) and ``interior(name)`` is its [6:jmax+7, 6:imax+7] view.
 """
@@ -222,6 +223,18 @@ class Cueva:
         if name in _abi.FACE_X:
             return a[6:self.jmax + 7, 5:self.imax + 7]
         return a[5:self.jmax + 7, 6:self.imax + 7]
+
+    def varfin(self):
+        """19_varfin.f95: psi, phi, B, q, D, tau, S += dt * their final sums."""
+        for n in _abi.FINSUM_FIELDS:
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_varfin(self.ctx))
+
+    def electricfield(self):
+        """20_electricfield.f95 (IMEX): E += dt * Exfinsum .."""
+        for n in _abi.FINSUM_FIELDS:
+            self.array(n)
+        _abi.check(self.L, self.L.cueva_electricfield(self.ctx))
 
     def con2prim(self):
         _abi.check(self.L, self.L.cueva_con2prim(self.ctx))

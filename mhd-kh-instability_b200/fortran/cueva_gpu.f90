@@ -49,6 +49,12 @@ module cueva_gpu
   integer(c_int32_t), parameter :: CUEVA_FTAUYLAX = 78, CUEVA_FSXXLAX = 79, CUEVA_FSXYLAX = 80
   integer(c_int32_t), parameter :: CUEVA_FSXZLAX = 81, CUEVA_FSYXLAX = 82, CUEVA_FSYYLAX = 83
   integer(c_int32_t), parameter :: CUEVA_FSYZLAX = 84
+  ! final stage sums (increments of varfin / electricfield)
+  integer(c_int32_t), parameter :: CUEVA_PSIFINSUM = 85, CUEVA_PHIFINSUM = 86, CUEVA_BXFINSUM = 87
+  integer(c_int32_t), parameter :: CUEVA_BYFINSUM = 88, CUEVA_BZFINSUM = 89, CUEVA_EXFINSUM = 90
+  integer(c_int32_t), parameter :: CUEVA_EYFINSUM = 91, CUEVA_EZFINSUM = 92, CUEVA_QFINSUM = 93
+  integer(c_int32_t), parameter :: CUEVA_DFINSUM = 94, CUEVA_TAUFINSUM = 95, CUEVA_SXFINSUM = 96
+  integer(c_int32_t), parameter :: CUEVA_SYFINSUM = 97, CUEVA_SZFINSUM = 98
 
   type, bind(c) :: cueva_params
      integer(c_int32_t) :: imax, jmax, order, flux_solver, rec_mp, c2p, bc_x, bc_y
@@ -141,6 +147,14 @@ module cueva_gpu
        type(c_ptr), value :: ctx
        integer(c_int32_t), value :: l
      end function cueva_fluxandsource
+     integer(c_int32_t) function cueva_varfin(ctx) bind(c, name="cueva_varfin")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_varfin
+     integer(c_int32_t) function cueva_electricfield(ctx) bind(c, name="cueva_electricfield")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+     end function cueva_electricfield
      integer(c_int32_t) function cueva_con2prim(ctx) bind(c, name="cueva_con2prim")
        import :: c_int32_t, c_ptr
        type(c_ptr), value :: ctx

@@ -276,3 +276,24 @@ def test_flux_routine_mirror_interface_fluxes_exact(oracle_mod, solver, rec):
         assert np.array_equal(split[n], g.interior(n, 1)), n
         assert np.array_equal(split[n], o.named(n, 1)), n
     g.close()
+
+
+def test_varfin_electricfield_mirrors(oracle_mod):
+    """cueva_varfin / cueva_electricfield: U + Delt * finsum after the last
+    stage's sumfin, on the oracle's own final sums and time-n state."""
+    imax, jmax = 45, 38
+    g, o = _pair(oracle_mod, imax, jmax, False, order=4, flux_solver=7, rec_mp=0, sigma=1e3)
+    _kh(g, o)
+    o.run_stages(g.lmax)
+    fin = {"psi": "psifinsum", "phi": "phifinsum", "Bx": "Bxfinsum", "By": "Byfinsum", "Bz": "Bzfinsum",
+           "q": "qfinsum", "D": "Dfinsum", "tau": "taufinsum", "Sx": "Sxfinsum", "Sy": "Syfinsum", "Sz": "Szfinsum",
+           "Ex": "Exfinsum", "Ey": "Eyfinsum", "Ez": "Ezfinsum"}
+    for n, f in fin.items():
+        g.set_interior(f, o.named(f))
+        g.set_interior(n, o.named(n))
+    g.varfin()
+    g.electricfield()
+    assert g.dt == o.dt
+    for n, f in fin.items():
+        assert np.array_equal(g.interior(n), o.named(n) + o.dt * o.named(f)), n
+    g.close()
