@@ -335,3 +335,86 @@ def test_lax_right_state_takes_the_slopes_of_p(oracle_mod):
     assert np.allclose(fdy[1:-2, :], -0.005, rtol=0, atol=1e-14)
     # the charge flux pairs J with q: both vanish here
     assert np.all(o.named("Jxlax", 1) == 0.0)
+
+
+def _uniform_prims(imax, jmax):
+    v = np.array([0.3, -0.2, 0.1])
+    B = np.array([0.1, 0.2, -0.05])
+    E = -np.cross(v, B)
+    shape = (jmax + 1, imax + 1)
+    pr = {"rho": np.full(shape, 1.3), "p": np.full(shape, 0.7), "psi": np.zeros(shape), "phi": np.zeros(shape),
+          "q": np.zeros(shape)}
+    for c, n in enumerate("xyz"):
+        pr["v" + n] = np.full(shape, v[c])
+        pr["E" + n] = np.full(shape, E[c])
+        pr["B" + n] = np.full(shape, B[c])
+    return pr, v, E, B
+
+
+@pytest.mark.parametrize("solver", [1, 2, 3, 4, 5, 6, 7])
+def test_interface_flux_consistent_on_uniform_state(oracle_mod, solver):
+    """F(U, U) = F(U): on a uniform state every flux routine returns the
+    physical flux of the state on every face (the Maxwell, cleaning and
+    fluid parts; the sign-flipped arrays EzlaxBy / BylaxEz / ExlaxBz /
+    BzlaxEx hold -F) -- except the reference's own HLLE-MC energy flux, which
+    is pinned to its closed form instead."""
+    imax, jmax = 16, 12
+    pr, v, E, B = _uniform_prims(imax, jmax)
+    o = oracle_mod.Oracle(imax, jmax, order=1, flux_solver=solver, bc_x=0, bc_y=1, sigma=1e3)
+    o.set_prims(pr)
+    assert o.run_stages(1) == 0
+    gam = 4.0 / 3.0
+    rho, p = 1.3, 0.7
+    W = 1.0 / np.sqrt(1.0 - v @ v)
+    h = rho * (1.0 + p / ((gam - 1.0) * rho)) + p
+    # stage-1 E is the implicit solve of E = -v x B, which returns it up to rounding
+    Ex, Ey, Ez = (o.named(n)[0, 0] for n in ("Exint", "Eyint", "Ezint"))
+    D = rho * W
+    expect = {
+        "Exlaxpsi": Ex, "Eylaxpsi": Ey, "Bxlaxphi": B[0], "Bylaxphi": B[1], "philaxBx": 0.0, "philaxBy": 0.0,
+        "psilaxEx": 0.0, "psilaxEy": 0.0, "EylaxBz": Ey, "EzlaxBx": Ez, "EzlaxBy": Ez, "ExlaxBz": Ex,
+        "BzlaxEy": B[2], "BxlaxEz": B[0], "BylaxEz": B[1], "BzlaxEx": B[2],
+        "FDxlax": D * v[0], "FDylax": D * v[1],
+        "Ftauxlax": (B[2] * Ey - B[1] * Ez) + h * W**2 * v[0],
+        "Ftauylax": (B[0] * Ez - B[2] * Ex) + h * W**2 * v[1],
+        "FSxylax": -Ex * Ey - B[0] * B[1] + h * W**2 * v[0] * v[1],
+    }
+    if solver == 3:
+        # the reference's HLLE-MC star energy (16_hlle_flow_mcl.f95, taustr_*)
+        # is not consistent: on a uniform state with v* = vn,
+        # tau*_L = tau - |E,B|^2/2 vn/(vn - s1) and tau*_R = tau + |E,B|^2/2 vn/(s2 - vn),
+        # so the star flux F + s (tau* - tau) is off by that much (s1, s2 the
+        # HLLE bounds, with the reference's vn under the root)
+        Cs = np.sqrt(gam * p / h)
+        V2 = v @ v
+        eb2 = 0.5 * ((Ex**2 + Ey**2 + Ez**2) + (B @ B))
+        for name, vn in (("Ftauxlax", v[0]), ("Ftauylax", v[1])):
+            root = np.sqrt((1.0 - V2) * (1.0 - V2 * Cs**2 - vn * (1.0 - Cs**2)))
+            s1 = (vn * (1.0 - Cs**2) - Cs * root) / (1.0 - Cs**2 * V2)
+            s2 = (vn * (1.0 - Cs**2) + Cs * root) / (1.0 - Cs**2 * V2)
+            assert s1 < 0.0 < s2
+            expect[name] += (-s1 * eb2 * vn / (vn - s1)) if vn >= 0.0 else (s2 * eb2 * vn / (s2 - vn))
+    for name, val in expect.items():
+        got = o.named(name)[1:-1, 1:-1]
+        np.testing.assert_allclose(got, val, rtol=1e-12, atol=1e-14, err_msg=f"{solver} {name}")
+
+
+def test_hllc_em_fluxes_equal_hll(oracle_mod):
+    """HLLC (flux_solver 7) keeps the HLL fluxes of the Maxwell equations
+    (16_hllc_flow_mpx.f95 star EM fluxes are the HLL ones), bit for bit; only
+    psi, phi and the fluid fluxes receive the contact correction."""
+    imax, jmax = 32, 16
+    pr = oracle_mod.kh_init(imax, jmax, v0=0.5, a=0.05)
+    arrs = {}
+    for solver in (5, 7):
+        o = oracle_mod.Oracle(imax, jmax, order=1, flux_solver=solver, sigma=1e3)
+        o.set_prims(pr)
+        assert o.run_stages(1) == 0
+        arrs[solver] = {n: o.named(n) for n in ("philaxBx", "EzlaxBy", "EylaxBz", "psilaxEx", "BzlaxEy", "BylaxEz",
+                                                 "EzlaxBx", "philaxBy", "ExlaxBz", "BzlaxEx", "psilaxEy", "BxlaxEz",
+                                                 "FDxlax")}
+    for n in arrs[5]:
+        if n == "FDxlax":
+            assert not np.array_equal(arrs[5][n], arrs[7][n]), n   # corrected by the contact
+        else:
+            assert np.array_equal(arrs[5][n], arrs[7][n]), n
