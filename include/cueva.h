@@ -129,6 +129,14 @@ int32_t cueva_upload(cueva_ctx* ctx, uint32_t groups);
  * caller's boundary routine, as main_cueva_code.f95:328 does); synchronises
  * and reports kernel status */
 int32_t cueva_download(cueva_ctx* ctx, uint32_t groups);
+/* cueva_download without the wait: the copies run on a second stream, after
+ * the work already queued on the context stream, one field after another.
+ * The host arrays hold the result after the next cueva_sync (or cueva_download,
+ * cueva_step, ...: every later call orders its work after the readback).  A
+ * following cueva_upload of the same arrays waits per field, so field f goes
+ * back up while field f+1 still comes down.  Kernel status is reported by the
+ * next call that synchronises. */
+int32_t cueva_download_async(cueva_ctx* ctx, uint32_t groups);
 
 /* ---- the hot path ----------------------------------------------------- */
 /* nsteps executions of the body of the time loop, main_cueva_code.f95:53-328

@@ -253,12 +253,33 @@ struct cueva_ctx {
   cueva_diag_record* d_diag_rec = nullptr;// ring of diag.capacity records
   long long diag_written = 0, diag_read = 0;
   cudaGraphExec_t graph_diag[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  // cueva_download_async: copies on a second stream, one event per field
+  // (14 prims, then the 6 conserved fields), so that the next upload of field
+  // f waits only for field f's readback
+  cudaStream_t xfer = nullptr;
+  cudaEvent_t ev_ready = nullptr, ev_xfer_done = nullptr;
+  cudaEvent_t ev_field[NPRIM + NAUX] = {};
+  bool dl_pending = false;
+  bool field_pending[NPRIM + NAUX] = {};
 };
 
 namespace {
 
-int32_t check_ctx(cueva_ctx* c) {
+// Orders the context stream after a pending cueva_download_async: its copies
+// read device buffers that later work on the stream overwrites.
+int32_t join_downloads(cueva_ctx* c) {
+  if (!c->dl_pending) return CUEVA_OK;
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_xfer_done, 0));
+  c->dl_pending = false;
+  for (bool& b : c->field_pending) b = false;
+  return CUEVA_OK;
+}
+
+// Every entry point starts here; join = false only where the caller orders
+// itself per field (cueva_upload) or only reads host state.
+int32_t check_ctx(cueva_ctx* c, bool join = true) {
   if (!c) return fail(CUEVA_ERR_ARG, "null context");
+  if (join) return join_downloads(c);
   return CUEVA_OK;
 }
 
@@ -459,16 +480,23 @@ int32_t cueva_ctx_destroy(cueva_ctx* c) {
   if (c->d_mlp) cudaFree(c->d_mlp);
   if (c->d_mlp_stats) cudaFree(c->d_mlp_stats);
   free_diag(c);
+  if (c->xfer) {
+    cudaStreamSynchronize(c->xfer);
+    cudaStreamDestroy(c->xfer);
+  }
+  for (cudaEvent_t ev : c->ev_field) if (ev) cudaEventDestroy(ev);
+  if (c->ev_ready) cudaEventDestroy(c->ev_ready);
+  if (c->ev_xfer_done) cudaEventDestroy(c->ev_xfer_done);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return CUEVA_OK;
 }
 
 int32_t cueva_set_stream(cueva_ctx* c, void* s) {
-  if (int32_t e = check_ctx(c)) return e;
+  if (int32_t e = check_ctx(c, false)) return e;
   destroy_graphs(c);
   c->stream = s ? (cudaStream_t)s : c->own_stream;
-  return CUEVA_OK;
+  return join_downloads(c);   // the new stream also follows a pending readback
 }
 
 double cueva_dt(const cueva_ctx* c) { return c ? c->dt : 0.0; }
@@ -490,19 +518,46 @@ int32_t cueva_unpin_host(void* ptr) {
   return CUEVA_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+const int kConsField[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
+
+// The stream waits for a pending asynchronous readback of transfer slot k
+// (0..13 prims, 14..19 conserved fields) before its next copy overwrites that
+// field's host array or device buffer.
+int32_t wait_field(cueva_ctx* c, int k) {
+  if (!c->field_pending[k]) return CUEVA_OK;
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_field[k], 0));
+  c->field_pending[k] = false;
+  return CUEVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int32_t cueva_upload(cueva_ctx* c, uint32_t groups) {
-  if (int32_t e = check_ctx(c)) return e;
+  if (int32_t e = check_ctx(c, false)) return e;
   CUDA_TRY(cudaSetDevice(c->dev));
   if (groups & CUEVA_G_PRIMS) {
-    for (int f = 0; f < NPRIM; ++f)
+    for (int f = 0; f < NPRIM; ++f) {
+      if (int32_t e = wait_field(c, f)) return e;
       if (int32_t e = h2d(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
-    if (int32_t e = run_begin_step(c)) return e;
+    }
   }
   if (groups & CUEVA_G_CONS) {
-    const int map[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
-    for (int f = 0; f < NAUX; ++f)
-      if (int32_t e = h2d(c, aux_f(c, c->cur, f), map[f], 1)) return e;
+    for (int f = 0; f < NAUX; ++f) {
+      if (int32_t e = wait_field(c, NPRIM + f)) return e;
+      if (int32_t e = h2d(c, aux_f(c, c->cur, f), kConsField[f], 1)) return e;
+    }
   }
+  // the stage-1 preparation writes the conserved buffers: the whole readback
+  // precedes it
+  if (int32_t e = join_downloads(c)) return e;
+  if (groups & CUEVA_G_PRIMS)
+    if (int32_t e = run_begin_step(c)) return e;
   return CUEVA_OK;
 }
 
@@ -512,12 +567,42 @@ int32_t cueva_download(cueva_ctx* c, uint32_t groups) {
   if (groups & CUEVA_G_PRIMS)
     for (int f = 0; f < NPRIM; ++f)
       if (int32_t e = d2h(c, prim_f(c, c->cur, f), CUEVA_RHO + f, 1)) return e;
-  if (groups & CUEVA_G_CONS) {
-    const int map[NAUX] = {CUEVA_D, CUEVA_TAU, CUEVA_SX, CUEVA_SY, CUEVA_SZ, CUEVA_W};
+  if (groups & CUEVA_G_CONS)
     for (int f = 0; f < NAUX; ++f)
-      if (int32_t e = d2h(c, aux_f(c, c->cur, f), map[f], 1)) return e;
-  }
+      if (int32_t e = d2h(c, aux_f(c, c->cur, f), kConsField[f], 1)) return e;
   return read_status(c);
+}
+
+int32_t cueva_download_async(cueva_ctx* c, uint32_t groups) {
+  if (int32_t e = check_ctx(c)) return e;
+  CUDA_TRY(cudaSetDevice(c->dev));
+  for (int k = 0; k < NPRIM + NAUX; ++k) {
+    int field = k < NPRIM ? CUEVA_RHO + k : kConsField[k - NPRIM];
+    bool want = k < NPRIM ? (groups & CUEVA_G_PRIMS) : (groups & CUEVA_G_CONS);
+    if (want && !c->bound[field]) return fail(CUEVA_ERR_UNBOUND, "field " + std::to_string(field) + " not bound");
+  }
+  if (!c->xfer) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_xfer_done, cudaEventDisableTiming));
+    for (cudaEvent_t& ev : c->ev_field) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  CUDA_TRY(cudaEventRecord(c->ev_ready, c->stream));
+  CUDA_TRY(cudaStreamWaitEvent(c->xfer, c->ev_ready, 0));
+  for (int k = 0; k < NPRIM + NAUX; ++k) {
+    bool prim = k < NPRIM;
+    if (!(groups & (prim ? CUEVA_G_PRIMS : CUEVA_G_CONS))) continue;
+    int field = prim ? CUEVA_RHO + k : kConsField[k - NPRIM];
+    const double* src = prim ? prim_f(c, c->cur, k) : aux_f(c, c->cur, k - NPRIM);
+    CUDA_TRY(cudaMemcpy2DAsync(host_interior(c, c->bound[field], 1), (size_t)(c->imax + 13) * 8, src,
+                               (size_t)c->pitch * 8, (size_t)c->nx * 8, (size_t)c->ny, cudaMemcpyDeviceToHost,
+                               c->xfer));
+    CUDA_TRY(cudaEventRecord(c->ev_field[k], c->xfer));
+    c->field_pending[k] = true;
+  }
+  CUDA_TRY(cudaEventRecord(c->ev_xfer_done, c->xfer));
+  c->dl_pending = true;
+  return CUEVA_OK;
 }
 
 int32_t cueva_step(cueva_ctx* c, int32_t nsteps) {

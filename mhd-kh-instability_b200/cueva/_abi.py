@@ -37,7 +37,7 @@ PER_STAGE = set(STAGE_FIELDS) | set(RHS_FIELDS) | set(FACE_FIELDS)
 
 EXPORTS = ["cueva_ctx_create", "cueva_ctx_destroy", "cueva_last_error", "cueva_set_stream", "cueva_dt",
            "cueva_tableau_stages", "cueva_bind_field", "cueva_pin_host", "cueva_unpin_host", "cueva_upload",
-           "cueva_download", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
+           "cueva_download", "cueva_download_async", "cueva_step", "cueva_sync", "cueva_status", "cueva_counters", "cueva_startconvar",
            "cueva_electricvarint", "cueva_flux_rhs", "cueva_flux_flow", "cueva_fluxandsource", "cueva_varfin", "cueva_electricfield", "cueva_con2prim", "cueva_kh_init", "cueva_profile_steps", "cueva_flux_rhs_noalloc", "cueva_mlp_create",
            "cueva_mlp_destroy", "cueva_mlp_get_params", "cueva_mlp_set_params", "cueva_mlp_synthetic_pairs",
            "cueva_mlp_fit_normalisation", "cueva_mlp_train", "cueva_mlp_gradients", "cueva_mlp_predict",
@@ -116,6 +116,7 @@ def load(fma=False):
     L.cueva_unpin_host.argtypes = [vp]
     L.cueva_upload.argtypes = [vp, u32]
     L.cueva_download.argtypes = [vp, u32]
+    L.cueva_download_async.argtypes = [vp, u32]
     L.cueva_step.argtypes = [vp, i32]
     L.cueva_sync.argtypes = [vp]
     L.cueva_status.argtypes = [vp, ctypes.POINTER(u32)]

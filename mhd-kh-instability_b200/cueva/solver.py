@@ -85,6 +85,11 @@ class Cueva:
     def download(self, groups=_abi.G_PRIMS):
         _abi.check(self.L, self.L.cueva_download(self.ctx, groups))
 
+    def download_async(self, groups=_abi.G_PRIMS):
+        """Queues the readback on a second stream; the arrays are complete
+        after sync(), and a following upload() waits field by field."""
+        _abi.check(self.L, self.L.cueva_download_async(self.ctx, groups))
+
     def step(self, n=1):
         _abi.check(self.L, self.L.cueva_step(self.ctx, int(n)))
 

@@ -109,6 +109,11 @@ module cueva_gpu
        type(c_ptr), value :: ctx
        integer(c_int32_t), value :: groups
      end function cueva_download
+     integer(c_int32_t) function cueva_download_async(ctx, groups) bind(c, name="cueva_download_async")
+       import :: c_ptr, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: groups
+     end function cueva_download_async
      integer(c_int32_t) function cueva_step(ctx, nsteps) bind(c, name="cueva_step")
        import :: c_int32_t, c_ptr
        type(c_ptr), value :: ctx
