@@ -1045,15 +1045,19 @@ int32_t cueva_flux_flow(cueva_ctx* c, int32_t l) {
                                  (size_t)(c->imax + 1) * 8, (size_t)(c->jmax + 2), cudaMemcpyDeviceToHost,
                                  c->stream));
   } else {
-    std::vector<float> tmp((size_t)NFACE * (size_t)I.ffs);
-    CUDA_TRY(cudaMemcpyAsync(tmp.data(), I.fy, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    // the mixed kernels' slabs, FP32 or FP64 by role (flux_slot)
+    std::vector<double> tmp((size_t)NFACE * (size_t)I.ffs);
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), I.fy, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    for (int r = 0; r < NFACE; ++r)
+    const float* tmpf = reinterpret_cast<const float*>(tmp.data());
+    for (int r = 0; r < NFACE; ++r) {
+      const FluxSlot sl = flux_slot(true, c->P.flux_solver, r, I.ffs);
       for (int j = -1; j <= c->jmax; ++j) {
         double* dst = host_at(c, kFaceY[r], l, 0, j);
-        const float* src = tmp.data() + (size_t)r * I.ffs + (size_t)(j + 1) * I.fpitch;
-        for (int i = 0; i <= c->imax; ++i) dst[i] = double(src[i]);
+        const size_t o = (size_t)sl.off + (size_t)(j + 1) * I.fpitch;
+        for (int i = 0; i <= c->imax; ++i) dst[i] = sl.f64 ? tmp[o + i] : double(tmpf[o + i]);
       }
+    }
   }
   return read_status(c);
 }

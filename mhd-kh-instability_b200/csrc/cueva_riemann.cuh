@@ -29,6 +29,7 @@ namespace cueva {
 
 enum Role { R_PSI = 0, R_PHI, R_BN, R_BT1, R_BT2, R_EN, R_ET1, R_ET2, R_Q, R_D, R_TAU, R_SN, R_ST1, R_ST2, NROLE };
 static_assert(NROLE == NFACE, "flux scratch holds one slab per role");
+static_assert(R_BN == 2 && R_ET2 == 7, "flux_slot keeps roles 2..7 (E/B transport) in FP64 for the mixed MP solvers");
 
 template <typename T>
 struct Side {

@@ -24,6 +24,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <type_traits>
+
 #include "cueva_common.cuh"
 #include "cueva_mp.cuh"
 #include "cueva_riemann.cuh"
@@ -118,23 +120,37 @@ __device__ __forceinline__ void prefetch_l2(const E* p, int n) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
 }
 
-// The y-flux scratch holds each flux in the type it is computed in: FP64,
-// or FP32 for the mixed-precision kernels (the update converts it to FP64
-// exactly as it would convert the register value, so the results are the
-// same and the scratch traffic halves).  Element e of field c of the slab
-// is at fy + c * ffs + e in units of that type.
-template <typename T>
-__device__ __forceinline__ void flux_store(double* fy, long long idx, T v) {
-  if constexpr (sizeof(T) == 8) fy[idx] = double(v);
-  else reinterpret_cast<float*>(fy)[idx] = float(v);
+// Type of the face fluxes a stage kernel produces: T, except that the
+// mixed-precision MP solvers return FP64 (their E/B transport roles are
+// computed in FP64, the others are FP32 values held exactly).
+template <typename T, int SV>
+constexpr bool kEmF64 = sizeof(T) == 4 && mixed_em_f64(SV);
+template <typename T, int SV>
+using flux_t = typename std::conditional<kEmF64<T, SV>, double, T>::type;
+
+// The y-flux scratch holds each flux in the type it is computed in (FP64,
+// or FP32 for the mixed-precision kernels, the update converting it to FP64
+// exactly as it would convert the register value), at the place flux_slot
+// gives; element e of role c is element e of that slab.
+template <typename T, int SV>
+__device__ __forceinline__ void flux_store(double* fy, long long ffs, int c, long long e, double v) {
+  const FluxSlot s = flux_slot(sizeof(T) == 4, SV, c, ffs);
+  if (s.f64) fy[s.off + e] = v;
+  else reinterpret_cast<float*>(fy)[s.off + e] = float(v);
 }
-template <typename T>
-__device__ __forceinline__ double flux_load(const double* fy, long long idx) {
-  if constexpr (sizeof(T) == 8) return fy[idx];
-  else return double(reinterpret_cast<const float*>(fy)[idx]);
+template <typename T, int SV>
+__device__ __forceinline__ double flux_load(const double* fy, long long ffs, int c, long long e) {
+  const FluxSlot s = flux_slot(sizeof(T) == 4, SV, c, ffs);
+  if (s.f64) return fy[s.off + e];
+  return double(reinterpret_cast<const float*>(fy)[s.off + e]);
 }
-template <typename T>
-__device__ __forceinline__ const T* flux_base(const double* fy) { return reinterpret_cast<const T*>(fy); }
+// L2 prefetch of n elements of role c from element e on
+template <typename T, int SV>
+__device__ __forceinline__ void flux_prefetch(const double* fy, long long ffs, int c, long long e, int n) {
+  const FluxSlot s = flux_slot(sizeof(T) == 4, SV, c, ffs);
+  if (s.f64) prefetch_l2(fy + s.off + e, n);
+  else prefetch_l2(reinterpret_cast<const float*>(fy) + s.off + e, n);
+}
 
 constexpr int NF_FACE = 20;   // 5 primitive slots + 14 conserved + the normal current
 
@@ -225,7 +241,7 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits
 template <int RM, int SOLVER, typename T, int D, int ROWS>
 __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
-                                              double sigma_d, T (&F)[NROLE]) {
+                                              double sigma_d, flux_t<T, SOLVER> (&F)[NROLE]) {
   using G = FaceGeom<RM, SOLVER, ROWS>;
   constexpr int R = G::R, NS = G::NS;
   auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
@@ -378,14 +394,48 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
       }
     }
   }
-  rec(5 + Q_PSI, L.psi, Rs.psi);
-  rec(5 + Q_PHI, L.phi, Rs.phi);
-  rec(5 + Q_EX, L.Ex, Rs.Ex);
-  rec(5 + Q_EY, L.Ey, Rs.Ey);
-  rec(5 + Q_EZ, L.Ez, Rs.Ez);
-  rec(5 + Q_BX, L.Bx, Rs.Bx);
-  rec(5 + Q_BY, L.By, Rs.By);
-  rec(5 + Q_BZ, L.Bz, Rs.Bz);
+  if constexpr (kEmF64<T, SOLVER>) {
+    // mixed precision: psi, phi, E and B are reconstructed as differences
+    // from the cell's FP64 value (the MP limiters are translation-equivariant:
+    // weights summing to 1, limiter tests on differences), so the FP32
+    // rounding is relative to the local variation rather than to the
+    // background field; the E/B transport fluxes, linear in these face values,
+    // are formed in FP64
+    auto rec_delta = [&](int f, double& Lv, double& Rv) {
+      const double c0 = nrmd(f, R);
+      T u[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) u[q] = T(nrmd(f, q) - c0);
+      const Pair<T> p = MPCall<RM, T>::template call<false>(u);
+      Lv = c0 + double(p.L); Rv = c0 + double(p.R);
+    };
+    Side<double> Ld{}, Rd{};
+    rec_delta(5 + Q_PSI, Ld.psi, Rd.psi);
+    rec_delta(5 + Q_PHI, Ld.phi, Rd.phi);
+    rec_delta(5 + Q_EX, Ld.Ex, Rd.Ex);
+    rec_delta(5 + Q_EY, Ld.Ey, Rd.Ey);
+    rec_delta(5 + Q_EZ, Ld.Ez, Rd.Ez);
+    rec_delta(5 + Q_BX, Ld.Bx, Rd.Bx);
+    rec_delta(5 + Q_BY, Ld.By, Rd.By);
+    rec_delta(5 + Q_BZ, Ld.Bz, Rd.Bz);
+    double Ad[NROLE];
+    em_fluxes<D>(Ld, Rd, Ad);
+#pragma unroll
+    for (int c = R_BN; c <= R_ET2; ++c) F[c] = Ad[c];
+    L.psi = T(Ld.psi); L.phi = T(Ld.phi); L.Ex = T(Ld.Ex); L.Ey = T(Ld.Ey); L.Ez = T(Ld.Ez);
+    L.Bx = T(Ld.Bx); L.By = T(Ld.By); L.Bz = T(Ld.Bz);
+    Rs.psi = T(Rd.psi); Rs.phi = T(Rd.phi); Rs.Ex = T(Rd.Ex); Rs.Ey = T(Rd.Ey); Rs.Ez = T(Rd.Ez);
+    Rs.Bx = T(Rd.Bx); Rs.By = T(Rd.By); Rs.Bz = T(Rd.Bz);
+  } else {
+    rec(5 + Q_PSI, L.psi, Rs.psi);
+    rec(5 + Q_PHI, L.phi, Rs.phi);
+    rec(5 + Q_EX, L.Ex, Rs.Ex);
+    rec(5 + Q_EY, L.Ey, Rs.Ey);
+    rec(5 + Q_EZ, L.Ez, Rs.Ez);
+    rec(5 + Q_BX, L.Bx, Rs.Bx);
+    rec(5 + Q_BY, L.By, Rs.By);
+    rec(5 + Q_BZ, L.Bz, Rs.Bz);
+  }
   rec(5 + Q_Q, L.q, Rs.q);
   rec(5 + Q_D, L.D, Rs.D);
   rec(5 + Q_TAU, L.tau, Rs.tau);
@@ -394,9 +444,20 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
   rec(5 + Q_SZ, L.Sz, Rs.Sz);
   rec(19, L.J, Rs.J);
   const T gamma = T(gamma_d);
-  if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, F);
-  else if constexpr (SOLVER == 6) hlle_fluxes<D>(L, Rs, gamma, F, stt);
-  else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, F, stt);
+  auto riemann = [&](T* A) {
+    if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, A);
+    else if constexpr (SOLVER == 6) hlle_fluxes<D>(L, Rs, gamma, A, stt);
+    else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, A, stt);
+  };
+  if constexpr (kEmF64<T, SOLVER>) {
+    T A[NROLE];
+    riemann(A);
+#pragma unroll
+    for (int c = 0; c < NROLE; ++c)
+      if (c < R_BN || c > R_ET2) F[c] = double(A[c]);
+  } else {
+    riemann(F);
+  }
   return stt;
 }
 
@@ -433,11 +494,11 @@ k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
     __syncthreads();
     const int i = i0 + lane, j = j0 + w;
     if (i <= ilast && j <= jlast) {
-      T F[NROLE];
+      flux_t<T, SOLVER> F[NROLE];
       const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
       const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
-      for (int c = 0; c < NROLE; ++c) flux_store<T>(I.fy, c * I.ffs + fo, F[c]);
+      for (int c = 0; c < NROLE; ++c) flux_store<T, SOLVER>(I.fy, I.ffs, c, fo, double(F[c]));
       if (stt) atomicOr(I.status, stt);
     }
     __syncthreads();   // the next tile's copies overwrite the staged values
@@ -456,7 +517,7 @@ struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
 // and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
 // valid == false (EP_LAST only): the lane computes a copy of a real point so
 // that its warp reaches con2prim converged, and stores nothing
-template <int EP, typename T>
+template <int EP, typename T, int SV = 0>
 __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
                                                  const double (&qx)[NROLE], const Centre& cv, bool valid = true) {
   const int pitch = I.pitch;
@@ -469,7 +530,7 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
   const double* __restrict__ fy = I.fy;
   const double dly = I.dely, iy2 = I.inv_dely_pow2;
   auto qy = [&](int r) {   // (dy)/dly
-    const double d = flux_load<T>(fy, r * I.ffs + fyo) - flux_load<T>(fy, r * I.ffs + fyo - I.fpitch);
+    const double d = flux_load<T, SV>(fy, I.ffs, r, fyo) - flux_load<T, SV>(fy, I.ffs, r, fyo - I.fpitch);
     return iy2 != 0.0 ? d * iy2 : d / dly;
   };
   auto qxf = [&](int r) { return qx[r]; };
@@ -642,7 +703,7 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
         prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
       } else {
         const int e2 = e - ncen * nr, r = e2 % (nr + 1), c = e2 / (nr + 1);
-        prefetch_l2(flux_base<T>(I.fy) + c * I.ffs + (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
+        flux_prefetch<T, SOLVER>(I.fy, I.ffs, c, (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
       }
     }
   }
@@ -650,9 +711,9 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
   __syncthreads();
   const int i = i0 + lane, j = j0 + w;
   if (j > jlast) return;   // whole warp; the caller synchronises before the next tile
-  T F[NROLE];
+  flux_t<T, SOLVER> F[NROLE];
 #pragma unroll
-  for (int c = 0; c < NROLE; ++c) F[c] = T(0);
+  for (int c = 0; c < NROLE; ++c) F[c] = 0;
   uint32_t stt = 0;
   if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
   if constexpr (EP == EP_RHS) {
@@ -689,7 +750,7 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
     auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + ln + R]; };
     const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
                     cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
-    stt |= update_point<EP, T>(I, sa, ii, j, qx, cv, valid);
+    stt |= update_point<EP, T, SOLVER>(I, sa, ii, j, qx, cv, valid);
   }
   if (stt) atomicOr(I.status, stt);
 }
