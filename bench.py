@@ -329,7 +329,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     net.close()
     nprof = max(args.profile_steps, 1)
     return {"value": world * cfg.nx * cfg.ny * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
-            "dtype": "f32 reconstruction + Riemann (E/B transport fluxes f64), f64 update / implicit E / con2prim",
+            "dtype": "f32 reconstruction + Riemann (psi, phi, E, B fluxes f64), f64 update / implicit E / con2prim",
             "con2prim": "network seed on the tcgen05 tensor cores (k_c2p_step), Newton in FP64, Cardano fall-back",
             "kernel_ms_per_step": {"k_yface": prof_ms[0] / nprof, "k_xupd": prof_ms[1] / nprof,
                                    "k_c2p_step": prof_ms[2] / nprof},
@@ -423,7 +423,7 @@ def run_ensemble(args):
         sizes[f"{i.nx}x{i.ny}"] = sizes.get(f"{i.nx}x{i.ny}", 0) + 1
     line = {"metric": ENS_METRIC, "value": rate(ms_mixed), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": warm,
             "ms_per_step": ms_mixed / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 reconstruction + Riemann (E/B transport fluxes f64), f64 update / implicit E / con2prim (learned seed)",
+            "dtype": "f32 reconstruction + Riemann (psi, phi, E, B fluxes f64), f64 update / implicit E / con2prim (learned seed)",
             "data": "synthetic KH ensemble (seed 2024)",
             "config": {"workload": f"kh-ensemble-{len(insts)}", "instances": len(insts), "zones": zones,
                        "grids": sizes, "solver": "MP5+HLLC", "imex": "SSP3(4,3,3), stage sums reset per stage"},

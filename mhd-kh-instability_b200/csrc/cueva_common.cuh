@@ -134,18 +134,18 @@ struct StageShape {
 inline int xupd_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 30) / 31) * ((jmax + 1 + rows - 1) / rows); }
 inline int yface_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 31) / 32) * ((jmax + 2 + rows - 1) / rows); }
 
-// The mixed-precision MP solvers (flux_solver 5..7) keep the six E/B
-// transport fluxes (roles 2..7: Bn, Bt1, Bt2, En, Et1, Et2) in FP64: they
-// carry the uniform background field (B ~ 0.1 in the KH runs), whose FP32
-// rounding (~4e-9) is not small against E itself, and the final IMEX
+// The mixed-precision MP solvers (flux_solver 5..7) keep the fluxes of the
+// field roles psi, phi, Bn, Bt1, Bt2, En, Et1, Et2 (roles 0..7) in FP64:
+// they carry the uniform background field (B ~ 0.1 in the KH runs), whose
+// FP32 rounding (~4e-9) is not small against E itself, and the final IMEX
 // combination passes that error into E(n+1) undamped.
 __host__ __device__ constexpr bool mixed_em_f64(int solver) { return solver >= 5 && solver <= 7; }
 
 // Place of role r in the y-flux scratch (NFACE slabs of ffs doubles): f64
 // tells the element type and off the slab's first element in units of that
 // type.  FP64 kernels: double slab r.  Mixed kernels: FP32 slab r; with
-// mixed_em_f64, double slabs 0..5 for roles 2..7, then FP32 slabs for roles
-// 0, 1, 8..13 from byte offset 48 * ffs on.
+// mixed_em_f64, double slabs 0..7 for roles 0..7, then FP32 slabs for roles
+// 8..13 from byte offset 64 * ffs on.
 struct FluxSlot {
   bool f64;
   long long off;
@@ -153,8 +153,8 @@ struct FluxSlot {
 __host__ __device__ inline FluxSlot flux_slot(bool mixed, int solver, int r, long long ffs) {
   if (!mixed) return {true, r * ffs};
   if (!mixed_em_f64(solver)) return {false, r * ffs};
-  if (r >= 2 && r <= 7) return {true, (r - 2) * ffs};
-  return {false, (12 + (r < 2 ? r : r - 6)) * ffs};
+  if (r <= 7) return {true, r * ffs};
+  return {false, (16 + (r - 8)) * ffs};
 }
 
 }  // namespace cueva

@@ -29,7 +29,7 @@ namespace cueva {
 
 enum Role { R_PSI = 0, R_PHI, R_BN, R_BT1, R_BT2, R_EN, R_ET1, R_ET2, R_Q, R_D, R_TAU, R_SN, R_ST1, R_ST2, NROLE };
 static_assert(NROLE == NFACE, "flux scratch holds one slab per role");
-static_assert(R_BN == 2 && R_ET2 == 7, "flux_slot keeps roles 2..7 (E/B transport) in FP64 for the mixed MP solvers");
+static_assert(R_PSI == 0 && R_ET2 == 7, "flux_slot keeps roles 0..7 (psi, phi, E, B) in FP64 for the mixed MP solvers");
 
 template <typename T>
 struct Side {
@@ -243,7 +243,8 @@ __device__ __forceinline__ T hllc_vel(T a, T b, T c, T rt, uint32_t& st) {
 
 // HLLC of Miranda-Aranguren et al. (2018), 16_hllc_flow_mpx.f95:2816-4610
 template <int D, typename T>
-__device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st) {
+__device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st,
+                                            T* vstar = nullptr) {
   using X = Dir<D>;
   em_fluxes<D>(L, R, A);
   const Phys<T> fl = physical<D>(L, gamma), fr = physical<D>(R, gamma);
@@ -293,6 +294,7 @@ __device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, 
   if (det_hll < T(0.0)) rt2 = c_hll / b_hll;
   T V = hllc_vel(a_hll, -b_hll, c_hll, rt2, st);
   if (fabs(V) <= T(1.0e-9)) V = T(0.0);
+  if (vstar) *vstar = V;   // the contact speed the flux choice below uses
   // star states (:3485-3570)
   const T pstr = Sn_f + (pw2(En_hll) + pw2(Bn_hll)) - (tau_f - ErotB_n) * V;
   const T omV = T(1.0) - V, opV = V + T(1.0);

@@ -121,8 +121,8 @@ __device__ __forceinline__ void prefetch_l2(const E* p, int n) {
 }
 
 // Type of the face fluxes a stage kernel produces: T, except that the
-// mixed-precision MP solvers return FP64 (their E/B transport roles are
-// computed in FP64, the others are FP32 values held exactly).
+// mixed-precision MP solvers return FP64 (their field roles psi, phi, E, B
+// are computed in FP64, the others are FP32 values held exactly).
 template <typename T, int SV>
 constexpr bool kEmF64 = sizeof(T) == 4 && mixed_em_f64(SV);
 template <typename T, int SV>
@@ -394,13 +394,14 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
       }
     }
   }
+  Side<double> Ld{}, Rd{};   // FP64 field face values (mixed MP solvers)
   if constexpr (kEmF64<T, SOLVER>) {
     // mixed precision: psi, phi, E and B are reconstructed as differences
     // from the cell's FP64 value (the MP limiters are translation-equivariant:
     // weights summing to 1, limiter tests on differences), so the FP32
     // rounding is relative to the local variation rather than to the
-    // background field; the E/B transport fluxes, linear in these face values,
-    // are formed in FP64
+    // background field; their fluxes, linear in these face values (plus the
+    // HLLC star correction of psi and phi, below), are formed in FP64
     auto rec_delta = [&](int f, double& Lv, double& Rv) {
       const double c0 = nrmd(f, R);
       T u[NS];
@@ -409,7 +410,6 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
       const Pair<T> p = MPCall<RM, T>::template call<false>(u);
       Lv = c0 + double(p.L); Rv = c0 + double(p.R);
     };
-    Side<double> Ld{}, Rd{};
     rec_delta(5 + Q_PSI, Ld.psi, Rd.psi);
     rec_delta(5 + Q_PHI, Ld.phi, Rd.phi);
     rec_delta(5 + Q_EX, Ld.Ex, Rd.Ex);
@@ -421,7 +421,7 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     double Ad[NROLE];
     em_fluxes<D>(Ld, Rd, Ad);
 #pragma unroll
-    for (int c = R_BN; c <= R_ET2; ++c) F[c] = Ad[c];
+    for (int c = R_PSI; c <= R_ET2; ++c) F[c] = Ad[c];
     L.psi = T(Ld.psi); L.phi = T(Ld.phi); L.Ex = T(Ld.Ex); L.Ey = T(Ld.Ey); L.Ez = T(Ld.Ez);
     L.Bx = T(Ld.Bx); L.By = T(Ld.By); L.Bz = T(Ld.Bz);
     Rs.psi = T(Rd.psi); Rs.phi = T(Rd.phi); Rs.Ex = T(Rd.Ex); Rs.Ey = T(Rd.Ey); Rs.Ez = T(Rd.Ez);
@@ -444,17 +444,37 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
   rec(5 + Q_SZ, L.Sz, Rs.Sz);
   rec(19, L.J, Rs.J);
   const T gamma = T(gamma_d);
+  T vstar = T(0);
   auto riemann = [&](T* A) {
     if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, A);
     else if constexpr (SOLVER == 6) hlle_fluxes<D>(L, Rs, gamma, A, stt);
-    else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, A, stt);
+    else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, A, stt, kEmF64<T, SOLVER> ? &vstar : nullptr);
   };
   if constexpr (kEmF64<T, SOLVER>) {
     T A[NROLE];
     riemann(A);
 #pragma unroll
-    for (int c = 0; c < NROLE; ++c)
-      if (c < R_BN || c > R_ET2) F[c] = double(A[c]);
+    for (int c = R_Q; c < NROLE; ++c) F[c] = double(A[c]);
+    if constexpr (SOLVER == 7) {
+      // the HLLC star correction of psi and phi (16_hllc_flow_mpx.f95:
+      // 3485-3520, 3908-4300), in FP64 on the FP64 field face values with
+      // the FP32 contact speed; HLL and HLLE keep the fixed-speed fluxes
+      using X = Dir<D>;
+      const double h = 0.5, V = double(vstar);
+      const double psi_hll = h * (((Rd.psi + Ld.psi) + X::En(Ld)) - X::En(Rd));
+      const double phi_hll = h * (((Rd.phi + Ld.phi) + X::Bn(Ld)) - X::Bn(Rd));
+      const double En_f = F[R_EN], Bn_f = F[R_BN];
+      if (V != 0.0 && V == V) {
+        const double omV = 1.0 - V, opV = V + 1.0, k = V > 0.0 ? omV : opV;
+        const double psiR = (psi_hll - V * En_f) / omV, psiL = (psi_hll + V * En_f) / opV;
+        const double phiR = (phi_hll - V * Bn_f) / omV, phiL = (phi_hll + V * Bn_f) / opV;
+        F[R_PSI] = F[R_PSI] + (k * (psiR - psiL)) * h;
+        F[R_PHI] = F[R_PHI] + (k * (phiR - phiL)) * h;
+      } else if (V != V) {
+        F[R_PSI] = double(A[R_PSI]);   // the failed contact: NaN fluxes and the status bit
+        F[R_PHI] = double(A[R_PHI]);
+      }
+    }
   } else {
     riemann(F);
   }
