@@ -87,3 +87,29 @@ def test_upload_of_conserved_group_after_async_readback():
     b.download()
     for n in PRIMS:
         assert np.array_equal(a.array(n), b.array(n)), n
+
+
+def test_stream_switch_with_pending_readback():
+    """set_stream while a readback is in flight: the new stream's work (the
+    next step overwrites the buffers being read) waits for the readback."""
+    import torch
+    a, b = _make(True), _make(True)
+    a.upload()
+    b.upload()
+    a.step(1)
+    a.download()
+    ref1 = _snapshot(a, PRIMS)
+    a.step(1)
+    a.download()
+    b.step(1)
+    b.download_async()
+    s = torch.cuda.Stream()
+    b.set_stream(s.cuda_stream)
+    b.step(1)
+    b.sync()
+    for n in PRIMS:          # the readback holds step 1, not step 2
+        assert np.array_equal(ref1[n], b.array(n)), n
+    b.download()
+    for n in PRIMS:
+        assert np.array_equal(a.array(n), b.array(n)), n
+    b.set_stream(None)
