@@ -582,10 +582,21 @@ int32_t cueva_download_async(cueva_ctx* c, uint32_t groups) {
     if (want && !c->bound[field]) return fail(CUEVA_ERR_UNBOUND, "field " + std::to_string(field) + " not bound");
   }
   if (!c->xfer) {
-    CUDA_TRY(cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_xfer_done, cudaEventDisableTiming));
-    for (cudaEvent_t& ev : c->ev_field) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    // the transfer stream and its events come into use together or not at all
+    cudaStream_t xs = nullptr;
+    cudaEvent_t evs[NPRIM + NAUX + 2] = {};
+    cudaError_t ce = cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking);
+    for (cudaEvent_t& ev : evs)
+      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (ce != cudaSuccess) {
+      for (cudaEvent_t ev : evs) if (ev) cudaEventDestroy(ev);
+      if (xs) cudaStreamDestroy(xs);
+      return fail(CUEVA_ERR_CUDA, std::string("transfer stream set-up: ") + cudaGetErrorString(ce));
+    }
+    c->xfer = xs;
+    c->ev_ready = evs[NPRIM + NAUX];
+    c->ev_xfer_done = evs[NPRIM + NAUX + 1];
+    for (int k = 0; k < NPRIM + NAUX; ++k) c->ev_field[k] = evs[k];
   }
   CUDA_TRY(cudaEventRecord(c->ev_ready, c->stream));
   CUDA_TRY(cudaStreamWaitEvent(c->xfer, c->ev_ready, 0));
