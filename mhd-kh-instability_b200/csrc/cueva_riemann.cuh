@@ -459,7 +459,8 @@ __device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, 
 // with |v*| <= 1e-6 taken as 0 (:2580-2600; the MPX routine uses 1e-9).
 template <int D, typename T>
 __device__ __forceinline__ void hllcmc_fluxes(const Side<T>& L, const Side<T>& R, const T (&m_et2)[2],
-                                              const T (&m_bt1)[2], T gamma, T sigma, T* A, uint32_t& st) {
+                                              const T (&m_bt1)[2], T gamma, T sigma, T* A, uint32_t& st,
+                                              T* vstar = nullptr) {
   using X = Dir<D>;
   mcl_fluxes<D>(L, R, m_et2, m_bt1, gamma, sigma, A);   // fixed-speed HLL fluxes of every role
   const Phys<T> fl = physical<D>(L, gamma, lorentz_hlle(L)), fr = physical<D>(R, gamma, lorentz_hlle(R));
@@ -497,6 +498,7 @@ __device__ __forceinline__ void hllcmc_fluxes(const Side<T>& L, const Side<T>& R
   if (det_hll < T(0.0)) rt2 = c_hll / b_hll;
   T V = hllc_vel(a_hll, -b_hll, c_hll, rt2, st);
   if (fabs(V) <= T(1.0e-6)) V = T(0.0);
+  if (vstar) *vstar = V;   // the contact speed the flux choice below uses
   const T pstr = Sn_f + (pw2(En_hll) + pw2(Bn_hll)) - (tau_f - ErotB_n) * V;
   const T omV = T(1.0) - V, opV = V + T(1.0);
   const T psiR = (psi_hll - V * En_f) / omV, psiL = (psi_hll + V * En_f) / opV;

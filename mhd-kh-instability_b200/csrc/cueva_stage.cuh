@@ -237,6 +237,32 @@ __device__ __forceinline__ void stage_tile(const InstDesc& I, const StageArgs& s
   }
 }
 
+// HLLC star correction of the psi and phi fluxes (16_hllc_flow_mpx.f95:
+// 3485-3520, 3908-4300; 16_hllc_flow_mcl.f95:3530-3620) in FP64 for the
+// mixed HLLC routines: F holds the FP64 fixed-speed fluxes of roles 0..7 from
+// the FP64 field face values Ld / Rd, V the FP32 contact speed after the
+// routine's zero threshold, A the routine's FP32 fluxes (NaN when it failed)
+template <int D, typename T>
+__device__ __forceinline__ void psiphi_star_f64(const Side<double>& Ld, const Side<double>& Rd, T vstar,
+                                                const T* A, double* F) {
+  using X = Dir<D>;
+  const double h = 0.5, V = double(vstar);
+  if (isnan(V)) {
+    F[R_PSI] = double(A[R_PSI]);
+    F[R_PHI] = double(A[R_PHI]);
+    return;
+  }
+  if (V == 0.0) return;
+  const double psi_hll = h * (((Rd.psi + Ld.psi) + X::En(Ld)) - X::En(Rd));
+  const double phi_hll = h * (((Rd.phi + Ld.phi) + X::Bn(Ld)) - X::Bn(Rd));
+  const double En_f = F[R_EN], Bn_f = F[R_BN];
+  const double omV = 1.0 - V, opV = V + 1.0, k = V > 0.0 ? omV : opV;
+  const double psiR = (psi_hll - V * En_f) / omV, psiL = (psi_hll + V * En_f) / opV;
+  const double phiR = (phi_hll - V * Bn_f) / omV, phiL = (phi_hll + V * Bn_f) / opV;
+  F[R_PSI] = F[R_PSI] + (k * (psiR - psiL)) * h;
+  F[R_PHI] = F[R_PHI] + (k * (phiR - phiL)) * h;
+}
+
 // flux of the face of (w, lane) from the staged tile (16_hll_flow_mpx.f95 /
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits
 template <int RM, int SOLVER, typename T, int D, int ROWS>
@@ -271,6 +297,7 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
 
   uint32_t stt = 0;
   Side<T> L, Rs;
+  Side<double> Ld{}, Rd{};   // FP64 field face values (mixed routines with FP64 field fluxes)
   if constexpr (SOLVER == 1) {
     // Lax-Friedrichs with MC slopes, 15_lax_flow.f95:920-1457: for stencil
     // cells 0..3 (the face lies between 1 and 2)
@@ -332,23 +359,72 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     recm(2, L.vz, Rs.vz, nullptr);
     recm(3, L.p, Rs.p, nullptr);
     recm(4, L.rho, Rs.rho, nullptr);
-    recm(5 + Q_PSI, L.psi, Rs.psi, nullptr);
-    recm(5 + Q_PHI, L.phi, Rs.phi, nullptr);
-    recm(5 + Q_EX, L.Ex, Rs.Ex, fEt2 == 5 + Q_EX ? m_et2 : nullptr);
-    recm(5 + Q_EY, L.Ey, Rs.Ey, nullptr);
-    recm(5 + Q_EZ, L.Ez, Rs.Ez, fEt2 == 5 + Q_EZ ? m_et2 : nullptr);
-    recm(5 + Q_BX, L.Bx, Rs.Bx, nullptr);
-    recm(5 + Q_BY, L.By, Rs.By, fBt1 == 5 + Q_BY ? m_bt1 : nullptr);
-    recm(5 + Q_BZ, L.Bz, Rs.Bz, fBt1 == 5 + Q_BZ ? m_bt1 : nullptr);
+    if constexpr (kEmF64<T, SOLVER>) {
+      // mixed precision: the field slots as differences from the FP64 value
+      // of stencil cell 1 (the MC slopes are differences), face and "_m"
+      // values back in FP64, their fluxes in FP64 (see the MP routines)
+      double md_et2[2], md_bt1[2];
+      auto recm_delta = [&](int f, double& Lv, double& Rv, double* m) {
+        const double c0 = nrmd(f, 1);
+        T u[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) u[q] = T(nrmd(f, q) - c0);
+        const T sl = T(0.5) * mc_slope(u[2] - u[1], u[1] - u[0]);
+        const T sr = T(0.5) * mc_slope(u[3] - u[2], u[2] - u[1]);
+        Lv = c0 + double(u[1] + sl);
+        Rv = c0 + double(u[2] - sr);
+        if (m) { m[0] = -(c0 + double(u[1])) + double(sl); m[1] = -(c0 + double(u[2])) - double(sr); }
+      };
+      recm_delta(5 + Q_PSI, Ld.psi, Rd.psi, nullptr);
+      recm_delta(5 + Q_PHI, Ld.phi, Rd.phi, nullptr);
+      recm_delta(5 + Q_EX, Ld.Ex, Rd.Ex, fEt2 == 5 + Q_EX ? md_et2 : nullptr);
+      recm_delta(5 + Q_EY, Ld.Ey, Rd.Ey, nullptr);
+      recm_delta(5 + Q_EZ, Ld.Ez, Rd.Ez, fEt2 == 5 + Q_EZ ? md_et2 : nullptr);
+      recm_delta(5 + Q_BX, Ld.Bx, Rd.Bx, nullptr);
+      recm_delta(5 + Q_BY, Ld.By, Rd.By, fBt1 == 5 + Q_BY ? md_bt1 : nullptr);
+      recm_delta(5 + Q_BZ, Ld.Bz, Rd.Bz, fBt1 == 5 + Q_BZ ? md_bt1 : nullptr);
+      double Ad[NROLE];
+      mcl_fluxes<D>(Ld, Rd, md_et2, md_bt1, gamma_d, sigma_d, Ad);   // roles 0..7 used
+#pragma unroll
+      for (int c = R_PSI; c <= R_ET2; ++c) F[c] = Ad[c];
+      L.psi = T(Ld.psi); L.phi = T(Ld.phi); L.Ex = T(Ld.Ex); L.Ey = T(Ld.Ey); L.Ez = T(Ld.Ez);
+      L.Bx = T(Ld.Bx); L.By = T(Ld.By); L.Bz = T(Ld.Bz);
+      Rs.psi = T(Rd.psi); Rs.phi = T(Rd.phi); Rs.Ex = T(Rd.Ex); Rs.Ey = T(Rd.Ey); Rs.Ez = T(Rd.Ez);
+      Rs.Bx = T(Rd.Bx); Rs.By = T(Rd.By); Rs.Bz = T(Rd.Bz);
+      m_et2[0] = T(md_et2[0]); m_et2[1] = T(md_et2[1]);
+      m_bt1[0] = T(md_bt1[0]); m_bt1[1] = T(md_bt1[1]);
+    } else {
+      recm(5 + Q_PSI, L.psi, Rs.psi, nullptr);
+      recm(5 + Q_PHI, L.phi, Rs.phi, nullptr);
+      recm(5 + Q_EX, L.Ex, Rs.Ex, fEt2 == 5 + Q_EX ? m_et2 : nullptr);
+      recm(5 + Q_EY, L.Ey, Rs.Ey, nullptr);
+      recm(5 + Q_EZ, L.Ez, Rs.Ez, fEt2 == 5 + Q_EZ ? m_et2 : nullptr);
+      recm(5 + Q_BX, L.Bx, Rs.Bx, nullptr);
+      recm(5 + Q_BY, L.By, Rs.By, fBt1 == 5 + Q_BY ? m_bt1 : nullptr);
+      recm(5 + Q_BZ, L.Bz, Rs.Bz, fBt1 == 5 + Q_BZ ? m_bt1 : nullptr);
+    }
     recm(5 + Q_Q, L.q, Rs.q, nullptr);
     recm(5 + Q_D, L.D, Rs.D, nullptr);
     recm(5 + Q_TAU, L.tau, Rs.tau, nullptr);
     recm(5 + Q_SX, L.Sx, Rs.Sx, nullptr);
     recm(5 + Q_SY, L.Sy, Rs.Sy, nullptr);
     recm(5 + Q_SZ, L.Sz, Rs.Sz, nullptr);
-    if constexpr (SOLVER == 2) mcl_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F);
-    else if constexpr (SOLVER == 3) hllemc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F, stt);
-    else hllcmc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), F, stt);
+    T vstar = T(0);
+    auto riemann_mc = [&](T* A) {
+      if constexpr (SOLVER == 2) mcl_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), A);
+      else if constexpr (SOLVER == 3) hllemc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), A, stt);
+      else hllcmc_fluxes<D>(L, Rs, m_et2, m_bt1, T(gamma_d), T(sigma_d), A, stt,
+                            kEmF64<T, SOLVER> ? &vstar : nullptr);
+    };
+    if constexpr (kEmF64<T, SOLVER>) {
+      T A[NROLE];
+      riemann_mc(A);
+#pragma unroll
+      for (int c = R_Q; c < NROLE; ++c) F[c] = double(A[c]);
+      if constexpr (SOLVER == 4) psiphi_star_f64<D>(Ld, Rd, vstar, A, F);
+    } else {
+      riemann_mc(F);
+    }
     return stt;
   }
   // primitive slots of this direction (21-25 for x, 58-62 for y)
@@ -394,7 +470,6 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
       }
     }
   }
-  Side<double> Ld{}, Rd{};   // FP64 field face values (mixed MP solvers)
   if constexpr (kEmF64<T, SOLVER>) {
     // mixed precision: psi, phi, E and B are reconstructed as differences
     // from the cell's FP64 value (the MP limiters are translation-equivariant:
@@ -455,26 +530,7 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     riemann(A);
 #pragma unroll
     for (int c = R_Q; c < NROLE; ++c) F[c] = double(A[c]);
-    if constexpr (SOLVER == 7) {
-      // the HLLC star correction of psi and phi (16_hllc_flow_mpx.f95:
-      // 3485-3520, 3908-4300), in FP64 on the FP64 field face values with
-      // the FP32 contact speed; HLL and HLLE keep the fixed-speed fluxes
-      using X = Dir<D>;
-      const double h = 0.5, V = double(vstar);
-      const double psi_hll = h * (((Rd.psi + Ld.psi) + X::En(Ld)) - X::En(Rd));
-      const double phi_hll = h * (((Rd.phi + Ld.phi) + X::Bn(Ld)) - X::Bn(Rd));
-      const double En_f = F[R_EN], Bn_f = F[R_BN];
-      if (V != 0.0 && V == V) {
-        const double omV = 1.0 - V, opV = V + 1.0, k = V > 0.0 ? omV : opV;
-        const double psiR = (psi_hll - V * En_f) / omV, psiL = (psi_hll + V * En_f) / opV;
-        const double phiR = (phi_hll - V * Bn_f) / omV, phiL = (phi_hll + V * Bn_f) / opV;
-        F[R_PSI] = F[R_PSI] + (k * (psiR - psiL)) * h;
-        F[R_PHI] = F[R_PHI] + (k * (phiR - phiL)) * h;
-      } else if (V != V) {
-        F[R_PSI] = double(A[R_PSI]);   // the failed contact: NaN fluxes and the status bit
-        F[R_PHI] = double(A[R_PHI]);
-      }
-    }
+    if constexpr (SOLVER == 7) psiphi_star_f64<D>(Ld, Rd, vstar, A, F);
   } else {
     riemann(F);
   }
