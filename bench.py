@@ -178,7 +178,7 @@ def run_reference(args, cfg):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cfg.nx * cfg.ny / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic KH initial data (BASELINE config 2 shapes)",
+            "data": f"synthetic KH initial data ({cfg.nx} x {cfg.ny} shear layer, reference orientation)",
             "config": {"workload": cfg.name, "nx": cfg.nx, "ny": cfg.ny, "rk_stages": 4, "solver": "MP5+HLLC",
                        "sigma": cfg.sigma},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
@@ -588,7 +588,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f64+f32",
-            "data": "synthetic KH initial data (BASELINE config 2 shapes)",
+            "data": f"synthetic KH initial data ({cfg.nx} x {cfg.ny} shear layer, reference orientation)",
             "config": {"workload": cfg.name, "nx": cfg.nx, "ny": cfg.ny, "points": zones_pts(cfg), "rk_stages": s,
                        "solver": "MP5+HLLC", "imex": "SSP3(4,3,3), stage sums reset per stage",
                        "sigma": cfg.sigma,

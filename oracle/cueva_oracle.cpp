@@ -2261,8 +2261,8 @@ void oracle_kh_init(int32_t imax, int32_t jmax, double lx, double ly, double v0,
   for (int j = 0; j <= jmax; ++j)
     for (int i = 0; i <= imax; ++i) {
       const size_t k = (size_t)i + (size_t)j * (imax + 1);
-      const double posx = -0.5 * lx + i * Delx;   // reference x = BASELINE y (shear normal)
-      const double posy = -0.5 * ly + j * Dely;   // reference y = BASELINE x (periodic)
+      const double posx = -0.5 * lx + i * Delx;   // reference x = problem y (shear normal)
+      const double posy = -0.5 * ly + j * Dely;   // reference y = problem x (periodic, along the flow)
       const double vx = amp * std::sin(kpert * posy + phase) * std::exp(-(posx * posx) / width);
       const double vy = v0 * std::tanh(posx / a);
       const double vz = 0.0;

@@ -71,8 +71,8 @@ int32_t oracle_get_named(void* h, const char* name, int32_t l, double* out);
 int32_t oracle_get_named_full(void* h, const char* name, int32_t l, double* out);
 void    oracle_counters(void* h, int64_t* out3);
 
-/* KH initial data in the reference orientation (x_ref = BASELINE y, copy;
- * y_ref = BASELINE x, periodic), conventions of 03_init_var_primitive.f95:2297-2336 */
+/* KH initial data in the reference orientation (x_ref = problem y, copy;
+ * y_ref = problem x, periodic), conventions of 03_init_var_primitive.f95:2297-2336 */
 void    oracle_kh_init(int32_t imax, int32_t jmax, double lx, double ly,
                        double v0, double a, double amp, double width,
                        double kpert, double phase, double bshear,
