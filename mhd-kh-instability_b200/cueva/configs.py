@@ -52,15 +52,15 @@ class KHConfig:
                     rho0=1.0, p0=1.0)
 
 
-# config 1: plain FP64, 128 x 256, sigma 1e3, MP5 + HLL, SSP2(2,2,2), 200 steps, Cardano
+# small plain-FP64 workload: 128 x 256, sigma 1e3, MP5 + HLL, SSP2(2,2,2), 200 steps, Cardano
 C1 = KHConfig("kh-128x256-mp5-hll-ssp222-sigma1e3", 128, 256, order=2, flux_solver=5, sigma=1e3, steps=200)
-# config 2: plain FP64 at 1024 x 2048, MP5 + HLLC, sigma 1e6, SSP3(4,3,3), 500 steps.
+# benchmark workload: plain FP64 at 1024 x 2048, MP5 + HLLC, sigma 1e6, SSP3(4,3,3), 500 steps.
 # The reference's SSP3(4,3,3) keeps accumulating the stage sums across stages
 # (cleanvarint runs once per step) and breaks down within a few steps; the
 # workload runs the tableau with the sums reset before every stage.
 C2 = KHConfig("kh-1024x2048-mp5-hllc-ssp433-sigma1e6", 1024, 2048, order=4, flux_solver=7, sigma=1e6, steps=500,
               intsum_reset=1)
-# config 3: 2048 x 4096, V0 = 0.8, sigma 1e5 (MP7 / MP9 variants; mixed precision)
+# large study workload: 2048 x 4096, V0 = 0.8, sigma 1e5 (MP7 / MP9 variants; mixed precision)
 C3 = KHConfig("kh-2048x4096-mp5-hllc-ssp433-v08-sigma1e5", 2048, 4096, order=4, flux_solver=7, sigma=1e5,
               v0=0.8, steps=1000, intsum_reset=1)
 # north-star target: 2048 x 4096 MP5 + HLLC resistive KH
