@@ -63,7 +63,7 @@ C2 = KHConfig("kh-1024x2048-mp5-hllc-ssp433-sigma1e6", 1024, 2048, order=4, flux
 # large study workload: 2048 x 4096, V0 = 0.8, sigma 1e5 (MP7 / MP9 variants; mixed precision)
 C3 = KHConfig("kh-2048x4096-mp5-hllc-ssp433-v08-sigma1e5", 2048, 4096, order=4, flux_solver=7, sigma=1e5,
               v0=0.8, steps=1000, intsum_reset=1)
-# north-star target: 2048 x 4096 MP5 + HLLC resistive KH
+# target workload: 2048 x 4096 MP5 + HLLC resistive KH, sigma 1e6
 TARGET = KHConfig("kh-2048x4096-mp5-hllc-ssp433-sigma1e6", 2048, 4096, order=4, flux_solver=7, sigma=1e6,
                   steps=500, intsum_reset=1)
 
