@@ -57,7 +57,7 @@ typedef struct cueva_params {
   int32_t c2p;          /* 1 Cardano, 0 Newton-Raphson (parameters.f95:37), 2 learned seed + Newton */
   int32_t bc_x, bc_y;   /* per-axis ghost rule: 0 copy, 1 periodic (BOUND 1 / 2 / 6 of 04_boundary.f95) */
   int32_t precision;    /* 0 FP64 throughout; 1 FP32 reconstruction + Riemann, FP64 elsewhere
-                           (flux_solver 2, 4..7: psi, phi, E, B reconstructed as differences
+                           (flux_solver 1, 2, 4..7: psi, phi, E, B reconstructed as differences
                            from a cell value and their fluxes kept in FP64) */
   int32_t device;       /* CUDA device ordinal */
   int32_t intsum_reset; /* 0: the stage sums are zeroed once per step and accumulate over the stages

@@ -134,16 +134,13 @@ struct StageShape {
 inline int xupd_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 30) / 31) * ((jmax + 1 + rows - 1) / rows); }
 inline int yface_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 31) / 32) * ((jmax + 2 + rows - 1) / rows); }
 
-// The mixed-precision HLL / HLLE / HLLC routines (flux_solver 2, 4 with the
-// MC reconstruction, 5..7 with MP) keep the fluxes of the field roles psi,
+// The mixed-precision flux routines keep the fluxes of the field roles psi,
 // phi, Bn, Bt1, Bt2, En, Et1, Et2 (roles 0..7) in FP64: they carry the
 // uniform background field (B ~ 0.1 in the KH runs), whose FP32 rounding
 // (~4e-9) is not small against E itself, and the final IMEX combination
-// passes that error into E(n+1) undamped.  The Lax pairs (1) and HLLE-MC
-// (3, field star states with the sound-speed bounds) stay FP32.
-__host__ __device__ constexpr bool mixed_em_f64(int solver) {
-  return solver == 2 || solver == 4 || (solver >= 5 && solver <= 7);
-}
+// passes that error into E(n+1) undamped.  All routines but HLLE-MC
+// (flux_solver 3, whose field star states use the sound-speed bounds).
+__host__ __device__ constexpr bool mixed_em_f64(int solver) { return solver >= 1 && solver <= 7 && solver != 3; }
 
 // Place of role r in the y-flux scratch (NFACE slabs of ffs doubles): f64
 // tells the element type and off the slab's first element in units of that

@@ -320,8 +320,38 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     T hW2[NS], EB[NS];
 #pragma unroll
     for (int q = 0; q < NS; ++q) lax_cell_scalars(cell(q), gamma, hW2[q], EB[q]);
+    if constexpr (kEmF64<T, SOLVER>) {
+      // mixed precision: the field roles (psi, phi, E, B) form p = F + U in
+      // FP64, take the MC slopes of the differences from p of cell 1 in FP32
+      // (the slopes are differences) and the face flux back in FP64
+      auto cell_d = [&](int q) {
+        Side<double> sd{};
+        sd.psi = nrmd(5 + Q_PSI, q); sd.phi = nrmd(5 + Q_PHI, q);
+        sd.Ex = nrmd(5 + Q_EX, q); sd.Ey = nrmd(5 + Q_EY, q); sd.Ez = nrmd(5 + Q_EZ, q);
+        sd.Bx = nrmd(5 + Q_BX, q); sd.By = nrmd(5 + Q_BY, q); sd.Bz = nrmd(5 + Q_BZ, q);
+        return sd;
+      };
 #pragma unroll
-    for (int r = 0; r < NROLE; ++r) {
+      for (int r = R_PSI; r <= R_ET2; ++r) {
+        double pd[NS], m2 = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          double f, u;
+          lax_pair<D>(r, cell_d(q), 0.0, 0.0, f, u);
+          pd[q] = f + u;
+          if (q == 2) m2 = f - u;
+        }
+        const double c0 = pd[1];
+        T d[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) d[q] = T(pd[q] - c0);
+        const double Lf = c0 + double(d[1] + T(0.5) * mc_slope(d[2] - d[1], d[1] - d[0]));
+        const double Rf = m2 - double(T(0.5) * mc_slope(d[3] - d[2], d[2] - d[1]));
+        F[r] = (r == R_BT1 || r == R_ET2) ? -(0.5 * (Lf + Rf)) : 0.5 * (Lf + Rf);
+      }
+    }
+#pragma unroll
+    for (int r = (kEmF64<T, SOLVER> ? R_Q : 0); r < NROLE; ++r) {
       T p[NS], m2 = T(0);
 #pragma unroll
       for (int q = 0; q < NS; ++q) {

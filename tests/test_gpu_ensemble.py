@@ -128,7 +128,7 @@ def test_primitive_reconstruction_ensemble_matches_single_runs():
     ens.close()
 
 
-@pytest.mark.parametrize("solver,precision", [(1, 0), (2, 0), (3, 1), (4, 0), (4, 1), (6, 1), (7, 1)])
+@pytest.mark.parametrize("solver,precision", [(1, 0), (1, 1), (2, 0), (3, 1), (4, 0), (4, 1), (6, 1), (7, 1)])
 def test_ensemble_other_flux_routines_match_single_runs(solver, precision):
     """The batched path runs every flux routine (and the mixed-precision
     kernels, whose FP64 field-flux slabs sit at offsets of each instance's
