@@ -2,9 +2,10 @@
 """Benchmark of the B200 CUEVA hot path: zone-updates/s of the resistive
 relativistic MHD Kelvin-Helmholtz run (plain FP64 and mixed precision).
 
-Workload: 1024 x 2048 cells, MP5 + HLLC, IMEX SSP3(4,3,3), sigma = 1e6
-(synthetic KH initial data, reference orientation).  One bench "step" is one
-full time step (4 RK stages) of that grid; the state stays resident in HBM.
+Workload: 2048 x 4096 cells, MP5 + HLLC, IMEX SSP3(4,3,3), sigma = 1e6
+(synthetic KH initial data, reference orientation), the resistive KH run the
+metric is quoted on.  One bench "step" is one full time step (4 RK stages) of
+that grid; the state stays resident in HBM.
 `e2e` repeats the measurement through the C-ABI with host buffers: each step
 uploads the 14 primitive fields from pinned host memory, advances one step
 and downloads them again, all inside the timed region (the readback of step k
@@ -58,6 +59,40 @@ def kernel_bytes_per_unit(s):
     its 20 stencil fields and 14 y fluxes (each y face is shared by two
     points) plus the stage's share of the resident state I/O."""
     return (FACE_BYTES, 8.0 * (20 + 14) + alg_bytes_per_zone(s) / s)
+
+
+# FP64 arithmetic of the B200: 64 FP64 lanes per SM and clock on 148 SMs
+# (NVIDIA's 37 TFLOP/s FP64 figure is this at 1965 MHz with an FMA counted as
+# two flops).  A spec value, not measured on this pool.
+FP64_LANES_PER_SM = 64
+N_SM = 148
+
+
+def fp64_roofline(kernels, units, name, sm_mhz):
+    """FP64 roofline of kernel `name`: counted FP64 instructions and flops per
+    unit (profiles/fp64_ops.json, from an ncu count of the same kernels)
+    times the units of a launch over the launch's average CUDA-event time,
+    against the FP64 lanes at the SM clock sampled during the timed region."""
+    path = os.path.join(ROOT, "profiles", "fp64_ops.json")
+    if not os.path.exists(path) or not sm_mhz:
+        return None
+    with open(path) as f:
+        ops = json.load(f)
+    k = ops.get("kernels", {}).get(name)
+    if not k or not kernels.get(name, {}).get("avg_ms"):
+        return None
+    idx = KERNELS.index(name)
+    sec = kernels[name]["avg_ms"] * 1e-3
+    instr_rate = k["fp64_instr_per_unit"] * units[idx] / sec
+    flop_rate = k["fp64_flops_per_unit"] * units[idx] / sec
+    lane_rate = FP64_LANES_PER_SM * N_SM * sm_mhz * 1e6
+    return {"bound": "fp64", "achieved": flop_rate / 1e12, "peak": 2 * lane_rate / 1e12, "unit": "TFLOP/s",
+            "frac": flop_rate / (2 * lane_rate), "pipe_frac": instr_rate / lane_rate, "kernel": name,
+            "fp64_instr_per_unit": k["fp64_instr_per_unit"], "fp64_flops_per_unit": k["fp64_flops_per_unit"],
+            "peak_kind": f"spec: {FP64_LANES_PER_SM} FP64 lanes/SM x {N_SM} SMs at the sampled {sm_mhz:.0f} MHz",
+            "note": "frac = counted FP64 flops (FMA = 2) over the lanes' FMA peak; pipe_frac = FP64 "
+                    "instructions over the lanes' issue rate (the no-FMA build keeps a multiply-add as two "
+                    "instructions); counts from " + ops.get("source", "profiles/fp64_ops.json")}
 
 
 def measured_peaks():
@@ -139,9 +174,10 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_port_rate(cfg, steps_budget_s=20.0, max_steps=2, threads=None):
+def cpu_port_rate(cfg, steps_budget_s=20.0, max_steps=2, threads=None, warmup=1):
     """Zone-updates/s of the CPU restatement (the oracle) on a bounded sample
-    of the workload: the full grid, as many whole steps as fit the budget."""
+    of the workload: the full grid, after `warmup` untimed steps as many whole
+    steps as fit the budget (at least one, at most max_steps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     oracle_py.build()
@@ -151,7 +187,8 @@ def cpu_port_rate(cfg, steps_budget_s=20.0, max_steps=2, threads=None):
     kw.pop("precision", None)
     o = oracle_py.Oracle(**kw)
     o.set_prims(oracle_py.kh_init(cfg.imax, cfg.jmax, **{k: v for k, v in cfg.kh_kwargs().items()}))
-    o.step(1)     # warm-up (page faults of the ~5 GB working set)
+    for _ in range(max(warmup, 1)):
+        o.step(1)     # warm-up (page faults of the working set)
     n, t0 = 0, time.perf_counter()
     while n < max_steps:
         o.step(1)
@@ -163,18 +200,17 @@ def cpu_port_rate(cfg, steps_budget_s=20.0, max_steps=2, threads=None):
 
 
 def run_reference(args, cfg):
+    """The reference arm: the CPU restatement of the Fortran (the Fortran
+    itself cannot be compiled here) on all host cores, same workload and
+    metric.  Its steps are whole time steps of the same grid; they are
+    bounded to about 90 s of CPU work, so a long --steps run stops early and
+    says so in `sample`."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    rates = []
-    for _ in range(max(args.warmup, 0)):
-        pass
     threads = os.cpu_count() or 1
-    for _ in range(args.steps):
-        r, threads, sample = cpu_port_rate(cfg, steps_budget_s=max(5.0, 60.0 / max(args.steps, 1)), max_steps=1,
-                                           threads=threads)
-        rates.append(r)
-    value = sum(rates) / len(rates)
+    value, threads, sample = cpu_port_rate(cfg, steps_budget_s=90.0, max_steps=max(args.steps, 1), threads=threads,
+                                           warmup=1)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cfg.nx * cfg.ny / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -182,8 +218,8 @@ def run_reference(args, cfg):
             "config": {"workload": cfg.name, "nx": cfg.nx, "ny": cfg.ny, "rk_stages": 4, "solver": "MP5+HLLC",
                        "sigma": cfg.sigma},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "per bench step one full time step of the 1024x2048 grid; CPU "
-                                       "restatement of the Fortran (no Fortran compiler on this image)"},
+                             "sample": sample + " after 1 untimed step, bounded to ~90 s; CPU restatement of "
+                                                "the Fortran (no Fortran compiler on this image)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -323,6 +359,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
         ms = float(t.item())
     m.download()
     errs = {n: rel_l1_field(n, m.interior(n), ref[n], ref) for n in PRIM_NAMES}
+    errs_vec = dict(errs, **vector_rel_l1(m, ref))
     its, pts, fails = learned_stats(m)
     prof_ms, prof_n = m.profile_steps(args.profile_steps) if args.profile_steps > 0 else ([0.0] * 3, [0] * 3)
     m.close()
@@ -340,6 +377,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
             "max_rel_l1_vs_fp64_one_step_vector_norm": max(one_vec.values()),
             "error_vs_fp64_after_steps": max(args.warmup, 3) + args.steps,
             "rel_l1_vs_fp64": errs, "max_rel_l1_vs_fp64": max(errs.values()),
+            "rel_l1_vs_fp64_vector_norm": errs_vec, "max_rel_l1_vs_fp64_vector_norm": max(errs_vec.values()),
             "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}
 
 
@@ -459,12 +497,12 @@ def main():
     ap.add_argument("--ens-n", type=int, default=64)
     args = ap.parse_args()
 
-    from cueva.configs import C2
-    cfg = C2
+    from cueva.configs import TARGET
+    cfg = TARGET
     if args.grid:
         import dataclasses
         nx, ny = (int(v) for v in args.grid.lower().split("x"))
-        cfg = dataclasses.replace(C2, nx=nx, ny=ny, name=C2.name.replace("1024x2048", f"{nx}x{ny}"))
+        cfg = dataclasses.replace(TARGET, nx=nx, ny=ny, name=TARGET.name.replace("2048x4096", f"{nx}x{ny}"))
     if args.impl == "reference":
         return run_reference(args, cfg)
     if args.mixed_study:
@@ -585,6 +623,8 @@ def main():
     if os.path.exists(tpath):
         with open(tpath) as f:
             traffic = json.load(f).get(KERNELS[top], {}).get("dram_bytes_per_launch_full")
+    clocks = clk.summary()
+    roof_fp64 = fp64_roofline(kernels, units, KERNELS[top], clocks.get("sm_mhz"))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f64+f32",
@@ -601,7 +641,8 @@ def main():
                          "kernel": KERNELS[top], "kernels": kernels,
                          "note": f"{KERNELS[top]}: {bpu[top]:.0f} algorithmic B per unit x {units[top]} units "
                                  f"per launch / avg launch {kernels[KERNELS[top]]['avg_ms']:.3f} ms"},
-            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 2 * s * args.steps, "mixed_learned": mixed}
+            "roofline_fp64": roof_fp64,
+            "clocks": clocks, "e2e": e2e, "gpu_launches": 2 * s * args.steps, "mixed_learned": mixed}
     if rank == 0 and not args.no_cpu_baseline:
         r, cores, sample = cpu_port_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

@@ -41,6 +41,8 @@ extern "C" {
 #define CUEVA_ST_NONFINITE 16u      /* con2prim returned NaN/Inf (the reference continues silently) */
 #define CUEVA_ST_HLLE_SPEED 32u     /* 16_hlle_flow_mpx.f95:2796-2803, 2974-2981 (NaN wave bounds) */
 #define CUEVA_ST_TC_TIMEOUT 64u     /* a bounded tensor-core (tcgen05) wait ran out; no reference counterpart */
+#define CUEVA_ST_TC_TEARDOWN 128u   /* after such a time-out the teardown's bounded wait ran out too: TMEM was
+                                       released while an MMA may still write it; destroy the context */
 
 typedef struct cueva_ctx cueva_ctx;
 
@@ -133,11 +135,13 @@ int32_t cueva_upload(cueva_ctx* ctx, uint32_t groups);
 int32_t cueva_download(cueva_ctx* ctx, uint32_t groups);
 /* cueva_download without the wait: the copies run on a second stream, after
  * the work already queued on the context stream, one field after another.
- * The host arrays hold the result after the next cueva_sync (or cueva_download,
- * cueva_step, ...: every later call orders its work after the readback).  A
- * following cueva_upload of the same arrays waits per field, so field f goes
- * back up while field f+1 still comes down.  Kernel status is reported by the
- * next call that synchronises. */
+ * The bound host arrays are being written until a call that waits for the
+ * host returns: cueva_sync, cueva_download or cueva_status.  Until then the
+ * caller must not read, modify, rebind or free them (later calls such as
+ * cueva_step only order their device work after the copies; they do not
+ * wait).  A following cueva_upload of the same arrays waits per field on the
+ * device, so field f goes back up while field f+1 still comes down.  Kernel
+ * status is reported by the next call that synchronises. */
 int32_t cueva_download_async(cueva_ctx* ctx, uint32_t groups);
 
 /* ---- the hot path ----------------------------------------------------- */
@@ -314,11 +318,14 @@ int32_t cueva_ens_learned_stats(cueva_ens* ens, int64_t out3[3]);
  * (jmax + 2) doubles plus a small header): grids that need more are
  * rejected with CUEVA_ERR_ARG and a message giving both sizes; 512 x 512
  * fits.  The first call on a device looks up the block's address and sets
- * the kernels' shared-memory limits there (no allocation); make that first
- * call before any stream capture.  The status word in the block is zeroed
- * by every call.  The block is shared by all calls on a device, so calls
- * that overlap in time (on different streams or host threads) race on it;
- * serialise them.
+ * the kernels' shared-memory limits there (no allocation), under a lock, so
+ * host threads that make their first calls together set up once.  The call
+ * uploads its kernel descriptor from host memory of the call itself and may
+ * wait for the stream, so it returns CUEVA_ERR_ARG on a stream that is being
+ * captured into a CUDA graph.  The status word in the block is zeroed by
+ * every call.  The block is shared by all calls on a device, so calls that
+ * overlap in time on the GPU (on different streams or host threads) race on
+ * it; serialise them.
  *
  * Asynchronous on `stream` (0 = the legacy default stream).  If
  * status_bits is non-null the call waits for the stream and stores the

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -314,7 +315,7 @@ int32_t read_status(cueva_ctx* c) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st) {
     char buf[160];
-    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed, 64 tensor-core wait)", st);
+    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed, 64 tensor-core wait, 128 tensor-core teardown: context suspect)", st);
     return fail(CUEVA_ERR_PHYSICS, buf);
   }
   return CUEVA_OK;
@@ -1234,6 +1235,9 @@ constexpr size_t kNoallocHeader = 256;
 constexpr size_t kNoallocDesc = (sizeof(InstDesc) + 255) / 256 * 256;
 constexpr int kMaxDevices = 64;
 void* g_noalloc_base[kMaxDevices] = {};
+// the once-per-device set-up (and every read of g_noalloc_base) runs under
+// this lock, so host threads making their first call together set up once
+std::mutex g_noalloc_mu;
 }  // namespace
 static __device__ __align__(256) double g_noalloc_scratch[kNoallocBytes / sizeof(double)];
 
@@ -1257,17 +1261,27 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
                                    " bytes, the static block holds " + std::to_string(kNoallocBytes));
   if (p->device < 0 || p->device >= kMaxDevices) return fail(CUEVA_ERR_ARG, "device ordinal out of range");
   CUDA_TRY(cudaSetDevice(p->device));
-  if (!g_noalloc_base[p->device]) {
-    // once per device, with that device current
-    void* base = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress(&base, g_noalloc_scratch));
-    for (int rm = 0; rm < 3; ++rm)
-      for (int sv : {5, 6, 7})
-        for (int pr = 0; pr < 2; ++pr) CUDA_TRY(prepare_stage(rm, sv, pr));
-    g_noalloc_base[p->device] = base;
-  }
-  char* base = (char*)g_noalloc_base[p->device];
   cudaStream_t st = (cudaStream_t)stream;
+  // the descriptor goes up from this call's stack and the status read waits
+  // for the stream: neither may be recorded into a graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(CUEVA_ERR_ARG, "cueva_flux_rhs_noalloc cannot run on a stream that is being captured");
+  char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[p->device]) {
+      // once per device, with that device current
+      void* b = nullptr;
+      CUDA_TRY(cudaGetSymbolAddress(&b, g_noalloc_scratch));
+      for (int rm = 0; rm < 3; ++rm)
+        for (int sv : {5, 6, 7})
+          for (int pr = 0; pr < 2; ++pr) CUDA_TRY(prepare_stage(rm, sv, pr));
+      g_noalloc_base[p->device] = b;
+    }
+    base = (char*)g_noalloc_base[p->device];
+  }
   InstDesc I{};
   I.status = (uint32_t*)base;
   I.counters = (unsigned long long*)(base + 8);

@@ -84,10 +84,12 @@ k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPD
   __shared__ MLPShared S;
   mlp_tc_setup(S, *mlp);
   uint32_t phase = 0;
+  uint32_t* tile_status = insts[0].status;   // the instance of the CTA's last tile (teardown status)
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     int b = tile;
     const InstDesc& I = tile_inst(insts, ninst, LK_C2P, b);
     if (!(I.c2p == 2 && I.c2p_tc)) continue;   // uniform over the CTA: a tile belongs to one instance
+    tile_status = I.status;
     if (tile + (int)gridDim.x < ntiles) {       // the next tile's inputs go to L2 meanwhile
       int bn = tile + (int)gridDim.x;
       const InstDesc& In = tile_inst(insts, ninst, LK_C2P, bn);
@@ -125,7 +127,7 @@ k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPD
       if (!I.primitive_rec) begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
     }
   }
-  mlp_tc_teardown(S, phase);
+  mlp_tc_teardown(S, phase, tile_status);
 }
 
 // network seeds of n states (SoA 11 x n conserved), tensor-core form
@@ -149,7 +151,7 @@ k_predict_tc(long long n, const MLPDevice* __restrict__ mlp, const double* __res
     }
     if (i0 < n) pseed[i] = cons[i] * (double)__expf(y * S.sd_y + S.mu_y);
   }
-  mlp_tc_teardown(S, phase);
+  mlp_tc_teardown(S, phase, err_status);
 }
 
 int c2p_grid(long long ntiles) {

@@ -35,6 +35,9 @@ enum StatusBits : uint32_t {
   ST_NONFINITE = 16u,      // con2prim returned NaN / Inf
   ST_HLLE_SPEED = 32u,     // 16_hlle_flow_mpx.f95:2796-2803, 2974-2981
   ST_TC_TIMEOUT = 64u,     // a bounded tensor-core wait ran out (no reference counterpart)
+  ST_TC_TEARDOWN = 128u,   // after such a time-out the teardown's bounded wait for the MMAs still in
+                           // flight ran out too: TMEM was released while an MMA may still write it, so
+                           // the context is suspect and should not be reused
 };
 
 // ---- per-instance descriptor (one grid of the ensemble) -------------------

@@ -95,11 +95,16 @@ __device__ __forceinline__ void mlp_tc_setup(MLPShared& S, const MLPDevice& M, u
 }
 
 // Releases the TMEM columns (all threads call it, after their last tile).
-__device__ __forceinline__ void mlp_tc_teardown(MLPShared& S, uint32_t phase) {
+// After a timed-out wait the MMAs of that commit may still be in flight: one
+// more bounded wait covers them, and if that runs out too, ST_TC_TEARDOWN
+// goes to *status (the columns are released regardless, since a CTA must not
+// exit holding TMEM).
+__device__ __forceinline__ void mlp_tc_teardown(MLPShared& S, uint32_t phase, uint32_t* status) {
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
-  if (S.fail && threadIdx.x == 0) umma::mbar_wait(&S.bar, phase, S.max_polls);   // MMAs still in flight
+  if (S.fail && threadIdx.x == 0 && !umma::mbar_wait(&S.bar, phase, S.max_polls))   // MMAs still in flight
+    atomicOr(status, ST_TC_TEARDOWN);
   __syncthreads();
   if (threadIdx.x < 32) umma::tmem_dealloc(S.taddr, TC_TMEM_COLS);
 }

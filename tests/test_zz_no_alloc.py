@@ -30,13 +30,16 @@ def _device_group(torch, arrays, pitch, ny):
     return slab
 
 
-@pytest.mark.parametrize("solver,rec", [(7, 0), (5, 2)])
-def test_noalloc_matches_flux_rhs(oracle_mod, solver, rec):
+@pytest.mark.parametrize("solver,rec,precision", [(7, 0, 0), (5, 2, 0), (7, 0, 1), (5, 2, 1)])
+def test_noalloc_matches_flux_rhs(oracle_mod, solver, rec, precision):
+    """precision = 1 runs the mixed kernels, whose scratch holds FP64 slabs
+    for the field roles and FP32 slabs for the rest; the reference call is
+    cueva_flux_rhs of a context with the same precision."""
     torch = pytest.importorskip("torch")
     from cueva import Cueva, _abi
     imax, jmax = 64, 32
     oracle_mod.set_libm_seed(0)
-    g = Cueva(imax, jmax, order=2, flux_solver=solver, rec_mp=rec, sigma=1e3)
+    g = Cueva(imax, jmax, order=2, flux_solver=solver, rec_mp=rec, sigma=1e3, precision=precision)
     o = oracle_mod.Oracle(imax, jmax, order=2, flux_solver=solver, rec_mp=rec, sigma=1e3)
     g.kh_init(v0=0.5, a=0.05)
     o.set_prims(g.prims())
@@ -84,3 +87,31 @@ def test_noalloc_rejects_oversized_grid():
                                   ctypes.byref(st))
     assert rc == _abi.CUEVA_ERR_ARG
     assert b"too large" in L.cueva_last_error()
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """The call uploads its descriptor from its own stack and may wait for
+    the stream, so a stream under capture is refused before anything is
+    enqueued."""
+    torch = pytest.importorskip("torch")
+    from cueva import _abi
+    L = _abi.load()
+    imax, jmax = 64, 32
+    p = _abi.Params(imax, jmax, 2, 7, 0, 1, 0, 1, 0, 0, 0, 0, 2.0, 1.0, 1.0, 0.25, 1e3, 4.0 / 3.0, 0.0)
+    pitch, ny = 72, jmax + 1
+    prim = torch.zeros((14, ny, pitch), dtype=torch.float64, device="cuda")
+    W = torch.ones((1, ny, pitch), dtype=torch.float64, device="cuda")
+    stage = torch.zeros((17, ny, pitch), dtype=torch.float64, device="cuda")
+    rhs = torch.zeros((17, ny, pitch), dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        graph.capture_begin()
+        rc = L.cueva_flux_rhs_noalloc(ctypes.byref(p), prim.data_ptr(), W.data_ptr(), stage.data_ptr(),
+                                      rhs.data_ptr(), pitch, pitch * ny, s.cuda_stream, None)
+        rhs.add_(0.0)   # keeps the captured graph non-empty
+        graph.capture_end()
+    assert rc == _abi.CUEVA_ERR_ARG
+    assert b"captured" in L.cueva_last_error()
+    del graph
