@@ -45,20 +45,21 @@ def alg_bytes_per_zone(s):
 
 
 FACE_BYTES = 8.0 * (20 + 14)   # per interface: 20 reconstructed fields read once, 14 fluxes written
-KERNELS = ("k_yface", "k_xupd")
 
 
-def kernel_units(cfg):
-    """Units one launch of each kernel processes: y faces, points."""
-    return ((cfg.imax + 1) * (cfg.jmax + 2), (cfg.imax + 1) * (cfg.jmax + 1))
-
-
-def kernel_bytes_per_unit(s):
-    """Algorithmic bytes per unit: a y face reads the 20 reconstructed fields
-    once and writes 14 fluxes; a point of the x-face + update kernel reads
-    its 20 stencil fields and 14 y fluxes (each y face is shared by two
-    points) plus the stage's share of the resident state I/O."""
-    return (FACE_BYTES, 8.0 * (20 + 14) + alg_bytes_per_zone(s) / s)
+def stage_kernels(cfg, s, kms, kcnt):
+    """The stage kernels of the profiled steps: name -> (units per launch,
+    algorithmic bytes per unit, summed ms, launches).  Slot 1 of the profile
+    is the kernel that updates the points: the fused k_stage (no y-face
+    launches in slot 0), or k_xupd after k_yface.  The fused kernel's bytes
+    per point are the stage's share of the whole-step figure, B_alg(s) / s;
+    the split kernels add the y-flux round trip and the twice-staged
+    stencil fields, which the fused kernel does not move."""
+    pts = (cfg.imax + 1) * (cfg.jmax + 1)
+    if kcnt[0] == 0:
+        return {"k_stage": (pts, alg_bytes_per_zone(s) / s, kms[1], kcnt[1])}
+    return {"k_yface": ((cfg.imax + 1) * (cfg.jmax + 2), FACE_BYTES, kms[0], kcnt[0]),
+            "k_xupd": (pts, 8.0 * (20 + 14) + alg_bytes_per_zone(s) / s, kms[1], kcnt[1])}
 
 
 # FP64 arithmetic of the B200: 64 FP64 lanes per SM and clock on 148 SMs
@@ -68,7 +69,7 @@ FP64_LANES_PER_SM = 64
 N_SM = 148
 
 
-def fp64_roofline(kernels, units, name, sm_mhz):
+def fp64_roofline(kernels, name, sm_mhz):
     """FP64 roofline of kernel `name`: counted FP64 instructions and flops per
     unit (profiles/fp64_ops.json, from an ncu count of the same kernels)
     times the units of a launch over the launch's average CUDA-event time,
@@ -81,10 +82,10 @@ def fp64_roofline(kernels, units, name, sm_mhz):
     k = ops.get("kernels", {}).get(name)
     if not k or not kernels.get(name, {}).get("avg_ms"):
         return None
-    idx = KERNELS.index(name)
+    units = kernels[name]["units"]
     sec = kernels[name]["avg_ms"] * 1e-3
-    instr_rate = k["fp64_instr_per_unit"] * units[idx] / sec
-    flop_rate = k["fp64_flops_per_unit"] * units[idx] / sec
+    instr_rate = k["fp64_instr_per_unit"] * units / sec
+    flop_rate = k["fp64_flops_per_unit"] * units / sec
     lane_rate = FP64_LANES_PER_SM * N_SM * sm_mhz * 1e6
     return {"bound": "fp64", "achieved": flop_rate / 1e12, "peak": 2 * lane_rate / 1e12, "unit": "TFLOP/s",
             "frac": flop_rate / (2 * lane_rate), "pipe_frac": instr_rate / lane_rate, "kernel": name,
@@ -368,8 +369,8 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     return {"value": world * cfg.nx * cfg.ny * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
             "dtype": "f32 reconstruction + Riemann (psi, phi, E, B fluxes f64), f64 update / implicit E / con2prim",
             "con2prim": "network seed on the tcgen05 tensor cores (k_c2p_step), Newton in FP64, Cardano fall-back",
-            "kernel_ms_per_step": {"k_yface": prof_ms[0] / nprof, "k_xupd": prof_ms[1] / nprof,
-                                   "k_c2p_step": prof_ms[2] / nprof},
+            "kernel_ms_per_step": dict({n: v[2] / nprof for n, v in stage_kernels(cfg, 4, prof_ms, prof_n).items()},
+                                       k_c2p_step=prof_ms[2] / nprof),
             "rel_l1_learned_vs_cardano_one_step": one_c2p,
             "max_rel_l1_learned_vs_cardano_one_step": max(one_c2p.values()),
             "rel_l1_vs_fp64_one_step": one_err, "max_rel_l1_vs_fp64_one_step": max(one_err.values()),
@@ -485,6 +486,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 mixed")
     ap.add_argument("--c2p", type=int, default=1, help="1 Cardano (reference), 0 NR, 2 learned seed + Newton")
+    ap.add_argument("--stage-kernel", type=int, default=None,
+                    help="1 one fused kernel per RK stage, 0 the y-face + x-face/update kernels (default: fused)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--profile-steps", type=int, default=3)
@@ -523,6 +526,8 @@ def main():
     from cueva import Cueva
 
     g = Cueva(device=local, pinned=True, **dict(cfg.solver_kwargs(), precision=args.precision, c2p=args.c2p))
+    if args.stage_kernel is not None:
+        g.set_stage_kernel(args.stage_kernel)
     if args.c2p == 2:
         from cueva.learned import LearnedSeed
         from cueva.train_seed import DEFAULT
@@ -608,23 +613,26 @@ def main():
     peak, peak_kind = measured_peaks()
     kms, kcnt = g.profile_steps(args.profile_steps)
     g.sync()
-    units = kernel_units(cfg)
-    bpu = kernel_bytes_per_unit(s)
     kernels = {}
-    for k, name in enumerate(KERNELS):
-        avg = kms[k] / max(kcnt[k], 1)
-        kernels[name] = {"avg_ms": avg, "launches": kcnt[k], "share": kms[k] / max(sum(kms), 1e-30),
-                         "alg_bytes_per_launch": bpu[k] * units[k],
-                         "gbs": bpu[k] * units[k] / (avg * 1e-3) / 1e9 if avg > 0 else None}
-    top = max(range(len(KERNELS)), key=lambda k: kms[k])
-    achieved = kernels[KERNELS[top]]["gbs"]
+    for name, (units, bpu, ms_sum, cnt) in stage_kernels(cfg, s, kms, kcnt).items():
+        avg = ms_sum / max(cnt, 1)
+        kernels[name] = {"avg_ms": avg, "launches": cnt, "share": ms_sum / max(sum(kms), 1e-30), "units": units,
+                         "alg_bytes_per_unit": bpu, "alg_bytes_per_launch": bpu * units,
+                         "gbs": bpu * units / (avg * 1e-3) / 1e9 if avg > 0 else None}
+    top = max(kernels, key=lambda n: kernels[n]["avg_ms"] * kernels[n]["launches"])
+    achieved = kernels[top]["gbs"]
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "kernel_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(KERNELS[top], {}).get("dram_bytes_per_launch_full")
+            tr = json.load(f)
+        per_unit = tr.get("kernels", {}).get(top, {}).get("dram_bytes_per_unit")
+        if per_unit is not None:
+            traffic = per_unit * kernels[top]["units"]
     clocks = clk.summary()
-    roof_fp64 = fp64_roofline(kernels, units, KERNELS[top], clocks.get("sm_mhz"))
+    roof_fp64 = fp64_roofline(kernels, top, clocks.get("sm_mhz"))
+    step_bytes = alg_bytes_per_zone(s) * zones_pts(cfg)
+    launches_per_step = sum(kcnt) / max(args.profile_steps, 1)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == 0 else "f64+f32",
@@ -633,16 +641,24 @@ def main():
                        "solver": "MP5+HLLC", "imex": "SSP3(4,3,3), stage sums reset per stage",
                        "sigma": cfg.sigma,
                        "precision": "fp64" if args.precision == 0 else "mixed",
-                       "l2": "working set ~2.2 GB >> 126 MB L2 (no flush needed)",
+                       "l2": f"working set {g.device_bytes() / 1e9:.1f} GB on the device >> 126 MB L2 "
+                             "(no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,
-                         "kernel": KERNELS[top], "kernels": kernels,
-                         "note": f"{KERNELS[top]}: {bpu[top]:.0f} algorithmic B per unit x {units[top]} units "
-                                 f"per launch / avg launch {kernels[KERNELS[top]]['avg_ms']:.3f} ms"},
+                         "kernel": top, "kernels": kernels,
+                         "whole_step_gbs": step_bytes / (ms_per_step * 1e-3) / 1e9,
+                         "whole_step_frac": step_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+                         "note": f"{top}: {kernels[top]['alg_bytes_per_unit']:.0f} algorithmic B per unit x "
+                                 f"{kernels[top]['units']} units per launch / avg launch "
+                                 f"{kernels[top]['avg_ms']:.3f} ms; whole step: B_alg(s) = "
+                                 f"{alg_bytes_per_zone(s):.0f} B per point over the timed ms per step; "
+                                 "traffic: DRAM bytes per unit of an ncu capture (profiles/kernel_traffic.json) "
+                                 "times the units of a launch"},
             "roofline_fp64": roof_fp64,
-            "clocks": clocks, "e2e": e2e, "gpu_launches": 2 * s * args.steps, "mixed_learned": mixed}
+            "clocks": clocks, "e2e": e2e, "gpu_launches": int(round(launches_per_step * args.steps)),
+            "mixed_learned": mixed}
     if rank == 0 and not args.no_cpu_baseline:
         r, cores, sample = cpu_port_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

@@ -152,6 +152,18 @@ int32_t cueva_download_async(cueva_ctx* ctx, uint32_t groups);
  * varfin, electricfield, varprimitivecardano or varprimitive_nr), on the
  * device-resident state.  Asynchronous on the context stream. */
 int32_t cueva_step(cueva_ctx* ctx, int32_t nsteps);
+/* No counterpart in the reference (an implementation choice of the step).
+ * fused = 1 runs each RK stage as one kernel (y faces, x faces and the point
+ * update of a strip of the grid in one CTA, the y fluxes kept in shared
+ * memory); fused = 0 as a y-face kernel and an x-face + update kernel that
+ * pass the y fluxes through device memory.  Both give bit-identical results.
+ * The default is 1 where the fused kernel exists (MP5 and the MC slopes of
+ * flux routines 1-4); elsewhere 1 is refused with CUEVA_ERR_ARG. */
+int32_t cueva_set_stage_kernel(cueva_ctx* ctx, int32_t fused);
+/* bytes of the context's device field slab (state, stage sums, stored stage
+ * right-hand sides, flux scratch); no counterpart in the reference */
+int32_t cueva_device_bytes(const cueva_ctx* ctx, uint64_t* bytes);
+int32_t cueva_get_stage_kernel(const cueva_ctx* ctx, int32_t* fused);
 int32_t cueva_sync(cueva_ctx* ctx);
 int32_t cueva_status(cueva_ctx* ctx, uint32_t* status_bits);
 int32_t cueva_counters(cueva_ctx* ctx, int64_t out3[3]);   /* contador_r, contador_p, contador_v */

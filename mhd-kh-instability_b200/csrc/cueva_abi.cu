@@ -451,13 +451,19 @@ int32_t cueva_ctx_create(const cueva_params* p, cueva_ctx** out) {
   fill_desc(p, G, c->nkslot, c->slab, c->d_status, c->d_counters, I);
   // x tiles: 31 points (32 faces) x FACE_ROWS rows; y tiles: 32 columns x
   // FACE_ROWS face rows of j = -1..jmax
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev);
   I.block_count[LK_XUPD] = xupd_tiles(c->imax, c->jmax, FACE_ROWS);
   I.block_count[LK_YFACE] = yface_tiles(c->imax, c->jmax, FACE_ROWS);
+  I.seg_rows = stage_seg_rows(c->imax, c->jmax, FACE_ROWS, 2 * nsm);
+  I.block_count[LK_STAGE] = stage_tiles(c->imax, c->jmax, I.seg_rows);
   c->shape.rows = FACE_ROWS;
-  for (int k = 0; k < 2; ++k) {
+  for (int k : {LK_XUPD, LK_YFACE, LK_STAGE}) {
     I.block_begin[k] = 0;
     c->shape.grid[k] = c->shape.ntiles[k] = I.block_count[k];   // one tile per CTA
   }
+  // the fused stage kernel where it exists (k_yface + k_xupd otherwise)
+  c->shape.fused = stage_fused_available(p->rec_mp, p->flux_solver);
   if (prepare_stage(p->rec_mp, p->flux_solver, p->precision) != cudaSuccess ||
       cudaMemcpy(c->d_inst, &I, sizeof(InstDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -490,6 +496,31 @@ int32_t cueva_ctx_destroy(cueva_ctx* c) {
   if (c->ev_xfer_done) cudaEventDestroy(c->ev_xfer_done);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
+  return CUEVA_OK;
+}
+
+int32_t cueva_device_bytes(const cueva_ctx* c, uint64_t* bytes) {
+  if (!c || !bytes) return fail(CUEVA_ERR_ARG, "null argument");
+  const InstGeom G = inst_geom(&c->P, c->nkslot);
+  *bytes = (uint64_t)G.nslab * sizeof(double);
+  return CUEVA_OK;
+}
+
+int32_t cueva_set_stage_kernel(cueva_ctx* c, int32_t fused) {
+  if (int32_t e = check_ctx(c)) return e;
+  if (fused != 0 && fused != 1) return fail(CUEVA_ERR_ARG, "fused must be 0 (two kernels per stage) or 1 (one)");
+  if (fused && !stage_fused_available(c->P.rec_mp, c->P.flux_solver))
+    return fail(CUEVA_ERR_ARG, "no fused stage kernel for this reconstruction (MP5 and the MC slopes have one)");
+  CUDA_TRY(cudaSetDevice(c->dev));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  destroy_graphs(c);
+  c->shape.fused = fused != 0;
+  return CUEVA_OK;
+}
+
+int32_t cueva_get_stage_kernel(const cueva_ctx* c, int32_t* fused) {
+  if (!c || !fused) return fail(CUEVA_ERR_ARG, "null argument");
+  *fused = c->shape.fused ? 1 : 0;
   return CUEVA_OK;
 }
 
@@ -690,6 +721,7 @@ int32_t cueva_profile_steps(cueva_ctx* c, int32_t nsteps, double ms_out[3], int3
       if (ce == cudaSuccess) ce = cudaEventSynchronize(ev[2]);
       if (ce != cudaSuccess) { rc = fail(CUEVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
       for (int k = 0; k < 2; ++k) {
+        if (k == 0 && c->shape.fused) continue;   // no separate y-face launch
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
         ms_out[k] += ms;
@@ -1313,9 +1345,11 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
     I.inv_dely_pow2 = inv_pow2(I.dely);
   }
   I.c2p = 1;
-  I.block_begin[LK_XUPD] = I.block_begin[LK_YFACE] = 0;
+  I.block_begin[LK_XUPD] = I.block_begin[LK_YFACE] = I.block_begin[LK_STAGE] = 0;
   I.block_count[LK_XUPD] = xupd_tiles(p->imax, p->jmax, FACE_ROWS);
   I.block_count[LK_YFACE] = yface_tiles(p->imax, p->jmax, FACE_ROWS);
+  I.block_count[LK_STAGE] = 0;   // the right-hand-side mode runs k_yface + k_xupd
+  I.seg_rows = FACE_ROWS;
   StageShape sh;
   sh.rows = FACE_ROWS;
   for (int k = 0; k < 2; ++k) sh.grid[k] = sh.ntiles[k] = I.block_count[k];
@@ -1387,17 +1421,21 @@ void ens_destroy_graphs(cueva_ens* e) {
 
 // tile ranges for a tile height and the launch grid for a CTA count per SM
 int32_t ens_apply_shape(cueva_ens* e, int rows, int ctas_per_sm) {
-  int begin[3] = {0, 0, 0};
+  int begin[4] = {0, 0, 0, 0};
   for (int k = 0; k < e->n; ++k) {
     InstDesc& I = e->I[k];
     I.block_count[LK_XUPD] = xupd_tiles(I.imax, I.jmax, rows);
     I.block_count[LK_YFACE] = yface_tiles(I.imax, I.jmax, rows);
     I.block_count[LK_C2P] = c2p_tiles(I.imax, I.jmax);
-    for (int t = 0; t < 3; ++t) { I.block_begin[t] = begin[t]; begin[t] += I.block_count[t]; }
+    I.seg_rows = stage_seg_rows(I.imax, I.jmax, FACE_ROWS, 2 * e->num_sms);
+    I.block_count[LK_STAGE] = stage_tiles(I.imax, I.jmax, I.seg_rows);
+    for (int t = 0; t < 4; ++t) { I.block_begin[t] = begin[t]; begin[t] += I.block_count[t]; }
   }
   e->c2p_ntiles = begin[LK_C2P];
   e->shape.rows = rows;
-  for (int t = 0; t < 2; ++t) {
+  // the fused stage kernel has the tile height FACE_ROWS; other heights run k_yface + k_xupd
+  e->shape.fused = rows == FACE_ROWS && stage_fused_available(e->P0.rec_mp, e->P0.flux_solver);
+  for (int t : {LK_XUPD, LK_YFACE, LK_STAGE}) {
     e->shape.ntiles[t] = begin[t];
     const long long persistent = (long long)ctas_per_sm * e->num_sms;
     e->shape.grid[t] = (ctas_per_sm > 0 && persistent < begin[t]) ? (int)persistent : begin[t];

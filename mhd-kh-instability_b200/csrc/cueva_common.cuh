@@ -78,9 +78,10 @@ struct InstDesc {
   int fpitch;
   long long ffs;       // doubles per flux field
   // work decomposition: tiles of each launch kind (x faces + update, y faces,
-  // learned con2prim)
-  int block_begin[3];
-  int block_count[3];
+  // learned con2prim, fused stage)
+  int block_begin[4];
+  int block_count[4];
+  int seg_rows;        // fused stage tiles: grid rows per tile (a multiple of the band height)
 };
 
 // ---- tableau data of one stage launch (by value, kernel parameter space) -----
@@ -123,19 +124,26 @@ __device__ __forceinline__ int map_idx(int i, int n, int periodic) {
 constexpr int FACE_ROWS = 8;   // default tile height
 constexpr int NFACE = 14;   // interface fluxes per face (the Riemann roles)
 constexpr int POINT_THREADS = 256;
-enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1, LK_C2P = 2 };
+enum LaunchKind { LK_XUPD = 0, LK_YFACE = 1, LK_C2P = 2, LK_STAGE = 3 };
 
 // launch shape of one RK stage: tile height, CTAs per launch kind and the
-// tiles they loop over (grid == ntiles: one tile per CTA; smaller: persistent)
+// tiles they loop over (grid == ntiles: one tile per CTA; smaller: persistent).
+// fused: the stage runs as one k_stage launch (grid[LK_STAGE] CTAs over
+// ntiles[LK_STAGE] tiles) instead of k_yface + k_xupd.
 struct StageShape {
   int rows = FACE_ROWS;
-  int grid[2] = {0, 0};
-  int ntiles[2] = {0, 0};
+  int grid[4] = {0, 0, 0, 0};
+  int ntiles[4] = {0, 0, 0, 0};
+  bool fused = false;
 };
 
 // tiles of one instance for a tile height (x tiles: 31 points by rows)
 inline int xupd_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 30) / 31) * ((jmax + 1 + rows - 1) / rows); }
 inline int yface_tiles(int imax, int jmax, int rows) { return ((imax + 1 + 31) / 32) * ((jmax + 2 + rows - 1) / rows); }
+// fused stage tiles: strips of 31 points by segments of seg_rows grid rows
+inline int stage_tiles(int imax, int jmax, int seg_rows) {
+  return ((imax + 1 + 30) / 31) * ((jmax + 1 + seg_rows - 1) / seg_rows);
+}
 
 // The mixed-precision flux routines keep the fluxes of the field roles psi,
 // phi, Bn, Bt1, Bt2, En, Et1, Et2 (roles 0..7) in FP64: they carry the

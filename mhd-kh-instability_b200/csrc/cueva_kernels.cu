@@ -131,7 +131,9 @@ __global__ void k_fluxandsource(const InstDesc* __restrict__ insts, StageArgs sa
     const Centre cv{Q[Q_Q * fs + pc], Q[Q_PSI * fs + pc], Q[Q_PHI * fs + pc], Q[Q_EX * fs + pc],
                     Q[Q_EY * fs + pc], Q[Q_EZ * fs + pc], Q[Q_BX * fs + pc], Q[Q_BY * fs + pc],
                     Q[Q_BZ * fs + pc], pv[P_VX * fs + pc], pv[P_VY * fs + pc], pv[P_VZ * fs + pc]};
-    const uint32_t st = update_point<EP_RHS, double>(I, sa, i, j, qx, cv);
+    const long long fyo = (long long)(j + 1) * I.fpitch + i;
+    auto fyd = [&](int r) { return I.fy[r * I.ffs + fyo] - I.fy[r * I.ffs + fyo - I.fpitch]; };
+    const uint32_t st = update_point<EP_RHS, double, 0>(I, sa, i, j, qx, fyd, cv);
     if (st) atomicOr(I.status, st);
   }
 }
@@ -185,6 +187,33 @@ __global__ void k_con2prim(const InstDesc* __restrict__ insts, int cur) {
 }
 
 // ------------------------------------------------------------- dispatch
+bool stage_fused_available(int rec_mp, int solver) {
+  const int rm = solver <= 4 ? 3 : rec_mp;   // the flux routines 1-4 use the MC slopes
+  switch (rm) {
+    case 0: return kFused<0>;
+    case 1: return kFused<1>;
+    case 2: return kFused<2>;
+    case 3: return kFused<3>;
+    default: return false;
+  }
+}
+
+int stage_seg_rows(int imax, int jmax, int rows, int slots) {
+  // A tile of nb bands costs about nb + 0.7 band times (its first bottom
+  // faces take one warp about as long as a band's faces); the launch takes
+  // about ceil(tiles / slots) tile times.  Pick the band count with the
+  // smallest product (the larger one on ties: fewer repeated faces).
+  const int strips = (imax + 1 + 30) / 31;
+  int best = 1;
+  double best_cost = 1e300;
+  for (int nb = 1; nb <= 32; ++nb) {
+    const long long tiles = (long long)strips * ((jmax + 1 + nb * rows - 1) / (nb * rows));
+    const double cost = (double)((tiles + slots - 1) / slots) * (nb + 0.7);
+    if (cost <= best_cost) { best_cost = cost; best = nb; }
+  }
+  return best * rows;
+}
+
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
   switch (solver) {
     case 1: return prepare_stage_lax(rec_mp, prec);

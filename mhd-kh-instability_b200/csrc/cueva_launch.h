@@ -44,6 +44,12 @@ cudaError_t launch_stage_hlle(int rec_mp, int prec, const StageShape& sh, cudaSt
 // are recorded before, between and after the launches
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev = nullptr);
+// whether the fused stage kernel k_stage exists for this reconstruction and
+// flux routine (tile height FACE_ROWS)
+bool stage_fused_available(int rec_mp, int solver);
+// grid rows per fused-stage tile for a grid: a multiple of rows, so that the
+// launch has enough tiles to balance over `slots` resident CTAs
+int stage_seg_rows(int imax, int jmax, int rows, int slots);
 cudaError_t launch_begin_step(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur, int qout,
                               double abt11);
 cudaError_t launch_startconvar(long long npts, cudaStream_t st, const InstDesc* d, int n, int cur);

@@ -263,16 +263,36 @@ __device__ __forceinline__ void psiphi_star_f64(const Side<double>& Ld, const Si
   F[R_PHI] = F[R_PHI] + (k * (phiR - phiL)) * h;
 }
 
-// flux of the face of (w, lane) from the staged tile (16_hll_flow_mpx.f95 /
-// 16_hllc_flow_mpx.f95 for one interface); returns status bits
-template <int RM, int SOLVER, typename T, int D, int ROWS>
-__device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st, int w, int lane, double gamma_d,
-                                              double sigma_d, flux_t<T, SOLVER> (&F)[NROLE]) {
+// Stencil values of a face of the split tiles: staged field f at normal
+// stencil point q (n), coupled field f at point q through the face's cell (t)
+template <int RM, int SOLVER, int D, int ROWS>
+struct SplitAcc {
   using G = FaceGeom<RM, SOLVER, ROWS>;
-  constexpr int R = G::R, NS = G::NS;
-  auto nrmd = [&](int f, int q) -> double { return sn[G::template nrm<D>(f, q, w, lane)]; };
+  const double* sn;
+  const double* st;
+  int w, lane;
+  __device__ __forceinline__ double n(int f, int q) const { return sn[G::template nrm<D>(f, q, w, lane)]; }
+  __device__ __forceinline__ double t(int f, int q) const { return st[G::template trn<D>(f, q, w, lane)]; }
+};
+
+// Face values of the primitive slots v, p, rho of one face, with the
+// superluminal fall-back and the density fix-ups already applied (the fused
+// stage kernel forms them once for the x and the y face of a point)
+template <typename T>
+struct FacePre {
+  T vL[3], vR[3], pL, pR, rhoL, rhoR;
+};
+
+// flux of one face from its stencil accessor (16_hll_flow_mpx.f95 /
+// 16_hllc_flow_mpx.f95 for one interface); returns status bits.  With PRE
+// the primitive slots come from *pre instead of being reconstructed here.
+template <int RM, int SOLVER, typename T, int D, bool PRE, class ACC>
+__device__ __forceinline__ uint32_t face_flux(const ACC& acc, const FacePre<T>* pre, double gamma_d, double sigma_d,
+                                              flux_t<T, SOLVER> (&F)[NROLE]) {
+  constexpr int R = MPR<RM>::R, NS = 2 * R + 2;
+  auto nrmd = [&](int f, int q) -> double { return acc.n(f, q); };
   auto nrm = [&](int f, int q) -> T { return T(nrmd(f, q)); };
-  auto trn = [&](int f, int q) -> T { return T(st[G::template trn<D>(f, q, w, lane)]); };
+  auto trn = [&](int f, int q) -> T { return T(acc.t(f, q)); };
   auto rec = [&](int f, T& L, T& Rv) {
     T u[NS];
 #pragma unroll
@@ -458,12 +478,19 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
     return stt;
   }
   // primitive slots of this direction (21-25 for x, 58-62 for y)
-  rec(0, L.vx, Rs.vx);
-  rec(1, L.vy, Rs.vy);
-  rec(2, L.vz, Rs.vz);
-  recp(3, L.p, Rs.p);
-  recp(4, L.rho, Rs.rho);
-  if constexpr (SOLVER == 5 || SOLVER == 7) {
+  if constexpr (PRE) {
+    L.vx = pre->vL[0]; L.vy = pre->vL[1]; L.vz = pre->vL[2];
+    Rs.vx = pre->vR[0]; Rs.vy = pre->vR[1]; Rs.vz = pre->vR[2];
+    L.p = pre->pL; Rs.p = pre->pR;
+    L.rho = pre->rhoL; Rs.rho = pre->rhoR;
+  } else {
+    rec(0, L.vx, Rs.vx);
+    rec(1, L.vy, Rs.vy);
+    rec(2, L.vz, Rs.vz);
+    recp(3, L.p, Rs.p);
+    recp(4, L.rho, Rs.rho);
+  }
+  if constexpr (!PRE && (SOLVER == 5 || SOLVER == 7)) {
     // superluminal fall-back, 16_hll_flow_mpx.f95:1393-1462: the x and y
     // reconstructions of the point fall back together if either is
     // superluminal; left states take cell (i,j), right states cell i-1 (x)
@@ -482,7 +509,7 @@ __device__ __forceinline__ uint32_t face_flux(const double* sn, const double* st
       Rs.vx = nrm(0, R - 1); Rs.vy = nrm(1, R - 1); Rs.vz = nrm(2, R - 1);
     }
   }
-  if constexpr (SOLVER == 7) {
+  if constexpr (!PRE && SOLVER == 7) {
     // density fix-up chain, 16_hllc_flow_mpx.f95:2663-2690: the first
     // negative of (yL, yR, xL, xR) becomes 0.1 rho(i,j); an x side is only
     // fixed when neither y side is negative
@@ -601,7 +628,8 @@ k_yface(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
     const int i = i0 + lane, j = j0 + w;
     if (i <= ilast && j <= jlast) {
       flux_t<T, SOLVER> F[NROLE];
-      const uint32_t stt = face_flux<RM, SOLVER, T, 1, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
+      const SplitAcc<RM, SOLVER, 1, ROWS> acc{sn, st, w, lane};
+      const uint32_t stt = face_flux<RM, SOLVER, T, 1, false>(acc, (const FacePre<T>*)nullptr, I.gamma, I.sigma, F);
       const long long fo = (long long)(j + 1) * I.fpitch + i;
 #pragma unroll
       for (int c = 0; c < NROLE; ++c) flux_store<T, SOLVER>(I.fy, I.ffs, c, fo, double(F[c]));
@@ -620,23 +648,23 @@ enum Epilogue { EP_RHS = 0, EP_MID = 1, EP_LAST = 2 };
 struct Centre { double q, psi, phi, Ex, Ey, Ez, Bx, By, Bz, vx, vy, vz; };
 
 // flux divergence + sources of point (i, j) (17_fluxandsource.f95:441-635)
-// and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role
+// and the fused epilogue; qx[r] = (Fx(i+1/2) - Fx(i-1/2)) / delx per role,
+// fyd(r) = Fy(j+1/2) - Fy(j-1/2) per role
 // valid == false (EP_LAST only): the lane computes a copy of a real point so
 // that its warp reaches con2prim converged, and stores nothing
-template <int EP, typename T, int SV = 0>
+template <int EP, typename T, int SV, class FYD>
 __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageArgs& sa, int i, int j,
-                                                 const double (&qx)[NROLE], const Centre& cv, bool valid = true) {
+                                                 const double (&qx)[NROLE], const FYD& fyd, const Centre& cv,
+                                                 bool valid = true) {
   const int pitch = I.pitch;
   const long long fs = I.fstride;
   const double* __restrict__ prim = I.prim[sa.cur];
   const double* __restrict__ aux = I.aux[sa.cur];
   uint32_t st = 0;
   const long long pc = (long long)j * pitch + i;
-  const long long fyo = (long long)(j + 1) * I.fpitch + i;      // Fy(i, j+1/2); Fy(i, j-1/2) at -fpitch
-  const double* __restrict__ fy = I.fy;
   const double dly = I.dely, iy2 = I.inv_dely_pow2;
   auto qy = [&](int r) {   // (dy)/dly
-    const double d = flux_load<T, SV>(fy, I.ffs, r, fyo) - flux_load<T, SV>(fy, I.ffs, r, fyo - I.fpitch);
+    const double d = fyd(r);
     return iy2 != 0.0 ? d * iy2 : d / dly;
   };
   auto qxf = [&](int r) { return qx[r]; };
@@ -821,7 +849,10 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
 #pragma unroll
   for (int c = 0; c < NROLE; ++c) F[c] = 0;
   uint32_t stt = 0;
-  if (i <= ilast) stt = face_flux<RM, SOLVER, T, 0, ROWS>(sn, st, w, lane, I.gamma, I.sigma, F);
+  if (i <= ilast) {
+    const SplitAcc<RM, SOLVER, 0, ROWS> acc{sn, st, w, lane};
+    stt = face_flux<RM, SOLVER, T, 0, false>(acc, (const FacePre<T>*)nullptr, I.gamma, I.sigma, F);
+  }
   if constexpr (EP == EP_RHS) {
     // the routine mirror of the flux routine (mode 2) also stores the x-face
     // fluxes; a face on a tile seam is stored by the tile of its right point
@@ -856,7 +887,11 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
     auto cs = [&](int f) { return sn[(w * NF_FACE + f) * LONG + ln + R]; };
     const Centre cv{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
                     cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
-    stt |= update_point<EP, T, SOLVER>(I, sa, ii, j, qx, cv, valid);
+    const long long fyo = (long long)(j + 1) * I.fpitch + ii;   // Fy(ii, j+1/2); Fy(ii, j-1/2) at -fpitch
+    auto fyd = [&](int r) {
+      return flux_load<T, SOLVER>(I.fy, I.ffs, r, fyo) - flux_load<T, SOLVER>(I.fy, I.ffs, r, fyo - I.fpitch);
+    };
+    stt |= update_point<EP, T, SOLVER>(I, sa, ii, j, qx, fyd, cv, valid);
   }
   if (stt) atomicOr(I.status, stt);
 }
@@ -876,12 +911,350 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) 
   }
 }
 
+// ------------------------------------------------------- fused stage kernel
+// k_stage: one launch per RK stage.  A CTA of 32 x ROWS threads owns a strip
+// of 31 points along x (lane 0 carries the strip's left face) and marches up
+// a segment of I.seg_rows grid rows in bands of ROWS rows.  The stencil rows
+// live in a shared-memory ring of ROWS + 2R + 1 rows, so a band copies in
+// only its ROWS new rows.  Thread (lane, w) of a band computes the y face
+// (i, j+1/2) and the x face (i+1/2, j) of point (i, j), j = j0 + w: the y
+// fluxes go to a shared buffer of ROWS + 1 face rows (a band's bottom faces
+// are the previous band's top faces; a segment computes its first bottom row
+// itself), the x flux of i-1/2 comes by warp shuffle, and the point is
+// updated as in k_xupd.  Against k_yface + k_xupd the y fluxes never leave
+// the SM, every stencil value is copied in once per stage, and the velocity
+// reconstructions that the superluminal fall-back of HLL / HLLC couples
+// between the two faces of a point are formed once.
+constexpr int NF_RING = 21;   // 0-4 time-n vx, vy, vz, p, rho; 5-18 stage psi .. Sz; 19 Jx; 20 Jy
+
+template <int RM, int ROWS>
+struct RingGeom {
+  static constexpr int R = MPR<RM>::R;
+  static constexpr int NS = 2 * R + 2;
+  static constexpr int NR = ROWS + 2 * R + 1;          // ring rows
+  static constexpr int LONG = 32 + 2 * R + 1;          // staged columns i0-R .. i0+32+R
+  static constexpr int ROWSZ = NF_RING * LONG;         // doubles per ring row
+  static constexpr int RING = NR * ROWSZ;
+  static constexpr int YF = (ROWS + 1) * NROLE * 32;   // y-flux face rows x roles x lanes
+  static constexpr size_t bytes() { return sizeof(double) * (size_t)(RING + YF); }
+  // ring row of grid row r (r > -16 NR)
+  static __device__ __forceinline__ int slot(int r) { return (int)((unsigned)(r + 16 * NR) % (unsigned)NR); }
+};
+// the fused kernel is built where two CTAs of FACE_ROWS warps fit an SM's
+// 228 KB of shared memory (MP5 and the MC slopes)
+template <int RM>
+constexpr bool kFused = RingGeom<RM, FACE_ROWS>::bytes() <= 113 * 1024;
+
+// copies grid rows ra .. rb of the strip (columns i0-R .. ilast+R+1) into
+// their ring rows, through the ghost maps
+template <int RM, int ROWS>
+__device__ __forceinline__ void ring_fill(const InstDesc& I, const StageArgs& sa, double* ring, int i0, int ilast,
+                                          int ra, int rb, int tid) {
+  using G = RingGeom<RM, ROWS>;
+  constexpr int R = G::R, LONG = G::LONG;
+  const long long fs = I.fstride;
+  const double* __restrict__ prim = I.prim[sa.cur];
+  const double* __restrict__ Q = I.stage[sa.qin];
+  const int ncell = ilast + R + 1 - (i0 - R) + 1;
+  const int n = (rb - ra + 1) * LONG;
+  for (int e = tid; e < n; e += 32 * ROWS) {
+    const int r = e / LONG, c = e - r * LONG;
+    if (c >= ncell) continue;
+    const int row = ra + r;
+    const long long off = (long long)map_idx(row, I.jmax, I.bc_y) * I.pitch + map_idx(i0 - R + c, I.imax, I.bc_x);
+    double* dst = ring + G::slot(row) * G::ROWSZ + c;
+    cp_async8(dst + 0 * LONG, prim + P_VX * fs + off);
+    cp_async8(dst + 1 * LONG, prim + P_VY * fs + off);
+    cp_async8(dst + 2 * LONG, prim + P_VZ * fs + off);
+    cp_async8(dst + 3 * LONG, prim + P_P * fs + off);
+    cp_async8(dst + 4 * LONG, prim + P_RHO * fs + off);
+#pragma unroll
+    for (int f = 0; f < 16; ++f) cp_async8(dst + (5 + f) * LONG, Q + f * fs + off);   // psi .. Sz, Jx, Jy
+  }
+}
+
+// stencil values of the face of (i, j) in direction D from the ring:
+// D = 0 row j, columns i-R .. i+R+1; D = 1 column i, rows j-R .. j+R+1
+template <int RM, int ROWS, int D>
+struct RingAcc {
+  using G = RingGeom<RM, ROWS>;
+  const double* ring;
+  int off[D == 0 ? 1 : G::NS];
+  __device__ __forceinline__ double n(int f, int q) const {
+    const int ff = (D == 1 && f == 19) ? 20 : f;   // field 19 is the normal current
+    if constexpr (D == 0) return ring[off[0] + ff * G::LONG + q];
+    else return ring[off[q] + ff * G::LONG];
+  }
+  __device__ __forceinline__ double t(int, int) const { return 0.0; }   // the fused faces take FacePre
+};
+
+template <int RM, typename T, bool POS, class ACC>
+__device__ __forceinline__ Pair<T> rec_acc(const ACC& a, int f) {
+  constexpr int NS = 2 * MPR<RM>::R + 2;
+  T u[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) u[q] = T(a.n(f, q));
+  return MPCall<RM, T>::template call<POS>(u);
+}
+
+// velocity slots of both faces of point (i, j) with the superluminal
+// fall-back of 16_hll_flow_mpx.f95:1393-1462: if any of the four
+// reconstructions is superluminal, both faces take cell (i, j) on the left
+// and cell (i-1, j) (x) or (i, j-1) (y) on the right
+template <int RM, typename T, class AX, class AY>
+__device__ __forceinline__ void point_velocities(const AX& ax, const AY& ay, T (&xL)[3], T (&xR)[3], T (&yL)[3],
+                                                 T (&yR)[3]) {
+  constexpr int R = MPR<RM>::R;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const Pair<T> px = rec_acc<RM, T, false>(ax, c);
+    xL[c] = px.L; xR[c] = px.R;
+    const Pair<T> py = rec_acc<RM, T, false>(ay, c);
+    yL[c] = py.L; yR[c] = py.R;
+  }
+  const T V2xl = pw2(xL[0]) + pw2(xL[1]) + pw2(xL[2]);
+  const T V2xr = pw2(xR[0]) + pw2(xR[1]) + pw2(xR[2]);
+  const T V2yl = pw2(yL[0]) + pw2(yL[1]) + pw2(yL[2]);
+  const T V2yr = pw2(yR[0]) + pw2(yR[1]) + pw2(yR[2]);
+  if (V2xl >= T(1) || V2xr >= T(1) || V2yl >= T(1) || V2yr >= T(1)) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      xL[c] = T(ax.n(c, R)); xR[c] = T(ax.n(c, R - 1));
+      yL[c] = T(ay.n(c, R)); yR[c] = T(ay.n(c, R - 1));
+    }
+  }
+}
+
+// y face (i, j+1/2) of point (i, j).  For HLL / HLLC the point's x-face
+// velocity slots are parked in xstash (6 doubles, stride 32: shared memory
+// that the caller reloads before it stores the y fluxes there) and yneg tells
+// whether a raw y density face value is negative (the x density fix-up of
+// 16_hllc_flow_mpx.f95:2663-2690 looks at the y pair first)
+template <int RM, int SOLVER, typename T, int ROWS>
+__device__ __forceinline__ uint32_t fused_yface(const RingAcc<RM, ROWS, 0>& ax, const RingAcc<RM, ROWS, 1>& ay,
+                                                const InstDesc& I, volatile double* xstash, bool& yneg,
+                                                flux_t<T, SOLVER> (&F)[NROLE]) {
+  constexpr int R = MPR<RM>::R;
+  yneg = false;
+  if constexpr (SOLVER == 5 || SOLVER == 7) {
+    FacePre<T> py;
+    {
+      T xL[3], xR[3];
+      point_velocities<RM, T>(ax, ay, xL, xR, py.vL, py.vR);
+      if (xstash) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { xstash[c * 32] = double(xL[c]); xstash[(3 + c) * 32] = double(xR[c]); }
+      }
+    }
+    const Pair<T> pp = rec_acc<RM, T, true>(ay, 3);
+    const Pair<T> pr = rec_acc<RM, T, true>(ay, 4);
+    py.pL = pp.L; py.pR = pp.R; py.rhoL = pr.L; py.rhoR = pr.R;
+    if constexpr (SOLVER == 7) {
+      yneg = (py.rhoL < T(0)) || (py.rhoR < T(0));
+      if (yneg) {
+        const T r10 = T(ay.n(4, R) * 1.0e-1);
+        if (py.rhoL < T(0)) py.rhoL = r10;
+        else py.rhoR = r10;
+      }
+    }
+    return face_flux<RM, SOLVER, T, 1, true>(ay, &py, I.gamma, I.sigma, F);
+  } else {
+    return face_flux<RM, SOLVER, T, 1, false>(ay, (const FacePre<T>*)nullptr, I.gamma, I.sigma, F);
+  }
+}
+
+// x face (i+1/2, j) of point (i, j); xv = the velocity slots fused_yface parked
+template <int RM, int SOLVER, typename T, int ROWS>
+__device__ __forceinline__ uint32_t fused_xface(const RingAcc<RM, ROWS, 0>& ax, const InstDesc& I, const T (&xv)[6],
+                                                bool yneg, flux_t<T, SOLVER> (&F)[NROLE]) {
+  constexpr int R = MPR<RM>::R;
+  if constexpr (SOLVER == 5 || SOLVER == 7) {
+    FacePre<T> px;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { px.vL[c] = xv[c]; px.vR[c] = xv[3 + c]; }
+    const Pair<T> pp = rec_acc<RM, T, true>(ax, 3);
+    const Pair<T> pr = rec_acc<RM, T, true>(ax, 4);
+    px.pL = pp.L; px.pR = pp.R; px.rhoL = pr.L; px.rhoR = pr.R;
+    if constexpr (SOLVER == 7) {
+      if ((px.rhoL < T(0) || px.rhoR < T(0)) && !yneg) {
+        const T r10 = T(ax.n(4, R) * 1.0e-1);
+        if (px.rhoL < T(0)) px.rhoL = r10;
+        else px.rhoR = r10;
+      }
+    }
+    return face_flux<RM, SOLVER, T, 0, true>(ax, &px, I.gamma, I.sigma, F);
+  } else {
+    return face_flux<RM, SOLVER, T, 0, false>(ax, (const FacePre<T>*)nullptr, I.gamma, I.sigma, F);
+  }
+}
+
+// L2 prefetch of the update's other inputs for rows j0 .. jl of a strip (see
+// xupd_tile)
+__device__ __forceinline__ void prefetch_update_rows(const InstDesc& I, const StageArgs& sa, int i0, int ilast, int j0,
+                                                     int jl, int tid, int nthr) {
+  const long long fs = I.fstride;
+  const int npt = ilast - i0, nr = jl - j0 + 1;
+  if (npt <= 0 || nr <= 0) return;
+  const int nfin = (sa.l > 1) ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
+  int nk = 0;
+  for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
+  const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;
+  for (int e = tid; e < ncen * nr; e += nthr) {
+    const int r = e % nr;
+    int f = e / nr;
+    const double* base;
+    if (f < NAUX) base = I.aux[sa.cur] + f * fs;
+    else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
+    else if ((f -= 9) < nfin) base = I.finsum + f * fs;
+    else if ((f -= nfin) < nint) base = I.intsum + f * fs;
+    else {
+      f -= nint;
+      int kk = f / NRHS, m = 1;
+      for (; m < sa.l; ++m)
+        if (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0) && kk-- == 0) break;
+      base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + f % NRHS) * fs;
+    }
+    prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
+  }
+}
+
+template <int RM, int SOLVER, typename T, int EP, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS, 16 / ROWS)
+k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) {
+  using G = RingGeom<RM, ROWS>;
+  constexpr int R = G::R, NS = G::NS, LONG = G::LONG;
+  constexpr bool kPre = SOLVER == 5 || SOLVER == 7;
+  extern __shared__ double smem[];
+  double* ring = smem;
+  double* yf = smem + G::RING;
+  const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int b = tile;
+    const InstDesc& I = tile_inst(insts, ninst, LK_STAGE, b);
+    const int nstrip = (I.imax + 1 + 30) / 31;
+    const int i0 = (b % nstrip) * 31 - 1, jseg = (b / nstrip) * I.seg_rows;
+    const int ilast = min(i0 + 31, I.imax), jend = min(jseg + I.seg_rows - 1, I.jmax);
+    const int i = i0 + lane;
+    uint32_t stt = 0;
+    auto x_acc = [&](int j) {
+      RingAcc<RM, ROWS, 0> a{ring, {G::slot(j) * G::ROWSZ + lane}};
+      return a;
+    };
+    auto y_acc = [&](int j) {
+      RingAcc<RM, ROWS, 1> a;
+      a.ring = ring;
+#pragma unroll
+      for (int q = 0; q < NS; ++q) a.off[q] = G::slot(j - R + q) * G::ROWSZ + lane + R;
+      return a;
+    };
+    // the segment's first bottom faces jseg - 1/2 (rows jseg-1-R .. jseg+R)
+    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jseg - 1 - R, jseg + R, tid);
+    cp_async_wait_all();
+    __syncthreads();
+    if (w == 0 && i <= ilast) {
+      flux_t<T, SOLVER> F[NROLE];
+      bool yneg;
+      stt |= fused_yface<RM, SOLVER, T, ROWS>(x_acc(jseg - 1), y_acc(jseg - 1), I, nullptr, yneg, F);
+#pragma unroll
+      for (int c = 0; c < NROLE; ++c) yf[c * 32 + lane] = double(F[c]);   // face row 0 of band 0
+    }
+    __syncthreads();   // the band's copies overwrite the ring row of grid row jseg-1-R
+    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jseg + R + 1, min(jseg + ROWS - 1, jend) + R + 1, tid);
+    int band = 0;
+    for (int j0 = jseg; j0 <= jend; j0 += ROWS, ++band) {
+      const int jl = min(j0 + ROWS - 1, jend);
+      if constexpr (EP != EP_RHS) prefetch_update_rows(I, sa, i0, ilast, j0, jl, tid, 32 * ROWS);
+      // the band's rows have arrived, and every warp has finished the previous
+      // band's update (its reads of the face rows that this band overwrites)
+      cp_async_wait_all();
+      __syncthreads();
+      // face row k of this band (k = 0 bottom faces, k = w + 1 the faces above row w)
+      const int rb = (band * ROWS) % (ROWS + 1);
+      auto frow = [&](int k) { const int r = k + rb; return yf + (r >= ROWS + 1 ? r - (ROWS + 1) : r) * (NROLE * 32); };
+      const int j = j0 + w;
+      const bool valid = lane >= 1 && i <= ilast;
+      const bool warp_c2p = EP == EP_LAST && I.c2p == 2 && !I.c2p_tc;
+      // point whose update this lane computes (lanes without one repeat a real
+      // point in the warp-wide con2prim, and store nothing)
+      const int ii = valid ? i : (lane == 0 ? i0 + 1 : ilast);
+      const int ln = ii - i0;
+      flux_t<T, SOLVER> Fx[NROLE];
+#pragma unroll
+      for (int c = 0; c < NROLE; ++c) Fx[c] = 0;
+      Centre cv{};
+      if (j <= jl) {
+        if (i <= ilast) {
+          const RingAcc<RM, ROWS, 0> ax = x_acc(j);
+          volatile double* top = frow(w + 1) + lane;
+          bool yneg;
+          T xv[6];
+          {
+            flux_t<T, SOLVER> Fy[NROLE];
+            stt |= fused_yface<RM, SOLVER, T, ROWS>(ax, y_acc(j), I, kPre ? top : nullptr, yneg, Fy);
+            if constexpr (kPre) {
+#pragma unroll
+              for (int c = 0; c < 6; ++c) xv[c] = T(top[c * 32]);
+            }
+#pragma unroll
+            for (int c = 0; c < NROLE; ++c) top[c * 32] = double(Fy[c]);
+          }
+          stt |= fused_xface<RM, SOLVER, T, ROWS>(ax, I, xv, yneg, Fx);
+        }
+        // centre values of the point, read before the next band's copies
+        // replace the ring rows
+        const double* cen = ring + G::slot(j) * G::ROWSZ + ln + R;
+        auto cs = [&](int f) { return cen[f * LONG]; };
+        cv = Centre{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
+                    cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
+      }
+      __syncthreads();   // the band's y fluxes are complete and its ring reads done
+      if (j0 + ROWS <= jend)   // the next band's rows arrive while this band updates
+        ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, j0 + ROWS + R + 1, min(j0 + 2 * ROWS - 1, jend) + R + 1, tid);
+      if (j <= jl) {
+        const double dlx = I.delx, ix2 = I.inv_delx_pow2;
+        double qx[NROLE];
+#pragma unroll
+        for (int c = 0; c < NROLE; ++c) {
+          const double fr = double(Fx[c]);
+          const double fl = __shfl_up_sync(0xffffffffu, fr, 1);
+          const double d = fr - fl;
+          qx[c] = ix2 != 0.0 ? d * ix2 : d / dlx;
+        }
+        if (valid || warp_c2p) {
+          if (warp_c2p) {
+#pragma unroll
+            for (int c = 0; c < NROLE; ++c) qx[c] = __shfl_sync(0xffffffffu, qx[c], ln);
+          }
+          const double* ytop = frow(w + 1) + ln;
+          const double* ybot = frow(w) + ln;
+          auto fyd = [&](int r) { return ytop[r * 32] - ybot[r * 32]; };
+          stt |= update_point<EP, T, SOLVER>(I, sa, ii, j, qx, fyd, cv, valid);
+        }
+      }
+    }
+    __syncthreads();   // the next tile's copies overwrite the ring and the face rows
+    if (stt) atomicOr(I.status, stt);
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 template <int RM, int SV, typename T, int ROWS>
 static void launch_tiles(const StageShape& sh, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
                          cudaEvent_t* ev) {
   using G = FaceGeom<RM, SV, ROWS>;
   const dim3 blk(32, ROWS);
+  if constexpr (kFused<RM> && ROWS == FACE_ROWS) {
+    if (sh.fused && sa.mode == 0) {
+      // one launch: ev[0] and ev[1] bracket no work (no separate y-face kernel)
+      using RG = RingGeom<RM, ROWS>;
+      if (ev) { cudaEventRecord(ev[0], st); cudaEventRecord(ev[1], st); }
+      const int gs = sh.grid[LK_STAGE], ns = sh.ntiles[LK_STAGE];
+      if (sa.l < sa.s) k_stage<RM, SV, T, EP_MID, ROWS><<<gs, blk, RG::bytes(), st>>>(d, n, ns, sa);
+      else k_stage<RM, SV, T, EP_LAST, ROWS><<<gs, blk, RG::bytes(), st>>>(d, n, ns, sa);
+      if (ev) cudaEventRecord(ev[2], st);
+      return;
+    }
+  }
   if (ev) cudaEventRecord(ev[0], st);
   k_yface<RM, SV, T, ROWS><<<sh.grid[LK_YFACE], blk, G::bytes(1), st>>>(d, n, sh.ntiles[LK_YFACE], sa);
   if (ev) cudaEventRecord(ev[1], st);
@@ -903,6 +1276,13 @@ static cudaError_t prepare_tiles() {
     e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_MID, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_xupd<RM, SV, T, EP_LAST, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, b0);
+  if constexpr (kFused<RM> && ROWS == FACE_ROWS) {
+    const int bs = (int)RingGeom<RM, ROWS>::bytes();
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_stage<RM, SV, T, EP_MID, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bs);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_stage<RM, SV, T, EP_LAST, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bs);
+  }
   return e;
 }
 

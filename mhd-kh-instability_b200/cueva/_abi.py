@@ -108,6 +108,9 @@ def load(fma=False):
     L.cueva_ctx_destroy.argtypes = [vp]
     L.cueva_last_error.restype = ctypes.c_char_p
     L.cueva_set_stream.argtypes = [vp, vp]
+    L.cueva_set_stage_kernel.argtypes = [vp, i32]
+    L.cueva_get_stage_kernel.argtypes = [vp, ctypes.POINTER(i32)]
+    L.cueva_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     L.cueva_dt.restype = dbl
     L.cueva_dt.argtypes = [vp]
     L.cueva_tableau_stages.argtypes = [vp]

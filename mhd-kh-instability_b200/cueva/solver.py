@@ -118,6 +118,23 @@ class Cueva:
         _abi.check(self.L, self.L.cueva_profile_steps(self.ctx, n, ms, cnt))
         return list(ms), list(cnt)
 
+    def set_stage_kernel(self, fused):
+        """1: one fused kernel per RK stage (the default where it exists: MP5
+        and the MC slopes); 0: the y-face and x-face + update kernels.  Both
+        give bit-identical results."""
+        _abi.check(self.L, self.L.cueva_set_stage_kernel(self.ctx, int(fused)))
+
+    def stage_kernel(self):
+        v = ctypes.c_int32()
+        _abi.check(self.L, self.L.cueva_get_stage_kernel(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def device_bytes(self):
+        """Bytes of device memory the context's field slab holds."""
+        v = ctypes.c_uint64()
+        _abi.check(self.L, self.L.cueva_device_bytes(self.ctx, ctypes.byref(v)))
+        return v.value
+
     def set_stream(self, stream_ptr):
         _abi.check(self.L, self.L.cueva_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
 

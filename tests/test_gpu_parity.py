@@ -393,3 +393,38 @@ def test_varfin_electricfield_mirrors(oracle_mod):
     for n, f in fin.items():
         assert np.array_equal(g.interior(n), o.named(n) + o.dt * o.named(f)), n
     g.close()
+
+
+@pytest.mark.parametrize("solver,order,reset,precision", [(7, 4, 1, 0), (5, 2, 0, 0), (6, 2, 0, 0), (2, 4, 1, 0),
+                                                          (1, 2, 0, 0), (3, 2, 0, 0), (4, 4, 1, 0), (7, 4, 1, 1),
+                                                          (5, 2, 0, 1), (4, 2, 0, 1)])
+def test_fused_stage_kernel_equals_split_kernels(solver, order, reset, precision):
+    """The fused stage kernel (y faces, x faces and update of a strip in one
+    CTA, y fluxes in shared memory) and the two-kernel form (y fluxes through
+    device memory) give bit-identical steps, on a grid with ragged strips and
+    segments and non-power-of-two spacings, with copy and periodic x."""
+    from cueva import Cueva
+    for bc_x in (0, 1):
+        runs = []
+        for fused in (1, 0):
+            g = Cueva(93, 70, order=order, flux_solver=solver, rec_mp=0, sigma=1e3, intsum_reset=reset,
+                      precision=precision, bc_x=bc_x)
+            g.set_stage_kernel(fused)
+            assert g.stage_kernel() == fused
+            g.kh_init(v0=0.5, a=0.05)
+            g.upload()
+            g.step(6)
+            g.download()
+            runs.append({n: g.interior(n).copy() for n in PRIMS})
+            g.close()
+        for n in PRIMS:
+            assert np.array_equal(runs[0][n], runs[1][n]), (bc_x, n)
+
+
+def test_fused_stage_kernel_refused_without_it():
+    from cueva import Cueva, CuevaError
+    g = Cueva(64, 32, order=2, flux_solver=7, rec_mp=1)
+    assert g.stage_kernel() == 0
+    with pytest.raises(CuevaError):
+        g.set_stage_kernel(1)
+    g.close()
