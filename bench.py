@@ -340,6 +340,36 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     # the same with v, E, B components measured against their vector's L1 norm
     one_vec = dict(one_err, **vector_rel_l1(one[(1, 2)], one[(0, 1)]))
     one_c2p = {n: rel_l1_field(n, one[(1, 2)][n], one[(1, 1)][n], one[(1, 1)]) for n in PRIM_NAMES}
+    # error trajectory: plain FP64 and mixed + learned stepped side by side
+    # from the initial state over the bench's step count; the largest
+    # per-variable error (v, E, B components against their vector's L1
+    # norm) after every step, and the step count up to which it stays <= 1e-6
+    nsteps = max(args.warmup, 3) + args.steps
+    traj = []
+    runs = []
+    for prec, c2p in ((0, 1), (1, 2)):
+        o = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=prec, c2p=c2p))
+        o.set_stream(stream.cuda_stream)
+        o.kh_init(**cfg.kh_kwargs())
+        o.upload()
+        if c2p == 2:
+            net.attach(o)
+        runs.append(o)
+    for n in range(1, nsteps + 1):
+        for o in runs:
+            o.step(1)
+            o.download()
+        rf = {k: runs[0].interior(k) for k in PRIM_NAMES}
+        e = dict({k: rel_l1_field(k, runs[1].interior(k), rf[k], rf) for k in PRIM_NAMES},
+                 **vector_rel_l1(runs[1], rf))
+        traj.append(max(e.values()))
+    for o in runs:
+        o.close()
+    within = 0
+    for n, e in enumerate(traj, 1):
+        if e > 1e-6:
+            break
+        within = n
     m = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=1, c2p=2))
     m.set_stream(stream.cuda_stream)
     m.kh_init(**cfg.kh_kwargs())
@@ -359,6 +389,25 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
     m.download()
+    # the same mixed precision with the reference's Cardano recovery in the
+    # last stage's update instead of the learned kernel, same steps
+    mc = Cueva(device=device, pinned=False, **dict(cfg.solver_kwargs(), precision=1, c2p=1))
+    mc.set_stream(stream.cuda_stream)
+    mc.kh_init(**cfg.kh_kwargs())
+    mc.upload()
+    mc.step(max(args.warmup, 3))
+    mc.sync()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    mc.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_card = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms_card], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_card = float(t.item())
+    mc.close()
     errs = {n: rel_l1_field(n, m.interior(n), ref[n], ref) for n in PRIM_NAMES}
     errs_vec = dict(errs, **vector_rel_l1(m, ref))
     its, pts, fails = learned_stats(m)
@@ -379,7 +428,13 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
             "error_vs_fp64_after_steps": max(args.warmup, 3) + args.steps,
             "rel_l1_vs_fp64": errs, "max_rel_l1_vs_fp64": max(errs.values()),
             "rel_l1_vs_fp64_vector_norm": errs_vec, "max_rel_l1_vs_fp64_vector_norm": max(errs_vec.values()),
-            "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails}
+            "max_rel_l1_vs_fp64_vector_norm_by_step": traj, "steps_within_1e-6": within,
+            "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails,
+            "mixed_cardano": {"value": world * cfg.nx * cfg.ny * args.steps / (ms_card * 1e-3),
+                              "ms_per_step": ms_card / args.steps,
+                              "note": "mixed precision with the reference's Cardano con2prim in the last "
+                                      "stage's update, same steps"},
+            "speedup_learned_vs_cardano": ms_card / ms}
 
 
 ENS_METRIC = "ensemble zone-updates/s: 64 KH instances batched (mixed + learned C2P) vs sequential plain FP64"

@@ -256,13 +256,18 @@ int32_t cueva_mlp_gradients(cueva_mlp* mlp, const double* d_cons, const double* 
  * writing seeds; the device stays usable. */
 int32_t cueva_mlp_predict(cueva_mlp* mlp, const double* d_cons, int64_t n, double* d_pseed, int32_t tensor_cores);
 /* batch con2prim for comparisons: method 1 Cardano, 2 network seed + Newton,
- * 3 Newton from d_seed; d_prev (5 x n) are the previous primitives the
- * Cardano path seeds from; d_iters (optional) gets the Newton iterations
- * (-1 = failed, then the Cardano result is stored; 0 for method 1) */
+ * 3 Newton from d_seed, 4 Newton from the network seed or the previous
+ * pressure, whichever leaves the smaller residual (the seed choice of the
+ * learned step); d_prev (5 x n: rho, p, vx, vy, vz) are the previous
+ * primitives the Cardano path and method 4 seed from; d_iters (optional)
+ * gets the Newton iterations (-1 = failed, then the Cardano result is
+ * stored; 0 for method 1) */
 int32_t cueva_c2p_batch(int32_t device, int32_t method, const cueva_mlp* mlp, double gamma, double eps1,
                         const double* d_cons, const double* d_prev, const double* d_seed, int64_t n, double* d_out,
                         int32_t* d_iters);
-/* copy a trained network into ctx; con2prim uses it when params.c2p == 2 */
+/* copy a trained network into ctx; con2prim uses it when params.c2p == 2:
+ * Newton from the network's pressure or the previous pressure, whichever
+ * leaves the smaller residual, Cardano where Newton fails */
 int32_t cueva_attach_mlp(cueva_ctx* ctx, const cueva_mlp* mlp);
 /* where the learned con2prim runs: 1 (set by cueva_attach_mlp) = a kernel of
  * its own after the last RK stage, network on the tcgen05 tensor cores in

@@ -21,7 +21,8 @@ namespace {
 constexpr int C2P_CTAS_PER_SM = 4;
 
 // one point of the learned con2prim (all 128 threads of the CTA call it, in
-// step): seeds p from the network, refines it, falls back to Cardano
+// step): seeds p from the network or the previous pressure (the one with the
+// smaller residual), refines it, falls back to Cardano
 struct LearnedOut {
   C2POut o;
   uint32_t st;
@@ -33,7 +34,7 @@ __device__ __forceinline__ bool learned_point(MLPShared& S, uint32_t& phase, con
   c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
   float y = 0.0f;
   if (!mlp_tc_tile(S, phase, f, y)) return false;
-  const double seed = in.D * (double)__expf(y * S.sd_y + S.mu_y);
+  const double seed = c2p_best_seed(in, gamma, in.D * (double)__expf(y * S.sd_y + S.mu_y));
   r.it = c2p_newton(in, gamma, seed, r.o);
   r.st = 0u;
   if (r.it <= 0) r.st = c2p_cardano_ool(in, gamma, eps1, r.o, count ? counters : nullptr);

@@ -246,6 +246,28 @@ __device__ __forceinline__ int c2p_newton(const C2PIn& in, double gamma, double 
   return it;
 }
 
+// |f(p)| of the Newton function of c2p_newton at a candidate seed (infinite
+// where the seed gives no physical state)
+__device__ __forceinline__ double c2p_residual(const C2PIn& in, double gamma, double p) {
+  const double g1 = (gamma - 1.0) / gamma;
+  const double Sfx = in.Sx - in.Ey * in.Bz + in.Ez * in.By;
+  const double Sfy = in.Sy - in.Ez * in.Bx + in.Ex * in.Bz;
+  const double Sfz = in.Sz - in.Ex * in.By + in.Ey * in.Bx;
+  const double Q = in.tau - e2b2_half(in) + p;
+  const double v2 = (Sfx * Sfx + Sfy * Sfy + Sfz * Sfz) / (Q * Q);
+  if (!(v2 < 1.0) || !(Q > 0.0) || !(p > 0.0)) return CUDART_INF;
+  return fabs(p - g1 * (Q * (1.0 - v2) - in.D * sqrt(1.0 - v2)));
+}
+
+// The seed Newton starts from: the network's pressure or the pressure of the
+// previous time level (the seed of 12_varprimitive_nr.f95:150-151), whichever
+// leaves the smaller residual.  Inside a smooth run the previous pressure is
+// usually within ~1e-4 of the root; after a restart, a large change of the
+// state or where the previous pressure is unusable, the network's is closer.
+__device__ __forceinline__ double c2p_best_seed(const C2PIn& in, double gamma, double p_net) {
+  return c2p_residual(in, gamma, in.p0) < c2p_residual(in, gamma, p_net) ? in.p0 : p_net;
+}
+
 // the Cardano recovery as a call (keeps the learned path's code small)
 static __device__ __noinline__ uint32_t c2p_cardano_ool(const C2PIn& in, double gamma, double eps1, C2POut& o,
                                                         unsigned long long* cnt) {
@@ -268,7 +290,7 @@ static __device__ __noinline__ uint32_t c2p_learned(const C2PIn& in, double gamm
   if (full_warp) __syncwarp();
   const unsigned mask = full_warp ? 0xffffffffu : __activemask();
   const float yn = (mask == 0xffffffffu) ? mlp_forward_warp(M, f) : mlp_forward(M, f);
-  const double seed = in.D * (double)__expf(yn * M.sd_y + M.mu_y);
+  const double seed = c2p_best_seed(in, gamma, in.D * (double)__expf(yn * M.sd_y + M.mu_y));
   const int it = c2p_newton(in, gamma, seed, o);
   if (M.stats) {
     // one atomic per warp and counter

@@ -144,6 +144,25 @@ __device__ __forceinline__ void mp_pair_pos(const T (&u)[N], T& L, T& R) {
   R = um1;
 }
 
+// positivity-fixed pair on differences u - c0 (mixed precision): the same
+// limiter (it is translation-equivariant) with the sign tests of the
+// positivity fix taken on the FP64 value c0 + u
+template <typename T>
+__device__ __forceinline__ void posfix_point_delta(double c0, T uk, T duk, T duk1, T& up, T& um) {
+  if (c0 + double(up) < 0.0) { up = uk + T(0.50) * DMM(duk, duk1); um = uk; }
+  if (c0 + double(um) < 0.0) { um = uk - T(0.50) * DMM(duk, duk1); up = uk; }
+}
+template <int RM, typename T, int N>
+__device__ __forceinline__ void mp_pair_pos_delta(const T (&u)[N], double c0, T& L, T& R) {
+  constexpr int C = MPR<RM>::R;
+  T up0 = mp_up<RM, C>(u), um0 = mp_um<RM, C>(u);
+  T up1 = mp_up<RM, C + 1>(u), um1 = mp_um<RM, C + 1>(u);
+  posfix_point_delta(c0, u[C], u[C] - u[C - 1], u[C + 1] - u[C], up0, um0);
+  posfix_point_delta(c0, u[C + 1], u[C + 1] - u[C], u[C + 2] - u[C + 1], up1, um1);
+  L = up0;
+  R = um1;
+}
+
 // Out-of-line entry points.  A sweep thread reconstructs ~45 slots per grid
 // point; inlining the limiter 45 times made the kernel larger than the
 // instruction cache (ncu: "no instruction" was the top stall).  One copy of
@@ -160,6 +179,11 @@ template <typename T> struct MPCall<0, T> {
     const T u[6] = {a0, a1, a2, a3, a4, a5};
     Pair<T> p; mp_pair_pos<0>(u, p.L, p.R); return p;
   }
+  static __device__ __noinline__ Pair<T> posd(T a0, T a1, T a2, T a3, T a4, T a5, double c0) {
+    const T u[6] = {a0, a1, a2, a3, a4, a5};
+    Pair<T> p; mp_pair_pos_delta<0>(u, c0, p.L, p.R); return p;
+  }
+  static __device__ __forceinline__ Pair<T> call_posd(const T (&u)[6], double c0) { return posd(u[0], u[1], u[2], u[3], u[4], u[5], c0); }
   template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[6]) {
     return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5]) : pair(u[0], u[1], u[2], u[3], u[4], u[5]);
   }
@@ -173,6 +197,11 @@ template <typename T> struct MPCall<1, T> {
     const T u[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
     Pair<T> p; mp_pair_pos<1>(u, p.L, p.R); return p;
   }
+  static __device__ __noinline__ Pair<T> posd(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7, double c0) {
+    const T u[8] = {a0, a1, a2, a3, a4, a5, a6, a7};
+    Pair<T> p; mp_pair_pos_delta<1>(u, c0, p.L, p.R); return p;
+  }
+  static __device__ __forceinline__ Pair<T> call_posd(const T (&u)[8], double c0) { return posd(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], c0); }
   template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[8]) {
     return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7])
                : pair(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7]);
@@ -187,6 +216,11 @@ template <typename T> struct MPCall<2, T> {
     const T u[10] = {a0, a1, a2, a3, a4, a5, a6, a7, a8, a9};
     Pair<T> p; mp_pair_pos<2>(u, p.L, p.R); return p;
   }
+  static __device__ __noinline__ Pair<T> posd(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7, T a8, T a9, double c0) {
+    const T u[10] = {a0, a1, a2, a3, a4, a5, a6, a7, a8, a9};
+    Pair<T> p; mp_pair_pos_delta<2>(u, c0, p.L, p.R); return p;
+  }
+  static __device__ __forceinline__ Pair<T> call_posd(const T (&u)[10], double c0) { return posd(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9], c0); }
   template <bool POS> static __device__ __forceinline__ Pair<T> call(const T (&u)[10]) {
     return POS ? pos(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9])
                : pair(u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7], u[8], u[9]);

@@ -34,6 +34,7 @@ static_assert(R_PSI == 0 && R_ET2 == 7, "flux_slot keeps roles 0..7 (psi, phi, E
 template <typename T>
 struct Side {
   T psi, phi, Ex, Ey, Ez, Bx, By, Bz, q, D, tau, Sx, Sy, Sz, vx, vy, vz, p, rho, J;
+  T dp;   // split-pressure solvers only: p minus the FP64 reference pressure of the face
 };
 
 // role accessors
@@ -84,7 +85,12 @@ __device__ __forceinline__ T lorentz_hlle(const Side<T>& s) {
   return T(1.0) / sqrt(T(1.0) - pw2(s.vx) - pw2(s.vy) - pw2(s.vz));
 }
 
-template <int D, typename T>
+// PS (split pressure, mixed precision): the isotropic pressure term of the
+// normal momentum flux is s.dp, the side's pressure minus a reference value
+// pc0 that the caller adds back in FP64 (the pressure, ~1 in the KH layer,
+// would otherwise be rounded to FP32 in a flux whose differences drive the
+// small normal velocity)
+template <int D, bool PS = false, typename T>
 __device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma, T W) {
   using X = Dir<D>;
   Phys<T> f;
@@ -97,16 +103,17 @@ __device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma, T W) {
   const T Bn = X::Bn(s), Bt1 = X::Bt1(s), Bt2 = X::Bt2(s);
   f.FD = s.D * vn;
   f.Ftau = (Bt2 * Et1 - Bt1 * Et2) + hW2 * vn;
-  f.FSn = -pw2(En) - pw2(Bn) + hW2 * pw2(vn) + T(0.5) * E2B2 + s.p;
+  if constexpr (PS) f.FSn = -pw2(En) - pw2(Bn) + hW2 * pw2(vn) + T(0.5) * E2B2 + s.dp;
+  else f.FSn = -pw2(En) - pw2(Bn) + hW2 * pw2(vn) + T(0.5) * E2B2 + s.p;
   f.FSt1 = -En * Et1 - Bn * Bt1 + hW2 * vn * vt1;
   if constexpr (D == 0) f.FSt2 = -En * Et2 - Bn * Bt2 + hW2 * vn * vt2;
   else                  f.FSt2 = -En * Et2 - Bn * Bt2 + hW2 * vt2 * vn;   // FSyx: vx before vy
   f.h = h;
   return f;
 }
-template <int D, typename T>
+template <int D, bool PS = false, typename T>
 __device__ __forceinline__ Phys<T> physical(const Side<T>& s, T gamma) {
-  return physical<D>(s, gamma, lorentz(s));
+  return physical<D, PS>(s, gamma, lorentz(s));
 }
 
 // fixed-speed (s1 = -1, s2 = +1) HLL combination
@@ -129,11 +136,13 @@ __device__ __forceinline__ void em_fluxes(const Side<T>& L, const Side<T>& R, T*
   A[R_Q] = hll(L.J, R.J, L.q, R.q);
 }
 
-template <int D, typename T>
+// PS: split pressure (see physical); A[R_SN] then lacks the reference
+// pressure, which the caller adds in FP64
+template <int D, bool PS = false, typename T>
 __device__ __forceinline__ void hll_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A) {
   using X = Dir<D>;
   em_fluxes<D>(L, R, A);
-  const Phys<T> fl = physical<D>(L, gamma), fr = physical<D>(R, gamma);
+  const Phys<T> fl = physical<D, PS>(L, gamma), fr = physical<D, PS>(R, gamma);
   A[R_D] = hll(fl.FD, fr.FD, L.D, R.D);
   A[R_TAU] = hll(fl.Ftau, fr.Ftau, L.tau, R.tau);
   A[R_SN] = hll(fl.FSn, fr.FSn, X::Sn(L), X::Sn(R));
@@ -241,13 +250,17 @@ __device__ __forceinline__ T hllc_vel(T a, T b, T c, T rt, uint32_t& st) {
   return fmax2(T(-1.0) + T(1.0e-3), fmin2(T(1.0) - T(1.0e-3), v));
 }
 
-// HLLC of Miranda-Aranguren et al. (2018), 16_hllc_flow_mpx.f95:2816-4610
-template <int D, typename T>
+// HLLC of Miranda-Aranguren et al. (2018), 16_hllc_flow_mpx.f95:2816-4610.
+// PS: split pressure with reference pressure pc0 (see physical): the normal
+// momentum fluxes and the star pressure lack pc0, which cancels in every
+// star-state difference; the contact-speed quadratic takes the full flux.
+// A[R_SN] then lacks pc0, which the caller adds in FP64.
+template <int D, bool PS = false, typename T>
 __device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st,
-                                            T* vstar = nullptr) {
+                                            T* vstar = nullptr, T pc0 = T(0)) {
   using X = Dir<D>;
   em_fluxes<D>(L, R, A);
-  const Phys<T> fl = physical<D>(L, gamma), fr = physical<D>(R, gamma);
+  const Phys<T> fl = physical<D, PS>(L, gamma), fr = physical<D, PS>(R, gamma);
   const T h = T(0.5);
   // HLL averages of the state (:2816-2900)
   const T psi_hll = h * (((R.psi + L.psi) + X::En(L)) - X::En(R));
@@ -286,7 +299,9 @@ __device__ __forceinline__ void hllc_fluxes(const Side<T>& L, const Side<T>& R, 
   const T E2B2_str = T(0.5) * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
   // contact speed (:3208-3335)
   const T a_hll = tau_f - ErotB_n;
-  const T b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
+  T b_hll;
+  if constexpr (PS) b_hll = E2_perp + B2_perp - tau_hll - (Sn_f + pc0);
+  else b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
   const T c_hll = Sn_hll - ErotB_n;
   const T det_hll = pw2(b_hll) - T(4.0) * a_hll * c_hll;
   const T q_root1 = -T(0.5) * (b_hll + fsgn1(b_hll) * fabs(sqrt(det_hll)));
@@ -357,11 +372,13 @@ __device__ __forceinline__ void hlle_bounds(const Side<T>& s, T h, T gamma, T& l
   lm = (vn * (T(1.0) - pw2(Cs)) - Cs * root) / (T(1.0) - pw2(Cs) * V2);
 }
 
-template <int D, typename T>
-__device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st) {
+// PS: split pressure with reference pressure pc0, as in hllc_fluxes
+template <int D, bool PS = false, typename T>
+__device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, T gamma, T* A, uint32_t& st,
+                                            T pc0 = T(0)) {
   using X = Dir<D>;
   em_fluxes<D>(L, R, A);   // psi, phi, E, B; the charge flux is replaced below
-  const Phys<T> fl = physical<D>(L, gamma, lorentz_hlle(L)), fr = physical<D>(R, gamma, lorentz_hlle(R));
+  const Phys<T> fl = physical<D, PS>(L, gamma, lorentz_hlle(L)), fr = physical<D, PS>(R, gamma, lorentz_hlle(R));
   const T h = T(0.5);
   // fixed-speed HLL states of E and B (the star E, B)
   const T En_hll = h * (((X::En(R) + X::En(L)) + L.psi) - R.psi);
@@ -403,7 +420,9 @@ __device__ __forceinline__ void hlle_fluxes(const Side<T>& L, const Side<T>& R, 
   else                  { Eys = En_hll; Ezs = Et1_hll; Exs = Et2_hll; Bys = Bn_hll; Bzs = Bt1_hll; Bxs = Bt2_hll; }
   const T E2B2_str = T(0.5) * ((pw2(Exs) + pw2(Eys) + pw2(Ezs)) + (pw2(Bxs) + pw2(Bys) + pw2(Bzs)));
   const T a_hll = tau_f - ErotB_n;
-  const T b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
+  T b_hll;
+  if constexpr (PS) b_hll = E2_perp + B2_perp - tau_hll - (Sn_f + pc0);
+  else b_hll = E2_perp + B2_perp - tau_hll - Sn_f;
   const T c_hll = Sn_hll - ErotB_n;
   const T det_hll = pw2(b_hll) - T(4.0) * a_hll * c_hll;
   const T q_root1 = -T(0.5) * (b_hll + fsgn1(b_hll) * fabs(sqrt(det_hll)));

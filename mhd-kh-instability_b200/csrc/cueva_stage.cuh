@@ -281,7 +281,19 @@ struct SplitAcc {
 template <typename T>
 struct FacePre {
   T vL[3], vR[3], pL, pR, rhoL, rhoR;
+  T dpL, dpR;    // split-pressure solvers: pL, pR minus pc0
+  double pc0;    // the face's FP64 reference pressure (cell i / j of the face)
 };
+
+// Mixed-precision HLL / HLLE / HLLC of the MP routines split the pressure:
+// p is reconstructed as differences from the FP64 pressure pc0 of the face's
+// cell (the MP limiter and its positivity fix are translation-equivariant),
+// the FP32 normal momentum flux carries p - pc0, and pc0 is added back to
+// that flux in FP64.  The pressure (~1 in the KH layer) would otherwise be
+// rounded to FP32 in the flux whose divergence drives the small normal
+// velocity of the perturbation.
+template <typename T, int SV>
+constexpr bool kSplitP = kEmF64<T, SV> && (SV == 5 || SV == 6 || SV == 7);
 
 // flux of one face from its stencil accessor (16_hll_flow_mpx.f95 /
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits.  With PRE
@@ -318,6 +330,7 @@ __device__ __forceinline__ uint32_t face_flux(const ACC& acc, const FacePre<T>* 
   uint32_t stt = 0;
   Side<T> L, Rs;
   Side<double> Ld{}, Rd{};   // FP64 field face values (mixed routines with FP64 field fluxes)
+  double pc0 = 0.0;          // reference pressure of the split-pressure solvers
   if constexpr (SOLVER == 1) {
     // Lax-Friedrichs with MC slopes, 15_lax_flow.f95:920-1457: for stencil
     // cells 0..3 (the face lies between 1 and 2)
@@ -483,11 +496,22 @@ __device__ __forceinline__ uint32_t face_flux(const ACC& acc, const FacePre<T>* 
     Rs.vx = pre->vR[0]; Rs.vy = pre->vR[1]; Rs.vz = pre->vR[2];
     L.p = pre->pL; Rs.p = pre->pR;
     L.rho = pre->rhoL; Rs.rho = pre->rhoR;
+    if constexpr (kSplitP<T, SOLVER>) { L.dp = pre->dpL; Rs.dp = pre->dpR; pc0 = pre->pc0; }
   } else {
     rec(0, L.vx, Rs.vx);
     rec(1, L.vy, Rs.vy);
     rec(2, L.vz, Rs.vz);
-    recp(3, L.p, Rs.p);
+    if constexpr (kSplitP<T, SOLVER>) {
+      pc0 = nrmd(3, R);
+      T u[NS];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) u[q] = T(nrmd(3, q) - pc0);
+      const Pair<T> pp = MPCall<RM, T>::call_posd(u, pc0);
+      L.dp = pp.L; Rs.dp = pp.R;
+      L.p = T(pc0 + double(pp.L)); Rs.p = T(pc0 + double(pp.R));
+    } else {
+      recp(3, L.p, Rs.p);
+    }
     recp(4, L.rho, Rs.rho);
   }
   if constexpr (!PRE && (SOLVER == 5 || SOLVER == 7)) {
@@ -577,16 +601,19 @@ __device__ __forceinline__ uint32_t face_flux(const ACC& acc, const FacePre<T>* 
   rec(19, L.J, Rs.J);
   const T gamma = T(gamma_d);
   T vstar = T(0);
+  constexpr bool PS = kSplitP<T, SOLVER>;
   auto riemann = [&](T* A) {
-    if constexpr (SOLVER == 5) hll_fluxes<D>(L, Rs, gamma, A);
-    else if constexpr (SOLVER == 6) hlle_fluxes<D>(L, Rs, gamma, A, stt);
-    else if constexpr (SOLVER == 7) hllc_fluxes<D>(L, Rs, gamma, A, stt, kEmF64<T, SOLVER> ? &vstar : nullptr);
+    if constexpr (SOLVER == 5) hll_fluxes<D, PS>(L, Rs, gamma, A);
+    else if constexpr (SOLVER == 6) hlle_fluxes<D, PS>(L, Rs, gamma, A, stt, T(pc0));
+    else if constexpr (SOLVER == 7)
+      hllc_fluxes<D, PS>(L, Rs, gamma, A, stt, kEmF64<T, SOLVER> ? &vstar : nullptr, T(pc0));
   };
   if constexpr (kEmF64<T, SOLVER>) {
     T A[NROLE];
     riemann(A);
 #pragma unroll
     for (int c = R_Q; c < NROLE; ++c) F[c] = double(A[c]);
+    if constexpr (PS) F[R_SN] = pc0 + double(A[R_SN]);
     if constexpr (SOLVER == 7) psiphi_star_f64<D>(Ld, Rd, vstar, A, F);
   } else {
     riemann(F);
@@ -997,6 +1024,26 @@ __device__ __forceinline__ Pair<T> rec_acc(const ACC& a, int f) {
   return MPCall<RM, T>::template call<POS>(u);
 }
 
+// pressure face values of one direction (positivity-fixed pair; the
+// split-pressure solvers reconstruct differences from the face cell's value)
+template <int RM, int SOLVER, typename T, class ACC>
+__device__ __forceinline__ void pressure_pair(const ACC& a, FacePre<T>& pre) {
+  if constexpr (kSplitP<T, SOLVER>) {
+    constexpr int R = MPR<RM>::R, NS = 2 * R + 2;
+    const double c0 = a.n(3, R);
+    T u[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) u[q] = T(a.n(3, q) - c0);
+    const Pair<T> pp = MPCall<RM, T>::call_posd(u, c0);
+    pre.pc0 = c0;
+    pre.dpL = pp.L; pre.dpR = pp.R;
+    pre.pL = T(c0 + double(pp.L)); pre.pR = T(c0 + double(pp.R));
+  } else {
+    const Pair<T> pp = rec_acc<RM, T, true>(a, 3);
+    pre.pL = pp.L; pre.pR = pp.R;
+  }
+}
+
 // velocity slots of both faces of point (i, j) with the superluminal
 // fall-back of 16_hll_flow_mpx.f95:1393-1462: if any of the four
 // reconstructions is superluminal, both faces take cell (i, j) on the left
@@ -1046,9 +1093,9 @@ __device__ __forceinline__ uint32_t fused_yface(const RingAcc<RM, ROWS, 0>& ax, 
         for (int c = 0; c < 3; ++c) { xstash[c * 32] = double(xL[c]); xstash[(3 + c) * 32] = double(xR[c]); }
       }
     }
-    const Pair<T> pp = rec_acc<RM, T, true>(ay, 3);
+    pressure_pair<RM, SOLVER, T>(ay, py);
     const Pair<T> pr = rec_acc<RM, T, true>(ay, 4);
-    py.pL = pp.L; py.pR = pp.R; py.rhoL = pr.L; py.rhoR = pr.R;
+    py.rhoL = pr.L; py.rhoR = pr.R;
     if constexpr (SOLVER == 7) {
       yneg = (py.rhoL < T(0)) || (py.rhoR < T(0));
       if (yneg) {
@@ -1072,9 +1119,9 @@ __device__ __forceinline__ uint32_t fused_xface(const RingAcc<RM, ROWS, 0>& ax, 
     FacePre<T> px;
 #pragma unroll
     for (int c = 0; c < 3; ++c) { px.vL[c] = xv[c]; px.vR[c] = xv[3 + c]; }
-    const Pair<T> pp = rec_acc<RM, T, true>(ax, 3);
+    pressure_pair<RM, SOLVER, T>(ax, px);
     const Pair<T> pr = rec_acc<RM, T, true>(ax, 4);
-    px.pL = pp.L; px.pR = pp.R; px.rhoL = pr.L; px.rhoR = pr.R;
+    px.rhoL = pr.L; px.rhoR = pr.R;
     if constexpr (SOLVER == 7) {
       if ((px.rhoL < T(0) || px.rhoR < T(0)) && !yneg) {
         const T r10 = T(ax.n(4, R) * 1.0e-1);

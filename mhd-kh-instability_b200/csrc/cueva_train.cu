@@ -238,7 +238,10 @@ __global__ void k_c2p_batch(long long n, int method, double gamma, double eps1, 
     if (method == 1) {
       c2p_cardano(in, gamma, eps1, o, nullptr);
     } else {
-      const double p0 = (method == 2) ? mlp_pressure_seed(*M, in) : seed[i];
+      // 2: the network's seed; 4: the network's or the previous pressure,
+      // whichever leaves the smaller residual; 3: the given seeds
+      const double p0 = (method == 2) ? mlp_pressure_seed(*M, in)
+                        : (method == 4) ? c2p_best_seed(in, gamma, mlp_pressure_seed(*M, in)) : seed[i];
       it = c2p_newton(in, gamma, p0, o);
       if (it < 0) c2p_cardano(in, gamma, eps1, o, nullptr);
     }
@@ -601,11 +604,13 @@ int32_t cueva_c2p_batch(int32_t device, int32_t method, const cueva_mlp* M, doub
                         const double* d_cons, const double* d_prev, const double* d_seed, int64_t n, double* d_out,
                         int32_t* d_iters) {
   if (n <= 0 || !d_cons || !d_prev || !d_out) return cueva_fail(CUEVA_ERR_ARG, "bad arguments");
-  if (method < 1 || method > 3) return cueva_fail(CUEVA_ERR_ARG, "method must be 1 (Cardano), 2 (network) or 3 (seed)");
-  if (method == 2 && (!M || !M->normed)) return cueva_fail(CUEVA_ERR_ARG, "method 2 needs a trained network");
+  if (method < 1 || method > 4)
+    return cueva_fail(CUEVA_ERR_ARG, "method must be 1 (Cardano), 2 (network), 3 (seed) or 4 (network or previous p)");
+  if ((method == 2 || method == 4) && (!M || !M->normed))
+    return cueva_fail(CUEVA_ERR_ARG, "methods 2 and 4 need a trained network");
   if (method == 3 && !d_seed) return cueva_fail(CUEVA_ERR_ARG, "method 3 needs seeds");
   TRY(cudaSetDevice(device));
-  k_c2p_batch<<<grid_for(n), 256>>>(n, method, gamma, eps1, method == 2 ? M->d_dev : nullptr, d_cons, d_prev, d_seed,
+  k_c2p_batch<<<grid_for(n), 256>>>(n, method, gamma, eps1, (method == 2 || method == 4) ? M->d_dev : nullptr, d_cons, d_prev, d_seed,
                                     d_out, d_iters);
   TRY(cudaGetLastError());
   TRY(cudaDeviceSynchronize());

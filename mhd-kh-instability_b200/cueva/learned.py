@@ -16,7 +16,10 @@ from . import _abi
 
 CONS_ORDER = ["D", "tau", "Sx", "Sy", "Sz", "Ex", "Ey", "Ez", "Bx", "By", "Bz"]
 PRIM_ORDER = ["rho", "p", "vx", "vy", "vz"]
-CARDANO, NETWORK, SEEDED = 1, 2, 3
+# batch con2prim methods: Cardano; Newton from the network's seed; Newton from
+# given seeds; Newton from the network's seed or the previous pressure,
+# whichever leaves the smaller residual (the form the step uses)
+CARDANO, NETWORK, SEEDED, BEST = 1, 2, 3, 4
 
 
 def _ptr(t):
@@ -107,8 +110,10 @@ class LearnedSeed:
         return out
 
     def c2p(self, method, cons, prev, seed=None, gamma=4.0 / 3.0, eps1=1e-6):
-        """Batch con2prim: CARDANO, NETWORK (seed + Newton) or SEEDED (Newton
-        from `seed`); returns (prims (5, n), Newton iterations per state)."""
+        """Batch con2prim: CARDANO, NETWORK (seed + Newton), SEEDED (Newton
+        from `seed`) or BEST (Newton from the network's seed or the previous
+        pressure prev[1], whichever has the smaller residual); returns
+        (prims (5, n), Newton iterations per state)."""
         import torch
         n = cons.shape[1]
         out = torch.empty((5, n), dtype=torch.float64, device=cons.device)
