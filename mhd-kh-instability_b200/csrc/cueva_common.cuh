@@ -152,12 +152,20 @@ inline int stage_tiles(int imax, int jmax, int seg_rows) {
 // passes that error into E(n+1) undamped.  All routines but HLLE-MC
 // (flux_solver 3, whose field star states use the sound-speed bounds).
 __host__ __device__ constexpr bool mixed_em_f64(int solver) { return solver >= 1 && solver <= 7 && solver != 3; }
+// The mixed-precision MP routines HLL, HLLE and HLLC (flux_solver 5..7) also
+// form the normal momentum flux in FP64: its pressure part, ~1 in the KH
+// layer, is added to the FP32 rest there (see the split pressure of the
+// stage kernels).
+__host__ __device__ constexpr bool mixed_split_p(int solver) { return solver >= 5 && solver <= 7; }
+constexpr int ROLE_SN = 11;   // the normal momentum flux (R_SN of the Riemann roles)
 
 // Place of role r in the y-flux scratch (NFACE slabs of ffs doubles): f64
 // tells the element type and off the slab's first element in units of that
 // type.  FP64 kernels: double slab r.  Mixed kernels: FP32 slab r; with
 // mixed_em_f64, double slabs 0..7 for roles 0..7, then FP32 slabs for roles
-// 8..13 from byte offset 64 * ffs on.
+// 8..13 from byte offset 64 * ffs on; with mixed_split_p also, the normal
+// momentum flux in double slab 8 and the other five FP32 slabs from byte
+// offset 72 * ffs on.
 struct FluxSlot {
   bool f64;
   long long off;
@@ -166,6 +174,10 @@ __host__ __device__ inline FluxSlot flux_slot(bool mixed, int solver, int r, lon
   if (!mixed) return {true, r * ffs};
   if (!mixed_em_f64(solver)) return {false, r * ffs};
   if (r <= 7) return {true, r * ffs};
+  if (mixed_split_p(solver)) {
+    if (r == ROLE_SN) return {true, 8 * ffs};
+    return {false, (18 + (r < ROLE_SN ? r - 8 : r - 9)) * ffs};
+  }
   return {false, (16 + (r - 8)) * ffs};
 }
 

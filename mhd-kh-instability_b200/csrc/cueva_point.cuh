@@ -182,6 +182,17 @@ __device__ __forceinline__ void chebyshev_roots(double y, double& c0, double& c1
   c2 = c;
 }
 // x^(1/3), x >= 0: Newton cube root on the mantissa (frexp/ldexp are exact)
+// d_2 + 2 z_1 under the square root of the one-real-root branch of
+// 12_varprimitive.f95 vanishes where the depressed quartic is biquadratic
+// (d_1 = 0), which the KH layer at V0 = 0.8 crosses at |v| ~ 0.74; there the
+// sum is zero up to rounding and can come out as -1e-15, and the square root
+// would return NaN with no status raised (the reference has no check on this
+// branch).  A negative value within rounding of zero (<= 1e-12 |d_2|) is
+// taken as zero, the biquadratic limit; anything else is left as it is.
+__device__ __forceinline__ double biquad_guard(double s2, double d_2) {
+  return (s2 < 0.0 && -s2 <= 1.0e-12 * fabs(d_2)) ? 0.0 : s2;
+}
+
 __device__ __forceinline__ double cbrt_newton(double x) {
   if (!(x > 0.0) || !(x < CUDART_INF)) return x;
   int e;
@@ -248,7 +259,7 @@ __device__ __forceinline__ uint32_t c2p_cardano(const C2PIn& in, double gamma, d
     const double AA_1 = -fsgn1(R_1) * copysign(fabs(cbrt_newton(xx1)), xx1);
     const double BB_1 = (AA_1 != 0.0) ? Q_1 / AA_1 : 0.0;
     z_1 = (AA_1 + BB_1) - e / 3.0;
-    s = fabs(sqrt(d_2 + 2.0 * z_1));
+    s = fabs(sqrt(biquad_guard(d_2 + 2.0 * z_1, d_2)));
     t = fabs(sqrt(pw2(z_1) + 2.0 * d_2 * z_1 + pw2(d_2) - d_0));
     det = pw2(s) - 4.0 * (d_2 + z_1 - t);
   }

@@ -30,6 +30,7 @@ namespace cueva {
 enum Role { R_PSI = 0, R_PHI, R_BN, R_BT1, R_BT2, R_EN, R_ET1, R_ET2, R_Q, R_D, R_TAU, R_SN, R_ST1, R_ST2, NROLE };
 static_assert(NROLE == NFACE, "flux scratch holds one slab per role");
 static_assert(R_PSI == 0 && R_ET2 == 7, "flux_slot keeps roles 0..7 (psi, phi, E, B) in FP64 for the mixed MP solvers");
+static_assert(R_SN == ROLE_SN, "flux_slot keeps the normal momentum flux in FP64 for the split-pressure solvers");
 
 template <typename T>
 struct Side {
@@ -244,7 +245,20 @@ __device__ __forceinline__ T hllc_vel(T a, T b, T c, T rt, uint32_t& st) {
     v = fmax2(T(-1.0), fmin2(T(1.0), oldv - fv / dfdv));
     const T err = fabs(oldv - v);
     oldv = v;
-    if (iter >= 100) { st |= ST_HLLC_NOCONV; break; }
+    if (iter >= 100) {
+      if constexpr (sizeof(T) == sizeof(double)) {
+        st |= ST_HLLC_NOCONV;
+      } else {
+        // FP32 (mixed precision): where the quadratic is flat near its root
+        // the FP32 steps can hover above the tolerance; the same Newton in
+        // FP64 from the same seed decides
+        uint32_t st64 = 0;
+        v = float(hllc_vel<double>(double(a), double(b), double(c), double(rt), st64));
+        st |= st64;
+        return v;
+      }
+      break;
+    }
     if (!(err > tol)) break;
   }
   return fmax2(T(-1.0) + T(1.0e-3), fmin2(T(1.0) - T(1.0e-3), v));

@@ -293,7 +293,7 @@ struct FacePre {
 // rounded to FP32 in the flux whose divergence drives the small normal
 // velocity of the perturbation.
 template <typename T, int SV>
-constexpr bool kSplitP = kEmF64<T, SV> && (SV == 5 || SV == 6 || SV == 7);
+constexpr bool kSplitP = kEmF64<T, SV> && mixed_split_p(SV);
 
 // flux of one face from its stencil accessor (16_hll_flow_mpx.f95 /
 // 16_hllc_flow_mpx.f95 for one interface); returns status bits.  With PRE

@@ -304,6 +304,16 @@ void chebyshev_roots(double y, double& c0, double& c1, double& c2) {
   c2 = c;
 }
 
+// Deviation from 12_varprimitive.f95 (one-real-root branch): d_2 + 2 z_1
+// vanishes where the depressed quartic is biquadratic (d_1 = 0), which the
+// V0 = 0.8 KH layer crosses at |v| ~ 0.74; rounding can leave it at -1e-15,
+// and the reference's sqrt then returns NaN with no status raised (W, rho, p
+// and v of the point become NaN).  A negative value within rounding of zero
+// (<= 1e-12 |d_2|) is taken as zero, the biquadratic limit; other values are
+// unchanged, so every state the reference inverts to a finite result is
+// unaffected.
+double biquad_guard(double s2, double d_2) { return (s2 < 0.0 && -s2 <= 1.0e-12 * std::fabs(d_2)) ? 0.0 : s2; }
+
 double cbrt_newton(double x) {
   if (!(x > 0.0) || !(x < INFINITY)) return x;
   int e;
@@ -403,7 +413,7 @@ int32_t c2p_cardano(const C2PIn& in, double gamma, double eps1, C2POut& o, int64
       const double AA_1 = -fsign(1.0, R_1) * fsign(std::fabs(cr), xx1);
       const double BB_1 = (AA_1 != 0.0) ? Q_1 / AA_1 : 0.0;
       z_1 = (AA_1 + BB_1) - e / 3.0;
-      s = std::fabs(std::sqrt(d_2 + 2.0 * z_1));
+      s = std::fabs(std::sqrt(biquad_guard(d_2 + 2.0 * z_1, d_2)));
       t = std::fabs(std::sqrt(pw2(z_1) + 2.0 * d_2 * z_1 + pw2(d_2) - d_0));
       det = pw2(s) - 4.0 * (d_2 + z_1 - t);
     }

@@ -157,3 +157,38 @@ def test_con2prim_routine_mirror(oracle_mod, method):
         nbad = int((got != want[n]).sum())
         assert nbad == 0, f"{n}: {nbad} of {got.size} points differ"
     g.close()
+
+
+def test_con2prim_biquadratic_state(oracle_mod):
+    """cueva_con2prim on the V0 = 0.8 state where the quartic of the Cardano
+    recovery is biquadratic to rounding (test_oracle_pins.BIQUAD_STATE): a
+    finite result, bit-identical to the oracle's, no status."""
+    from test_oracle_pins import BIQUAD_STATE
+    from cueva import Cueva
+    imax, jmax = 8, 8
+    inp = np.array(BIQUAD_STATE)
+    g = Cueva(imax, jmax, order=4, flux_solver=7, rec_mp=0, c2p=1, sigma=1e5)
+    vals = {"D": inp[0], "tau": inp[1], "Sx": inp[2], "Sy": inp[3], "Sz": inp[4], "Ex": inp[5], "Ey": inp[6],
+            "Ez": inp[7], "Bx": inp[8], "By": inp[9], "Bz": inp[10], "vx": inp[11], "vy": inp[12], "vz": inp[13],
+            "rho": inp[14], "p": inp[15], "psi": 0.0, "phi": 0.0, "q": 0.0}
+    for n, v in vals.items():
+        g.set_interior(n, np.full((jmax + 1, imax + 1), v))
+    g.con2prim()
+    assert g.status() == 0
+    st, want = oracle_mod.c2p(inp, method=1, eps1=float(np.float32(1e-6)))
+    assert st == 0
+    for k, n in enumerate(("vx", "vy", "vz", "rho", "p")):
+        got = g.interior(n)
+        assert np.all(np.isfinite(got)) and np.all(got == want[k]), n
+    g.close()
+
+
+def test_v08_layer_runs_past_the_biquadratic_state(oracle_mod):
+    """The V0 = 0.8, sigma = 1e5 layer (MP5 + HLLC, SSP3(4,3,3) with per-stage
+    reset) with a = 0.05 on 256 x 512: the reference's Cardano returned NaN at
+    step 5 (point (277, 90)); with the biquadratic limit both sides run on,
+    1 step <= 1e-12 and 20 steps <= 1e-9 apart, with no status."""
+    import dataclasses
+    from cueva.configs import C3
+    cfg = dataclasses.replace(C3, nx=256, ny=512, a=0.05, rec_mp=0)
+    _run_pair(oracle_mod, cfg, [(1, 1e-12), (20, 1e-9)])

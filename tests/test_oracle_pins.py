@@ -418,3 +418,29 @@ def test_hllc_em_fluxes_equal_hll(oracle_mod):
             assert not np.array_equal(arrs[5][n], arrs[7][n]), n   # corrected by the contact
         else:
             assert np.array_equal(arrs[5][n], arrs[7][n]), n
+
+
+# A state of the V0 = 0.8 KH layer (256 x 512, a = 0.05, step 5, point
+# (277, 90)) where the depressed quartic of the Cardano recovery is
+# biquadratic to rounding (d_1 = 3e-9): d_2 + 2 z_1 of the one-real-root
+# branch comes out as -1.3e-15.  Exact bits; D, tau, S, E, B, then the seeds.
+BIQUAD_STATE = [float.fromhex(h) for h in (
+    "0x1.7dcd0bb9e7a81p+0", "0x1.442aaecbba2e9p+3", "-0x1.7bf2784f7b54cp-5", "0x1.0830b1d8ae4d0p+3", "0x0.0p+0",
+    "0x0.0p+0", "0x0.0p+0", "0x1.ba9505f926cc5p-12", "0x1.300b04ea65465p-17", "0x1.9976c538ce886p-4", "0x0.0p+0",
+    "-0x1.101b440068168p-8", "0x1.7bf60cdc988bep-1", "0x0.0p+0", "0x1.ffd74b35d9abcp-1", "0x1.ffc9c1aa05e5bp-1")]
+
+
+def test_cardano_biquadratic_state_recovered(oracle_mod):
+    """Where the reference's square root of d_2 + 2 z_1 would take a
+    rounding-level negative argument (a silent NaN in 12_varprimitive.f95),
+    the recovery takes the biquadratic limit: a finite state whose conserved
+    variables reproduce the input, and that agrees with the NR recovery."""
+    inp = np.array(BIQUAD_STATE)
+    st, out = oracle_mod.c2p(inp, method=1, eps1=float(np.float32(1e-6)))
+    assert st == 0 and np.all(np.isfinite(out))
+    vx, vy, vz, rho, p, W = out
+    D, tau, S = _cons(np.array([rho]), np.array([p]), np.array([[vx, vy, vz]]), inp[None, 5:8], inp[None, 8:11])
+    assert abs(D[0] / inp[0] - 1) < 1e-9 and abs(tau[0] / inp[1] - 1) < 1e-9
+    assert np.abs(S[0] - inp[2:5]).max() < 1e-9 * np.abs(inp[2:5]).max()
+    st_nr, out_nr = oracle_mod.c2p(inp, method=0)
+    assert st_nr == 0 and abs(out_nr[3] / rho - 1) < 1e-4 and abs(out_nr[1] / vy - 1) < 1e-4
