@@ -21,7 +21,7 @@ namespace {
 constexpr int C2P_CTAS_PER_SM = 4;
 
 // one point of the learned con2prim (all 128 threads of the CTA call it, in
-// step): seeds p from the network or the previous pressure (the one with the
+// step): seeds p from the previous pressure or the network (the one with the
 // smaller residual), refines it, falls back to Cardano
 struct LearnedOut {
   C2POut o;
@@ -30,11 +30,20 @@ struct LearnedOut {
 };
 __device__ __forceinline__ bool learned_point(MLPShared& S, uint32_t& phase, const C2PIn& in, double gamma,
                                               double eps1, unsigned long long* counters, bool count, LearnedOut& r) {
-  float f[MLP_IN];
-  c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
-  float y = 0.0f;
-  if (!mlp_tc_tile(S, phase, f, y)) return false;
-  const double seed = c2p_best_seed(in, gamma, in.D * (double)__expf(y * S.sd_y + S.mu_y));
+  // The network's seeds leave Newton about 1e-2 from the root.  Where the
+  // previous pressure is already closer than that for every point of the
+  // tile (residual <= 1e-2 p), the tile skips the network; otherwise the
+  // tile runs it and each point starts from the better of the two seeds.
+  const double r_prev = c2p_residual(in, gamma, in.p0);
+  double seed = in.p0;
+  if (!__syncthreads_and(r_prev <= 1.0e-2 * in.p0)) {   // uniform over the CTA (one tile)
+    float f[MLP_IN];
+    c2p_features(in.D, in.tau, in.Sx, in.Sy, in.Sz, in.Ex, in.Ey, in.Ez, in.Bx, in.By, in.Bz, f);
+    float y = 0.0f;
+    if (!mlp_tc_tile(S, phase, f, y)) return false;
+    const double p_net = in.D * (double)__expf(y * S.sd_y + S.mu_y);
+    seed = c2p_residual(in, gamma, p_net) < r_prev ? p_net : in.p0;
+  }
   r.it = c2p_newton(in, gamma, seed, r.o);
   r.st = 0u;
   if (r.it <= 0) r.st = c2p_cardano_ool(in, gamma, eps1, r.o, count ? counters : nullptr);

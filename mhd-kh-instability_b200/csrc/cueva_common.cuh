@@ -81,7 +81,7 @@ struct InstDesc {
   // learned con2prim, fused stage)
   int block_begin[4];
   int block_count[4];
-  int seg_rows;        // fused stage tiles: grid rows per tile (a multiple of the band height)
+  int seg_rows;        // fused stage tiles: grid rows per tile (bands of the tile height, less one row)
 };
 
 // ---- tableau data of one stage launch (by value, kernel parameter space) -----

@@ -199,19 +199,20 @@ bool stage_fused_available(int rec_mp, int solver) {
 }
 
 int stage_seg_rows(int imax, int jmax, int rows, int slots) {
-  // A tile of nb bands costs about nb + 0.7 band times (its first bottom
-  // faces take one warp about as long as a band's faces); the launch takes
-  // about ceil(tiles / slots) tile times.  Pick the band count with the
-  // smallest product (the larger one on ties: fewer repeated faces).
+  // A tile of nb bands updates nb * rows - 1 grid rows (its first band also
+  // computes the faces below the segment) and costs about nb band times; the
+  // launch takes about ceil(tiles / slots) tile times.  Pick the band count
+  // with the smallest product (the larger one on ties: fewer repeated faces).
   const int strips = (imax + 1 + 30) / 31;
   int best = 1;
-  double best_cost = 1e300;
+  long long best_cost = -1;
   for (int nb = 1; nb <= 32; ++nb) {
-    const long long tiles = (long long)strips * ((jmax + 1 + nb * rows - 1) / (nb * rows));
-    const double cost = (double)((tiles + slots - 1) / slots) * (nb + 0.7);
-    if (cost <= best_cost) { best_cost = cost; best = nb; }
+    const int seg = nb * rows - 1;
+    const long long tiles = (long long)strips * ((jmax + 1 + seg - 1) / seg);
+    const long long cost = (tiles + slots - 1) / slots * nb;
+    if (best_cost < 0 || cost <= best_cost) { best_cost = cost; best = nb; }
   }
-  return best * rows;
+  return best * rows - 1;
 }
 
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {

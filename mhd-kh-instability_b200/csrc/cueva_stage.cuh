@@ -946,8 +946,9 @@ k_xupd(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa) 
 // only its ROWS new rows.  Thread (lane, w) of a band computes the y face
 // (i, j+1/2) and the x face (i+1/2, j) of point (i, j), j = j0 + w: the y
 // fluxes go to a shared buffer of ROWS + 1 face rows (a band's bottom faces
-// are the previous band's top faces; a segment computes its first bottom row
-// itself), the x flux of i-1/2 comes by warp shuffle, and the point is
+// are the previous band's top faces; the first band of a segment starts one
+// row lower, where warp 0 computes the segment's bottom faces), the x flux of
+// i-1/2 comes by warp shuffle, and the point is
 // updated as in k_xupd.  Against k_yface + k_xupd the y fluxes never leave
 // the SM, every stencil value is copied in once per stage, and the velocity
 // reconstructions that the superluminal fall-back of HLL / HLLC couples
@@ -1194,23 +1195,17 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
       for (int q = 0; q < NS; ++q) a.off[q] = G::slot(j - R + q) * G::ROWSZ + lane + R;
       return a;
     };
-    // the segment's first bottom faces jseg - 1/2 (rows jseg-1-R .. jseg+R)
-    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jseg - 1 - R, jseg + R, tid);
-    cp_async_wait_all();
-    __syncthreads();
-    if (w == 0 && i <= ilast) {
-      flux_t<T, SOLVER> F[NROLE];
-      bool yneg;
-      stt |= fused_yface<RM, SOLVER, T, ROWS>(x_acc(jseg - 1), y_acc(jseg - 1), I, nullptr, yneg, F);
-#pragma unroll
-      for (int c = 0; c < NROLE; ++c) yf[c * 32 + lane] = double(F[c]);   // face row 0 of band 0
-    }
-    __syncthreads();   // the band's copies overwrite the ring row of grid row jseg-1-R
-    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jseg + R + 1, min(jseg + ROWS - 1, jend) + R + 1, tid);
+    // The bands start one row below the segment: warp 0 of the first band
+    // computes only the y faces jseg - 1/2 (the segment's bottom faces; row
+    // jseg - 1 belongs to the segment below and is not updated here), every
+    // other warp the y face, the x face and the update of its row.  With
+    // seg_rows = 8 nb - 1 the bands are full.
+    const int jfirst = jseg - 1;
+    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jfirst - R, min(jfirst + ROWS - 1, jend) + R + 1, tid);
     int band = 0;
-    for (int j0 = jseg; j0 <= jend; j0 += ROWS, ++band) {
+    for (int j0 = jfirst; j0 <= jend; j0 += ROWS, ++band) {
       const int jl = min(j0 + ROWS - 1, jend);
-      if constexpr (EP != EP_RHS) prefetch_update_rows(I, sa, i0, ilast, j0, jl, tid, 32 * ROWS);
+      if constexpr (EP != EP_RHS) prefetch_update_rows(I, sa, i0, ilast, max(j0, jseg), jl, tid, 32 * ROWS);
       // the band's rows have arrived, and every warp has finished the previous
       // band's update (its reads of the face rows that this band overwrites)
       cp_async_wait_all();
@@ -1219,6 +1214,7 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
       const int rb = (band * ROWS) % (ROWS + 1);
       auto frow = [&](int k) { const int r = k + rb; return yf + (r >= ROWS + 1 ? r - (ROWS + 1) : r) * (NROLE * 32); };
       const int j = j0 + w;
+      const bool face_only = j < jseg;   // warp 0 of the first band
       const bool valid = lane >= 1 && i <= ilast;
       const bool warp_c2p = EP == EP_LAST && I.c2p == 2 && !I.c2p_tc;
       // point whose update this lane computes (lanes without one repeat a real
@@ -1245,7 +1241,7 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
 #pragma unroll
             for (int c = 0; c < NROLE; ++c) top[c * 32] = double(Fy[c]);
           }
-          stt |= fused_xface<RM, SOLVER, T, ROWS>(ax, I, xv, yneg, Fx);
+          if (!face_only) stt |= fused_xface<RM, SOLVER, T, ROWS>(ax, I, xv, yneg, Fx);
         }
         // centre values of the point, read before the next band's copies
         // replace the ring rows
@@ -1257,7 +1253,7 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
       __syncthreads();   // the band's y fluxes are complete and its ring reads done
       if (j0 + ROWS <= jend)   // the next band's rows arrive while this band updates
         ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, j0 + ROWS + R + 1, min(j0 + 2 * ROWS - 1, jend) + R + 1, tid);
-      if (j <= jl) {
+      if (j <= jl && !face_only) {
         const double dlx = I.delx, ix2 = I.inv_delx_pow2;
         double qx[NROLE];
 #pragma unroll
