@@ -119,6 +119,18 @@ module cueva_gpu
        type(c_ptr), value :: ctx
        integer(c_int32_t), value :: nsteps
      end function cueva_step
+     ! one fused kernel per RK stage (1, the default for MP5 and the MC slopes)
+     ! or the y-face and x-face + update kernels (0); bit-identical results
+     integer(c_int32_t) function cueva_set_stage_kernel(ctx, fused) bind(c, name="cueva_set_stage_kernel")
+       import :: c_int32_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: fused
+     end function cueva_set_stage_kernel
+     integer(c_int32_t) function cueva_device_bytes(ctx, nbytes) bind(c, name="cueva_device_bytes")
+       import :: c_int32_t, c_int64_t, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), intent(out) :: nbytes
+     end function cueva_device_bytes
      integer(c_int32_t) function cueva_sync(ctx) bind(c, name="cueva_sync")
        import :: c_int32_t, c_ptr
        type(c_ptr), value :: ctx
