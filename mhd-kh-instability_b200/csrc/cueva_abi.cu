@@ -334,6 +334,15 @@ StageArgs stage_args_of(const Tableau& T, const int* kslot_of, int intsum_reset,
   sa.abt_diag_first = T.Abt[0][0];
   for (int m = 1; m < l; ++m) sa.kslot[m - 1] = kslot_of[m - 1];
   sa.store_k_slot = (l < T.s) ? kslot_of[l - 1] : -1;
+  // K_l is read by rows r >= l+2 only through its E sources when every such
+  // row has Ab(r, l) = 0 (SSP3(4,3,3): K_1, whose only later use is Abt(4,1))
+  sa.store_k_src = 1;
+  for (int r = l + 1; r < T.s; ++r) sa.store_k_src = sa.store_k_src && T.Ab[r][l - 1] == 0.0;
+  // the final sums stay zero while every stage so far has zero weights
+  // (SSP3(4,3,3): wb(1) = wbt(1) = 0)
+  sa.fin_load = 0;
+  for (int m = 1; m < l; ++m) sa.fin_load = sa.fin_load || T.wb[m - 1] != 0.0 || T.wbt[m - 1] != 0.0;
+  sa.fin_store = sa.fin_load || T.wb[l - 1] != 0.0 || T.wbt[l - 1] != 0.0;
   // the reference zeroes the stage sums once per step, so stage l+1 starts
   // from the sums of stage l; with intsum_reset every stage starts from zero
   sa.need_intsum_load = (!intsum_reset && l >= 2 && l < T.s) ? 1 : 0;
@@ -1360,6 +1369,7 @@ int32_t cueva_flux_rhs_noalloc(const cueva_params* p, const double* prim, const 
   sa.l = 1; sa.s = 1; sa.cur = 0; sa.qin = 0; sa.mode = 1;
   for (int m = 0; m < 8; ++m) sa.kslot[m] = -1;
   sa.store_k_slot = -1;
+  sa.store_k_src = 0; sa.fin_load = 0; sa.fin_store = 0;
   CUDA_TRY(launch_stage(p->rec_mp, p->flux_solver, p->precision, sh, st, d_inst, 1, sa));
   if (status_bits) {
     uint32_t h = 0;

@@ -97,6 +97,11 @@ struct StageArgs {
   double abt_diag_first;// Abt(1,1) (next step's stage 1)
   int kslot[8];        // slot of stored K_m in kbuf, -1 if not stored
   int store_k_slot;    // slot to store K_l, -1 if not needed
+  int store_k_src;     // K_l is only read through its E sources (every later row has Ab = 0 in
+                       // column l): store the 3 sources, not the 14 fluxes
+  int fin_load;        // the final sums of earlier stages are not all zero (some wb, wbt of m < l
+                       // is non-zero): load them; else they start from zero
+  int fin_store;       // the final sums after this stage are not identically zero: store them
   int need_intsum_load;  // stage l >= 2 and s >= 3: intsum_l is stored
   int need_intsum_store; // l + 1 < s
   int mode;            // 0 fused (next stage / final), 1 store rhs only, 2 also the x-face fluxes (I.fx)

@@ -725,7 +725,8 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
     double fin[NCONS];
 #pragma unroll
     for (int c = 0; c < NCONS; ++c) {
-      const double prev = (sa.l == 1) ? 0.0 : I.finsum[c * fs + pc];
+      // sums of stages with zero weights are zero (up to the sign of zero)
+      const double prev = sa.fin_load ? I.finsum[c * fs + pc] : 0.0;
       if (c >= Q_EX && c <= Q_EZ) fin[c] = prev + (sa.wb * K[c] - sa.wbt * K[K_SEX + (c - Q_EX)]);
       else fin[c] = prev + sa.wb * K[c];
     }
@@ -738,8 +739,10 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
     U[Q_D] = aux[A_D * fs + pc]; U[Q_TAU] = aux[A_TAU * fs + pc];
     U[Q_SX] = aux[A_SX * fs + pc]; U[Q_SY] = aux[A_SY * fs + pc]; U[Q_SZ] = aux[A_SZ * fs + pc];
     if constexpr (EP == EP_MID) {
+      if (sa.fin_store) {
 #pragma unroll
-      for (int c = 0; c < NCONS; ++c) I.finsum[c * fs + pc] = fin[c];
+        for (int c = 0; c < NCONS; ++c) I.finsum[c * fs + pc] = fin[c];
+      }
       // sumint for stage l+1 (09_sumint.f95:18-67); intsum is zeroed only
       // once per step (07_clean_var.f95), so it accumulates across stages
       double acc[NCONS];
@@ -749,13 +752,21 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
         const double ab = sa.ab_next[m - 1], abt = sa.abt_next[m - 1];
         if (ab == 0.0 && abt == 0.0) continue;
         const double* Km = (m < sa.l) ? I.kbuf + (long long)sa.kslot[m - 1] * NRHS * fs : nullptr;
+        // with Ab = 0 the term ab * F is a zero: the flux of K_m is not read
+        // (a stored K_m may hold its E sources only), which changes at most
+        // the sign of a zero sum
 #pragma unroll
         for (int c = 0; c < NCONS; ++c) {
-          const double F = Km ? Km[c * fs + pc] : K[c];
           if (c >= Q_EX && c <= Q_EZ) {
             const double S = Km ? Km[(K_SEX + c - Q_EX) * fs + pc] : K[K_SEX + c - Q_EX];
-            acc[c] = acc[c] + (ab * F - abt * S);
-          } else {
+            if (ab == 0.0) {
+              acc[c] = acc[c] + (0.0 - abt * S);
+            } else {
+              const double F = Km ? Km[c * fs + pc] : K[c];
+              acc[c] = acc[c] + (ab * F - abt * S);
+            }
+          } else if (ab != 0.0) {
+            const double F = Km ? Km[c * fs + pc] : K[c];
             acc[c] = acc[c] + ab * F;
           }
         }
@@ -767,7 +778,8 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
       if (sa.store_k_slot >= 0) {
         double* Ko = I.kbuf + (long long)sa.store_k_slot * NRHS * fs;
 #pragma unroll
-        for (int c = 0; c < NRHS; ++c) Ko[c * fs + pc] = K[c];
+        for (int c = 0; c < NRHS; ++c)
+          if (!sa.store_k_src || c >= K_SEX) Ko[c * fs + pc] = K[c];
       }
       // varint (10_varint.f95:23-63), electricvarint and flowinit of stage l+1
       double Qn[NCONS];
@@ -824,6 +836,43 @@ __device__ __forceinline__ uint32_t update_point(const InstDesc& I, const StageA
   return st;
 }
 
+// L2 prefetch of the update's other inputs for the points i0+1 .. ilast of
+// rows j0 .. jl: the 6 aux and 9 time-n primitive fields, the final sums and
+// stage sums when loaded, and the stored stage right-hand sides a later row
+// reads (their E sources only where that row's Ab is zero)
+__device__ __forceinline__ void prefetch_update_rows(const InstDesc& I, const StageArgs& sa, int i0, int ilast, int j0,
+                                                     int jl, int tid, int nthr) {
+  const long long fs = I.fstride;
+  const int npt = ilast - i0, nr = jl - j0 + 1;
+  if (npt <= 0 || nr <= 0) return;
+  const int nfin = sa.fin_load ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
+  int nkf = 0;   // stored K fields read
+  for (int m = 1; m < sa.l; ++m)
+    if (sa.kslot[m - 1] >= 0) nkf += sa.ab_next[m - 1] != 0.0 ? NRHS : (sa.abt_next[m - 1] != 0.0 ? 3 : 0);
+  const int ncen = NAUX + 9 + nfin + nint + nkf;
+  for (int e = tid; e < ncen * nr; e += nthr) {
+    const int r = e % nr;
+    int f = e / nr;
+    const double* base;
+    if (f < NAUX) base = I.aux[sa.cur] + f * fs;
+    else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
+    else if ((f -= 9) < nfin) base = I.finsum + f * fs;
+    else if ((f -= nfin) < nint) base = I.intsum + f * fs;
+    else {
+      f -= nint;
+      base = nullptr;
+      for (int m = 1; m < sa.l && !base; ++m) {
+        if (sa.kslot[m - 1] < 0) continue;
+        const int nm = sa.ab_next[m - 1] != 0.0 ? NRHS : (sa.abt_next[m - 1] != 0.0 ? 3 : 0);
+        if (f < nm) base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + (nm == NRHS ? f : K_SEX + f)) * fs;
+        else f -= nm;
+      }
+      if (!base) continue;
+    }
+    prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
+  }
+}
+
 template <int RM, int SOLVER, typename T, int EP, int ROWS>
 __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa, int b, double* sn, double* st) {
   using G = FaceGeom<RM, SOLVER, ROWS>;
@@ -835,37 +884,13 @@ __device__ __forceinline__ void xupd_tile(const InstDesc& I, const StageArgs& sa
   const int ilast = min(i0 + 31, I.imax), jlast = min(j0 + ROWS - 1, I.jmax);
   stage_tile<RM, SOLVER, 0, ROWS>(I, sa, sn, st, i0, j0, ilast, jlast, w * 32 + lane);
   if constexpr (EP != EP_RHS) {
-    // the update's other inputs go to L2 while the faces are computed: per
-    // row of the tile, the 6 aux and 9 time-n primitive fields, finsum and
-    // intsum when loaded, stored stage right-hand sides, and the y fluxes
-    const long long fs = I.fstride;
+    // the update's other inputs and the y fluxes go to L2 while the faces
+    // are computed
+    prefetch_update_rows(I, sa, i0, ilast, j0, jlast, w * 32 + lane, 32 * ROWS);
     const int npt = ilast - i0, nr = jlast - j0 + 1;
-    const int nfin = (sa.l > 1) ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
-    int nk = 0;
-    for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
-    const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;   // fields read at the point
-    const int total = ncen * nr + NROLE * (nr + 1);
-    for (int e = w * 32 + lane; e < total && npt > 0; e += 32 * ROWS) {
-      if (e < ncen * nr) {
-        const int r = e % nr;
-        int f = e / nr;
-        const double* base;
-        if (f < NAUX) base = I.aux[sa.cur] + f * fs;
-        else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
-        else if ((f -= 9) < nfin) base = I.finsum + f * fs;
-        else if ((f -= nfin) < nint) base = I.intsum + f * fs;
-        else {
-          f -= nint;
-          int kk = f / NRHS, m = 1;
-          for (; m < sa.l; ++m)
-            if (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0) && kk-- == 0) break;
-          base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + f % NRHS) * fs;
-        }
-        prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
-      } else {
-        const int e2 = e - ncen * nr, r = e2 % (nr + 1), c = e2 / (nr + 1);
-        flux_prefetch<T, SOLVER>(I.fy, I.ffs, c, (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
-      }
+    for (int e = w * 32 + lane; e < NROLE * (nr + 1) && npt > 0; e += 32 * ROWS) {
+      const int r = e % (nr + 1), c = e / (nr + 1);
+      flux_prefetch<T, SOLVER>(I.fy, I.ffs, c, (long long)(j0 + r) * I.fpitch + i0 + 1, npt);
     }
   }
   cp_async_wait_all();
@@ -1133,36 +1158,6 @@ __device__ __forceinline__ uint32_t fused_xface(const RingAcc<RM, ROWS, 0>& ax, 
     return face_flux<RM, SOLVER, T, 0, true>(ax, &px, I.gamma, I.sigma, F);
   } else {
     return face_flux<RM, SOLVER, T, 0, false>(ax, (const FacePre<T>*)nullptr, I.gamma, I.sigma, F);
-  }
-}
-
-// L2 prefetch of the update's other inputs for rows j0 .. jl of a strip (see
-// xupd_tile)
-__device__ __forceinline__ void prefetch_update_rows(const InstDesc& I, const StageArgs& sa, int i0, int ilast, int j0,
-                                                     int jl, int tid, int nthr) {
-  const long long fs = I.fstride;
-  const int npt = ilast - i0, nr = jl - j0 + 1;
-  if (npt <= 0 || nr <= 0) return;
-  const int nfin = (sa.l > 1) ? NCONS : 0, nint = sa.need_intsum_load ? NCONS : 0;
-  int nk = 0;
-  for (int m = 1; m < sa.l; ++m) nk += (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0)) ? 1 : 0;
-  const int ncen = NAUX + 9 + nfin + nint + nk * NRHS;
-  for (int e = tid; e < ncen * nr; e += nthr) {
-    const int r = e % nr;
-    int f = e / nr;
-    const double* base;
-    if (f < NAUX) base = I.aux[sa.cur] + f * fs;
-    else if ((f -= NAUX) < 9) base = I.prim[sa.cur] + (P_PSI + f) * fs;
-    else if ((f -= 9) < nfin) base = I.finsum + f * fs;
-    else if ((f -= nfin) < nint) base = I.intsum + f * fs;
-    else {
-      f -= nint;
-      int kk = f / NRHS, m = 1;
-      for (; m < sa.l; ++m)
-        if (sa.kslot[m - 1] >= 0 && (sa.ab_next[m - 1] != 0.0 || sa.abt_next[m - 1] != 0.0) && kk-- == 0) break;
-      base = I.kbuf + ((long long)sa.kslot[m - 1] * NRHS + f % NRHS) * fs;
-    }
-    prefetch_l2(base + (long long)(j0 + r) * I.pitch + i0 + 1, npt);
   }
 }
 
