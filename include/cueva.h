@@ -43,6 +43,8 @@ extern "C" {
 #define CUEVA_ST_TC_TIMEOUT 64u     /* a bounded tensor-core (tcgen05) wait ran out; no reference counterpart */
 #define CUEVA_ST_TC_TEARDOWN 128u   /* after such a time-out the teardown's bounded wait ran out too: TMEM was
                                        released while an MMA may still write it; destroy the context */
+#define CUEVA_ST_COPY_TIMEOUT 256u  /* a bounded wait for the stage kernel's bulk copies of stencil rows ran
+                                       out; the state of that step is incomplete; no reference counterpart */
 
 typedef struct cueva_ctx cueva_ctx;
 

@@ -315,7 +315,7 @@ int32_t read_status(cueva_ctx* c) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (st) {
     char buf[160];
-    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed, 64 tensor-core wait, 128 tensor-core teardown: context suspect)", st);
+    snprintf(buf, sizeof buf, "kernel status 0x%x (1 con2prim, 2 superluminal, 4 hllc_vel, 8 v* not finite, 16 non-finite state, 32 HLLE wave speed, 64 tensor-core wait, 128 tensor-core teardown: context suspect, 256 stencil copy wait)", st);
     return fail(CUEVA_ERR_PHYSICS, buf);
   }
   return CUEVA_OK;

@@ -38,6 +38,8 @@ enum StatusBits : uint32_t {
   ST_TC_TEARDOWN = 128u,   // after such a time-out the teardown's bounded wait for the MMAs still in
                            // flight ran out too: TMEM was released while an MMA may still write it, so
                            // the context is suspect and should not be reused
+  ST_COPY_TIMEOUT = 256u,  // a bounded wait for the bulk copies of the stage kernel's stencil rows ran
+                           // out (no reference counterpart); the CTA stopped
 };
 
 // ---- per-instance descriptor (one grid of the ensemble) -------------------

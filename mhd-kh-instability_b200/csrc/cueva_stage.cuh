@@ -31,6 +31,7 @@
 #include "cueva_riemann.cuh"
 #include "cueva_point.cuh"
 #include "cueva_mlp.cuh"
+#include "cueva_umma.cuh"
 
 namespace cueva {
 
@@ -985,7 +986,10 @@ struct RingGeom {
   static constexpr int R = MPR<RM>::R;
   static constexpr int NS = 2 * R + 2;
   static constexpr int NR = ROWS + 2 * R + 1;          // ring rows
-  static constexpr int LONG = 32 + 2 * R + 1;          // staged columns i0-R .. i0+32+R
+  // staged columns: cs .. cs + LONG - 1 with cs = (i0 - R) rounded down to
+  // an even column (16-byte aligned rows for the bulk copies), covering the
+  // stencils' i0-R .. i0+32+R
+  static constexpr int LONG = 32 + 2 * R + 2;
   static constexpr int ROWSZ = NF_RING * LONG;         // doubles per ring row
   static constexpr int RING = NR * ROWSZ;
   static constexpr int YF = (ROWS + 1) * NROLE * 32;   // y-flux face rows x roles x lanes
@@ -998,23 +1002,77 @@ struct RingGeom {
 template <int RM>
 constexpr bool kFused = RingGeom<RM, FACE_ROWS>::bytes() <= 113 * 1024;
 
-// copies grid rows ra .. rb of the strip (columns i0-R .. ilast+R+1) into
-// their ring rows, through the ghost maps
+// first staged column of a strip (see RingGeom::LONG)
+template <int R>
+__device__ __forceinline__ int ring_col0(int i0) { return (i0 - R) & ~1; }
+
+// Whether a strip's staged columns are all interior points: then every ring
+// row is one contiguous, 16-byte aligned segment of LONG doubles per field
+// (rows outside 0..jmax map to interior rows), copied by the bulk-copy
+// engine; strips at the x boundaries go element by element through the
+// ghost map.
+template <int RM, int ROWS>
+__device__ __forceinline__ bool ring_bulk(const InstDesc& I, int i0) {
+  const int cs = ring_col0<MPR<RM>::R>(i0);
+  return cs >= 0 && cs + RingGeom<RM, ROWS>::LONG - 1 <= I.imax;
+}
+
+// staged field f (0-4 time-n vx, vy, vz, p, rho; 5-20 stage psi .. Sz, Jx, Jy)
+__device__ __forceinline__ const double* ring_field(const double* prim, const double* Q, long long fs, int f) {
+  if (f < 5) return prim + (long long)(f < 3 ? P_VX + f : (f == 3 ? P_P : P_RHO)) * fs;
+  return Q + (long long)(f - 5) * fs;
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// one bulk copy global -> shared of `bytes` (16-byte aligned addresses, a
+// multiple of 16 bytes) completing on the CTA's mbarrier `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   umma::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(umma::smem_u32(bar))
+               : "memory");
+}
+
+// copies grid rows ra .. rb of the strip into their ring rows: with bulk,
+// one bulk copy per field and row issued by warp 0 (completion on bar, which
+// the caller waits for), else element by element through the ghost maps
+// (columns i0-R .. ilast+R+1; the caller waits with cp.async.wait_all)
 template <int RM, int ROWS>
 __device__ __forceinline__ void ring_fill(const InstDesc& I, const StageArgs& sa, double* ring, int i0, int ilast,
-                                          int ra, int rb, int tid) {
+                                          int ra, int rb, int tid, bool bulk, uint64_t* bar) {
   using G = RingGeom<RM, ROWS>;
   constexpr int R = G::R, LONG = G::LONG;
   const long long fs = I.fstride;
   const double* __restrict__ prim = I.prim[sa.cur];
   const double* __restrict__ Q = I.stage[sa.qin];
-  const int ncell = ilast + R + 1 - (i0 - R) + 1;
+  const int cs = ring_col0<R>(i0);
+  if (bulk) {
+    // every thread arrives once per fill (the barrier counts all of them),
+    // announcing the bytes of the copies it issues itself
+    const int n = (rb - ra + 1) * NF_RING;
+    constexpr uint32_t kRowBytes = LONG * sizeof(double);
+    uint32_t mine = 0;
+    for (int e = tid; e < n; e += 32 * ROWS) mine += kRowBytes;
+    // the ring rows being replaced were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_arrive_expect_tx(bar, mine);
+    for (int e = tid; e < n; e += 32 * ROWS) {
+      const int r = e / NF_RING, f = e - r * NF_RING, row = ra + r;
+      const double* src = ring_field(prim, Q, fs, f) + (long long)map_idx(row, I.jmax, I.bc_y) * I.pitch + cs;
+      bulk_g2s(ring + G::slot(row) * G::ROWSZ + f * LONG, src, kRowBytes, bar);
+    }
+    return;
+  }
+  const int cfirst = i0 - R - cs, clast = ilast + R + 1 - cs;   // needed ring columns
   const int n = (rb - ra + 1) * LONG;
   for (int e = tid; e < n; e += 32 * ROWS) {
     const int r = e / LONG, c = e - r * LONG;
-    if (c >= ncell) continue;
+    if (c < cfirst || c > clast) continue;
     const int row = ra + r;
-    const long long off = (long long)map_idx(row, I.jmax, I.bc_y) * I.pitch + map_idx(i0 - R + c, I.imax, I.bc_x);
+    const long long off = (long long)map_idx(row, I.jmax, I.bc_y) * I.pitch + map_idx(cs + c, I.imax, I.bc_x);
     double* dst = ring + G::slot(row) * G::ROWSZ + c;
     cp_async8(dst + 0 * LONG, prim + P_VX * fs + off);
     cp_async8(dst + 1 * LONG, prim + P_VY * fs + off);
@@ -1167,10 +1225,18 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
   using G = RingGeom<RM, ROWS>;
   constexpr int R = G::R, NS = G::NS, LONG = G::LONG;
   constexpr bool kPre = SOLVER == 5 || SOLVER == 7;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(128) double smem[];
+  __shared__ __align__(8) uint64_t bar;   // completion of the bulk copies of a band's rows
   double* ring = smem;
   double* yf = smem + G::RING;
   const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+  if (tid == 0) {
+    umma::mbar_init(&bar, 32 * ROWS);   // every thread arrives once per bulk fill
+    umma::mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t bulk_phase = 0;   // parity of the next bulk fill to complete
+  constexpr uint32_t kCopyPolls = 1u << 22;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     int b = tile;
     const InstDesc& I = tile_inst(insts, ninst, LK_STAGE, b);
@@ -1178,16 +1244,18 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
     const int i0 = (b % nstrip) * 31 - 1, jseg = (b / nstrip) * I.seg_rows;
     const int ilast = min(i0 + 31, I.imax), jend = min(jseg + I.seg_rows - 1, I.jmax);
     const int i = i0 + lane;
+    const bool bulk = ring_bulk<RM, ROWS>(I, i0);
+    const int sh = i0 - R - ring_col0<R>(i0);   // ring column of grid column i0 - R (0 or 1)
     uint32_t stt = 0;
     auto x_acc = [&](int j) {
-      RingAcc<RM, ROWS, 0> a{ring, {G::slot(j) * G::ROWSZ + lane}};
+      RingAcc<RM, ROWS, 0> a{ring, {G::slot(j) * G::ROWSZ + lane + sh}};
       return a;
     };
     auto y_acc = [&](int j) {
       RingAcc<RM, ROWS, 1> a;
       a.ring = ring;
 #pragma unroll
-      for (int q = 0; q < NS; ++q) a.off[q] = G::slot(j - R + q) * G::ROWSZ + lane + R;
+      for (int q = 0; q < NS; ++q) a.off[q] = G::slot(j - R + q) * G::ROWSZ + lane + R + sh;
       return a;
     };
     // The bands start one row below the segment: warp 0 of the first band
@@ -1196,15 +1264,30 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
     // other warp the y face, the x face and the update of its row.  With
     // seg_rows = 8 nb - 1 the bands are full.
     const int jfirst = jseg - 1;
-    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jfirst - R, min(jfirst + ROWS - 1, jend) + R + 1, tid);
+    ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, jfirst - R, min(jfirst + ROWS - 1, jend) + R + 1, tid, bulk, &bar);
     int band = 0;
     for (int j0 = jfirst; j0 <= jend; j0 += ROWS, ++band) {
       const int jl = min(j0 + ROWS - 1, jend);
       if constexpr (EP != EP_RHS) prefetch_update_rows(I, sa, i0, ilast, max(j0, jseg), jl, tid, 32 * ROWS);
       // the band's rows have arrived, and every warp has finished the previous
       // band's update (its reads of the face rows that this band overwrites)
-      cp_async_wait_all();
-      __syncthreads();
+      if (bulk) {
+        const bool ok = umma::mbar_wait(&bar, bulk_phase, kCopyPolls);
+        if (!__syncthreads_and(ok)) {
+          // the copies did not arrive in time: report, wait (bounded) for the
+          // ones still in flight, and stop the CTA
+          if (tid == 0) {
+            atomicOr(I.status, ST_COPY_TIMEOUT);
+            umma::mbar_wait(&bar, bulk_phase, kCopyPolls);
+          }
+          __syncthreads();
+          return;
+        }
+        bulk_phase ^= 1u;
+      } else {
+        cp_async_wait_all();
+        __syncthreads();
+      }
       // face row k of this band (k = 0 bottom faces, k = w + 1 the faces above row w)
       const int rb = (band * ROWS) % (ROWS + 1);
       auto frow = [&](int k) { const int r = k + rb; return yf + (r >= ROWS + 1 ? r - (ROWS + 1) : r) * (NROLE * 32); };
@@ -1240,14 +1323,15 @@ k_stage(const InstDesc* __restrict__ insts, int ninst, int ntiles, StageArgs sa)
         }
         // centre values of the point, read before the next band's copies
         // replace the ring rows
-        const double* cen = ring + G::slot(j) * G::ROWSZ + ln + R;
+        const double* cen = ring + G::slot(j) * G::ROWSZ + ln + R + sh;
         auto cs = [&](int f) { return cen[f * LONG]; };
         cv = Centre{cs(5 + Q_Q), cs(5 + Q_PSI), cs(5 + Q_PHI), cs(5 + Q_EX), cs(5 + Q_EY), cs(5 + Q_EZ),
                     cs(5 + Q_BX), cs(5 + Q_BY), cs(5 + Q_BZ), cs(0), cs(1), cs(2)};
       }
       __syncthreads();   // the band's y fluxes are complete and its ring reads done
       if (j0 + ROWS <= jend)   // the next band's rows arrive while this band updates
-        ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, j0 + ROWS + R + 1, min(j0 + 2 * ROWS - 1, jend) + R + 1, tid);
+        ring_fill<RM, ROWS>(I, sa, ring, i0, ilast, j0 + ROWS + R + 1, min(j0 + 2 * ROWS - 1, jend) + R + 1, tid,
+                            bulk, &bar);
       if (j <= jl && !face_only) {
         const double dlx = I.delx, ix2 = I.inv_delx_pow2;
         double qx[NROLE];
