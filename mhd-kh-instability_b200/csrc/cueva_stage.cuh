@@ -1037,8 +1037,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 // copies grid rows ra .. rb of the strip into their ring rows: with bulk,
-// one bulk copy per field and row issued by warp 0 (completion on bar, which
-// the caller waits for), else element by element through the ghost maps
+// one bulk copy per field and row, spread over all the CTA's threads
+// (completion on bar, which the caller waits for), else element by element
+// through the ghost maps
 // (columns i0-R .. ilast+R+1; the caller waits with cp.async.wait_all)
 template <int RM, int ROWS>
 __device__ __forceinline__ void ring_fill(const InstDesc& I, const StageArgs& sa, double* ring, int i0, int ilast,
