@@ -216,30 +216,38 @@ int stage_seg_rows(int imax, int jmax, int rows, int slots) {
 }
 
 cudaError_t prepare_stage(int rec_mp, int solver, int prec) {
+#define CUEVA_PREPARE_CASE(K, NAME) \
+  case K: return prec ? prepare_stage_##NAME##_mixed(rec_mp) : prepare_stage_##NAME##_fp64(rec_mp);
   switch (solver) {
-    case 1: return prepare_stage_lax(rec_mp, prec);
-    case 2: return prepare_stage_mcl(rec_mp, prec);
-    case 3: return prepare_stage_hllemc(rec_mp, prec);
-    case 4: return prepare_stage_hllcmc(rec_mp, prec);
-    case 5: return prepare_stage_hll(rec_mp, prec);
-    case 6: return prepare_stage_hlle(rec_mp, prec);
-    case 7: return prepare_stage_hllc(rec_mp, prec);
+    CUEVA_PREPARE_CASE(1, lax)
+    CUEVA_PREPARE_CASE(2, mcl)
+    CUEVA_PREPARE_CASE(3, hllemc)
+    CUEVA_PREPARE_CASE(4, hllcmc)
+    CUEVA_PREPARE_CASE(5, hll)
+    CUEVA_PREPARE_CASE(6, hlle)
+    CUEVA_PREPARE_CASE(7, hllc)
     default: return cudaErrorInvalidValue;
   }
+#undef CUEVA_PREPARE_CASE
 }
 
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
                          int n, const StageArgs& sa, cudaEvent_t* ev) {
+#define CUEVA_LAUNCH_CASE(K, NAME)                                                 \
+  case K:                                                                        \
+    return prec ? launch_stage_##NAME##_mixed(rec_mp, sh, st, d, n, sa, ev)      \
+                : launch_stage_##NAME##_fp64(rec_mp, sh, st, d, n, sa, ev);
   switch (solver) {
-    case 1: return launch_stage_lax(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 2: return launch_stage_mcl(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 3: return launch_stage_hllemc(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 4: return launch_stage_hllcmc(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 5: return launch_stage_hll(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 6: return launch_stage_hlle(rec_mp, prec, sh, st, d, n, sa, ev);
-    case 7: return launch_stage_hllc(rec_mp, prec, sh, st, d, n, sa, ev);
+    CUEVA_LAUNCH_CASE(1, lax)
+    CUEVA_LAUNCH_CASE(2, mcl)
+    CUEVA_LAUNCH_CASE(3, hllemc)
+    CUEVA_LAUNCH_CASE(4, hllcmc)
+    CUEVA_LAUNCH_CASE(5, hll)
+    CUEVA_LAUNCH_CASE(6, hlle)
+    CUEVA_LAUNCH_CASE(7, hllc)
     default: return cudaErrorInvalidValue;
   }
+#undef CUEVA_LAUNCH_CASE
 }
 
 static dim3 point_grid(long long npts, int ninst) {

@@ -18,28 +18,20 @@ int mlp_device_of(const cueva_mlp* M);
 // sets the shared-memory limits of the stage kernels (call once per device
 // before the first launch or capture)
 cudaError_t prepare_stage(int rec_mp, int solver, int prec);
-// per-solver halves of prepare_stage / launch_stage (cueva_stage_*.cu)
-cudaError_t prepare_stage_lax(int rec_mp, int prec);
-cudaError_t prepare_stage_hll(int rec_mp, int prec);
-cudaError_t prepare_stage_mcl(int rec_mp, int prec);
-cudaError_t prepare_stage_hllemc(int rec_mp, int prec);
-cudaError_t prepare_stage_hllcmc(int rec_mp, int prec);
-cudaError_t prepare_stage_hllc(int rec_mp, int prec);
-cudaError_t prepare_stage_hlle(int rec_mp, int prec);
-cudaError_t launch_stage_lax(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                             const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_hll(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                             const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_mcl(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                             const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_hllemc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
-                                int n, const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_hllcmc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,
-                                int n, const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_hllc(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                              const StageArgs& sa, cudaEvent_t* ev);
-cudaError_t launch_stage_hlle(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                              const StageArgs& sa, cudaEvent_t* ev);
+// per-solver, per-precision halves of prepare_stage / launch_stage
+// (cueva_stage_*.cu; _fp64 plain FP64, _mixed the mixed-precision kernels)
+#define CUEVA_DECLARE_STAGE_UNIT(NAME, P)                                                                   \
+  cudaError_t prepare_stage_##NAME##_##P(int rec_mp);                                                       \
+  cudaError_t launch_stage_##NAME##_##P(int rec_mp, const StageShape& sh, cudaStream_t st, const InstDesc* d, \
+                                        int n, const StageArgs& sa, cudaEvent_t* ev);
+#define CUEVA_DECLARE_STAGE_SOLVER(NAME) CUEVA_DECLARE_STAGE_UNIT(NAME, fp64) CUEVA_DECLARE_STAGE_UNIT(NAME, mixed)
+CUEVA_DECLARE_STAGE_SOLVER(lax)
+CUEVA_DECLARE_STAGE_SOLVER(mcl)
+CUEVA_DECLARE_STAGE_SOLVER(hllemc)
+CUEVA_DECLARE_STAGE_SOLVER(hllcmc)
+CUEVA_DECLARE_STAGE_SOLVER(hll)
+CUEVA_DECLARE_STAGE_SOLVER(hlle)
+CUEVA_DECLARE_STAGE_SOLVER(hllc)
 // one RK stage: y faces, then x faces + update; with ev non-null, ev[0..2]
 // are recorded before, between and after the launches
 cudaError_t launch_stage(int rec_mp, int solver, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d,

@@ -1409,55 +1409,71 @@ static cudaError_t prepare_tiles() {
   return e;
 }
 
-template <int RM, int SV>
-static void launch_rm_sv(int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                         const StageArgs& sa, cudaEvent_t* ev) {
-  if (prec == 0) {
-    if (sh.rows == 4) launch_tiles<RM, SV, double, 4>(sh, st, d, n, sa, ev);
-    else launch_tiles<RM, SV, double, 8>(sh, st, d, n, sa, ev);
-  } else {
-    if (sh.rows == 4) launch_tiles<RM, SV, float, 4>(sh, st, d, n, sa, ev);
-    else launch_tiles<RM, SV, float, 8>(sh, st, d, n, sa, ev);
-  }
+template <int RM, int SV, typename T>
+static void launch_rm_sv(const StageShape& sh, cudaStream_t st, const InstDesc* d, int n, const StageArgs& sa,
+                         cudaEvent_t* ev) {
+  if (sh.rows == 4) launch_tiles<RM, SV, T, 4>(sh, st, d, n, sa, ev);
+  else launch_tiles<RM, SV, T, 8>(sh, st, d, n, sa, ev);
 }
 
-template <int RM, int SV>
-static cudaError_t prepare_rm_sv(int prec) {
-  cudaError_t e = prec == 0 ? prepare_tiles<RM, SV, double, 8>() : prepare_tiles<RM, SV, float, 8>();
-  if (e == cudaSuccess) e = prec == 0 ? prepare_tiles<RM, SV, double, 4>() : prepare_tiles<RM, SV, float, 4>();
+template <int RM, int SV, typename T>
+static cudaError_t prepare_rm_sv() {
+  cudaError_t e = prepare_tiles<RM, SV, T, 8>();
+  if (e == cudaSuccess) e = prepare_tiles<RM, SV, T, 4>();
   return e;
 }
 
-// one solver's stage launch / kernel set-up over rec_mp and the precision
-template <int SV>
-cudaError_t launch_stage_solver(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
+// one solver's stage launch / kernel set-up over rec_mp in one precision
+// (T = double: plain FP64; T = float: the mixed-precision kernels, which the
+// build compiles in translation units of their own)
+template <int SV, typename T>
+cudaError_t launch_stage_solver(int rec_mp, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
                                 const StageArgs& sa, cudaEvent_t* ev) {
   if (sh.rows != 4 && sh.rows != 8) return cudaErrorInvalidValue;
   if constexpr (SV >= 1 && SV <= 4) {   // the MC family uses MC slopes; rec_mp does not apply
-    launch_rm_sv<3, SV>(prec, sh, st, d, n, sa, ev);
+    launch_rm_sv<3, SV, T>(sh, st, d, n, sa, ev);
   } else {
     switch (rec_mp) {
-      case 0: launch_rm_sv<0, SV>(prec, sh, st, d, n, sa, ev); break;
-      case 1: launch_rm_sv<1, SV>(prec, sh, st, d, n, sa, ev); break;
-      case 2: launch_rm_sv<2, SV>(prec, sh, st, d, n, sa, ev); break;
+      case 0: launch_rm_sv<0, SV, T>(sh, st, d, n, sa, ev); break;
+      case 1: launch_rm_sv<1, SV, T>(sh, st, d, n, sa, ev); break;
+      case 2: launch_rm_sv<2, SV, T>(sh, st, d, n, sa, ev); break;
       default: return cudaErrorInvalidValue;
     }
   }
   return cudaGetLastError();
 }
 
-template <int SV>
-cudaError_t prepare_stage_solver(int rec_mp, int prec) {
+template <int SV, typename T>
+cudaError_t prepare_stage_solver(int rec_mp) {
   if constexpr (SV >= 1 && SV <= 4) {
-    return prepare_rm_sv<3, SV>(prec);
+    return prepare_rm_sv<3, SV, T>();
   } else {
     switch (rec_mp) {
-      case 0: return prepare_rm_sv<0, SV>(prec);
-      case 1: return prepare_rm_sv<1, SV>(prec);
-      case 2: return prepare_rm_sv<2, SV>(prec);
+      case 0: return prepare_rm_sv<0, SV, T>();
+      case 1: return prepare_rm_sv<1, SV, T>();
+      case 2: return prepare_rm_sv<2, SV, T>();
       default: return cudaErrorInvalidValue;
     }
   }
 }
+
+// A solver's translation unit defines its launcher and set-up for one
+// precision: compiled plain for FP64 (<name>_fp64), or with
+// CUEVA_STAGE_MIXED for the mixed-precision kernels (<name>_mixed).
+#if defined(CUEVA_STAGE_MIXED)
+#define CUEVA_STAGE_UNIT(NAME, SV)                                                                              \
+  cudaError_t launch_stage_##NAME##_mixed(int rec_mp, const StageShape& sh, cudaStream_t st, const InstDesc* d, \
+                                          int n, const StageArgs& sa, cudaEvent_t* ev) {                       \
+    return launch_stage_solver<SV, float>(rec_mp, sh, st, d, n, sa, ev);                                       \
+  }                                                                                                            \
+  cudaError_t prepare_stage_##NAME##_mixed(int rec_mp) { return prepare_stage_solver<SV, float>(rec_mp); }
+#else
+#define CUEVA_STAGE_UNIT(NAME, SV)                                                                             \
+  cudaError_t launch_stage_##NAME##_fp64(int rec_mp, const StageShape& sh, cudaStream_t st, const InstDesc* d, \
+                                         int n, const StageArgs& sa, cudaEvent_t* ev) {                       \
+    return launch_stage_solver<SV, double>(rec_mp, sh, st, d, n, sa, ev);                                     \
+  }                                                                                                           \
+  cudaError_t prepare_stage_##NAME##_fp64(int rec_mp) { return prepare_stage_solver<SV, double>(rec_mp); }
+#endif
 
 }  // namespace cueva

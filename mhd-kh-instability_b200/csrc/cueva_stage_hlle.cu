@@ -1,15 +1,12 @@
 // cueva_stage_hlle.cu -- stage kernels instantiated for the HLLE + MPX (16_hlle_flow_mpx.f95)
 // solver (one translation unit per solver keeps the builds parallel).
+// Built twice: plain for the FP64 kernels and with CUEVA_STAGE_MIXED for the
+// mixed-precision ones.
 #include "cueva_launch.h"
 #include "cueva_stage.cuh"
 
 namespace cueva {
 
-cudaError_t launch_stage_hlle(int rec_mp, int prec, const StageShape& sh, cudaStream_t st, const InstDesc* d, int n,
-                              const StageArgs& sa, cudaEvent_t* ev) {
-  return launch_stage_solver<6>(rec_mp, prec, sh, st, d, n, sa, ev);
-}
-
-cudaError_t prepare_stage_hlle(int rec_mp, int prec) { return prepare_stage_solver<6>(rec_mp, prec); }
+CUEVA_STAGE_UNIT(hlle, 6)
 
 }  // namespace cueva
