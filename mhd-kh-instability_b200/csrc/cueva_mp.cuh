@@ -88,15 +88,26 @@ __device__ __forceinline__ T mp_vorm(const T (&u)[N]) {
   }
 }
 
-// limited up(k) for the cell at register index C (mp5.f95:104-136)
+// up(k) for the cell at register index C (mp5.f95:104-136) in two steps:
+// mp_up_fast gives the unlimited value vorp and whether it passes the
+// monotonicity test (then vorp is up(k)); mp_up_lim gives the limited value
+// of a vorp that failed it.  mp_up chains them; the interface pairs below
+// take all their tests first (independent chains for the scheduler) and
+// limit only the values that failed.  The operations are the same.
 template <int RM, int C, typename T, int N>
-__device__ __forceinline__ T mp_up(const T (&u)[N]) {
-  const T alpha = T(2.0), b2 = T(4.0 / 3.0), epsm = T(1.0e-10);
+__device__ __forceinline__ T mp_up_fast(const T (&u)[N], bool& ok) {
+  const T alpha = T(2.0), epsm = T(1.0e-10);
   const T du0 = u[C] - u[C - 1];
   const T du1 = u[C + 1] - u[C];
   const T vorp = mp_vorp<RM, C>(u);
   const T vmpp = u[C] + DMM(du1, alpha * du0);
-  if ((vorp - u[C]) * (vorp - vmpp) <= epsm) return vorp;
+  ok = (vorp - u[C]) * (vorp - vmpp) <= epsm;
+  return vorp;
+}
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_up_lim(const T (&u)[N], T vorp) {
+  const T alpha = T(2.0), b2 = T(4.0 / 3.0);
+  const T du0 = u[C] - u[C - 1];
   const T d2m = u[C - 2] - T(2.0) * u[C - 1] + u[C];
   const T d20 = u[C - 1] - T(2.0) * u[C] + u[C + 1];
   const T d2p = u[C] - T(2.0) * u[C + 1] + u[C + 2];
@@ -110,16 +121,28 @@ __device__ __forceinline__ T mp_up(const T (&u)[N]) {
   const T vmax = fmin2(fmax2(fmax2(u[C], u[C + 1]), vmd), fmax2(fmax2(u[C], vul), vlc));
   return vorp + DMM(vmin - vorp, vmax - vorp);
 }
-
-// limited um(k) for the cell at register index C (mp5.f95:142-167)
 template <int RM, int C, typename T, int N>
-__device__ __forceinline__ T mp_um(const T (&u)[N]) {
-  const T alpha = T(2.0), b2 = T(4.0 / 3.0), epsm = T(1.0e-10);
+__device__ __forceinline__ T mp_up(const T (&u)[N]) {
+  bool ok;
+  const T v = mp_up_fast<RM, C>(u, ok);
+  return ok ? v : mp_up_lim<RM, C>(u, v);
+}
+
+// um(k) for the cell at register index C (mp5.f95:142-167), same two steps
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_um_fast(const T (&u)[N], bool& ok) {
+  const T alpha = T(2.0), epsm = T(1.0e-10);
   const T du0 = u[C] - u[C - 1];
   const T du1 = u[C + 1] - u[C];
   const T vorm = mp_vorm<RM, C>(u);
   const T vmpm = u[C] + DMM(-du0, -alpha * du1);
-  if ((vorm - u[C]) * (vorm - vmpm) <= epsm) return vorm;
+  ok = (vorm - u[C]) * (vorm - vmpm) <= epsm;
+  return vorm;
+}
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_um_lim(const T (&u)[N], T vorm) {
+  const T alpha = T(2.0), b2 = T(4.0 / 3.0);
+  const T du1 = u[C + 1] - u[C];
   const T d2m = u[C - 2] - T(2.0) * u[C - 1] + u[C];
   const T d20 = u[C - 1] - T(2.0) * u[C] + u[C + 1];
   const T d2p = u[C] - T(2.0) * u[C + 1] + u[C + 2];
@@ -133,13 +156,38 @@ __device__ __forceinline__ T mp_um(const T (&u)[N]) {
   const T vmax = fmin2(fmax2(fmax2(u[C], u[C - 1]), vmd), fmax2(fmax2(u[C], vul), vlc));
   return vorm + DMM(vmin - vorm, vmax - vorm);
 }
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ T mp_um(const T (&u)[N]) {
+  bool ok;
+  const T v = mp_um_fast<RM, C>(u, ok);
+  return ok ? v : mp_um_lim<RM, C>(u, v);
+}
 
 // interface pair: u holds cells i-R .. i+1+R; returns L = up(i), R = um(i+1)
+// (both monotonicity tests first: two independent chains before the rare
+// limiting steps)
 template <int RM, typename T, int N>
 __device__ __forceinline__ void mp_pair(const T (&u)[N], T& L, T& R) {
   constexpr int C = MPR<RM>::R;
-  L = mp_up<RM, C>(u);
-  R = mp_um<RM, C + 1>(u);
+  bool okL, okR;
+  L = mp_up_fast<RM, C>(u, okL);
+  R = mp_um_fast<RM, C + 1>(u, okR);
+  if (!okL) L = mp_up_lim<RM, C>(u, L);
+  if (!okR) R = mp_um_lim<RM, C + 1>(u, R);
+}
+// up(k), um(k) of the cells at C and C + 1 (the positivity-fixed pairs),
+// the four tests first
+template <int RM, int C, typename T, int N>
+__device__ __forceinline__ void mp_quad(const T (&u)[N], T& up0, T& um0, T& up1, T& um1) {
+  bool o0, o1, o2, o3;
+  up0 = mp_up_fast<RM, C>(u, o0);
+  um0 = mp_um_fast<RM, C>(u, o1);
+  up1 = mp_up_fast<RM, C + 1>(u, o2);
+  um1 = mp_um_fast<RM, C + 1>(u, o3);
+  if (!o0) up0 = mp_up_lim<RM, C>(u, up0);
+  if (!o1) um0 = mp_um_lim<RM, C>(u, um0);
+  if (!o2) up1 = mp_up_lim<RM, C + 1>(u, up1);
+  if (!o3) um1 = mp_um_lim<RM, C + 1>(u, um1);
 }
 
 // pair for the p / rho slots: the positivity fix-up of mp5.f95:177-216 makes
@@ -152,8 +200,8 @@ __device__ __forceinline__ void posfix_point(T uk, T duk, T duk1, T& up, T& um) 
 template <int RM, typename T, int N>
 __device__ __forceinline__ void mp_pair_pos(const T (&u)[N], T& L, T& R) {
   constexpr int C = MPR<RM>::R;
-  T up0 = mp_up<RM, C>(u), um0 = mp_um<RM, C>(u);
-  T up1 = mp_up<RM, C + 1>(u), um1 = mp_um<RM, C + 1>(u);
+  T up0, um0, up1, um1;
+  mp_quad<RM, C>(u, up0, um0, up1, um1);
   posfix_point(u[C], u[C] - u[C - 1], u[C + 1] - u[C], up0, um0);
   posfix_point(u[C + 1], u[C + 1] - u[C], u[C + 2] - u[C + 1], up1, um1);
   L = up0;
@@ -171,8 +219,8 @@ __device__ __forceinline__ void posfix_point_delta(double c0, T uk, T duk, T duk
 template <int RM, typename T, int N>
 __device__ __forceinline__ void mp_pair_pos_delta(const T (&u)[N], double c0, T& L, T& R) {
   constexpr int C = MPR<RM>::R;
-  T up0 = mp_up<RM, C>(u), um0 = mp_um<RM, C>(u);
-  T up1 = mp_up<RM, C + 1>(u), um1 = mp_um<RM, C + 1>(u);
+  T up0, um0, up1, um1;
+  mp_quad<RM, C>(u, up0, um0, up1, um1);
   posfix_point_delta(c0, u[C], u[C] - u[C - 1], u[C + 1] - u[C], up0, um0);
   posfix_point_delta(c0, u[C + 1], u[C + 1] - u[C], u[C + 2] - u[C + 1], up1, um1);
   L = up0;
