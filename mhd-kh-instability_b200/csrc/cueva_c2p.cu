@@ -19,6 +19,9 @@ namespace cueva {
 namespace {
 
 constexpr int C2P_CTAS_PER_SM = 4;
+// k_c2p_step holds a tile's inputs in registers while it works on the one
+// before: three CTAs per SM leave it the registers for that
+constexpr int C2P_STEP_CTAS_PER_SM = 3;
 
 // one point of the learned con2prim (all 128 threads of the CTA call it, in
 // step): seeds p from the previous pressure or the network (the one with the
@@ -64,8 +67,6 @@ __device__ __forceinline__ void learned_stats(unsigned long long* stats, bool co
   }
 }
 
-// the tail of the step for the instances with the learned method: tiles of
-// 128 points over all instances (block ranges of launch kind LK_C2P)
 // L2 prefetch of the inputs of tile b of instance I (the 19 fields the
 // tile reads; its 128 points cover at most two row segments per field)
 __device__ __forceinline__ void c2p_prefetch(const InstDesc& I, int b, int cur) {
@@ -88,54 +89,89 @@ __device__ __forceinline__ void c2p_prefetch(const InstDesc& I, int b, int cur) 
   prefetch_l2(base + (long long)row * I.pitch + ia, ib - ia + 1);
 }
 
-__global__ void __launch_bounds__(TC_ROWS, C2P_CTAS_PER_SM)
+// One thread's inputs of a tile: the con2prim state and the time n+1
+// fields that varfin completed.  k_c2p_step loads them a tile ahead, so
+// that their latency is spent under the previous tile's work.
+struct C2PTileIn {
+  C2PIn in;
+  double fn[NPRIM - P_PSI];   // psi .. q of time n+1
+  long long pc;               // the point's offset in its instance's slabs
+  const InstDesc* I;
+  int b;                      // the tile within its instance
+  bool valid;                 // a real point (rows past the end repeat the last one)
+  bool use;                   // the instance runs the learned method on the tensor cores
+};
+
+__device__ __forceinline__ void c2p_load(const InstDesc* __restrict__ insts, int ninst, int tile, int cur,
+                                         C2PTileIn& t) {
+  int b = tile;
+  const InstDesc& I = tile_inst(insts, ninst, LK_C2P, b);
+  t.I = &I;
+  t.b = b;
+  t.use = I.c2p == 2 && I.c2p_tc;   // uniform over the CTA: a tile belongs to one instance
+  if (!t.use) return;
+  const int nx = I.imax + 1;
+  const long long npts = (long long)nx * (I.jmax + 1);
+  const long long p0 = (long long)b * TC_ROWS + threadIdx.x;
+  t.valid = p0 < npts;
+  const long long p = t.valid ? p0 : npts - 1;
+  const int i = int(p % nx), j = int(p / nx);
+  const long long fs = I.fstride, pc = (long long)j * I.pitch + i;
+  t.pc = pc;
+  const double* un = I.finsum;        // varfin's D, tau, S in the slabs Q_D .. Q_SZ
+  const double* pold = I.prim[cur];
+  const double* pn = I.prim[1 - cur];
+  t.in = C2PIn{un[Q_D * fs + pc], un[Q_TAU * fs + pc], un[Q_SX * fs + pc], un[Q_SY * fs + pc],
+               un[Q_SZ * fs + pc], pn[P_EX * fs + pc], pn[P_EY * fs + pc], pn[P_EZ * fs + pc],
+               pn[P_BX * fs + pc], pn[P_BY * fs + pc], pn[P_BZ * fs + pc], pold[P_VX * fs + pc],
+               pold[P_VY * fs + pc], pold[P_VZ * fs + pc], pold[P_RHO * fs + pc], pold[P_P * fs + pc]};
+#pragma unroll
+  for (int c = P_PSI; c < NPRIM; ++c) t.fn[c - P_PSI] = pn[c * fs + pc];
+}
+
+// the tail of the step for the instances with the learned method: tiles of
+// 128 points over all instances (block ranges of launch kind LK_C2P)
+__global__ void __launch_bounds__(TC_ROWS, C2P_STEP_CTAS_PER_SM)
 k_c2p_step(const InstDesc* __restrict__ insts, int ninst, int ntiles, const MLPDevice* __restrict__ mlp, int cur,
            int qout, double abt11) {
   __shared__ MLPShared S;
   mlp_tc_setup(S, *mlp);
   uint32_t phase = 0;
   uint32_t* tile_status = insts[0].status;   // the instance of the CTA's last tile (teardown status)
+  C2PTileIn t{}, tn{};
+  if ((int)blockIdx.x < ntiles) c2p_load(insts, ninst, blockIdx.x, cur, t);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int b = tile;
-    const InstDesc& I = tile_inst(insts, ninst, LK_C2P, b);
-    if (!(I.c2p == 2 && I.c2p_tc)) continue;   // uniform over the CTA: a tile belongs to one instance
-    tile_status = I.status;
-    if (tile + (int)gridDim.x < ntiles) {       // the next tile's inputs go to L2 meanwhile
-      int bn = tile + (int)gridDim.x;
+    const int next = tile + (int)gridDim.x;
+    if (next < ntiles) c2p_load(insts, ninst, next, cur, tn);   // in flight during this tile
+    if (next + (int)gridDim.x < ntiles) {                        // the tile after it goes to L2
+      int bn = next + (int)gridDim.x;
       const InstDesc& In = tile_inst(insts, ninst, LK_C2P, bn);
       if (In.c2p == 2 && In.c2p_tc) c2p_prefetch(In, bn, cur);
     }
-    const int nx = I.imax + 1;
-    const long long npts = (long long)nx * (I.jmax + 1);
-    const long long p0 = (long long)b * TC_ROWS + threadIdx.x;
-    const bool valid = p0 < npts;
-    const long long p = valid ? p0 : npts - 1;   // rows past the end repeat the last point
-    const int i = int(p % nx), j = int(p / nx);
-    const long long fs = I.fstride, pc = (long long)j * I.pitch + i;
-    const double* un = I.finsum;        // varfin's D, tau, S in the slabs Q_D .. Q_SZ
-    const double* pold = I.prim[cur];
-    double* pn = I.prim[1 - cur];
-    const C2PIn in{un[Q_D * fs + pc], un[Q_TAU * fs + pc], un[Q_SX * fs + pc], un[Q_SY * fs + pc],
-                   un[Q_SZ * fs + pc], pn[P_EX * fs + pc], pn[P_EY * fs + pc], pn[P_EZ * fs + pc],
-                   pn[P_BX * fs + pc], pn[P_BY * fs + pc], pn[P_BZ * fs + pc], pold[P_VX * fs + pc],
-                   pold[P_VY * fs + pc], pold[P_VZ * fs + pc], pold[P_RHO * fs + pc], pold[P_P * fs + pc]};
-    LearnedOut r;
-    if (!learned_point(S, phase, in, I.gamma, I.eps1_c2p, I.counters, valid, r)) {
-      if (threadIdx.x == 0) atomicOr(I.status, ST_TC_TIMEOUT);
-      break;   // every thread of the CTA sees the same result
-    }
-    learned_stats(mlp->stats, valid, r.it);
-    const uint32_t st = __reduce_or_sync(0xffffffffu, valid ? r.st : 0u);
-    if (st && (threadIdx.x & 31) == 0) atomicOr(I.status, st);
-    if (valid) {
-      double pv[NPRIM];
-      pv[P_RHO] = r.o.rho; pv[P_P] = r.o.p; pv[P_VX] = r.o.vx; pv[P_VY] = r.o.vy; pv[P_VZ] = r.o.vz;
-      pn[P_RHO * fs + pc] = r.o.rho; pn[P_P * fs + pc] = r.o.p;
-      pn[P_VX * fs + pc] = r.o.vx; pn[P_VY * fs + pc] = r.o.vy; pn[P_VZ * fs + pc] = r.o.vz;
+    if (t.use) {
+      const InstDesc& I = *t.I;
+      tile_status = I.status;
+      LearnedOut r;
+      if (!learned_point(S, phase, t.in, I.gamma, I.eps1_c2p, I.counters, t.valid, r)) {
+        if (threadIdx.x == 0) atomicOr(I.status, ST_TC_TIMEOUT);
+        break;   // every thread of the CTA sees the same result
+      }
+      learned_stats(mlp->stats, t.valid, r.it);
+      const uint32_t st = __reduce_or_sync(0xffffffffu, t.valid ? r.st : 0u);
+      if (st && (threadIdx.x & 31) == 0) atomicOr(I.status, st);
+      if (t.valid) {
+        const long long fs = I.fstride, pc = t.pc;
+        double* pn = I.prim[1 - cur];
+        double pv[NPRIM];
+        pv[P_RHO] = r.o.rho; pv[P_P] = r.o.p; pv[P_VX] = r.o.vx; pv[P_VY] = r.o.vy; pv[P_VZ] = r.o.vz;
+        pn[P_RHO * fs + pc] = r.o.rho; pn[P_P * fs + pc] = r.o.p;
+        pn[P_VX * fs + pc] = r.o.vx; pn[P_VY * fs + pc] = r.o.vy; pn[P_VZ * fs + pc] = r.o.vz;
 #pragma unroll
-      for (int c = P_PSI; c < NPRIM; ++c) pv[c] = pn[c * fs + pc];
-      if (!I.primitive_rec) begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
+        for (int c = P_PSI; c < NPRIM; ++c) pv[c] = t.fn[c - P_PSI];
+        if (!I.primitive_rec) begin_step_point(I, abt11, I.aux[1 - cur], I.stage[qout], pc, pv);
+      }
     }
+    t = tn;
   }
   mlp_tc_teardown(S, phase, tile_status);
 }
@@ -164,8 +200,8 @@ k_predict_tc(long long n, const MLPDevice* __restrict__ mlp, const double* __res
   mlp_tc_teardown(S, phase, err_status);
 }
 
-int c2p_grid(long long ntiles) {
-  const long long g = (long long)C2P_CTAS_PER_SM * 148;
+int c2p_grid(long long ntiles, int ctas_per_sm = C2P_CTAS_PER_SM) {
+  const long long g = (long long)ctas_per_sm * 148;
   return (int)(ntiles < g ? (ntiles < 1 ? 1 : ntiles) : g);
 }
 
@@ -177,7 +213,7 @@ int c2p_tiles(int imax, int jmax) {
 
 cudaError_t launch_c2p_step(cudaStream_t st, const InstDesc* d, int ninst, int ntiles, const MLPDevice* mlp, int cur,
                             int qout, double abt11) {
-  k_c2p_step<<<c2p_grid(ntiles), TC_ROWS, 0, st>>>(d, ninst, ntiles, mlp, cur, qout, abt11);
+  k_c2p_step<<<c2p_grid(ntiles, C2P_STEP_CTAS_PER_SM), TC_ROWS, 0, st>>>(d, ninst, ntiles, mlp, cur, qout, abt11);
   return cudaGetLastError();
 }
 
