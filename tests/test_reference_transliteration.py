@@ -13,7 +13,13 @@ rounded operations, as gfortran's code without -ffast-math).  They cover
   DM4 and DMM in the sign arithmetic of funciones.f95:148-185, and the
   positivity fix of the p and rho slots (mp5.f95:177-216);
 - get_hllc_vel (funciones.f95:188-259), with the first evaluation at the
-  clamped seed (the Fortran reads an uninitialised v there).
+  clamped seed (the Fortran reads an uninitialised v there);
+- varprimitivecardano (12_varprimitive.f95:48-813, l_swap = 1, no drift,
+  no low-velocity branch, no electric-field recovery) with the C library's
+  acos, cos and pow, as the Fortran calls them.  The states here all take
+  the one-real-root branch, as nearly every point of a KH run does; the
+  three-root branch's seed arithmetic is pinned against acos / cos in
+  test_oracle_pins.py.
 """
 import math
 
@@ -205,3 +211,165 @@ def test_hllc_vel_equals_fortran_statements(oracle_mod):
         assert got == want, (a, b, c, rt, got, want)
         checked += 1
     assert checked > 2500
+
+
+def varprimitivecardano_fortran(inp, gamma=4.0 / 3.0, eps1=1.0e-6, stats=None):
+    """12_varprimitive.f95:48-813 for one point with l_swap = 1, VDRIFT = 0,
+    low_vel = 0, REC_ELEC = 0 (one pass of the n_elec loop): the Cardano
+    quartic in W with the C library's acos, cos and x**THIRD as the Fortran
+    has them, the Newton polish of W, the pressure iteration and the
+    velocities.  inp = D, tau, S, E, B, v(seed), rho(seed), p(seed).
+    Returns (vx, vy, vz, rho, p, W), or None where the reference stops."""
+    D, tau, Sx, Sy, Sz, Ex0, Ey0, Ez0, Bx, By, Bz, vx0, vy0, vz0, rho_old, p_old = (float(x) for x in inp)
+    TOL, nrmax, THIRD, pi = 1.0e-10, 40, 0.333333333333333333333333333333, 3.14159265358979323846264338327950288
+    stats = {} if stats is None else stats
+    V2c = vx0 * vx0 + vy0 * vy0 + vz0 * vz0
+    if V2c > 1:
+        V2c = max(-1.0 + eps1, min(1.0 - eps1, V2c))
+    E2B2 = 0.5 * (Ex0 * Ex0 + Ey0 * Ey0 + Ez0 * Ez0 + Bx * Bx + By * By + Bz * Bz)
+    gamma_1 = (gamma - 1.0) / gamma
+    c1x, c1y, c1z = Sx - Ey0 * Bz + Ez0 * By, Sy - Ez0 * Bx + Ex0 * Bz, Sz - Ex0 * By + Ey0 * Bx
+    C_1 = c1x * c1x + c1y * c1y + c1z * c1z
+    C_2 = tau - E2B2
+    a_4 = C_1 - C_2 * C_2
+    a_3 = 2.0 * gamma_1 * C_2 * D
+    a_2 = C_2 * C_2 - 2.0 * gamma_1 * C_1 - (gamma_1 * gamma_1) * (D * D)
+    a_1 = -(2.0 * gamma_1 * C_2 * D)
+    a_0 = (gamma_1 * gamma_1) * (C_1 + D * D)
+    b_3, b_2, b_1, b_0 = a_3 / a_4, a_2 / a_4, a_1 / a_4, a_0 / a_4
+    b32 = b_3 * b_3
+    d_2 = b_2 - (3.0 * b32) / 8.0
+    d_1 = b_1 - (b_3 * b_2) / 2.0 + (b32 * b_3) / 8.0
+    d_0 = b_0 - (b_3 * b_1) / 4.0 + (b32 * b_2) / 16.0 - (3.0 * (b32 * b32)) / 256.0
+    e = (20.0 * d_2) / 8.0
+    f = -(d_0 - 2.0 * (d_2 * d_2))
+    g = -((d_1 * d_1 + 4.0 * d_2 * d_0 - 4.0 * ((d_2 * d_2) * d_2)) / 8.0)
+    Q_1 = (e * e - 3.0 * f) / 9.0
+    R_1 = (2.0 * ((e * e) * e) - 9.0 * e * f + 27.0 * g) / 54.0
+    Q_13 = (Q_1 * Q_1) * Q_1
+    if R_1 * R_1 < Q_13:
+        stats["trig"] = stats.get("trig", 0) + 1
+        T_1 = math.acos(R_1 / abs(math.sqrt(Q_13)))
+        z_1 = s = t = det = None
+        for Tk in (T_1, T_1 + 2.0 * pi, T_1 - 2.0 * pi):
+            z = -(2.0 * abs(math.sqrt(Q_1)) * math.cos(Tk / 3.0)) - e / 3.0
+            s_1 = d_2 + 2.0 * z
+            t_1 = z * z + 2.0 * d_2 * z + d_2 * d_2 - d_0
+            if s_1 >= 0.0 and t_1 >= 0.0:
+                s, t, z_1 = abs(math.sqrt(s_1)), abs(math.sqrt(t_1)), z
+                det = s * s - 4.0 * (d_2 + z - t)
+                if det < 0.0:
+                    return None
+                break
+        if z_1 is None:
+            return None
+    else:
+        stats["real"] = stats.get("real", 0) + 1
+        xx1 = abs(R_1) + abs(math.sqrt(R_1 * R_1 - Q_13))
+        AA_1 = -(math.copysign(1.0, R_1) * math.copysign(abs(xx1 ** THIRD), xx1))
+        BB_1 = Q_1 / AA_1 if AA_1 != 0.0 else 0.0
+        z_1 = (AA_1 + BB_1) - e / 3.0
+        s2 = d_2 + 2.0 * z_1
+        if s2 < 0.0:
+            return None                      # the reference's sqrt gives NaN here
+        s = abs(math.sqrt(s2))
+        t = abs(math.sqrt(z_1 * z_1 + 2.0 * d_2 * z_1 + d_2 * d_2 - d_0))
+        det = s * s - 4.0 * (d_2 + z_1 - t)
+    if det < 0.0:
+        return None
+    Q_2 = -0.5 * (-s + math.copysign(1.0, -s) * abs(math.sqrt(det)))
+    y_1 = Q_2 - b_3 / 4.0
+    y_2 = (d_2 + z_1 - t) / Q_2 - b_3 / 4.0
+    Wnro = math.nan
+    if y_1 >= 1.0 and y_2 >= 1.0:
+        Wnro = min(y_1, y_2)
+    if y_1 <= 1.0 and y_2 <= 1.0:
+        return None
+    if y_1 >= 1.0 and y_2 <= 1.0:
+        Wnro = y_1
+    if y_1 <= 1.0 and y_2 >= 1.0:
+        Wnro = y_2
+    nrw, CHA1 = 1, 1.0
+    while CHA1 > TOL and nrw < nrmax:
+        W2 = Wnro * Wnro
+        W3 = W2 * Wnro
+        Wnr = Wnro - (W2 * W2 + b_3 * W3 + b_2 * W2 + b_1 * Wnro + b_0) / (4.0 * W3 + 3.0 * b_3 * W2 + 2.0 * b_2 * Wnro + b_1)
+        CHA1 = abs(Wnr - Wnro) / (0.5 * (Wnr + Wnro))
+        Wnro = Wnr
+        nrw += 1
+    W = Wnro
+    rho = D / W
+    if rho < 0.0:
+        rho = max(rho_old * 1.0e-1, rho)
+    enthpy = (tau - E2B2 - gamma_1 * rho) / (W * W - gamma_1)
+    p = gamma_1 * (enthpy - rho)
+    pnro = p
+    epsilonnr = (tau - E2B2 - D * W + pnro * (1.0 - W * W)) / (D * W)
+    Cs2 = (gamma * (gamma - 1.0) * epsilonnr) / (1.0 + gamma * epsilonnr)
+    CHA, nr = 1.0, 1
+    while CHA >= TOL and nr <= nrmax:
+        pnr = pnro - ((gamma - 1.0) * rho * epsilonnr - pnro) / (V2c * Cs2 - 1.0)
+        CHA = abs(pnr - pnro) / (0.5 * (pnr + pnro))
+        pnro = pnr
+        nr += 1
+    if pnro < 0.0:
+        pnro = max(p_old * 1.0e-4, pnro)
+    p = pnro
+    tau_n = E2B2 + enthpy * (W * W) - p
+    den = tau_n - E2B2 + p
+    vx, vy, vz = c1x / den, c1y / den, c1z / den
+    V2c = vx * vx + vy * vy + vz * vz
+    if V2c >= 1.0:
+        return None                          # the drift fall-back is not transliterated here
+    W = 1.0 / math.sqrt(1.0 - V2c)
+    return vx, vy, vz, rho, p, W
+
+
+def _c2p_states(n, seed):
+    """Conserved states from random primitives (W up to 3, magnetised, E
+    near the ideal -v x B) and seeds near the true state."""
+    rng = np.random.default_rng(seed)
+    gamma = 4.0 / 3.0
+    rho = 10 ** rng.uniform(-1, 1, n)
+    p = 10 ** rng.uniform(-2, 1, n)
+    W = rng.uniform(1.0, 3.0, n)
+    vdir = rng.standard_normal((n, 3))
+    vdir /= np.linalg.norm(vdir, axis=1)[:, None]
+    v = vdir * np.sqrt(1 - 1 / W ** 2)[:, None]
+    B = rng.standard_normal((n, 3)) * 0.5
+    E = -np.cross(v, B) + rng.standard_normal((n, 3)) * 1e-3
+    h = rho + gamma / (gamma - 1) * p
+    D = rho * W
+    tau = 0.5 * ((E ** 2).sum(1) + (B ** 2).sum(1)) + h * W ** 2 - p
+    S = np.cross(E, B) + (h * W ** 2)[:, None] * v
+    v0 = v * (1 + 1e-3 * rng.standard_normal((n, 3)))
+    return [np.r_[D[k], tau[k], S[k], E[k], B[k], v0[k], rho[k], p[k]] for k in range(n)]
+
+
+def test_cardano_equals_fortran_statements(oracle_mod):
+    """The oracle's Cardano recovery with the C library's acos / cos / pow
+    (the reference's own seed arithmetic, oracle_set_libm_seed(1)) equals the
+    transliteration bit for bit; with the deterministic seeds of the default
+    build it agrees to a few ulps of W."""
+    stats = {}
+    checked = 0
+    oracle_mod.set_libm_seed(1)
+    try:
+        for inp in _c2p_states(400, 11):
+            want = varprimitivecardano_fortran(inp, stats=stats)
+            if want is None:
+                continue
+            st, got = oracle_mod.c2p(inp, method=1)
+            assert st == 0
+            assert np.array_equal(got, np.array(want)), (inp, got, want)
+            checked += 1
+    finally:
+        oracle_mod.set_libm_seed(0)
+    assert checked > 350 and stats.get("real", 0) > 0
+    for inp in _c2p_states(100, 12):
+        want = varprimitivecardano_fortran(inp)
+        if want is None:
+            continue
+        st, got = oracle_mod.c2p(inp, method=1)
+        assert st == 0
+        np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-15)
