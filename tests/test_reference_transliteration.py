@@ -19,7 +19,9 @@ rounded operations, as gfortran's code without -ffast-math).  They cover
   acos, cos and pow, as the Fortran calls them.  The states here all take
   the one-real-root branch, as nearly every point of a KH run does; the
   three-root branch's seed arithmetic is pinned against acos / cos in
-  test_oracle_pins.py.
+  test_oracle_pins.py;
+- varprimitive_nr (12_varprimitive_nr.f95:6-343, l_swap = 1, no
+  electric-field recovery).
 """
 import math
 
@@ -373,3 +375,59 @@ def test_cardano_equals_fortran_statements(oracle_mod):
         st, got = oracle_mod.c2p(inp, method=1)
         assert st == 0
         np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-15)
+
+
+def varprimitive_nr_fortran(inp, gamma=4.0 / 3.0):
+    """12_varprimitive_nr.f95:6-343 for one point with l_swap = 1 and
+    REC_ELEC = 0: velocities from the conserved state at the seed pressure,
+    the pressure iteration, and the velocities again.  inp as for the
+    Cardano routine; returns (vx, vy, vz, rho, p, W), or None where the
+    reference stops."""
+    D, tau, Sx, Sy, Sz, Ex0, Ey0, Ez0, Bx, By, Bz, vx0, vy0, vz0, rho_old, p_old = (float(x) for x in inp)
+    TOL, nrmax = 1.0e-10, 40
+    E2B2 = 0.5 * (Ex0 * Ex0 + Ey0 * Ey0 + Ez0 * Ez0 + Bx * Bx + By * By + Bz * Bz)
+    c1x, c1y, c1z = Sx - Ey0 * Bz + Ez0 * By, Sy - Ez0 * Bx + Ex0 * Bz, Sz - Ex0 * By + Ey0 * Bx
+    p = p_old
+    den = tau - E2B2 + p
+    vx, vy, vz = c1x / den, c1y / den, c1z / den
+    V2c = vx * vx + vy * vy + vz * vz
+    if V2c >= 1.0:
+        return None                          # sqrt of a negative number in the reference
+    W = 1.0 / math.sqrt(1.0 - V2c)
+    W_2 = 1.0 / (1.0 - V2c)
+    rho = D / W
+    epsilonnr = (tau - E2B2 - D * W + p * (1.0 - W_2)) / (D * W)
+    Cs2 = (gamma * (gamma - 1.0) * epsilonnr) / (1.0 + gamma * epsilonnr)
+    CHA, nr, pnro = 1.0, 1, p
+    while CHA >= TOL and nr <= nrmax:
+        pnr = pnro - ((gamma - 1.0) * rho * epsilonnr - pnro) / (V2c * Cs2 - 1.0)
+        CHA = abs(pnr - pnro) / (0.5 * (pnr + pnro))
+        pnro = pnr
+        nr += 1
+    p = pnro
+    den = tau - E2B2 + p
+    vx, vy, vz = c1x / den, c1y / den, c1z / den
+    V2c = vx * vx + vy * vy + vz * vz
+    if V2c >= 1.0:
+        return None
+    W = 1.0 / math.sqrt(1.0 - V2c)
+    rho = D / W
+    return vx, vy, vz, rho, p, W
+
+
+def test_newton_raphson_con2prim_equals_fortran_statements(oracle_mod):
+    """The oracle's varprimitive_nr equals the transliteration bit for bit,
+    seeded with the pressure of the state and with pressures off by up to
+    30 %."""
+    checked = 0
+    rng = np.random.default_rng(13)
+    for inp in _c2p_states(400, 14):
+        inp = inp.copy()
+        inp[15] *= 1.0 + 0.3 * rng.uniform(-1, 1)
+        want = varprimitive_nr_fortran(inp)
+        if want is None:
+            continue
+        st, got = oracle_mod.c2p(inp, method=0)
+        assert np.array_equal(got, np.array(want)), (inp, got, want)
+        checked += 1
+    assert checked > 300
