@@ -175,6 +175,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(ms, pg, device="cuda"):
+    """The largest of the ranks' device times (every rank takes part); ms
+    itself without a process group."""
+    if pg is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, zones, steps, ms):
+    """Whole-job zone-updates/s: every replica advances its own grid of
+    `zones` cells `steps` times; the job takes the slowest replica's ms."""
+    return world * zones * steps / (ms * 1e-3)
+
+
 def cpu_port_rate(cfg, steps_budget_s=20.0, max_steps=2, threads=None, warmup=1):
     """Zone-updates/s of the CPU restatement (the oracle) on a bounded sample
     of the workload: the full grid, after `warmup` untimed steps as many whole
@@ -383,11 +400,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     m.step(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), pg)
     m.download()
     # the same mixed precision with the reference's Cardano recovery in the
     # last stage's update instead of the learned kernel, same steps
@@ -402,11 +415,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     mc.step(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_card = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms_card], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_card = float(t.item())
+    ms_card = max_over_ranks(e0.elapsed_time(e1), pg)
     mc.close()
     errs = {n: rel_l1_field(n, m.interior(n), ref[n], ref) for n in PRIM_NAMES}
     errs_vec = dict(errs, **vector_rel_l1(m, ref))
@@ -415,7 +424,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
     m.close()
     net.close()
     nprof = max(args.profile_steps, 1)
-    return {"value": world * cfg.nx * cfg.ny * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+    return {"value": aggregate_rate(world, cfg.nx * cfg.ny, args.steps, ms), "unit": UNIT, "ms_per_step": ms / args.steps,
             "dtype": "f32 reconstruction + Riemann (psi, phi, E, B fluxes f64), f64 update / implicit E / con2prim",
             "con2prim": "network seed on the tcgen05 tensor cores (k_c2p_step), Newton in FP64, Cardano fall-back",
             "kernel_ms_per_step": dict({n: v[2] / nprof for n, v in stage_kernels(cfg, 4, prof_ms, prof_n).items()},
@@ -430,7 +439,7 @@ def run_mixed_learned(args, cfg, stream, g, device, world, pg):
             "rel_l1_vs_fp64_vector_norm": errs_vec, "max_rel_l1_vs_fp64_vector_norm": max(errs_vec.values()),
             "max_rel_l1_vs_fp64_vector_norm_by_step": traj, "steps_within_1e-6": within,
             "newton_iterations_per_point": its / max(pts, 1), "cardano_fallbacks": fails,
-            "mixed_cardano": {"value": world * cfg.nx * cfg.ny * args.steps / (ms_card * 1e-3),
+            "mixed_cardano": {"value": aggregate_rate(world, cfg.nx * cfg.ny, args.steps, ms_card),
                               "ms_per_step": ms_card / args.steps,
                               "note": "mixed precision with the reference's Cardano con2prim in the last "
                                       "stage's update, same steps"},
@@ -618,13 +627,9 @@ def main():
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     g.sync()                                    # raises on a reference STOP condition
-    ms_max = ms
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, pg)
     zones = cfg.nx * cfg.ny
-    value = world * zones * args.steps / (ms_max * 1e-3)
+    value = aggregate_rate(world, zones, args.steps, ms_max)
     ms_per_step = ms_max / args.steps
 
     # the mixed-precision + learned-seed form on the same workload and steps
@@ -649,12 +654,8 @@ def main():
         g.sync()                                # the last readback is complete
         e1.record(stream)
         torch.cuda.synchronize()
-        ms_ = e0.elapsed_time(e1)
-        if pg is not None:
-            t = torch.tensor([ms_], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms_ = float(t.item())
-        return world * zones * args.e2e_steps / (ms_ * 1e-3)
+        ms_ = max_over_ranks(e0.elapsed_time(e1), pg)
+        return aggregate_rate(world, zones, args.e2e_steps, ms_)
 
     e2e_sync = e2e_loop(False)
     e2e_async = e2e_loop(True)
